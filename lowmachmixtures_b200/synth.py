@@ -1,0 +1,135 @@
+"""Seeded synthetic Stokes problems with the shapes of the benchmark workloads.
+
+The reference benchmarks nothing and ships no input data, so every workload
+is synthetic (periodic box, one grid, isotropic dx = 1/n):
+
+* log-viscosity field g(x) = sum_{m=1..6} cos(2 pi k_m . x + phi_m) with integer
+  wave vectors 0 < |k_m| <= 4 and phases phi_m ~ U[0, 2 pi), normalised to
+  max |g| = 1 over every sample point; beta = exp(ln(C)/2 * g), so the
+  viscosity contrast is about C;
+* beta at cell centres, beta_ed at nodes (2D) or at xy/xz/yz edge midpoints
+  (3D), i.e. the layouts gmres(...) receives (src_gmres/gmres.f90:41-42,
+  src_gmres/stag_mg_solver.f90:178-194);
+* alpha_fc = 1 (the density rhotot_fc the time steppers pass,
+  src_multiSpec/advance_timestep_overdamped.f90:317);
+* b_u ~ N(0,1) i.i.d. per unique face with each component's mean removed,
+  b_p = 0, zero initial guess.
+
+Arrays are numpy float64 in the compact layout: shape (ny, nx) in 2D or
+(nz, ny, nx) in 3D, i fastest, periodic seam stored once.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class StokesProblem:
+    dm: int
+    n: tuple
+    dx: float
+    theta_alpha: float
+    alpha_fc: list
+    beta: np.ndarray
+    beta_ed: list
+    gamma: np.ndarray
+    b_u: list
+    b_p: np.ndarray
+    contrast: float
+    seed: int
+
+    @property
+    def shape(self):
+        return tuple(reversed(self.n[: self.dm]))
+
+    def zeros_like_solution(self):
+        return [np.zeros(self.shape) for _ in range(self.dm)], np.zeros(self.shape)
+
+
+def _wave_vectors(rng, dm, count=6, kmax=4):
+    ks = []
+    while len(ks) < count:
+        k = rng.integers(-kmax, kmax + 1, size=dm)
+        r2 = int((k * k).sum())
+        if 0 < r2 <= kmax * kmax:
+            ks.append(k.astype(np.float64))
+    return ks
+
+
+def _logfield(ks, phases, coords):
+    g = np.zeros(np.broadcast_shapes(*[c.shape for c in coords]))
+    for k, ph in zip(ks, phases):
+        arg = ph + 2.0 * math.pi * sum(k[d] * coords[d] for d in range(len(coords)))
+        g = g + np.cos(arg)
+    return g
+
+
+def _grids(n, dm, offsets):
+    """Coordinates (x, y[, z]) broadcast to the compact array shape, with
+    per-direction offsets in units of dx (0 = nodal, 0.5 = cell centred)."""
+    dx = 1.0 / n[0]
+    axes = []
+    for d in range(dm):
+        axes.append((np.arange(n[d]) + offsets[d]) * dx)
+    if dm == 2:
+        y, x = np.meshgrid(axes[1], axes[0], indexing="ij")
+        return [x, y]
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return [x, y, z]
+
+
+def viscosity_fields(dm, n, contrast, seed):
+    """beta at cells and beta_ed at nodes (2D) / edges xy, xz, yz (3D)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ks = _wave_vectors(rng, dm)
+    phases = rng.uniform(0.0, 2.0 * math.pi, size=len(ks))
+    cc = _logfield(ks, phases, _grids(n, dm, [0.5] * dm))
+    if dm == 2:
+        eds = [_logfield(ks, phases, _grids(n, dm, [0.0, 0.0]))]
+    else:
+        eds = [
+            _logfield(ks, phases, _grids(n, dm, [0.0, 0.0, 0.5])),  # xy edges
+            _logfield(ks, phases, _grids(n, dm, [0.0, 0.5, 0.0])),  # xz edges
+            _logfield(ks, phases, _grids(n, dm, [0.5, 0.0, 0.0])),  # yz edges
+        ]
+    gmax = max(np.abs(cc).max(), *[np.abs(e).max() for e in eds])
+    s = math.log(contrast) / 2.0 / gmax
+    beta = np.exp(s * cc)
+    beta_ed = [np.exp(s * e) for e in eds]
+    return beta, beta_ed, rng
+
+
+def make_problem(dm: int, n: int, contrast: float, seed: int, theta_alpha: float = 0.0,
+                 gamma_value: float = 0.0) -> StokesProblem:
+    nn = (n,) * dm
+    beta, beta_ed, rng = viscosity_fields(dm, nn, contrast, seed)
+    shape = tuple(reversed(nn))
+    b_u = []
+    for _ in range(dm):
+        r = rng.standard_normal(size=shape)
+        b_u.append(np.ascontiguousarray(r - r.mean()))
+    return StokesProblem(
+        dm=dm, n=nn + (1,) * (3 - dm), dx=1.0 / n, theta_alpha=float(theta_alpha),
+        alpha_fc=[np.ones(shape) for _ in range(dm)], beta=beta, beta_ed=beta_ed,
+        gamma=np.full(shape, float(gamma_value)), b_u=b_u, b_p=np.zeros(shape),
+        contrast=float(contrast), seed=int(seed))
+
+
+# Named workloads (the parity and benchmark configurations).
+def config_2d_64(seed: int = 0) -> StokesProblem:
+    """2D 64^2, contrast 10, steady (theta_alpha = 0)."""
+    return make_problem(2, 64, 10.0, seed, theta_alpha=0.0)
+
+
+def config_3d_128(seed: int = 0, n: int = 128) -> StokesProblem:
+    """3D n^3, contrast 100, inertial alpha = rho/dt with alpha*dx^2/beta0 = 0.1."""
+    dx = 1.0 / n
+    return make_problem(3, n, 100.0, seed, theta_alpha=0.1 / (dx * dx))
+
+
+def config_3d_64_learned(seed: int = 0, contrast: float = 1000.0) -> StokesProblem:
+    """3D 64^3 steady problems of the learned-preconditioner workload."""
+    return make_problem(3, 64, contrast, seed, theta_alpha=0.0)
