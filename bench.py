@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Benchmark: Stokes solves/s to 1e-9 relative residual on one B200.
+
+Workload: 3D 128^3 periodic variable-viscosity Stokes problem (contrast 100,
+inertial alpha = rho/dt with alpha*dx^2/beta0 = 0.1, seeded synthetic
+6-mode log-viscosity, N(0,1) mean-removed velocity rhs), block
+lower-triangular preconditioner (precon_type 2), visc_type -2.
+
+A step is one full solve.  Reported:
+  value   solves/s of the mixed-precision method (FP64 flexible GMRES around
+          an FP32 staggered V-cycle + FP32 pressure V-cycle), inputs resident
+          in HBM, each solve to |b-Ax|/|b| <= 1e-9 in FP64;
+  e2e     the same through the C ABI with host buffers (pinned numpy arrays,
+          host->device and device->host copies inside the timed region);
+  plain_fp64  the same FGMRES with the FP64 V-cycle (reference arithmetic);
+  reference_gmres  the reference's own algorithm (left-preconditioned
+          GMRES, FP64) timed on the GPU;
+  roofline of the dominant kernel (one Gauss-Seidel smooth of the finest
+          level), measured live with CUDA events on the solver's stream;
+  cpu_baseline  the CPU oracle (C++ restatement of the reference algorithm)
+          on a bounded sample of the same solve, rank 0 only.
+
+N > 1 GPUs: replicas only (one independent solve per GPU, a different seed
+per rank, no collective on the data path); value = total solves / max time.
+`--impl reference` times the CPU oracle (the reference Fortran cannot be
+built on this machine) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Stokes solves/s to 1e-9 rel. residual: plain FP64 vs mixed+learned, same B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_sample(prob, sample_iters: int, full_precon_applications: int, knobs_kw: dict):
+    """Time the oracle's reference GMRES on `sample_iters` inner iterations of
+    the same solve and scale to a full solve by preconditioner applications
+    (the V-cycles dominate both codes)."""
+    from oracle import oracle as O
+    k = O.default_knobs(**knobs_kw, gmres_max_iter=sample_iters)
+    t0 = time.perf_counter()
+    rc, _, _, _, _, st = O.solve(prob, k)
+    dt = time.perf_counter() - t0
+    # applications in the sample: |M^-1 b|, one per restart residual, one per inner iteration
+    sample_apps = 1 + (st["outer_iter"] + 1) + st["total_iter"]
+    solve_s = dt * full_precon_applications / sample_apps
+    return dt, sample_apps, solve_s
+
+
+def omp_threads():
+    try:
+        return int(os.environ.get("OMP_NUM_THREADS", "")) or os.cpu_count()
+    except ValueError:
+        return os.cpu_count()
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from lowmachmixtures_b200 import synth
+    from oracle import oracle as O
+    O.build()
+    prob = synth.config_3d_128(0, n=args.n)
+    kn = dict(precon_type=2, visc_type=-2)
+    # calibration: the oracle's preconditioner applications for the full solve
+    # come from one full solve on a 4x smaller grid in the number of
+    # iterations this workload needs (the GMRES iteration count is nearly
+    # size independent for this multigrid preconditioner)
+    calib = synth.config_3d_128(0, n=max(16, args.n // 4))
+    _, _, _, _, _, stc = O.solve(calib, O.default_knobs(**kn))
+    full_apps = 1 + (stc["outer_iter"] + 1) + stc["total_iter"]
+    sample_iters = 2
+    times = []
+    for s in range(args.warmup + args.steps):
+        dt, apps, solve_s = cpu_sample(prob, sample_iters, full_apps, kn)
+        if s >= args.warmup:
+            times.append(solve_s)
+    solve_s = sum(times) / len(times)
+    v = 1.0 / solve_s
+    cores = omp_threads()
+    sample = (f"{sample_iters} GMRES iterations ({apps} preconditioner applications) of the {args.n}^3 solve per step, "
+              f"scaled to a full solve's {full_apps} applications (counted on the {calib.n[0]}^3 solve)")
+    line = {
+        "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"stokes_3d_{args.n}^3_inertial_contrast100", "precon_type": 2,
+                   "method": "reference GMRES(5), FP64 (CPU oracle restating the Fortran; the Fortran itself "
+                             "cannot be built: no Fortran compiler, BoxLib not vendored)"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ product arm
+def run_product(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from lowmachmixtures_b200 import abi, synth
+    from lowmachmixtures_b200 import build as B
+    from lowmachmixtures_b200.gmres import StokesSolver
+
+    B.build()
+    torch.cuda.set_device(local)
+    n = args.n
+    prob = synth.config_3d_128(seed=rank, n=n)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    d_in = dict(b_u=[dev(a) for a in prob.b_u], b_p=dev(prob.b_p), alpha_fc=[dev(a) for a in prob.alpha_fc],
+                beta=dev(prob.beta), beta_ed=[dev(a) for a in prob.beta_ed], gamma=dev(prob.gamma))
+    d_xu = [torch.zeros_like(d_in["b_u"][0]) for _ in range(3)]
+    d_xp = torch.zeros_like(d_in["b_p"])
+    base = dict(precon_type=2, visc_type=-2)
+    mixed_kn = abi.make_knobs(**base, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
+    plain_kn = abi.make_knobs(**base, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP64)
+    ref_kn = abi.make_knobs(**base, method=abi.LMM_METHOD_GMRES)
+
+    def solve_dev(s):
+        for t in d_xu:
+            t.zero_()
+        d_xp.zero_()
+        return s.solve_device(d_in["b_u"], d_in["b_p"], d_xu, d_xp, d_in["alpha_fc"], d_in["beta"], d_in["beta_ed"],
+                              d_in["gamma"], prob.theta_alpha)
+
+    def timed_device(s, steps, warmup, clocks=None):
+        ext = torch.cuda.ExternalStream(s.stream_ptr())
+        for _ in range(warmup):
+            solve_dev(s)
+        barrier(world)
+        torch.cuda.synchronize()
+        l0 = s.lib.lmm_kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        if clocks:
+            clocks.__enter__()
+        e0.record(ext)
+        for _ in range(steps):
+            _, _, st = solve_dev(s)
+            stats.append(st)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.__exit__(None, None, None)
+        ms = e0.elapsed_time(e1)
+        barrier(world)
+        launches = s.lib.lmm_kernel_launches() - l0
+        return ms, stats, launches
+
+    mixed = StokesSolver(3, (n, n, n), prob.dx, knobs=mixed_kn, device=local)
+    plain = StokesSolver(3, (n, n, n), prob.dx, knobs=plain_kn, device=local)
+    refg = StokesSolver(3, (n, n, n), prob.dx, knobs=ref_kn, device=local)
+
+    clocks = ClockSampler(local)
+    ms_mixed, st_mixed, launches = timed_device(mixed, args.steps, args.warmup, clocks)
+    ms_mixed = max_over_ranks(world, ms_mixed)
+    total = sum_over_ranks(world, float(args.steps))
+    value = total / (ms_mixed / 1e3)
+
+    ms_plain, st_plain, _ = timed_device(plain, max(2, args.steps // 2), 1)
+    ms_plain = max_over_ranks(world, ms_plain)
+    plain_steps = max(2, args.steps // 2)
+    ms_ref, st_ref, _ = timed_device(refg, max(2, args.steps // 2), 1)
+    ms_ref = max_over_ranks(world, ms_ref)
+
+    # e2e through the C ABI with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    h_in = dict(b_u=[pin(a) for a in prob.b_u], b_p=pin(prob.b_p), alpha_fc=[pin(a) for a in prob.alpha_fc],
+                beta=pin(prob.beta), beta_ed=[pin(a) for a in prob.beta_ed], gamma=pin(prob.gamma))
+    h_xu = [pin(np.zeros(prob.shape)) for _ in range(3)]
+    h_xp = pin(np.zeros(prob.shape))
+
+    def solve_host():
+        for a in h_xu:
+            a[...] = 0.0
+        h_xp[...] = 0.0
+        return mixed.solve(h_in["b_u"], h_in["b_p"], h_xu, h_xp, h_in["alpha_fc"], h_in["beta"], h_in["beta_ed"],
+                           h_in["gamma"], prob.theta_alpha)
+
+    solve_host()
+    barrier(world)
+    torch.cuda.synchronize()
+    ext = torch.cuda.ExternalStream(mixed.stream_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solve_host()
+    t1 = time.perf_counter()
+    e1.record(ext)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(world, (t1 - t0) * 1e3)
+    e2e_value = total / (ms_e2e / 1e3)
+    nf = prob.shape[0] * prob.shape[1] * prob.shape[2]
+    h2d = 8 * nf * (3 + 1 + 3 + 1 + 3 + 1 + 3 + 1)  # b_u b_p alpha beta beta_ed gamma x0_u x0_p
+    d2h = 8 * nf * 4
+
+    # roofline: one Gauss-Seidel smooth of the finest level (6 colour kernels)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    ms_smooth32 = mixed.time_op(1, reps=20)
+    ms_smooth64 = plain.time_op(0, reps=20)
+    ms_apply64 = plain.time_op(2, reps=20)
+    ms_vc32 = mixed.time_op(5, reps=5)
+    ms_vc64 = plain.time_op(4, reps=5)
+    bytes_smooth32 = 16 * 4 * nf  # w(4F + N + E) with w = 4: phi r/w, rhs, alpha, beta_cc, 3 edges
+    bytes_smooth64 = 16 * 8 * nf
+    bytes_apply64 = 13 * 8 * nf   # w(3F + N + E): phi, alpha, beta, edges in; L out
+    gbs = lambda b, ms: b / (ms * 1e-3) / 1e9  # noqa: E731
+    roofline = {"bound": "hbm", "kernel": "gs_colour_fp32 (one full smooth: 6 colours, 128^3)",
+                "achieved": gbs(bytes_smooth32, ms_smooth32), "peak": peak, "unit": "GB/s",
+                "frac": gbs(bytes_smooth32, ms_smooth32) / peak, "traffic": None,
+                "peak_source": peak_src,
+                "algorithmic_bytes": bytes_smooth32, "ms_per_launch": ms_smooth32 / 6.0,
+                "ms_per_smooth": ms_smooth32}
+    kernels = {
+        "gs_smooth_fp64": {"ms": ms_smooth64, "GB/s": gbs(bytes_smooth64, ms_smooth64),
+                           "frac": gbs(bytes_smooth64, ms_smooth64) / peak},
+        "stag_applyop_fp64": {"ms": ms_apply64, "GB/s": gbs(bytes_apply64, ms_apply64),
+                              "frac": gbs(bytes_apply64, ms_apply64) / peak},
+        "vcycle_fp32_ms": ms_vc32, "vcycle_fp64_ms": ms_vc64,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 Krylov + f32 preconditioner", "data": "synthetic",
+        "config": {"workload": f"stokes_3d_{n}^3_inertial_contrast100", "n": n, "precon_type": 2, "visc_type": -2,
+                   "method": "FGMRES(5) FP64 + FP32 V-cycles", "rel_tol": 1e-9,
+                   "l2": "inputs larger than L2 (device working set > 2 GB per solve)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "iterations": [s["total_iter"] for s in st_mixed],
+        "true_rel_residual": [s["norm_resid_true"] / s["norm_b"] for s in st_mixed],
+        "plain_fp64": {"value": sum_over_ranks(world, float(plain_steps)) / (ms_plain / 1e3),
+                       "ms_per_step": ms_plain / plain_steps, "iterations": [s["total_iter"] for s in st_plain]},
+        "reference_gmres_gpu": {"value": sum_over_ranks(world, float(plain_steps)) / (ms_ref / 1e3),
+                                "ms_per_step": ms_ref / plain_steps,
+                                "iterations": [s["total_iter"] for s in st_ref]},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "kernels": kernels,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        full_apps = 1 + st_ref[-1]["outer_iter"] + 1 + st_ref[-1]["total_iter"]
+        dt, apps, solve_s = cpu_sample(prob, 2, full_apps, base)
+        line["cpu_baseline"] = {
+            "value": 1.0 / solve_s, "unit": "solves/s", "cores": omp_threads(), "kind": "port",
+            "sample": (f"oracle reference GMRES: 2 inner iterations ({apps} preconditioner applications, "
+                       f"{dt:.1f} s) of the same {n}^3 solve, scaled to the full solve's {full_apps} applications")}
+    for s in (mixed, plain, refg):
+        s.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # the CPU oracle runs on rank 0 only; other ranks exit without work
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        run_product(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -225,6 +225,23 @@ int lmm_op_sum_umac_press(lmm_handle* h, const double* const u[3], const double*
 /* Number of staggered MG levels (compute_nlevs_mg, stag_mg_layout.f90:179-222). */
 int lmm_op_num_levels(lmm_handle* h);
 
+/* ---- measurement hooks (no counterpart in the reference) ---------------- */
+
+/* Kernels this library has launched in this process so far. */
+int64_t lmm_kernel_launches(void);
+
+/* Average device time (CUDA events on the handle's stream) of `reps`
+ * repetitions of one hot operation on the finest level, using the
+ * coefficients and level-0 buffers of the last solve:
+ *   0 one Gauss-Seidel smooth, all 2*dm colours, FP64
+ *   1 the same in FP32
+ *   2 stag_applyop (all faces), FP64
+ *   3 apply_matrix, FP64
+ *   4 one staggered V-cycle, FP64
+ *   5 one staggered V-cycle, FP32
+ *   6 one pressure V-cycle, FP64                                        */
+int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_rep);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,70 @@
+"""Build liblmmstokes.so in-tree for sm_100a (B200).
+
+    python -m lowmachmixtures_b200.build
+
+The FP64 translation units are compiled with -fmad=false so that every
+multiply and add rounds separately in the reference's operand order; the FP32
+preconditioner unit keeps FMA contraction.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "liblmmstokes.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+          "--expt-relaxed-constexpr", "-I" + os.path.join(os.path.dirname(PKG), "include")]
+
+UNITS = [
+    ("kernels_fp64.cu", ["-fmad=false"]),
+    ("kernels_fp32.cu", ["-fmad=true"]),
+    ("krylov.cu", ["-fmad=false"]),
+    ("solver.cu", ["-fmad=false"]),
+]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(src_list, target) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in src_list)
+
+
+def build(verbose: bool = False, force: bool = False, extra: list | None = None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(os.path.dirname(PKG), "include", "lmm_stokes.h"))
+    objs = []
+    cc = nvcc()
+    for src, flags in UNITS:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _stale([s] + headers, o):
+            cmd = [cc, "-c", s, "-o", o] + ARCH + COMMON + flags + (extra or [])
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if force or _stale(objs, LIB):
+        cmd = [cc, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fPIC"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)

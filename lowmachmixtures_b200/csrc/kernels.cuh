@@ -1,0 +1,748 @@
+// kernels.cuh - implementations of the staggered Stokes kernels (templated on
+// the arithmetic type).  Included once per precision by kernels_fp64.cu and
+// kernels_fp32.cu, which instantiate the launchers of kernels.h.
+//
+// Reference loops restated (compact periodic layout, no ghost cells):
+//   stag_applyop_2d/_3d        src_common/stag_applyop.f90:204-1067
+//   stag_mg_update (+colours)  src_gmres/stag_mg_solver.f90:1637-2463
+//   residual + stag_restriction src_gmres/stag_mg_solver.f90:406-437, 1033-1175
+//   stag_prolongation          src_gmres/stag_mg_solver.f90:1424-1633
+//   coefficient coarsening     src_gmres/stag_mg_solver.f90:214-230, 873-968,
+//                              1229-1244, 1326-1367
+//   compute_div / compute_grad src_common/div_and_grad.f90:16-455
+//   subtract_weighted_gradp    src_gmres/macproject.f90:320-364
+//   norms / sum_umac_press     src_gmres/norm_inner_product.f90:16-794
+// The pressure multigrid kernels (cc_*) are this library's own cell-centred
+// V-cycle (the reference delegates to BoxLib F_MG, which it does not ship).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.h"
+#include "stencil.cuh"
+
+namespace lmm {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ void unflat(const Dims& D, int64_t t, int& i, int& j, int& k) {
+    i = (int)(t % D.nx);
+    int64_t r = t / D.nx;
+    j = (int)(r % D.ny);
+    k = (int)(r / D.ny);
+}
+
+static inline int nblocks_for(int64_t n, int threads = kThreads) {
+    int64_t b = (n + threads - 1) / threads;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// --------------------------------------------------------------- applyop
+template <class T, int DM, int VISC>
+__global__ void __launch_bounds__(kThreads) k_applyop(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
+                                                      const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
+                                                      T* __restrict__ o2, T dxsqinv, int color) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(D, t, i, j, k);
+    Nb nb = make_nb(D, i, j, k);
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    // colour c >= 1 covers component (c-1)/2, faces with (i+j+k) even for odd c
+    const int ccomp = (color - 1) / 2;
+    const bool on = (color == 0) || ((((i + j + k) & 1) == ((color % 2 == 1) ? 0 : 1)));
+    if (color == 0 || (ccomp == 0 && on)) o0[t] = face_L<T, DM, VISC, 0>(phi, C, nb, dxsqinv, b, c);
+    if (color == 0 || (ccomp == 1 && on)) o1[t] = face_L<T, DM, VISC, 1>(phi, C, nb, dxsqinv, b, c);
+    if constexpr (DM == 3)
+        if (color == 0 || (ccomp == 2 && on)) o2[t] = face_L<T, DM, VISC, 2>(phi, C, nb, dxsqinv, b, c);
+}
+
+// --------------------------------------------------------------- GS colour
+// One colour of stag_applyop_level(color) + stag_mg_update(color): faces of
+// component COMP with (i+j+k) % 2 == parity are updated in place.  Faces of
+// one colour never read each other (even cell counts), so the in-place
+// update equals the reference's compute-all-then-update order.
+template <class T, int DM, int VISC, int COMP>
+__global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const T* __restrict__ rhs, T* p0, T* p1, T* p2,
+                                                        int parity, T omega, T dxsqinv) {
+    const int hx = D.nx >> 1;
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)hx * D.ny * D.nz;
+    if (t >= n) return;
+    int ih = (int)(t % hx);
+    int64_t r = t / hx;
+    int j = (int)(r % D.ny);
+    int k = (int)(r / D.ny);
+    int i = 2 * ih + ((j + k + parity) & 1);
+    Nb nb = make_nb(D, i, j, k);
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    T Lp = face_L<T, DM, VISC, COMP>(phi, C, nb, dxsqinv, b, c);
+    T fac = face_diag<T, DM, VISC, COMP>(C, nb, dxsqinv, b, c);
+    T* p = (COMP == 0) ? p0 : (COMP == 1 ? p1 : p2);
+    T cur = p[nb.s];
+    p[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
+}
+
+// --------------------------------------------------------------- Jacobi
+template <class T, int DM, int VISC>
+__global__ void __launch_bounds__(kThreads) k_jacobi(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
+                                                     const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
+                                                     const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
+                                                     T* __restrict__ o2, T omega, T dxsqinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(D, t, i, j, k);
+    Nb nb = make_nb(D, i, j, k);
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    {
+        T Lp = face_L<T, DM, VISC, 0>(phi, C, nb, dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, 0>(C, nb, dxsqinv, b, c);
+        o0[t] = ld(p0, t) + omega * (ld(r0, t) - Lp) / fac;
+    }
+    {
+        T Lp = face_L<T, DM, VISC, 1>(phi, C, nb, dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, 1>(C, nb, dxsqinv, b, c);
+        o1[t] = ld(p1, t) + omega * (ld(r1, t) - Lp) / fac;
+    }
+    if constexpr (DM == 3) {
+        T Lp = face_L<T, DM, VISC, 2>(phi, C, nb, dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, 2>(C, nb, dxsqinv, b, c);
+        o2[t] = ld(p2, t) + omega * (ld(r2, t) - Lp) / fac;
+    }
+}
+
+// --------------------------------------------------------------- residual + restriction
+// residual of one fine face: (L phi - rhs) * -1  (stag_mg_solver.f90:414-415)
+template <class T, int DM, int VISC, int D_>
+__device__ __forceinline__ T fine_resid(const Dims& F, const Coef<T>& C, const T* const phi[3], const T* rhs, int i, int j, int k,
+                                        T dxsqinv, T b, T c) {
+    i = (i + F.nx) % F.nx;
+    j = (j + F.ny) % F.ny;
+    k = (DM == 3) ? (k + F.nz) % F.nz : 0;
+    Nb nb = make_nb(F, i, j, k);
+    T v = face_L<T, DM, VISC, D_>(phi, C, nb, dxsqinv, b, c) - ld(rhs, nb.s);
+    return v * T(-1);
+}
+
+template <class T, int DM, int VISC>
+__global__ void __launch_bounds__(kThreads) k_residual_restrict(Dims F, Coef<T> C, const T* __restrict__ r0,
+                                                                const T* __restrict__ r1, const T* __restrict__ r2,
+                                                                const T* __restrict__ p0, const T* __restrict__ p1,
+                                                                const T* __restrict__ p2, Dims Dc, T* __restrict__ c0,
+                                                                T* __restrict__ c1, T* __restrict__ c2, T dxsqinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)Dc.nx * Dc.ny * Dc.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(Dc, t, i, j, k);
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), cc = ld(C.gamma, 0);
+    const int I = 2 * i, J = 2 * j, K = 2 * k;
+#define RX(a, bb, ccc) fine_resid<T, DM, VISC, 0>(F, C, phi, r0, a, bb, ccc, dxsqinv, b, cc)
+#define RY(a, bb, ccc) fine_resid<T, DM, VISC, 1>(F, C, phi, r1, a, bb, ccc, dxsqinv, b, cc)
+#define RZ(a, bb, ccc) fine_resid<T, DM, VISC, 2>(F, C, phi, r2, a, bb, ccc, dxsqinv, b, cc)
+    if constexpr (DM == 2) {
+        c0[t] = T(0.25) * (RX(I, J, 0) + RX(I, J + 1, 0)) + T(0.125) * (RX(I + 1, J, 0) + RX(I + 1, J + 1, 0) + RX(I - 1, J, 0) + RX(I - 1, J + 1, 0));
+        c1[t] = T(0.25) * (RY(I, J, 0) + RY(I + 1, J, 0)) + T(0.125) * (RY(I, J + 1, 0) + RY(I + 1, J + 1, 0) + RY(I, J - 1, 0) + RY(I + 1, J - 1, 0));
+    } else {
+        c0[t] = T(0.125) * (RX(I, J, K) + RX(I, J + 1, K) + RX(I, J, K + 1) + RX(I, J + 1, K + 1)) +
+                T(0.0625) * (RX(I + 1, J, K) + RX(I + 1, J + 1, K) + RX(I + 1, J, K + 1) + RX(I + 1, J + 1, K + 1)) +
+                T(0.0625) * (RX(I - 1, J, K) + RX(I - 1, J + 1, K) + RX(I - 1, J, K + 1) + RX(I - 1, J + 1, K + 1));
+        c1[t] = T(0.125) * (RY(I, J, K) + RY(I + 1, J, K) + RY(I, J, K + 1) + RY(I + 1, J, K + 1)) +
+                T(0.0625) * (RY(I, J + 1, K) + RY(I + 1, J + 1, K) + RY(I, J + 1, K + 1) + RY(I + 1, J + 1, K + 1)) +
+                T(0.0625) * (RY(I, J - 1, K) + RY(I + 1, J - 1, K) + RY(I, J - 1, K + 1) + RY(I + 1, J - 1, K + 1));
+        c2[t] = T(0.125) * (RZ(I, J, K) + RZ(I + 1, J, K) + RZ(I, J + 1, K) + RZ(I + 1, J + 1, K)) +
+                T(0.0625) * (RZ(I, J, K + 1) + RZ(I + 1, J, K + 1) + RZ(I, J + 1, K + 1) + RZ(I + 1, J + 1, K + 1)) +
+                T(0.0625) * (RZ(I, J, K - 1) + RZ(I + 1, J, K - 1) + RZ(I, J + 1, K - 1) + RZ(I + 1, J + 1, K - 1));
+    }
+#undef RX
+#undef RY
+#undef RZ
+}
+
+// --------------------------------------------------------------- prolongation
+template <class T>
+__device__ __forceinline__ T cat(const T* a, const Dims& Dc, int i, int j, int k) {
+    i = (i + Dc.nx) % Dc.nx;
+    j = (j + Dc.ny) % Dc.ny;
+    k = (Dc.dm == 3) ? (k + Dc.nz) % Dc.nz : 0;
+    return ld(a, i + (int64_t)Dc.nx * (j + (int64_t)Dc.ny * k));
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_prolong_add(Dims F, Dims Dc, const T* __restrict__ q0, const T* __restrict__ q1,
+                                                          const T* __restrict__ q2, T* __restrict__ f0, T* __restrict__ f1,
+                                                          T* __restrict__ f2) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)F.nx * F.ny * F.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(F, t, i, j, k);
+    const int i2 = i / 2, j2 = j / 2, k2 = k / 2;
+    if constexpr (DM == 2) {
+        {
+            int joff = (j % 2 == 0) ? -1 : 1;
+            T v = f0[t];
+            if (i % 2 == 0)
+                v = v + T(0.75) * cat(q0, Dc, i2, j2, 0) + T(0.25) * cat(q0, Dc, i2, j2 + joff, 0);
+            else
+                v = v + T(0.375) * cat(q0, Dc, i2, j2, 0) + T(0.125) * cat(q0, Dc, i2, j2 + joff, 0) + T(0.375) * cat(q0, Dc, i2 + 1, j2, 0) +
+                    T(0.125) * cat(q0, Dc, i2 + 1, j2 + joff, 0);
+            f0[t] = v;
+        }
+        {
+            int ioff = (i % 2 == 0) ? -1 : 1;
+            T v = f1[t];
+            if (j % 2 == 0)
+                v = v + T(0.75) * cat(q1, Dc, i2, j2, 0) + T(0.25) * cat(q1, Dc, i2 + ioff, j2, 0);
+            else
+                v = v + T(0.375) * cat(q1, Dc, i2, j2, 0) + T(0.125) * cat(q1, Dc, i2 + ioff, j2, 0) + T(0.375) * cat(q1, Dc, i2, j2 + 1, 0) +
+                    T(0.125) * cat(q1, Dc, i2 + ioff, j2 + 1, 0);
+            f1[t] = v;
+        }
+    } else {
+        const T n16 = T(9.0 / 16.0), t16 = T(3.0 / 16.0), o16 = T(1.0 / 16.0);
+        const T n32 = T(9.0 / 32.0), t32 = T(3.0 / 32.0), o32 = T(1.0 / 32.0);
+        const int ioff = (i % 2 == 0) ? -1 : 1, joff = (j % 2 == 0) ? -1 : 1, koff = (k % 2 == 0) ? -1 : 1;
+        {
+            T v = f0[t];
+            if (i % 2 == 0)
+                v = v + n16 * cat(q0, Dc, i2, j2, k2) + t16 * cat(q0, Dc, i2, j2 + joff, k2) + t16 * cat(q0, Dc, i2, j2, k2 + koff) +
+                    o16 * cat(q0, Dc, i2, j2 + joff, k2 + koff);
+            else
+                v = v + n32 * cat(q0, Dc, i2, j2, k2) + t32 * cat(q0, Dc, i2, j2 + joff, k2) + t32 * cat(q0, Dc, i2, j2, k2 + koff) +
+                    o32 * cat(q0, Dc, i2, j2 + joff, k2 + koff) + n32 * cat(q0, Dc, i2 + 1, j2, k2) +
+                    t32 * cat(q0, Dc, i2 + 1, j2 + joff, k2) + t32 * cat(q0, Dc, i2 + 1, j2, k2 + koff) +
+                    o32 * cat(q0, Dc, i2 + 1, j2 + joff, k2 + koff);
+            f0[t] = v;
+        }
+        {
+            T v = f1[t];
+            if (j % 2 == 0)
+                v = v + n16 * cat(q1, Dc, i2, j2, k2) + t16 * cat(q1, Dc, i2 + ioff, j2, k2) + t16 * cat(q1, Dc, i2, j2, k2 + koff) +
+                    o16 * cat(q1, Dc, i2 + ioff, j2, k2 + koff);
+            else
+                v = v + n32 * cat(q1, Dc, i2, j2, k2) + t32 * cat(q1, Dc, i2 + ioff, j2, k2) + t32 * cat(q1, Dc, i2, j2, k2 + koff) +
+                    o32 * cat(q1, Dc, i2 + ioff, j2, k2 + koff) + n32 * cat(q1, Dc, i2, j2 + 1, k2) +
+                    t32 * cat(q1, Dc, i2 + ioff, j2 + 1, k2) + t32 * cat(q1, Dc, i2, j2 + 1, k2 + koff) +
+                    o32 * cat(q1, Dc, i2 + ioff, j2 + 1, k2 + koff);
+            f1[t] = v;
+        }
+        {
+            T v = f2[t];
+            if (k % 2 == 0)
+                v = v + n16 * cat(q2, Dc, i2, j2, k2) + t16 * cat(q2, Dc, i2 + ioff, j2, k2) + t16 * cat(q2, Dc, i2, j2 + joff, k2) +
+                    o16 * cat(q2, Dc, i2 + ioff, j2 + joff, k2);
+            else
+                v = v + n32 * cat(q2, Dc, i2, j2, k2) + t32 * cat(q2, Dc, i2 + ioff, j2, k2) + t32 * cat(q2, Dc, i2, j2 + joff, k2) +
+                    o32 * cat(q2, Dc, i2 + ioff, j2 + joff, k2) + n32 * cat(q2, Dc, i2, j2, k2 + 1) +
+                    t32 * cat(q2, Dc, i2 + ioff, j2, k2 + 1) + t32 * cat(q2, Dc, i2, j2 + joff, k2 + 1) +
+                    o32 * cat(q2, Dc, i2 + ioff, j2 + joff, k2 + 1);
+            f2[t] = v;
+        }
+    }
+}
+
+// --------------------------------------------------------------- coefficient coarsening
+template <class T>
+__device__ __forceinline__ T fat(const T* a, const Dims& F, int i, int j, int k) {
+    return ld(a, (i % F.nx) + (int64_t)F.nx * ((j % F.ny) + (int64_t)F.ny * (F.dm == 3 ? (k % F.nz) : 0)));
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> Cf, T* a0, T* a1, T* a2, T* beta, T* gamma,
+                                                      T* e0, T* e1, T* e2, int do_visc) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)Dc.nx * Dc.ny * Dc.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(Dc, t, i, j, k);
+    const int I = 2 * i, J = 2 * j, K = 2 * k;
+    if constexpr (DM == 2) {
+        a0[t] = T(0.5) * (fat(Cf.alpha[0], F, I, J, 0) + fat(Cf.alpha[0], F, I, J + 1, 0));
+        a1[t] = T(0.5) * (fat(Cf.alpha[1], F, I, J, 0) + fat(Cf.alpha[1], F, I + 1, J, 0));
+        if (do_visc) {
+            const T* b = Cf.beta;
+            beta[t] = T(0.25) * (fat(b, F, I, J, 0) + fat(b, F, I + 1, J, 0) + fat(b, F, I, J + 1, 0) + fat(b, F, I + 1, J + 1, 0));
+            const T* g = Cf.gamma;
+            gamma[t] = T(0.25) * (fat(g, F, I, J, 0) + fat(g, F, I + 1, J, 0) + fat(g, F, I, J + 1, 0) + fat(g, F, I + 1, J + 1, 0));
+            e0[t] = fat(Cf.bed[0], F, I, J, 0);  // nodal injection
+        }
+    } else {
+        const T* A0 = Cf.alpha[0];
+        const T* A1 = Cf.alpha[1];
+        const T* A2 = Cf.alpha[2];
+        a0[t] = T(0.25) * (fat(A0, F, I, J, K) + fat(A0, F, I, J + 1, K) + fat(A0, F, I, J, K + 1) + fat(A0, F, I, J + 1, K + 1));
+        a1[t] = T(0.25) * (fat(A1, F, I, J, K) + fat(A1, F, I + 1, J, K) + fat(A1, F, I, J, K + 1) + fat(A1, F, I + 1, J, K + 1));
+        a2[t] = T(0.25) * (fat(A2, F, I, J, K) + fat(A2, F, I + 1, J, K) + fat(A2, F, I, J + 1, K) + fat(A2, F, I + 1, J + 1, K));
+        if (do_visc) {
+            const T* b = Cf.beta;
+            beta[t] = T(0.125) * (fat(b, F, I, J, K) + fat(b, F, I + 1, J, K) + fat(b, F, I, J + 1, K) + fat(b, F, I + 1, J + 1, K) +
+                                  fat(b, F, I, J, K + 1) + fat(b, F, I + 1, J, K + 1) + fat(b, F, I, J + 1, K + 1) +
+                                  fat(b, F, I + 1, J + 1, K + 1));
+            const T* g = Cf.gamma;
+            gamma[t] = T(0.125) * (fat(g, F, I, J, K) + fat(g, F, I + 1, J, K) + fat(g, F, I, J + 1, K) + fat(g, F, I + 1, J + 1, K) +
+                                   fat(g, F, I, J, K + 1) + fat(g, F, I + 1, J, K + 1) + fat(g, F, I, J + 1, K + 1) +
+                                   fat(g, F, I + 1, J + 1, K + 1));
+            e0[t] = T(0.5) * (fat(Cf.bed[0], F, I, J, K) + fat(Cf.bed[0], F, I, J, K + 1));
+            e1[t] = T(0.5) * (fat(Cf.bed[1], F, I, J, K) + fat(Cf.bed[1], F, I, J + 1, K));
+            e2[t] = T(0.5) * (fat(Cf.bed[2], F, I, J, K) + fat(Cf.bed[2], F, I + 1, J, K));
+        }
+    }
+}
+
+// --------------------------------------------------------------- pressure multigrid
+template <class T, int DM>
+__device__ __forceinline__ T cc_lap(const T* const a[3], const T* phi, const Nb& n, T dxsqinv) {
+    const int64_t s = n.s;
+    const T p = ld(phi, s);
+    T v = (ld(a[0], s + n.op[0]) * (ld(phi, s + n.op[0]) - p) - ld(a[0], s) * (p - ld(phi, s + n.om[0]))) +
+          (ld(a[1], s + n.op[1]) * (ld(phi, s + n.op[1]) - p) - ld(a[1], s) * (p - ld(phi, s + n.om[1])));
+    if constexpr (DM == 3) v = v + (ld(a[2], s + n.op[2]) * (ld(phi, s + n.op[2]) - p) - ld(a[2], s) * (p - ld(phi, s + n.om[2])));
+    return v * dxsqinv;
+}
+template <class T, int DM>
+__device__ __forceinline__ T cc_diag(const T* const a[3], const Nb& n, T dxsqinv) {
+    const int64_t s = n.s;
+    T sum = ld(a[0], s) + ld(a[0], s + n.op[0]) + ld(a[1], s) + ld(a[1], s + n.op[1]);
+    if constexpr (DM == 3) sum = sum + ld(a[2], s) + ld(a[2], s + n.op[2]);
+    return -(sum * dxsqinv);
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ rhs,
+                                                        T* phi, int parity, T dxsqinv) {
+    const int hx = D.nx >> 1;
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)hx * D.ny * D.nz;
+    if (t >= n) return;
+    int ih = (int)(t % hx);
+    int64_t r = t / hx;
+    int j = (int)(r % D.ny);
+    int k = (int)(r / D.ny);
+    int i = 2 * ih + ((j + k + parity) & 1);
+    Nb nb = make_nb(D, i, j, k);
+    const T* a[3] = {a0, a1, a2};
+    T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
+    T cur = phi[nb.s];
+    phi[nb.s] = cur + res / cc_diag<T, DM>(a, nb, dxsqinv);
+}
+
+template <class T, int DM>
+__device__ __forceinline__ T cc_res_at(const Dims& F, const T* const a[3], const T* phi, const T* rhs, int i, int j, int k,
+                                       T dxsqinv) {
+    Nb nb = make_nb(F, i, j, k);
+    return ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const T* a0, const T* a1, const T* a2,
+                                                                   const T* __restrict__ rhs, const T* __restrict__ phi, Dims Dc,
+                                                                   T* __restrict__ rc, T dxsqinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)Dc.nx * Dc.ny * Dc.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(Dc, t, i, j, k);
+    const T* a[3] = {a0, a1, a2};
+    const int I = 2 * i, J = 2 * j, K = 2 * k;
+#define R(ii, jj, kk) cc_res_at<T, DM>(F, a, phi, rhs, ii, jj, kk, dxsqinv)
+    if constexpr (DM == 2)
+        rc[t] = T(0.25) * (R(I, J, 0) + R(I + 1, J, 0) + R(I, J + 1, 0) + R(I + 1, J + 1, 0));
+    else
+        rc[t] = T(0.125) * (R(I, J, K) + R(I + 1, J, K) + R(I, J + 1, K) + R(I + 1, J + 1, K) + R(I, J, K + 1) + R(I + 1, J, K + 1) +
+                            R(I, J + 1, K + 1) + R(I + 1, J + 1, K + 1));
+#undef R
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_cc_prolong_add(Dims F, Dims Dc, const T* __restrict__ pc, T* __restrict__ pf) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)F.nx * F.ny * F.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(F, t, i, j, k);
+    pf[t] = pf[t] + ld(pc, (i / 2) + (int64_t)Dc.nx * ((j / 2) + (int64_t)Dc.ny * (k / 2)));
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_neg_cc_lap(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ phi,
+                                                         T* __restrict__ out, T dxsqinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(D, t, i, j, k);
+    Nb nb = make_nb(D, i, j, k);
+    const T* a[3] = {a0, a1, a2};
+    out[t] = -cc_lap<T, DM>(a, phi, nb, dxsqinv);
+}
+
+// --------------------------------------------------------------- div / grad pieces
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_div_plus(Dims D, const T* __restrict__ u0, const T* __restrict__ u1,
+                                                       const T* __restrict__ u2, const T* __restrict__ bp, T* __restrict__ out,
+                                                       T dxinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(D, t, i, j, k);
+    Nb nb = make_nb(D, i, j, k);
+    T v = (ld(u0, t + nb.op[0]) - ld(u0, t)) * dxinv + (ld(u1, t + nb.op[1]) - ld(u1, t)) * dxinv;
+    if constexpr (DM == 3) v = v + (ld(u2, t + nb.op[2]) - ld(u2, t)) * dxinv;
+    out[t] = v + ld(bp, t);
+}
+
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_sub_weighted_grad(Dims D, const T* c0, const T* c1, const T* c2,
+                                                                const T* __restrict__ phi, T* u0, T* u1, T* u2, T dxinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat(D, t, i, j, k);
+    Nb nb = make_nb(D, i, j, k);
+    const T p = ld(phi, t);
+    T* u[3] = {u0, u1, u2};
+    const T* c[3] = {c0, c1, c2};
+#pragma unroll
+    for (int d = 0; d < DM; ++d) {
+        T g = (p - ld(phi, t + nb.om[d])) * dxinv;
+        if (c[d]) g = g * ld(c[d], t);
+        u[d][t] = u[d][t] + T(-1) * g;
+    }
+}
+
+// --------------------------------------------------------------- small vector ops
+template <class Tin, class Tout>
+__global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) out[t] = (Tout)in[t];
+}
+template <class T>
+__global__ void k_scale_copy(const T* __restrict__ in, T* __restrict__ out, T s, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) out[t] = in[t] * s;
+}
+template <class T>
+__global__ void k_recip(const T* __restrict__ in, T* __restrict__ out, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) out[t] = T(1) / in[t];
+}
+template <class T>
+__global__ void k_fill(T* __restrict__ out, T v, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) out[t] = v;
+}
+
+// --------------------------------------------------------------- deterministic reductions
+// Each block accumulates a fixed grid-stride subset in double, reduces it in
+// a fixed tree, writes its partials; the last block to finish sums all
+// partials in block order.  The result depends only on n and the launch
+// shape, never on scheduling.
+// MODE 0: weighted dot, MODE 1: weighted sum, MODE 2: max |a - b| (inf norm).
+// out[0..dm] per component; out[4] = sum_d out[d] + pw^2 out[dm] (the
+// Hessenberg entry of gmres.f90:344), out[5] = sqrt(|u|^2 + (pw |p|)^2)
+// (the Stokes norm of gmres.f90:127-130).
+template <class T, int DM, int MODE>
+__global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const T* a1, const T* a2, const T* a3, const T* b0,
+                                                     const T* b1, const T* b2, const T* b3, double w0, double w1, double w2,
+                                                     double pw, double* partials, unsigned* counter, double* out) {
+    constexpr int NC = DM + 1;
+    const T* A[4] = {a0, a1, a2, a3};
+    const T* B[4] = {b0, b1, b2, b3};
+    const double W[3] = {w0, w1, w2};
+    double acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+    const int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) {
+        int i, j, k;
+        unflat(D, t, i, j, k);
+        const int idx[3] = {i, j, k};
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const T* a = (c < DM) ? A[c] : A[3];
+            const T* b = (c < DM) ? B[c] : B[3];
+            if (!a) continue;
+            double v = (double)ld(a, t);
+            if (MODE == 2) {
+                v = fabs(v - (b ? (double)ld(b, t) : 0.0));
+                acc[c] = fmax(acc[c], v);
+                continue;
+            }
+            if (MODE == 0) v = v * (double)ld(b, t);
+            if (c < DM && idx[c] == 0) v = v * W[c];
+            acc[c] += v;
+        }
+    }
+    __shared__ double sh[NC][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) {
+            double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = (MODE == 2) ? fmax(v, u) : v + u;
+        }
+        if (lane == 0) sh[c][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < NC; ++c) {
+            double v = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) v = (MODE == 2) ? fmax(v, sh[c][w]) : v + sh[c][w];
+            partials[(int64_t)blockIdx.x * NC + c] = v;
+        }
+        __threadfence();
+    }
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        unsigned prev = atomicAdd(counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // fixed-order final sum: thread c handles component c over all blocks
+    __shared__ double fin[4];
+    if (threadIdx.x < NC) {
+        const int c = threadIdx.x;
+        double v = 0.0;
+        for (unsigned bidx = 0; bidx < gridDim.x; ++bidx) {
+            double q = ((volatile double*)partials)[(int64_t)bidx * NC + c];
+            v = (MODE == 2) ? fmax(v, q) : v + q;
+        }
+        fin[c] = v;
+        out[c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double su = 0.0;
+        for (int c = 0; c < DM; ++c) su = su + fin[c];
+        out[4] = su + (pw * pw) * fin[DM];
+        double nu = sqrt(su);
+        double np = pw * sqrt(fin[DM]);
+        out[5] = sqrt(nu * nu + np * np);
+        *counter = 0u;
+    }
+}
+
+// =============================================================== launchers
+#define LMM_VISC_DISPATCH(VISC, ...)                      \
+    switch (VISC) {                                       \
+    case -1: { constexpr int V = -1; __VA_ARGS__; } break; \
+    case 1: { constexpr int V = 1; __VA_ARGS__; } break;   \
+    case -2: { constexpr int V = -2; __VA_ARGS__; } break; \
+    case 2: { constexpr int V = 2; __VA_ARGS__; } break;   \
+    case -3: { constexpr int V = -3; __VA_ARGS__; } break; \
+    case 3: { constexpr int V = 3; __VA_ARGS__; } break;   \
+    default: break;                                       \
+    }
+
+template <class T>
+void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color) {
+    const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    const int nb = nblocks_for(L.n);
+    if (L.D.dm == 2) {
+        LMM_VISC_DISPATCH(visc, (k_applyop<T, 2, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+    } else {
+        LMM_VISC_DISPATCH(visc, (k_applyop<T, 3, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+    }
+}
+
+template <class T>
+void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega,
+                      cudaStream_t s) {
+    const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    const int comp = (color - 1) / 2;
+    const int parity = (color % 2 == 1) ? 0 : 1;
+    const int nb = nblocks_for(L.n / 2);
+    const T om = (T)omega;
+#define GS(DM_, COMP_) k_gs_colour<T, DM_, V, COMP_><<<nb, kThreads, 0, s>>>(L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
+    if (L.D.dm == 2) {
+        if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
+        else { LMM_VISC_DISPATCH(visc, GS(2, 1)) }
+    } else {
+        if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(3, 0)) }
+        else if (comp == 1) { LMM_VISC_DISPATCH(visc, GS(3, 1)) }
+        else { LMM_VISC_DISPATCH(visc, GS(3, 2)) }
+    }
+#undef GS
+}
+
+template <class T>
+void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const pin[3], T* const pout[3],
+                   double omega, cudaStream_t s) {
+    const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    const int nb = nblocks_for(L.n);
+    const T om = (T)omega;
+    if (L.D.dm == 2) {
+        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 2, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+    } else {
+        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 3, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+    }
+}
+
+template <class T>
+void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
+                              const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s) {
+    const T dxsqinv = T(1.0 / (F.dx * F.dx));
+    const int nb = nblocks_for(Cc.n);
+    if (F.D.dm == 2) {
+        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 2, V><<<nb, kThreads, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
+    } else {
+        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 3, V><<<nb, kThreads, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
+    }
+}
+
+template <class T>
+void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3],
+                        cudaStream_t s) {
+    const int nb = nblocks_for(F.n);
+    if (F.D.dm == 2)
+        k_prolong_add<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+    else
+        k_prolong_add<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+}
+
+template <class T>
+void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s) {
+    const int nb = nblocks_for(Cc.n);
+    Coef<T> cf = F.coef();
+    if (pressure_faces) {
+        for (int d = 0; d < 3; ++d) cf.alpha[d] = F.pa[d];
+        if (F.D.dm == 2)
+            k_coarsen<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+        else
+            k_coarsen<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+        return;
+    }
+    if (F.D.dm == 2)
+        k_coarsen<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
+    else
+        k_coarsen<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
+}
+
+template <class T>
+void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s) {
+    const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    const int nb = nblocks_for(L.n / 2);
+    if (L.D.dm == 2)
+        k_cc_smooth<T, 2><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+    else
+        k_cc_smooth<T, 3><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+}
+
+template <class T>
+void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s) {
+    const T dxsqinv = T(1.0 / (F.dx * F.dx));
+    const int nb = nblocks_for(Cc.n);
+    if (F.D.dm == 2)
+        k_cc_residual_restrict<T, 2><<<nb, kThreads, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+    else
+        k_cc_residual_restrict<T, 3><<<nb, kThreads, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+}
+
+template <class T>
+void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s) {
+    const int nb = nblocks_for(F.n);
+    if (F.D.dm == 2)
+        k_cc_prolong_add<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
+    else
+        k_cc_prolong_add<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
+}
+
+template <class T>
+void launch_neg_cc_lap(const LevelDev<T>& L, const T* phi, T* out, cudaStream_t s) {
+    const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    const int nb = nblocks_for(L.n);
+    if (L.D.dm == 2)
+        k_neg_cc_lap<T, 2><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
+    else
+        k_neg_cc_lap<T, 3><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
+}
+
+template <class T>
+void launch_div_plus(const LevelDev<T>& L, const T* const u[3], const T* bp, T* out, cudaStream_t s) {
+    const T dxinv = T(1.0 / L.dx);
+    const int nb = nblocks_for(L.n);
+    if (L.D.dm == 2)
+        k_div_plus<T, 2><<<nb, kThreads, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+    else
+        k_div_plus<T, 3><<<nb, kThreads, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+}
+
+template <class T>
+void launch_sub_weighted_grad(const LevelDev<T>& L, const T* const coef[3], const T* phi, T* const u[3], cudaStream_t s) {
+    const T dxinv = T(1.0 / L.dx);
+    const int nb = nblocks_for(L.n);
+    const T* c0 = coef ? coef[0] : nullptr;
+    const T* c1 = coef ? coef[1] : nullptr;
+    const T* c2 = coef ? coef[2] : nullptr;
+    if (L.D.dm == 2)
+        k_sub_weighted_grad<T, 2><<<nb, kThreads, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+    else
+        k_sub_weighted_grad<T, 3><<<nb, kThreads, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+}
+
+template <class Tin, class Tout>
+void launch_convert(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
+    k_convert<Tin, Tout><<<nblocks_for(n), kThreads, 0, s>>>(in, out, n);
+}
+template <class T>
+void launch_scale_copy(const T* in, T* out, double scale, int64_t n, cudaStream_t s) {
+    k_scale_copy<T><<<nblocks_for(n), kThreads, 0, s>>>(in, out, (T)scale, n);
+}
+template <class T>
+void launch_recip(const T* in, T* out, int64_t n, cudaStream_t s) {
+    k_recip<T><<<nblocks_for(n), kThreads, 0, s>>>(in, out, n);
+}
+template <class T>
+void launch_fill(T* out, double v, int64_t n, cudaStream_t s) {
+    k_fill<T><<<nblocks_for(n), kThreads, 0, s>>>(out, (T)v, n);
+}
+
+template <class T>
+void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const b[4], const double wseam[3], double pw,
+                   double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s) {
+#define RED(DM_, M_) k_reduce<T, DM_, M_><<<nblocks, kThreads, 0, s>>>(D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out)
+    if (D.dm == 2) {
+        if (mode == 0) RED(2, 0); else if (mode == 1) RED(2, 1); else RED(2, 2);
+    } else {
+        if (mode == 0) RED(3, 0); else if (mode == 1) RED(3, 1); else RED(3, 2);
+    }
+#undef RED
+}
+
+#define LMM_INSTANTIATE(T)                                                                                                     \
+    template void launch_applyop<T>(const LevelDev<T>&, int, const T* const[3], T* const[3], cudaStream_t, int);              \
+    template void launch_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t);     \
+    template void launch_jacobi<T>(const LevelDev<T>&, int, const T* const[3], const T* const[3], T* const[3], double,         \
+                                   cudaStream_t);                                                                              \
+    template void launch_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, int, const T* const[3],                  \
+                                              const T* const[3], T* const[3], cudaStream_t);                                   \
+    template void launch_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, const T* const[3], T* const[3], cudaStream_t); \
+    template void launch_coarsen_coeffs<T>(const LevelDev<T>&, const LevelDev<T>&, bool, cudaStream_t);                        \
+    template void launch_cc_smooth<T>(const LevelDev<T>&, int, cudaStream_t);                                                   \
+    template void launch_cc_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, cudaStream_t);                        \
+    template void launch_cc_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, cudaStream_t);                              \
+    template void launch_neg_cc_lap<T>(const LevelDev<T>&, const T*, T*, cudaStream_t);                                        \
+    template void launch_div_plus<T>(const LevelDev<T>&, const T* const[3], const T*, T*, cudaStream_t);                        \
+    template void launch_sub_weighted_grad<T>(const LevelDev<T>&, const T* const[3], const T*, T* const[3], cudaStream_t);     \
+    template void launch_scale_copy<T>(const T*, T*, double, int64_t, cudaStream_t);                                           \
+    template void launch_recip<T>(const T*, T*, int64_t, cudaStream_t);                                                        \
+    template void launch_fill<T>(T*, double, int64_t, cudaStream_t);                                                           \
+    template void launch_reduce<T>(const Dims&, int, const T* const[4], const T* const[4], const double[3], double,            \
+                                   double*, unsigned*, double*, int, cudaStream_t);
+
+}  // namespace lmm

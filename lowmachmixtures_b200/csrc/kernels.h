@@ -1,0 +1,106 @@
+// kernels.h - host-side launchers of the staggered Stokes kernels.
+//
+// Every launcher is templated on the arithmetic type T (double for the
+// reference-faithful path, float for the mixed-precision preconditioner) and
+// explicitly instantiated in kernels_fp64.cu (built with -fmad=false) and
+// kernels_fp32.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "stencil.cuh"
+
+namespace lmm {
+
+// One level of the staggered hierarchy on the device (compact layout).
+template <class T>
+struct LevelDev {
+    Dims D;
+    double dx;
+    int64_t n;          // cells (= faces per component)
+    T* alpha[3];        // theta*alpha at this level
+    T* beta;
+    T* bed[3];
+    T* gamma;
+    T* phi[3];
+    T* rhs[3];
+    T* tmp[3];          // Jacobi output / scratch
+    // pressure (cell-centred) multigrid level
+    T* pa[3];           // face coefficient 1/alpha (coarsened)
+    T* pphi;
+    T* prhs;
+    T* ptmp;
+    Coef<T> coef() const {
+        Coef<T> c;
+        for (int d = 0; d < 3; ++d) { c.alpha[d] = alpha[d]; c.bed[d] = bed[d]; }
+        c.beta = beta;
+        c.gamma = gamma;
+        return c;
+    }
+};
+
+// ---- staggered operator / multigrid ----
+// color 0: every face; 1..2*dm: only the faces of that Gauss-Seidel colour
+template <class T>
+void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color);
+template <class T>
+void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega,
+                      cudaStream_t s);
+template <class T>
+void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const phi_in[3], T* const phi_out[3],
+                   double omega, cudaStream_t s);
+template <class T>
+void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
+                              const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s);
+template <class T>
+void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3],
+                        cudaStream_t s);
+template <class T>
+void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s);
+
+// ---- pressure multigrid (this library's cell-centred V-cycle) ----
+template <class T>
+void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s);
+template <class T>
+void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s);
+template <class T>
+void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s);
+template <class T>
+void launch_neg_cc_lap(const LevelDev<T>& L, const T* phi, T* out, cudaStream_t s);
+
+// ---- elementwise pieces of apply_precon (level-0 geometry) ----
+// mac_rhs = div(u) + b_p
+template <class T>
+void launch_div_plus(const LevelDev<T>& L, const T* const u[3], const T* bp, T* out, cudaStream_t s);
+// u -= coef * grad(phi); coef == nullptr means coefficient 1
+template <class T>
+void launch_sub_weighted_grad(const LevelDev<T>& L, const T* const coef[3], const T* phi, T* const u[3], cudaStream_t s);
+
+// ---- conversions and small vector ops ----
+template <class Tin, class Tout>
+void launch_convert(const Tin* in, Tout* out, int64_t n, cudaStream_t s);
+template <class T>
+void launch_scale_copy(const T* in, T* out, double scale, int64_t n, cudaStream_t s);
+template <class T>
+void launch_recip(const T* in, T* out, int64_t n, cudaStream_t s);
+template <class T>
+void launch_fill(T* out, double v, int64_t n, cudaStream_t s);
+
+// Deterministic weighted sums over one level-0 vector:
+//   mode 0: out[c] = sum_w a_c * b_c   (stag_inner_prod / cc_inner_prod weights)
+//   mode 1: out[c] = sum_w a_c         (sum_umac_press weights)
+//   mode 2: out[c] = max |a_c - b_c|   (multifab_norm_inf_c)
+// components c = 0..dm-1 are faces, c = dm the cell field (weight 1).
+// a entries may be nullptr to skip a component.  out[4] and out[5] receive
+// the combined Hessenberg entry and Stokes norm (see k_reduce).
+template <class T>
+void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const b[4], const double wseam[3], double pw,
+                   double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s);
+
+int reduce_blocks(int64_t n);
+// one kernel launch issued (counted by check_launch after every launch site)
+void count_launch();
+int64_t launches_total();
+
+}  // namespace lmm

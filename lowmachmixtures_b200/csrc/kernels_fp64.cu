@@ -1,0 +1,11 @@
+// kernels_fp64.cu - FP64 instantiation of the staggered Stokes kernels.
+// Built with -fmad=false: every multiply and add is rounded separately, in
+// the operand order of the reference Fortran, so face values match the
+// reference arithmetic (and the CPU oracle) bit for bit.
+#include "kernels.cuh"
+
+namespace lmm {
+LMM_INSTANTIATE(double)
+template void launch_convert<double, float>(const double*, float*, int64_t, cudaStream_t);
+template void launch_convert<float, double>(const float*, double*, int64_t, cudaStream_t);
+}  // namespace lmm

@@ -1,0 +1,283 @@
+// krylov.cu - FP64 Krylov-side kernels (see krylov.cuh).  Built with
+// -fmad=false so every operation rounds like the reference Fortran.
+#include "krylov.cuh"
+#include "stencil.cuh"
+
+namespace lmm {
+
+namespace {
+constexpr int kT = 256;
+inline int nb(int64_t n) { return (int)((n + kT - 1) / kT < 1 ? 1 : (n + kT - 1) / kT); }
+
+__device__ __forceinline__ void unflat3(const Dims& D, int64_t t, int& i, int& j, int& k) {
+    i = (int)(t % D.nx);
+    int64_t r = t / D.nx;
+    j = (int)(r % D.ny);
+    k = (int)(r / D.ny);
+}
+}  // namespace
+
+// b_u = stag_applyop(x_u) + grad(x_p);  b_p = -div(x_u)   (apply_matrix.f90:96-112)
+template <int DM, int VISC>
+__global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, const double* __restrict__ u0,
+                                                     const double* __restrict__ u1, const double* __restrict__ u2,
+                                                     const double* __restrict__ p, double* __restrict__ o0,
+                                                     double* __restrict__ o1, double* __restrict__ o2, double* __restrict__ op,
+                                                     double dxsqinv, double dxinv) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat3(D, t, i, j, k);
+    Nb nbr = make_nb(D, i, j, k);
+    const double* phi[3] = {u0, u1, u2};
+    const double b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    const double pc = ld(p, t);
+    {
+        double L = face_L<double, DM, VISC, 0>(phi, C, nbr, dxsqinv, b, c);
+        double g = (pc - ld(p, t + nbr.om[0])) * dxinv;
+        o0[t] = L + g;
+    }
+    {
+        double L = face_L<double, DM, VISC, 1>(phi, C, nbr, dxsqinv, b, c);
+        double g = (pc - ld(p, t + nbr.om[1])) * dxinv;
+        o1[t] = L + g;
+    }
+    double dv = (ld(u0, t + nbr.op[0]) - ld(u0, t)) * dxinv + (ld(u1, t + nbr.op[1]) - ld(u1, t)) * dxinv;
+    if constexpr (DM == 3) {
+        double L = face_L<double, DM, VISC, 2>(phi, C, nbr, dxsqinv, b, c);
+        double g = (pc - ld(p, t + nbr.om[2])) * dxinv;
+        o2[t] = L + g;
+        dv = dv + (ld(u2, t + nbr.op[2]) - ld(u2, t)) * dxinv;
+    }
+    op[t] = dv * -1.0;
+}
+
+void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s) {
+    const double dxsqinv = 1.0 / (L0.dx * L0.dx);
+    const double dxinv = 1.0 / L0.dx;
+    const int g = nb(L0.n);
+    const double* x2 = (x.dm == 3) ? x.c(2) : x.c(0);
+    double* b2 = (b.dm == 3) ? b.c(2) : b.c(0);
+#define AM(DM_, V_) k_apply_matrix<DM_, V_><<<g, kT, 0, s>>>(L0.D, L0.coef(), x.c(0), x.c(1), x2, x.p(), b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
+#define AMV(DM_)                    \
+    switch (visc) {                 \
+    case -1: AM(DM_, -1); break;    \
+    case 1: AM(DM_, 1); break;      \
+    case -2: AM(DM_, -2); break;    \
+    case 2: AM(DM_, 2); break;      \
+    case -3: AM(DM_, -3); break;    \
+    case 3: AM(DM_, 3); break;      \
+    }
+    if (x.dm == 2) {
+        AMV(2)
+    } else {
+        AMV(3)
+    }
+#undef AMV
+#undef AM
+}
+
+__global__ void k_neg_resid(double* __restrict__ out, const double* __restrict__ b, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        double v = out[t] - b[t];
+        out[t] = v * -1.0;
+    }
+}
+void launch_neg_resid(double* out, const double* b, int64_t n, cudaStream_t s) { k_neg_resid<<<nb(n), kT, 0, s>>>(out, b, n); }
+
+__global__ void k_div_by(const double* __restrict__ w, double* __restrict__ v, const double* __restrict__ den, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) v[t] = w[t] / *den;
+}
+void launch_div_by(const double* w, double* v, const double* den, int64_t n, cudaStream_t s) {
+    k_div_by<<<nb(n), kT, 0, s>>>(w, v, den, n);
+}
+
+__global__ void k_sub_scaled(double* __restrict__ w, const double* __restrict__ V, const double* __restrict__ h, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        double tmp = V[t] * *h;
+        w[t] = w[t] - tmp;
+    }
+}
+void launch_sub_scaled(double* w, const double* V, const double* h, int64_t n, cudaStream_t s) {
+    k_sub_scaled<<<nb(n), kT, 0, s>>>(w, V, h, n);
+}
+
+__global__ void k_add_scaled(double* __restrict__ x, const double* __restrict__ V, double y, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        double tmp = V[t] * y;
+        x[t] = x[t] + tmp;
+    }
+}
+void launch_add_scaled(double* x, const double* V, double y, int64_t n, cudaStream_t s) { k_add_scaled<<<nb(n), kT, 0, s>>>(x, V, y, n); }
+
+__global__ void k_add_scaled_f32(double* __restrict__ x, const float* __restrict__ Z, double y, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        double tmp = (double)Z[t] * y;
+        x[t] = x[t] + tmp;
+    }
+}
+void launch_add_scaled_f32(double* x, const float* Z, double y, int64_t n, cudaStream_t s) {
+    k_add_scaled_f32<<<nb(n), kT, 0, s>>>(x, Z, y, n);
+}
+
+// ---------------------------------------------------------------- Schur complement pieces
+template <class T>
+__global__ void k_schur(int mode, int pt, int av, double theta, const T* __restrict__ mac, const T* __restrict__ src,
+                        const T* __restrict__ beta, const T* __restrict__ gamma, T* __restrict__ phi, const T* __restrict__ bp,
+                        T* __restrict__ xp, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const T th = (T)theta;
+    T x = 0;
+    if (mode == 0) {  // simple_schur_complement (apply_precon.f90:485-528) [+ sign flip :244-249]
+        if (av == 1 || av == 2) {
+            x = mac[t] * T(-1);
+            x = x * beta[t];
+            if (av == 2) x = x * T(2);
+        } else {
+            x = mac[t] * T(-4.0 / 3.0);
+            x = x * beta[t];
+            T m2 = mac[t] * T(-1);
+            m2 = m2 * gamma[t];
+            x = x + m2;
+        }
+        if (fabs(theta) > 0.0) {
+            T ph = phi[t] * th;
+            phi[t] = ph;
+            x = x + ph;
+        }
+        if (pt == -2 || pt == -5) x = x * T(-1);
+    } else if (mode == 1) {  // projection preconditioner (apply_precon.f90:140-188)
+        T sv = (pt == 1 || theta == 0.0) ? mac[t] * T(-1) : src[t];
+        if (av == 1 || av == 2) {
+            x = sv * beta[t];
+            if (av == 2) x = x * T(2);
+        } else {
+            T m2 = sv * gamma[t];
+            x = sv * beta[t];
+            x = x * T(4.0 / 3.0);
+            x = x + m2;
+        }
+        T ph = phi[t] * th;
+        phi[t] = ph;
+        x = x + ph;
+    } else {  // block diagonal (apply_precon.f90:380-416)
+        T ph = phi[t];
+        if (fabs(theta) > 0.0) {
+            ph = ph * th;
+            phi[t] = ph;
+        }
+        x = bp[t] * beta[t];
+        x = x - ph;
+        if (av == 1 && pt == 4) {
+            x = x * T(-1);
+        } else if (av == 2 && pt == 4) {
+            x = x * T(-2);
+        } else if (av == 2 && pt == -4) {
+            x = x * T(2);
+        } else if (av == 3 && pt == 4) {
+            x = x * T(-4.0 / 3.0);
+            T q = bp[t] * gamma[t];
+            q = q * T(-1);
+            x = x + q;
+        } else if (av == 3 && pt == -4) {
+            x = x * T(4.0 / 3.0);
+            T q = bp[t] * gamma[t];
+            x = x + q;
+        }
+    }
+    xp[t] = x;
+}
+
+template <class T>
+void launch_schur(int mode, int precon_type, int visc_abs, double theta_alpha, const T* mac_rhs, const T* src,
+                  const T* beta, const T* gamma, T* phi, const T* bp, T* xp, int64_t n, cudaStream_t s) {
+    k_schur<T><<<nb(n), kT, 0, s>>>(mode, precon_type, visc_abs, theta_alpha, mac_rhs, src, beta, gamma, phi, bp, xp, n);
+}
+template void launch_schur<double>(int, int, int, double, const double*, const double*, const double*, const double*, double*,
+                                   const double*, double*, int64_t, cudaStream_t);
+template void launch_schur<float>(int, int, int, double, const float*, const float*, const float*, const float*, float*,
+                                  const float*, float*, int64_t, cudaStream_t);
+
+// ---------------------------------------------------------------- mean removal
+template <class T, int DM>
+__global__ void k_sub_means(Dims D, T* u0, T* u1, T* u2, T* p, const double* __restrict__ sums, double total_volume, int sub_u) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    const double mp = sums[DM] / total_volume;
+    p[t] = (T)((double)p[t] - mp);
+    if (sub_u) {
+        T* u[3] = {u0, u1, u2};
+#pragma unroll
+        for (int d = 0; d < DM; ++d) {
+            const double mu = sums[d] / total_volume;
+            u[d][t] = (T)((double)u[d][t] - mu);
+        }
+    }
+}
+
+template <class T>
+void launch_sub_means(const Dims& D, T* const u[3], T* p, const double* sums, double total_volume, int sub_u, cudaStream_t s) {
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (D.dm == 2)
+        k_sub_means<T, 2><<<nb(n), kT, 0, s>>>(D, u[0], u[1], u[2], p, sums, total_volume, sub_u);
+    else
+        k_sub_means<T, 3><<<nb(n), kT, 0, s>>>(D, u[0], u[1], u[2], p, sums, total_volume, sub_u);
+}
+template void launch_sub_means<double>(const Dims&, double* const[3], double*, const double*, double, int, cudaStream_t);
+template void launch_sub_means<float>(const Dims&, float* const[3], float*, const double*, double, int, cudaStream_t);
+
+// ---------------------------------------------------------------- layouts
+int64_t boxlib_size(const Dims& D, const int nodal[3], int ng) {
+    int64_t s = 1;
+    const int n[3] = {D.nx, D.ny, D.nz};
+    for (int d = 0; d < D.dm; ++d) s *= (int64_t)(n[d] + nodal[d] + 2 * ng);
+    return s;
+}
+
+__global__ void k_gather_boxlib(Dims D, int ex, int ey, int ng, const double* __restrict__ in, double* __restrict__ out) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    if (t >= n) return;
+    int i, j, k;
+    unflat3(D, t, i, j, k);
+    const int kg = (D.dm == 3) ? ng : 0;
+    out[t] = in[(int64_t)(i + ng) + (int64_t)ex * ((j + ng) + (int64_t)ey * (k + kg))];
+}
+
+__global__ void k_scatter_boxlib(Dims D, int ex, int ey, int ez, int ng, const double* __restrict__ in, double* __restrict__ out) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t n = (int64_t)ex * ey * ez;
+    if (t >= n) return;
+    int I = (int)(t % ex);
+    int64_t r = t / ex;
+    int J = (int)(r % ey);
+    int K = (int)(r / ey);
+    const int kg = (D.dm == 3) ? ng : 0;
+    int i = ((I - ng) % D.nx + D.nx) % D.nx;
+    int j = ((J - ng) % D.ny + D.ny) % D.ny;
+    int k = (D.dm == 3) ? ((K - kg) % D.nz + D.nz) % D.nz : 0;
+    out[t] = in[(int64_t)i + (int64_t)D.nx * (j + (int64_t)D.ny * k)];
+}
+
+void launch_gather_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s) {
+    const int ex = D.nx + nodal[0] + 2 * ng, ey = D.ny + nodal[1] + 2 * ng;
+    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    k_gather_boxlib<<<nb(n), kT, 0, s>>>(D, ex, ey, ng, in, out);
+}
+
+void launch_scatter_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s) {
+    const int ex = D.nx + nodal[0] + 2 * ng, ey = D.ny + nodal[1] + 2 * ng;
+    const int ez = (D.dm == 3) ? D.nz + nodal[2] + 2 * ng : 1;
+    int64_t n = (int64_t)ex * ey * ez;
+    k_scatter_boxlib<<<nb(n), kT, 0, s>>>(D, ex, ey, ez, ng, in, out);
+}
+
+}  // namespace lmm

@@ -1,0 +1,58 @@
+// krylov.cuh - FP64 Krylov-side kernels: the fused Stokes operator, the
+// BLAS-1 steps of GMRES, the block-preconditioner pointwise steps and the
+// BoxLib <-> compact layout converters.  Built into krylov.cu with
+// -fmad=false (reference rounding).
+//
+//   apply_matrix      src_gmres/apply_matrix.f90:96-112
+//   residual, MGS, V(i+1) = w/H, update_sol
+//                     src_gmres/gmres.f90:186-194, 338-375, 481-515
+//   simple_schur_complement / P1 / P4 pressure updates
+//                     src_gmres/apply_precon.f90:140-188, 380-416, 479-534
+//   mean removal      src_gmres/apply_precon.f90:433-460
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.h"
+
+namespace lmm {
+
+// Stokes vector: dm face components then the cell field, each n entries,
+// contiguous (c * n offsets).
+struct SVec {
+    double* base = nullptr;
+    int64_t n = 0;
+    int dm = 0;
+    double* c(int k) const { return base + (int64_t)k * n; }
+    double* p() const { return base + (int64_t)dm * n; }
+    int64_t size() const { return (int64_t)(dm + 1) * n; }
+};
+
+void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s);
+// out = (out - b) * -1  (gmres.f90:186-194)
+void launch_neg_resid(double* out, const double* b, int64_t n, cudaStream_t s);
+// v = w / (*den)   (multifab_div_div_s_c)
+void launch_div_by(const double* w, double* v, const double* den, int64_t n, cudaStream_t s);
+// w = w - V * (*h)
+void launch_sub_scaled(double* w, const double* V, const double* h, int64_t n, cudaStream_t s);
+// x = x + V * y
+void launch_add_scaled(double* x, const double* V, double y, int64_t n, cudaStream_t s);
+void launch_add_scaled_f32(double* x, const float* Z, double y, int64_t n, cudaStream_t s);
+
+// pressure updates of apply_precon: mode 0 simple Schur (P2/P3/P5),
+// mode 1 projection (P1), mode 2 block diagonal (P4)
+template <class T>
+void launch_schur(int mode, int precon_type, int visc_abs, double theta_alpha, const T* mac_rhs, const T* src,
+                  const T* beta, const T* gamma, T* phi, const T* bp, T* xp, int64_t n, cudaStream_t s);
+// x_p -= <p>; x_u[d] -= <u_d> when sub_u (means from reduction slots)
+template <class T>
+void launch_sub_means(const Dims& D, T* const u[3], T* p, const double* sums, double total_volume, int sub_u,
+                      cudaStream_t s);
+
+// BoxLib <-> compact (ng ghost layers, nodal flags per direction)
+void launch_gather_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s);
+void launch_scatter_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s);
+int64_t boxlib_size(const Dims& D, const int nodal[3], int ng);
+
+}  // namespace lmm

@@ -1,0 +1,1534 @@
+// solver.cu - the gmres(...) replacement: persistent device workspace, the
+// staggered V-cycle driver, the pressure V-cycle, apply_precon for every
+// precon_type, the reference GMRES and the flexible GMRES, and the C ABI.
+//
+// Reference control flow restated here:
+//   gmres             src_gmres/gmres.f90:30-605
+//   apply_precon      src_gmres/apply_precon.f90:29-536
+//   stag_mg_solver    src_gmres/stag_mg_solver.f90:37-868 (V-cycle order,
+//                     colour order 1..2*dm, bottom smooths, coefficient
+//                     coarsening hoisted to once per solve)
+//   macproject        src_gmres/macproject.f90:34-318 (front end; the
+//                     V-cycle is this library's own design)
+// Scalars of the Arnoldi process (H, norms) stay on the device; the host
+// reads one Hessenberg column per inner iteration to run the Givens
+// rotations and the stopping tests exactly as the reference does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lmm_stokes.h"
+#include "kernels.h"
+#include "krylov.cuh"
+
+using namespace lmm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define LMM_CK(call)                                                                     \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);           \
+            throw LmmError(LMM_ERR_CUDA);                                                \
+        }                                                                                \
+    } while (0)
+
+struct LmmError {
+    int code;
+    explicit LmmError(int c) : code(c) {}
+};
+
+inline void check_launch() {
+    lmm::count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_last_error = std::string("kernel launch: ") + cudaGetErrorString(e);
+        throw LmmError(LMM_ERR_CUDA);
+    }
+}
+
+int compute_nlevs(const int n[3], int dm, int minwidth) {
+    int nl = -1;
+    for (int d = 0; d < dm; ++d) {
+        int temp = n[d], rdir = 1;
+        while (temp % 2 == 0 && temp / minwidth != 1) {
+            temp /= 2;
+            ++rdir;
+        }
+        nl = (nl == -1) ? rdir : std::min(nl, rdir);
+    }
+    return nl;
+}
+
+}  // namespace
+
+// ============================================================ handle
+struct lmm_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    lmm_grid grid{};
+    lmm_knobs knobs{};
+    int dm = 0;
+    int64_t n = 0;
+    Dims D0{};
+    int nlev = 0;      // staggered levels
+    int nlev_p = 0;    // pressure levels
+    std::vector<LevelDev<double>> L64;
+    std::vector<LevelDev<float>> L32;
+    // arena
+    char* arena = nullptr;
+    size_t arena_bytes = 0, arena_used = 0;
+    // level-0 unscaled inputs (compact)
+    double* alpha_fc[3] = {nullptr, nullptr, nullptr};
+    double* alphainv[3] = {nullptr, nullptr, nullptr};
+    float* alphainv32[3] = {nullptr, nullptr, nullptr};
+    // Krylov storage
+    int m = 0;
+    std::vector<SVec> V;
+    std::vector<SVec> Z64;
+    std::vector<float*> Z32;  // (dm+1)*n floats each
+    SVec b, x, r, w, tmp, zt;
+    // apply_precon scratch (FP64 and FP32)
+    double *mac64 = nullptr, *src64 = nullptr, *xptmp64 = nullptr, *butmp64[3] = {nullptr, nullptr, nullptr};
+    float *mac32 = nullptr, *src32 = nullptr, *xptmp32 = nullptr, *butmp32[3] = {nullptr, nullptr, nullptr};
+    float* pin32 = nullptr;   // FP32 copy of a Stokes vector (precon input)
+    float* pout32 = nullptr;  // FP32 precon output
+    // reductions
+    double* partials = nullptr;
+    unsigned* counter = nullptr;
+    double* scal = nullptr;       // device scalar slots (8 doubles per slot)
+    double* hscal = nullptr;      // pinned host mirror
+    int red_blocks = 0;
+    static constexpr int kSlots = 256;
+    // BoxLib staging
+    double* stage = nullptr;
+    int64_t stage_elems = 0;
+    // statistics
+    int vcycles = 0, pvcycles = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool coeffs_loaded = false;
+    double theta_loaded = 0.0;
+
+    template <class T>
+    T* alloc(int64_t count) {
+        size_t bytes = ((size_t)count * sizeof(T) + 255) & ~(size_t)255;
+        if (arena_used + bytes > arena_bytes) throw LmmError(LMM_ERR_CUDA);
+        T* p = reinterpret_cast<T*>(arena + arena_used);
+        arena_used += bytes;
+        return p;
+    }
+    double* slot(int k) { return scal + 8 * k; }
+};
+
+namespace {
+
+int64_t level_cells(const int n[3], int dm, int lev) {
+    int64_t c = 1;
+    for (int d = 0; d < dm; ++d) c *= (n[d] >> lev);
+    return c;
+}
+
+size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
+    const int dm = g.dm;
+    const int ne = (dm == 2) ? 1 : 3;
+    size_t tot = 0;
+    auto add = [&](int64_t count, size_t sz) { tot += ((size_t)count * sz + 255) & ~(size_t)255; };
+    for (int l = 0; l < std::max(nlev, nlev_p); ++l) {
+        int64_t c = level_cells(g.n, dm, l);
+        for (int prec = 0; prec < 2; ++prec) {
+            size_t sz = prec ? sizeof(float) : sizeof(double);
+            if (l < nlev) {
+                for (int q = 0; q < 4 * dm + ne + 2; ++q) add(c, sz);  // alpha, phi, rhs, tmp, bed, beta, gamma
+            }
+            if (l < nlev_p) {
+                for (int q = 0; q < dm + 3; ++q) add(c, sz);
+            }
+        }
+    }
+    int64_t n = level_cells(g.n, dm, 0);
+    int64_t vec = (int64_t)(dm + 1) * n;
+    add(n, sizeof(double) * 2 * dm);                    // alpha_fc, alphainv
+    add(n, sizeof(float) * dm);                         // alphainv32
+    add(vec * (k.gmres_max_inner + 1), sizeof(double)); // V
+    if (k.method == LMM_METHOD_FGMRES) {
+        if (k.precision == LMM_PRECISION_FP32)
+            add(vec * k.gmres_max_inner, sizeof(float));
+        else
+            add(vec * k.gmres_max_inner, sizeof(double));
+    }
+    for (int q = 0; q < 6; ++q) add(vec, sizeof(double));  // b x r w tmp zt
+    for (int q = 0; q < 3 + dm; ++q) add(n, sizeof(double));
+    for (int q = 0; q < 3 + dm; ++q) add(n, sizeof(float));
+    add(vec, sizeof(float));
+    add(vec, sizeof(float));
+    add(4096 * 4, sizeof(double));
+    add(64, sizeof(unsigned));
+    add(8 * lmm_handle::kSlots, sizeof(double));
+    // BoxLib staging: the largest field with up to 4 ghost layers
+    int64_t st = 1;
+    for (int d = 0; d < dm; ++d) st *= (g.n[d] + 1 + 8);
+    add(st, sizeof(double));
+    return tot + (1 << 20);
+}
+
+template <class T>
+std::vector<LevelDev<T>>& levels(lmm_handle* h);
+template <>
+std::vector<LevelDev<double>>& levels<double>(lmm_handle* h) { return h->L64; }
+template <>
+std::vector<LevelDev<float>>& levels<float>(lmm_handle* h) { return h->L32; }
+
+template <class T>
+void build_levels(lmm_handle* h) {
+    auto& L = levels<T>(h);
+    const int dm = h->dm;
+    const int nl = std::max(h->nlev, h->nlev_p);
+    L.resize(nl);
+    for (int l = 0; l < nl; ++l) {
+        LevelDev<T>& v = L[l];
+        std::memset(&v, 0, sizeof(v));
+        v.D.dm = dm;
+        v.D.nx = h->grid.n[0] >> l;
+        v.D.ny = h->grid.n[1] >> l;
+        v.D.nz = (dm == 3) ? (h->grid.n[2] >> l) : 1;
+        v.dx = h->grid.dx * (double)(1 << l);
+        v.n = (int64_t)v.D.nx * v.D.ny * v.D.nz;
+        if (l < h->nlev) {
+            for (int d = 0; d < dm; ++d) {
+                v.alpha[d] = h->alloc<T>(v.n);
+                v.phi[d] = h->alloc<T>(v.n);
+                v.rhs[d] = h->alloc<T>(v.n);
+                v.tmp[d] = h->alloc<T>(v.n);
+            }
+            for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) v.bed[e] = h->alloc<T>(v.n);
+            v.beta = h->alloc<T>(v.n);
+            v.gamma = h->alloc<T>(v.n);
+        }
+        if (l < h->nlev_p) {
+            for (int d = 0; d < dm; ++d) v.pa[d] = h->alloc<T>(v.n);
+            v.pphi = h->alloc<T>(v.n);
+            v.prhs = h->alloc<T>(v.n);
+            v.ptmp = h->alloc<T>(v.n);
+        }
+    }
+}
+
+SVec make_svec(lmm_handle* h) {
+    SVec s;
+    s.n = h->n;
+    s.dm = h->dm;
+    s.base = h->alloc<double>(s.size());
+    return s;
+}
+
+// ------------------------------------------------------------ reductions
+void stokes_reduce(lmm_handle* h, int mode, const double* const a[4], const double* const b[4], int slot) {
+    double w[3];
+    if (mode == 0) {
+        w[0] = w[1] = w[2] = 3.0;  // each seam face is stored twice and weighed 1.5 per copy
+    } else {
+        // sum_umac_press: the x tiles span the box (weight 3 at the seam);
+        // y/z tiles of 8 cells span it only when n < 16 (else weight 2).
+        const int tile[3] = {1024000, 8, 8};
+        for (int d = 0; d < 3; ++d) {
+            int nd = (d < h->dm) ? h->grid.n[d] : 1;
+            w[d] = (nd / tile[d] < 2) ? 3.0 : 2.0;
+        }
+    }
+    launch_reduce<double>(h->D0, mode, a, b, w, h->knobs.p_norm_weight, h->partials, h->counter, h->slot(slot),
+                          h->red_blocks, h->stream);
+    check_launch();
+}
+
+void svec_ptrs(const SVec& v, const double* p[4]) {
+    for (int c = 0; c < 3; ++c) p[c] = (c < v.dm) ? v.c(c) : nullptr;
+    p[3] = v.p();
+}
+
+// slot[4] = Hessenberg dot, slot[5] = Stokes norm
+void stokes_dot(lmm_handle* h, const SVec& a, const SVec& b, int slot) {
+    const double* pa[4];
+    const double* pb[4];
+    svec_ptrs(a, pa);
+    svec_ptrs(b, pb);
+    stokes_reduce(h, 0, pa, pb, slot);
+}
+void stokes_norm(lmm_handle* h, const SVec& a, int slot) { stokes_dot(h, a, a, slot); }
+
+double read_slot(lmm_handle* h, int slot, int idx) {
+    LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(slot), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    LMM_CK(cudaStreamSynchronize(h->stream));
+    return h->hscal[idx];
+}
+
+// ------------------------------------------------------------ coefficients
+// Level-0 coefficients in FP64 (theta*alpha, beta, beta_ed, gamma), the
+// hierarchy by coarsening (stag_mg_solver.f90:200-230, hoisted out of the
+// V-cycle), 1/alpha for the pressure solve and the FP32 copies.
+void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* beta, const double* const bed[3],
+                 const double* gamma, double theta) {
+    const int dm = h->dm;
+    LevelDev<double>& L0 = h->L64[0];
+    const int64_t n = h->n;
+    for (int d = 0; d < dm; ++d) {
+        if (alpha_dev[d] != h->alpha_fc[d])
+            LMM_CK(cudaMemcpyAsync(h->alpha_fc[d], alpha_dev[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        launch_scale_copy<double>(h->alpha_fc[d], L0.alpha[d], theta, n, h->stream);
+        launch_recip<double>(h->alpha_fc[d], h->alphainv[d], n, h->stream);
+        check_launch();
+    }
+    if (beta != L0.beta) LMM_CK(cudaMemcpyAsync(L0.beta, beta, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (gamma) {
+        if (gamma != L0.gamma) LMM_CK(cudaMemcpyAsync(L0.gamma, gamma, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        LMM_CK(cudaMemsetAsync(L0.gamma, 0, n * sizeof(double), h->stream));
+    }
+    for (int e = 0; e < (dm == 2 ? 1 : 3); ++e)
+        if (bed[e] != L0.bed[e]) LMM_CK(cudaMemcpyAsync(L0.bed[e], bed[e], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    for (int l = 1; l < h->nlev; ++l) {
+        launch_coarsen_coeffs<double>(h->L64[l - 1], h->L64[l], false, h->stream);
+        check_launch();
+    }
+    // pressure face coefficients 1/alpha_fc, coarsened by face averaging
+    if (h->nlev_p > 0) {
+        for (int d = 0; d < dm; ++d)
+            LMM_CK(cudaMemcpyAsync(h->L64[0].pa[d], h->alphainv[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        for (int l = 1; l < h->nlev_p; ++l) {
+            launch_coarsen_coeffs<double>(h->L64[l - 1], h->L64[l], true, h->stream);
+            check_launch();
+        }
+    }
+    if (h->knobs.precision == LMM_PRECISION_FP32) {
+        for (int l = 0; l < (int)h->L64.size(); ++l) {
+            LevelDev<double>& a = h->L64[l];
+            LevelDev<float>& b = h->L32[l];
+            if (l < h->nlev) {
+                for (int d = 0; d < dm; ++d) launch_convert<double, float>(a.alpha[d], b.alpha[d], a.n, h->stream);
+                for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) launch_convert<double, float>(a.bed[e], b.bed[e], a.n, h->stream);
+                launch_convert<double, float>(a.beta, b.beta, a.n, h->stream);
+                launch_convert<double, float>(a.gamma, b.gamma, a.n, h->stream);
+            }
+            if (l < h->nlev_p)
+                for (int d = 0; d < dm; ++d) launch_convert<double, float>(a.pa[d], b.pa[d], a.n, h->stream);
+            check_launch();
+        }
+        for (int d = 0; d < dm; ++d) launch_convert<double, float>(h->alphainv[d], h->alphainv32[d], n, h->stream);
+        check_launch();
+    }
+    h->coeffs_loaded = true;
+    h->theta_loaded = theta;
+}
+
+// ------------------------------------------------------------ staggered V-cycle
+template <class T>
+void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
+    const lmm_knobs& K = h->knobs;
+    for (int m = 0; m < nsm; ++m) {
+        if (K.stag_mg_smoother == 0) {
+            launch_jacobi<T>(L, K.visc_type, L.rhs, L.phi, L.tmp, K.stag_mg_omega, h->stream);
+            check_launch();
+            for (int d = 0; d < h->dm; ++d)
+                LMM_CK(cudaMemcpyAsync(L.phi[d], L.tmp[d], L.n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+        } else {
+            for (int color = 1; color <= 2 * h->dm; ++color) {
+                launch_gs_colour<T>(L, K.visc_type, color, L.rhs, L.phi, K.stag_mg_omega, h->stream);
+                check_launch();
+            }
+        }
+    }
+}
+
+template <class T>
+void vcycle(lmm_handle* h, std::vector<LevelDev<T>>& L) {
+    const lmm_knobs& K = h->knobs;
+    const int nl = h->nlev;
+    for (int l = 1; l < nl; ++l)
+        for (int d = 0; d < h->dm; ++d) LMM_CK(cudaMemsetAsync(L[l].phi[d], 0, L[l].n * sizeof(T), h->stream));
+    for (int l = 0; l < nl - 1; ++l) {
+        smooth<T>(h, L[l], K.stag_mg_nsmooths_down);
+        launch_residual_restrict<T>(L[l], L[l + 1], K.visc_type, L[l].rhs, L[l].phi, L[l + 1].rhs, h->stream);
+        check_launch();
+    }
+    smooth<T>(h, L[nl - 1], K.stag_mg_nsmooths_bottom);
+    for (int l = nl - 2; l >= 0; --l) {
+        launch_prolong_add<T>(L[l], L[l + 1], L[l + 1].phi, L[l].phi, h->stream);
+        check_launch();
+        smooth<T>(h, L[l], K.stag_mg_nsmooths_up);
+    }
+}
+
+// inf-norm of (L phi - rhs) per component at level 0 (stag_mg_solver.f90:259-270, 766-786)
+template <class T>
+void mg_resid_inf(lmm_handle* h, LevelDev<T>& L0, int slot);
+
+template <>
+void mg_resid_inf<double>(lmm_handle* h, LevelDev<double>& L0, int slot) {
+    launch_applyop<double>(L0, h->knobs.visc_type, L0.phi, L0.tmp, h->stream, 0);
+    check_launch();
+    const double* a[4] = {L0.tmp[0], L0.tmp[1], h->dm == 3 ? L0.tmp[2] : nullptr, nullptr};
+    const double* b[4] = {L0.rhs[0], L0.rhs[1], h->dm == 3 ? L0.rhs[2] : nullptr, nullptr};
+    const double w[3] = {1, 1, 1};
+    launch_reduce<double>(h->D0, 2, a, b, w, 0.0, h->partials, h->counter, h->slot(slot), h->red_blocks, h->stream);
+    check_launch();
+}
+template <>
+void mg_resid_inf<float>(lmm_handle* h, LevelDev<float>& L0, int slot) {
+    launch_applyop<float>(L0, h->knobs.visc_type, L0.phi, L0.tmp, h->stream, 0);
+    check_launch();
+    const float* a[4] = {L0.tmp[0], L0.tmp[1], h->dm == 3 ? L0.tmp[2] : nullptr, nullptr};
+    const float* b[4] = {L0.rhs[0], L0.rhs[1], h->dm == 3 ? L0.rhs[2] : nullptr, nullptr};
+    const double w[3] = {1, 1, 1};
+    launch_reduce<float>(h->D0, 2, a, b, w, 0.0, h->partials, h->counter, h->slot(slot), h->red_blocks, h->stream);
+    check_launch();
+}
+
+// stag_mg_solver: phi (initial guess) and rhs live in L[0].phi / L[0].rhs
+template <class T>
+void stag_mg_solver(lmm_handle* h) {
+    auto& L = levels<T>(h);
+    const lmm_knobs& K = h->knobs;
+    const int dm = h->dm;
+    if (K.stag_mg_max_vcycles <= 1) {
+        vcycle<T>(h, L);
+    } else {
+        const int s0 = h->kSlots - 2, s1 = h->kSlots - 1;
+        mg_resid_inf<T>(h, L[0], s0);
+        double r0[3] = {0, 0, 0};
+        LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(s0), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        bool all_zero = true, any_zero = false;
+        for (int d = 0; d < dm; ++d) {
+            r0[d] = h->hscal[d];
+            all_zero = all_zero && r0[d] == 0.0;
+            any_zero = any_zero || r0[d] == 0.0;
+        }
+        if (!all_zero) {
+            if (any_zero) {
+                double mx = 0;
+                for (int d = 0; d < dm; ++d) mx = std::max(mx, r0[d]);
+                for (int d = 0; d < dm; ++d) r0[d] = mx;
+            }
+            for (int vc = 1; vc <= K.stag_mg_max_vcycles; ++vc) {
+                vcycle<T>(h, L);
+                mg_resid_inf<T>(h, L[0], s1);
+                LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(s1), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                LMM_CK(cudaStreamSynchronize(h->stream));
+                bool done = true;
+                for (int d = 0; d < dm; ++d) done = done && (h->hscal[d] / r0[d] < K.stag_mg_rel_tol);
+                if (done) break;
+            }
+        }
+    }
+    h->vcycles += dm * K.stag_mg_max_vcycles;
+}
+
+// ------------------------------------------------------------ pressure V-cycle
+template <class T>
+void cc_smooth(lmm_handle* h, LevelDev<T>& L, int nsweeps) {
+    for (int s = 0; s < nsweeps; ++s)
+        for (int parity = 0; parity < 2; ++parity) {
+            launch_cc_smooth<T>(L, parity, h->stream);
+            check_launch();
+        }
+}
+
+// phi (L[0].pphi) <- mg_max_vcycles V-cycles of div(a grad phi) = L[0].prhs
+template <class T>
+void macproject(lmm_handle* h) {
+    auto& L = levels<T>(h);
+    const lmm_knobs& K = h->knobs;
+    const int nl = h->nlev_p;
+    LMM_CK(cudaMemsetAsync(L[0].pphi, 0, L[0].n * sizeof(T), h->stream));
+    for (int vc = 0; vc < K.mg_max_vcycles; ++vc) {
+        for (int l = 1; l < nl; ++l) LMM_CK(cudaMemsetAsync(L[l].pphi, 0, L[l].n * sizeof(T), h->stream));
+        for (int l = 0; l < nl - 1; ++l) {
+            cc_smooth<T>(h, L[l], K.mg_nsmooths_down);
+            launch_cc_residual_restrict<T>(L[l], L[l + 1], h->stream);
+            check_launch();
+        }
+        cc_smooth<T>(h, L[nl - 1], K.mg_nsmooths_bottom);
+        for (int l = nl - 2; l >= 0; --l) {
+            launch_cc_prolong_add<T>(L[l], L[l + 1], h->stream);
+            check_launch();
+            cc_smooth<T>(h, L[l], K.mg_nsmooths_up);
+        }
+    }
+    h->pvcycles += K.mg_max_vcycles;
+}
+
+// ------------------------------------------------------------ apply_precon
+template <class T>
+struct PrecScratch {
+    T* mac;
+    T* src;
+    T* xptmp;
+    T* butmp[3];
+    T* alphainv[3];
+};
+template <class T>
+PrecScratch<T> prec_scratch(lmm_handle* h);
+template <>
+PrecScratch<double> prec_scratch<double>(lmm_handle* h) {
+    return {h->mac64, h->src64, h->xptmp64, {h->butmp64[0], h->butmp64[1], h->butmp64[2]},
+            {h->alphainv[0], h->alphainv[1], h->alphainv[2]}};
+}
+template <>
+PrecScratch<float> prec_scratch<float>(lmm_handle* h) {
+    return {h->mac32, h->src32, h->xptmp32, {h->butmp32[0], h->butmp32[1], h->butmp32[2]},
+            {h->alphainv32[0], h->alphainv32[1], h->alphainv32[2]}};
+}
+
+template <class T>
+void reduce_means(lmm_handle* h, T* const u[3], const T* p, int slot);
+template <>
+void reduce_means<double>(lmm_handle* h, double* const u[3], const double* p, int slot) {
+    const double* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
+    const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
+    stokes_reduce(h, 1, a, b, slot);
+}
+template <>
+void reduce_means<float>(lmm_handle* h, float* const u[3], const float* p, int slot) {
+    const float* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
+    const float* b[4] = {nullptr, nullptr, nullptr, nullptr};
+    const int tile[3] = {1024000, 8, 8};
+    double w[3];
+    for (int d = 0; d < 3; ++d) {
+        int nd = (d < h->dm) ? h->grid.n[d] : 1;
+        w[d] = (nd / tile[d] < 2) ? 3.0 : 2.0;
+    }
+    launch_reduce<float>(h->D0, 1, a, b, w, 0.0, h->partials, h->counter, h->slot(slot), h->red_blocks, h->stream);
+    check_launch();
+}
+
+// x = M^-1 b.  b_u / b_p and x_u / x_p are level-0 arrays of type T (they
+// may alias the level-0 rhs / phi arrays of the hierarchy).
+template <class T>
+void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x_u[3], T* x_p) {
+    const lmm_knobs& K = h->knobs;
+    const int dm = h->dm;
+    const int64_t n = h->n;
+    const int pt = K.precon_type;
+    const int av = std::abs(K.visc_type);
+    const double theta = h->theta_loaded;
+    auto& L = levels<T>(h);
+    LevelDev<T>& L0 = L[0];
+    PrecScratch<T> S = prec_scratch<T>(h);
+    const int mean_slot = h->kSlots - 3;
+
+    // the staggered solve reads its rhs from L0.rhs and iterates on L0.phi
+    auto vel_solve = [&](const T* const rhs[3], bool zero_guess) {
+        for (int d = 0; d < dm; ++d) {
+            if (rhs[d] != L0.rhs[d]) LMM_CK(cudaMemcpyAsync(L0.rhs[d], rhs[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+            if (zero_guess) LMM_CK(cudaMemsetAsync(L0.phi[d], 0, n * sizeof(T), h->stream));
+        }
+        stag_mg_solver<T>(h);
+        for (int d = 0; d < dm; ++d)
+            if (x_u[d] != L0.phi[d]) LMM_CK(cudaMemcpyAsync(x_u[d], L0.phi[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+    };
+    auto pres_solve = [&](const T* rhs) {
+        if (rhs != L0.prhs) LMM_CK(cudaMemcpyAsync(L0.prhs, rhs, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+        macproject<T>(h);
+    };
+    const T* xu_c[3] = {x_u[0], x_u[1], x_u[2]};
+    switch (std::abs(pt)) {
+    case 1: {
+        vel_solve(b_u, true);
+        launch_div_plus<T>(L0, xu_c, b_p, S.mac, h->stream);
+        check_launch();
+        pres_solve(S.mac);
+        const T* ai[3] = {S.alphainv[0], S.alphainv[1], S.alphainv[2]};
+        launch_sub_weighted_grad<T>(L0, ai, L0.pphi, x_u, h->stream);
+        check_launch();
+        if (!(pt == 1 || theta == 0.0)) {
+            launch_neg_cc_lap<T>(L0, L0.pphi, S.src, h->stream);
+            check_launch();
+        }
+        launch_schur<T>(1, pt, av, theta, S.mac, S.src, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+        check_launch();
+        break;
+    }
+    case 2:
+    case 5: {
+        vel_solve(b_u, true);
+        launch_div_plus<T>(L0, xu_c, b_p, S.mac, h->stream);
+        check_launch();
+        if (std::fabs(theta) > 0.0)
+            pres_solve(S.mac);
+        else
+            LMM_CK(cudaMemsetAsync(L0.pphi, 0, n * sizeof(T), h->stream));
+        launch_schur<T>(0, pt, av, theta, S.mac, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+        check_launch();
+        if (std::abs(pt) == 5) {
+            for (int d = 0; d < dm; ++d)
+                LMM_CK(cudaMemcpyAsync(S.butmp[d], b_u[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+            launch_sub_weighted_grad<T>(L0, nullptr, x_p, S.butmp, h->stream);
+            check_launch();
+            const T* bt[3] = {S.butmp[0], S.butmp[1], S.butmp[2]};
+            // second viscous solve starts from the current x_u (apply_precon.f90:276)
+            for (int d = 0; d < dm; ++d)
+                if (x_u[d] != L0.phi[d])
+                    LMM_CK(cudaMemcpyAsync(L0.phi[d], x_u[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+            vel_solve(bt, false);
+        }
+        break;
+    }
+    case 3: {
+        LMM_CK(cudaMemcpyAsync(S.mac, b_p, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+        if (pt == -3) {
+            launch_scale_copy<T>(S.mac, S.mac, -1.0, n, h->stream);
+            check_launch();
+        }
+        if (std::fabs(theta) > 0.0)
+            pres_solve(S.mac);
+        else
+            LMM_CK(cudaMemsetAsync(L0.pphi, 0, n * sizeof(T), h->stream));
+        launch_schur<T>(0, 3, av, theta, S.mac, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+        check_launch();
+        for (int d = 0; d < dm; ++d) LMM_CK(cudaMemcpyAsync(S.butmp[d], b_u[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+        launch_sub_weighted_grad<T>(L0, nullptr, x_p, S.butmp, h->stream);
+        check_launch();
+        const T* bt[3] = {S.butmp[0], S.butmp[1], S.butmp[2]};
+        vel_solve(bt, true);
+        break;
+    }
+    case 4: {
+        vel_solve(b_u, true);
+        if (std::fabs(theta) > 0.0)
+            pres_solve(b_p);
+        else
+            LMM_CK(cudaMemsetAsync(L0.pphi, 0, n * sizeof(T), h->stream));
+        launch_schur<T>(2, pt, av, theta, nullptr, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+        check_launch();
+        break;
+    }
+    default:
+        throw LmmError(LMM_ERR_INVALID);
+    }
+    // mean removal (apply_precon.f90:433-460); periodic: no no-slip walls
+    reduce_means<T>(h, x_u, x_p, mean_slot);
+    double tv = 1.0;
+    for (int d = 0; d < dm; ++d) tv *= (double)h->grid.n[d];
+    launch_sub_means<T>(h->D0, x_u, x_p, h->slot(mean_slot), tv, theta == 0.0 ? 1 : 0, h->stream);
+    check_launch();
+}
+
+// FP64 Stokes vector in, FP64 Stokes vector out
+void precon64(lmm_handle* h, const SVec& bin, const SVec& xout) {
+    const double* bu[3] = {bin.c(0), bin.c(1), h->dm == 3 ? bin.c(2) : nullptr};
+    double* xu[3] = {xout.c(0), xout.c(1), h->dm == 3 ? xout.c(2) : nullptr};
+    apply_precon<double>(h, bu, bin.p(), xu, xout.p());
+}
+
+// FP64 Stokes vector in, FP32 Stokes vector out (Z storage)
+void precon32(lmm_handle* h, const SVec& bin, float* zout) {
+    const int dm = h->dm;
+    const int64_t n = h->n;
+    launch_convert<double, float>(bin.base, h->pin32, (int64_t)(dm + 1) * n, h->stream);
+    check_launch();
+    const float* bu[3] = {h->pin32, h->pin32 + n, dm == 3 ? h->pin32 + 2 * n : nullptr};
+    float* xu[3] = {zout, zout + n, dm == 3 ? zout + 2 * n : nullptr};
+    apply_precon<float>(h, bu, h->pin32 + (int64_t)dm * n, xu, zout + (int64_t)dm * n);
+}
+
+// ------------------------------------------------------------ Givens (host, gmres.f90:517-605)
+void rotmat(double a, double b, double& cs, double& sn) {
+    if (b == 0.0) {
+        cs = 1.0;
+        sn = 0.0;
+    } else if (std::fabs(b) > std::fabs(a)) {
+        double temp = a / b;
+        sn = 1.0 / std::sqrt(1.0 + temp * temp);
+        cs = temp * sn;
+    } else {
+        double temp = b / a;
+        cs = 1.0 / std::sqrt(1.0 + temp * temp);
+        sn = temp * cs;
+    }
+}
+
+struct Hess {
+    int ld;
+    std::vector<double> v;
+    double& operator()(int r, int c) { return v[(size_t)(r - 1) + (size_t)ld * (c - 1)]; }
+};
+
+void least_squares(int i, Hess& H, std::vector<double>& cs, std::vector<double>& sn, std::vector<double>& s) {
+    for (int k = 1; k <= i - 1; ++k) {
+        double temp = cs[k] * H(k, i) + sn[k] * H(k + 1, i);
+        H(k + 1, i) = -sn[k] * H(k, i) + cs[k] * H(k + 1, i);
+        H(k, i) = temp;
+    }
+    rotmat(H(i, i), H(i + 1, i), cs[i], sn[i]);
+    double temp = cs[i] * s[i];
+    s[i + 1] = -sn[i] * s[i];
+    s[i] = temp;
+    H(i, i) = cs[i] * H(i, i) + sn[i] * H(i + 1, i);
+    H(i + 1, i) = 0.0;
+}
+
+void solve_utri(int k, Hess& H, std::vector<double>& s, std::vector<double>& y) {
+    y[k + 1] = s[k + 1] / H(k + 1, k + 1);
+    for (int i = k; i >= 1; --i) {
+        double dot = 0.0;
+        for (int q = i + 1; q <= k + 1; ++q) dot = dot + H(i, q) * y[q];
+        y[i] = (s[i] - dot) / H(i, i);
+    }
+}
+
+void push_hist(lmm_stats* st, double v) {
+    if (st && st->n_history < LMM_HISTORY_MAX) st->history[st->n_history++] = v;
+}
+
+// MGS of w against V_0..V_{i-1} with H(k,i) kept on the device, then
+// H(i+1,i) = |w|; returns the Hessenberg column on the host.
+void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
+    const int64_t len = h->w.size();
+    for (int k = 1; k <= i; ++k) {
+        stokes_dot(h, h->w, h->V[k - 1], k);
+        launch_sub_scaled(h->w.base, h->V[k - 1].base, h->slot(k) + 4, len, h->stream);
+        check_launch();
+    }
+    stokes_norm(h, h->w, i + 1);
+    LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
+    LMM_CK(cudaStreamSynchronize(h->stream));
+    col.assign(i + 2, 0.0);
+    for (int k = 1; k <= i; ++k) col[k] = h->hscal[8 * k + 4];
+    col[i + 1] = h->hscal[8 * (i + 1) + 5];
+}
+
+// ------------------------------------------------------------ the reference GMRES
+int run_gmres(lmm_handle* h, double* theta_alpha, double* norm_pre_rhs, lmm_stats* st) {
+    const lmm_knobs& K = h->knobs;
+    const int m = K.gmres_max_inner;
+    const int64_t len = h->b.size();
+    std::vector<double> cs(m + 2), sn(m + 2), y(m + 2), s(m + 3), col;
+    Hess H{m + 1, std::vector<double>((size_t)(m + 1) * m, 0.0)};
+
+    h->vcycles = 0;
+    precon64(h, h->b, h->tmp);
+    stokes_norm(h, h->tmp, 0);
+    const double norm_pre_b = read_slot(h, 0, 5);
+    if (norm_pre_rhs) *norm_pre_rhs = norm_pre_b;
+    stokes_norm(h, h->b, 0);
+    const double norm_b = read_slot(h, 0, 5);
+    if (st) {
+        st->norm_b = norm_b;
+        st->norm_pre_b = norm_pre_b;
+    }
+    if (!std::isfinite(norm_b) || !std::isfinite(norm_pre_b)) return LMM_ERR_NONFINITE;
+    if (norm_b <= 0.0) {
+        LMM_CK(cudaMemsetAsync(h->x.base, 0, len * sizeof(double), h->stream));
+        return LMM_OK;
+    }
+    int status = LMM_OK;
+    int total_iter = 0, iter = 0, i_copy = 0;
+    double norm_init_resid = 0, norm_init_Stokes = 0;
+    h->vcycles = 0;
+    for (;;) {
+        launch_apply_matrix(h->L64[0], K.visc_type, h->x, h->tmp, h->stream);
+        check_launch();
+        launch_neg_resid(h->tmp.base, h->b.base, len, h->stream);
+        check_launch();
+        stokes_norm(h, h->tmp, 0);
+        int vtemp = h->vcycles;
+        precon64(h, h->tmp, h->r);
+        h->vcycles = vtemp;
+        stokes_norm(h, h->r, 1);
+        LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        const double norm_resid_Stokes = h->hscal[5];
+        const double norm_resid = h->hscal[8 + 5];
+        if (!std::isfinite(norm_resid) || !std::isfinite(norm_resid_Stokes)) return LMM_ERR_NONFINITE;
+        if (iter == 0) {
+            norm_init_Stokes = norm_resid_Stokes;
+            norm_init_resid = norm_resid;
+        }
+        if (st) {
+            st->norm_resid = norm_resid;
+            st->norm_init_resid = norm_init_resid;
+            st->norm_resid_true = norm_resid_Stokes;
+            st->norm_init_true = norm_init_Stokes;
+        }
+        if (total_iter >= K.gmres_max_iter) {
+            status = LMM_WARN_MAX_ITER;
+            break;
+        }
+        if (total_iter >= K.gmres_min_iter) {
+            if (norm_resid <= K.gmres_rel_tol * std::min(norm_pre_b, norm_init_resid)) {
+                if (norm_resid_Stokes >= 10 * K.gmres_rel_tol * std::min(norm_b, norm_init_Stokes)) status = LMM_WARN_RESID_MISMATCH;
+                break;
+            } else if (norm_resid <= K.gmres_abs_tol) {
+                break;
+            }
+        }
+        if (iter >= K.gmres_max_outer) {
+            status = LMM_WARN_MAX_OUTER;
+            break;
+        }
+        iter = iter + 1;
+        launch_div_by(h->r.base, h->V[0].base, h->slot(1) + 5, len, h->stream);
+        check_launch();
+        std::fill(s.begin(), s.end(), 0.0);
+        s[1] = norm_resid;
+        int i;
+        for (i = 1; i <= m; ++i) {
+            total_iter = total_iter + 1;
+            i_copy = i;
+            launch_apply_matrix(h->L64[0], K.visc_type, h->V[i - 1], h->tmp, h->stream);
+            check_launch();
+            precon64(h, h->tmp, h->w);
+            arnoldi_column(h, i, col);
+            for (int k = 1; k <= i + 1; ++k) H(k, i) = col[k];
+            for (int k = 1; k <= i + 1; ++k)
+                if (!std::isfinite(col[k])) return LMM_ERR_NONFINITE;
+            if (H(i + 1, i) != 0.0) {
+                launch_div_by(h->w.base, h->V[i].base, h->slot(i + 1) + 5, len, h->stream);
+                check_launch();
+            } else {
+                g_last_error = "gmres: error in orthogonalization (H(i+1,i) == 0)";
+                return LMM_ERR_BREAKDOWN;
+            }
+            least_squares(i, H, cs, sn, s);
+            const double est = std::fabs(s[i + 1]);
+            push_hist(st, est);
+            if (total_iter >= K.gmres_max_iter) break;
+            if (total_iter >= K.gmres_min_iter) {
+                if (est <= K.gmres_rel_tol * std::min(norm_pre_b, norm_init_resid) || est <= K.gmres_abs_tol) break;
+            }
+        }
+        solve_utri(i_copy - 1, H, s, y);
+        for (int it = 1; it <= i_copy; ++it) {
+            launch_add_scaled(h->x.base, h->V[it - 1].base, y[it], len, h->stream);
+            check_launch();
+        }
+    }
+    if (st) {
+        st->total_iter = total_iter;
+        st->outer_iter = iter;
+        st->vcycles = h->vcycles;
+    }
+    (void)theta_alpha;
+    return status;
+}
+
+// ------------------------------------------------------------ flexible GMRES
+int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
+    const lmm_knobs& K = h->knobs;
+    const int m = K.gmres_max_inner;
+    const int64_t len = h->b.size();
+    const bool fp32 = (K.precision == LMM_PRECISION_FP32);
+    std::vector<double> cs(m + 2), sn(m + 2), y(m + 2), s(m + 3), col;
+    Hess H{m + 1, std::vector<double>((size_t)(m + 1) * m, 0.0)};
+    h->vcycles = 0;
+    if (norm_pre_rhs) *norm_pre_rhs = 0.0;
+    stokes_norm(h, h->b, 0);
+    const double norm_b = read_slot(h, 0, 5);
+    if (st) st->norm_b = norm_b;
+    if (!std::isfinite(norm_b)) return LMM_ERR_NONFINITE;
+    if (norm_b <= 0.0) {
+        LMM_CK(cudaMemsetAsync(h->x.base, 0, len * sizeof(double), h->stream));
+        return LMM_OK;
+    }
+    int status = LMM_OK, total_iter = 0, iter = 0;
+    double norm_init = 0.0;
+    for (;;) {
+        launch_apply_matrix(h->L64[0], K.visc_type, h->x, h->tmp, h->stream);
+        check_launch();
+        launch_neg_resid(h->tmp.base, h->b.base, len, h->stream);
+        check_launch();
+        stokes_norm(h, h->tmp, 0);
+        const double norm_r = read_slot(h, 0, 5);
+        if (!std::isfinite(norm_r)) return LMM_ERR_NONFINITE;
+        if (iter == 0) norm_init = norm_r;
+        if (st) {
+            st->norm_resid_true = norm_r;
+            st->norm_init_true = norm_init;
+            st->norm_resid = norm_r;
+        }
+        if (total_iter >= K.gmres_min_iter && (norm_r <= K.gmres_rel_tol * norm_b || norm_r <= K.gmres_abs_tol)) break;
+        if (total_iter >= K.gmres_max_iter) {
+            status = LMM_WARN_MAX_ITER;
+            break;
+        }
+        if (iter >= K.gmres_max_outer) {
+            status = LMM_WARN_MAX_OUTER;
+            break;
+        }
+        iter = iter + 1;
+        launch_div_by(h->tmp.base, h->V[0].base, h->slot(0) + 5, len, h->stream);
+        check_launch();
+        std::fill(s.begin(), s.end(), 0.0);
+        s[1] = norm_r;
+        int i, i_copy = 0;
+        bool happy = false;
+        for (i = 1; i <= m; ++i) {
+            total_iter = total_iter + 1;
+            i_copy = i;
+            if (fp32) {
+                precon32(h, h->V[i - 1], h->Z32[i - 1]);
+                launch_convert<float, double>(h->Z32[i - 1], h->zt.base, len, h->stream);
+                check_launch();
+                launch_apply_matrix(h->L64[0], K.visc_type, h->zt, h->w, h->stream);
+            } else {
+                precon64(h, h->V[i - 1], h->Z64[i - 1]);
+                launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[i - 1], h->w, h->stream);
+            }
+            check_launch();
+            arnoldi_column(h, i, col);
+            for (int k = 1; k <= i + 1; ++k) H(k, i) = col[k];
+            for (int k = 1; k <= i + 1; ++k)
+                if (!std::isfinite(col[k])) return LMM_ERR_NONFINITE;
+            if (H(i + 1, i) != 0.0) {
+                launch_div_by(h->w.base, h->V[i].base, h->slot(i + 1) + 5, len, h->stream);
+                check_launch();
+            } else {
+                happy = true;
+            }
+            least_squares(i, H, cs, sn, s);
+            const double est = std::fabs(s[i + 1]);
+            push_hist(st, est);
+            if (happy || total_iter >= K.gmres_max_iter) break;
+            if (total_iter >= K.gmres_min_iter && (est <= K.gmres_rel_tol * norm_b || est <= K.gmres_abs_tol)) break;
+        }
+        solve_utri(i_copy - 1, H, s, y);
+        for (int it = 1; it <= i_copy; ++it) {
+            if (fp32)
+                launch_add_scaled_f32(h->x.base, h->Z32[it - 1], y[it], len, h->stream);
+            else
+                launch_add_scaled(h->x.base, h->Z64[it - 1].base, y[it], len, h->stream);
+            check_launch();
+        }
+    }
+    if (st) {
+        st->total_iter = total_iter;
+        st->outer_iter = iter;
+        st->vcycles = h->vcycles;
+    }
+    return status;
+}
+
+int validate(const lmm_grid* g, const lmm_knobs* k) {
+    if (!g || !k) return LMM_ERR_INVALID;
+    if (g->dm != 2 && g->dm != 3) return LMM_ERR_INVALID;
+    if (!(g->dx > 0.0)) return LMM_ERR_INVALID;
+    for (int d = 0; d < g->dm; ++d) {
+        if (g->n[d] < 2) return LMM_ERR_INVALID;
+        if (g->bc_lo[d] != LMM_BC_PERIODIC || g->bc_hi[d] != LMM_BC_PERIODIC) {
+            g_last_error = "only periodic boundaries are supported";
+            return LMM_ERR_INVALID;
+        }
+    }
+    const int av = std::abs(k->visc_type);
+    if (av < 1 || av > 3) return LMM_ERR_INVALID;
+    const int ap = std::abs(k->precon_type);
+    if (ap < 1 || ap > 5) {
+        g_last_error = "unsupported precon_type";
+        return LMM_ERR_INVALID;
+    }
+    if (k->visc_schur_approx != 0) {
+        g_last_error = "visc_schur_approx /= 0 (BFBt) is not built";
+        return LMM_ERR_INVALID;
+    }
+    if (k->gmres_max_inner < 1 || k->gmres_max_inner > 120) return LMM_ERR_INVALID;
+    if (k->method != LMM_METHOD_GMRES && k->method != LMM_METHOD_FGMRES) return LMM_ERR_INVALID;
+    if (k->precision == LMM_PRECISION_FP32 && k->method != LMM_METHOD_FGMRES) {
+        g_last_error = "the FP32 preconditioner needs LMM_METHOD_FGMRES";
+        return LMM_ERR_INVALID;
+    }
+    if (k->stag_mg_smoother != 0 && k->stag_mg_smoother != 1) return LMM_ERR_INVALID;
+    // every multigrid level the colour kernels touch needs even cell counts
+    int nl = compute_nlevs(g->n, g->dm, k->stag_mg_minwidth);
+    int nlp = compute_nlevs(g->n, g->dm, k->mg_minwidth);
+    for (int d = 0; d < g->dm; ++d) {
+        if (((g->n[d] >> (nl - 1)) % 2) != 0 || ((g->n[d] >> (nlp - 1)) % 2) != 0) {
+            g_last_error = "a multigrid level with an odd cell count is not supported";
+            return LMM_ERR_INVALID;
+        }
+        if ((g->n[d] >> (nl - 1)) << (nl - 1) != g->n[d]) return LMM_ERR_INVALID;
+    }
+    return LMM_OK;
+}
+
+}  // namespace
+
+// ============================================================ C ABI
+extern "C" {
+
+int lmm_version(void) { return 100; }
+
+const char* lmm_strerror(int code) {
+    switch (code) {
+    case LMM_OK: return "converged";
+    case LMM_WARN_MAX_ITER: return "GMRES did not converge in max number of total inner iterations";
+    case LMM_WARN_MAX_OUTER: return "GMRES did not converge in max number of outer iterations";
+    case LMM_WARN_RESID_MISMATCH: return "gmres may not have converged: true residual disagrees with preconditioned residual";
+    case LMM_ERR_INVALID: return g_last_error.empty() ? "invalid argument" : g_last_error.c_str();
+    case LMM_ERR_BREAKDOWN: return "gmres: error in orthogonalization";
+    case LMM_ERR_NONFINITE: return "non-finite value in an input or a residual";
+    case LMM_ERR_CUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
+    case LMM_ERR_WATCHDOG: return "a bounded device wait gave up";
+    case LMM_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+void lmm_default_knobs(lmm_knobs* k) {
+    std::memset(k, 0, sizeof(*k));
+    k->precon_type = 1;
+    k->visc_schur_approx = 0;
+    k->p_norm_weight = 1.0;
+    k->scale_factor = 1.0;
+    k->mg_max_vcycles = 1;
+    k->mg_minwidth = 2;
+    k->mg_bottom_solver = 4;
+    k->mg_nsmooths_down = 2;
+    k->mg_nsmooths_up = 2;
+    k->mg_nsmooths_bottom = 8;
+    k->mg_max_bottom_nlevels = 10;
+    k->mg_rel_tol = 1e-9;
+    k->stag_mg_max_vcycles = 1;
+    k->stag_mg_minwidth = 2;
+    k->stag_mg_bottom_solver = 4;
+    k->stag_mg_nsmooths_down = 2;
+    k->stag_mg_nsmooths_up = 2;
+    k->stag_mg_nsmooths_bottom = 8;
+    k->stag_mg_max_bottom_nlevels = 10;
+    k->stag_mg_omega = 1.0;
+    k->stag_mg_smoother = 1;
+    k->stag_mg_rel_tol = 1e-9;
+    k->gmres_rel_tol = 1e-9;
+    k->gmres_abs_tol = 0.0;
+    k->gmres_verbose = 1;
+    k->gmres_max_outer = 20;
+    k->gmres_max_inner = 5;
+    k->gmres_max_iter = 100;
+    k->gmres_min_iter = 1;
+    k->visc_type = 1;
+    k->method = LMM_METHOD_GMRES;
+    k->precision = LMM_PRECISION_FP64;
+    k->learned_stage = 0;
+}
+
+int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_handle** out) {
+    if (!out) return LMM_ERR_INVALID;
+    *out = nullptr;
+    g_last_error.clear();
+    int rc = validate(g, k);
+    if (rc != LMM_OK) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_last_error = "no CUDA device";
+        return LMM_ERR_NO_DEVICE;
+    }
+    lmm_handle* h = new lmm_handle();
+    try {
+        h->device = device;
+        LMM_CK(cudaSetDevice(device));
+        h->grid = *g;
+        h->knobs = *k;
+        h->dm = g->dm;
+        h->D0.dm = g->dm;
+        h->D0.nx = g->n[0];
+        h->D0.ny = g->n[1];
+        h->D0.nz = (g->dm == 3) ? g->n[2] : 1;
+        h->n = (int64_t)h->D0.nx * h->D0.ny * h->D0.nz;
+        h->nlev = compute_nlevs(g->n, g->dm, k->stag_mg_minwidth);
+        const int ap = std::abs(k->precon_type);
+        h->nlev_p = compute_nlevs(g->n, g->dm, k->mg_minwidth);
+        (void)ap;
+        h->m = k->gmres_max_inner;
+        LMM_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        LMM_CK(cudaEventCreate(&h->ev0));
+        LMM_CK(cudaEventCreate(&h->ev1));
+        h->arena_bytes = plan_bytes(*g, *k, h->nlev, h->nlev_p);
+        LMM_CK(cudaMalloc(&h->arena, h->arena_bytes));
+        LMM_CK(cudaMemset(h->arena, 0, h->arena_bytes));
+        build_levels<double>(h);
+        if (k->precision == LMM_PRECISION_FP32) build_levels<float>(h);
+        const int dm = h->dm;
+        for (int d = 0; d < dm; ++d) {
+            h->alpha_fc[d] = h->alloc<double>(h->n);
+            h->alphainv[d] = h->alloc<double>(h->n);
+            h->alphainv32[d] = h->alloc<float>(h->n);
+        }
+        for (int q = 0; q <= h->m; ++q) h->V.push_back(make_svec(h));
+        if (k->method == LMM_METHOD_FGMRES) {
+            for (int q = 0; q < h->m; ++q) {
+                if (k->precision == LMM_PRECISION_FP32)
+                    h->Z32.push_back(h->alloc<float>((int64_t)(dm + 1) * h->n));
+                else
+                    h->Z64.push_back(make_svec(h));
+            }
+        }
+        h->b = make_svec(h);
+        h->x = make_svec(h);
+        h->r = make_svec(h);
+        h->w = make_svec(h);
+        h->tmp = make_svec(h);
+        h->zt = make_svec(h);
+        h->mac64 = h->alloc<double>(h->n);
+        h->src64 = h->alloc<double>(h->n);
+        h->xptmp64 = h->alloc<double>(h->n);
+        for (int d = 0; d < dm; ++d) h->butmp64[d] = h->alloc<double>(h->n);
+        h->mac32 = h->alloc<float>(h->n);
+        h->src32 = h->alloc<float>(h->n);
+        h->xptmp32 = h->alloc<float>(h->n);
+        for (int d = 0; d < dm; ++d) h->butmp32[d] = h->alloc<float>(h->n);
+        h->pin32 = h->alloc<float>((int64_t)(dm + 1) * h->n);
+        h->pout32 = h->alloc<float>((int64_t)(dm + 1) * h->n);
+        h->red_blocks = reduce_blocks(h->n);
+        h->partials = h->alloc<double>(4096 * 4);
+        h->counter = h->alloc<unsigned>(64);
+        h->scal = h->alloc<double>(8 * lmm_handle::kSlots);
+        int64_t st = 1;
+        for (int d = 0; d < dm; ++d) st *= (g->n[d] + 1 + 8);
+        h->stage_elems = st;
+        h->stage = h->alloc<double>(st);
+        LMM_CK(cudaMallocHost(&h->hscal, 8 * sizeof(double) * lmm_handle::kSlots));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+    } catch (const LmmError& e) {
+        lmm_stokes_destroy(h);
+        return e.code;
+    }
+    *out = h;
+    return LMM_OK;
+}
+
+int lmm_stokes_destroy(lmm_handle* h) {
+    if (!h) return LMM_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->arena) cudaFree(h->arena);
+    if (h->hscal) cudaFreeHost(h->hscal);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LMM_OK;
+}
+
+void* lmm_stream(lmm_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int lmm_op_num_levels(lmm_handle* h) { return h ? h->nlev : -1; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------ solve entry points
+namespace {
+
+// device inputs (compact) -> handle buffers, the solve, solution -> x (device)
+int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], const double* x0_p, double* theta_alpha,
+               double* norm_pre_rhs, lmm_stats* st) {
+    const lmm_knobs& K = h->knobs;
+    const int dm = h->dm;
+    const int64_t n = h->n;
+    double theta = *theta_alpha;
+    const double sf = K.scale_factor;
+    // scale_factor (gmres.f90:106-122): applied to device copies only
+    if (sf != 1.0) theta = theta * sf;
+    LevelDev<double>& L0 = h->L64[0];
+    // b = (scaled) rhs, x = (scaled) initial guess
+    for (int d = 0; d < dm; ++d) {
+        if (sf != 1.0)
+            launch_scale_copy<double>(in->b_u[d], h->b.c(d), sf, n, h->stream);
+        else
+            LMM_CK(cudaMemcpyAsync(h->b.c(d), in->b_u[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaMemcpyAsync(h->x.c(d), x0_u[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    LMM_CK(cudaMemcpyAsync(h->b.p(), in->b_p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (sf != 1.0)
+        launch_scale_copy<double>(x0_p, h->x.p(), sf, n, h->stream);
+    else
+        LMM_CK(cudaMemcpyAsync(h->x.p(), x0_p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    check_launch();
+    // coefficients (beta, beta_ed, gamma scaled by scale_factor)
+    const double* beta = in->beta;
+    const double* bed[3] = {in->beta_ed[0], in->beta_ed[1], in->beta_ed[2]};
+    const double* gamma = in->gamma;
+    if (sf != 1.0) {
+        launch_scale_copy<double>(in->beta, L0.beta, sf, n, h->stream);
+        beta = L0.beta;
+        for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) {
+            launch_scale_copy<double>(in->beta_ed[e], L0.bed[e], sf, n, h->stream);
+            bed[e] = L0.bed[e];
+        }
+        if (gamma) {
+            launch_scale_copy<double>(in->gamma, L0.gamma, sf, n, h->stream);
+            gamma = L0.gamma;
+        }
+        check_launch();
+    }
+    const double* al[3] = {in->alpha_fc[0], in->alpha_fc[1], in->alpha_fc[2]};
+    load_coeffs(h, al, beta, bed, gamma, theta);
+    h->pvcycles = 0;
+    int rc = (K.method == LMM_METHOD_FGMRES) ? run_fgmres(h, norm_pre_rhs, st) : run_gmres(h, theta_alpha, norm_pre_rhs, st);
+    if (sf != 1.0) {
+        theta = theta / sf;
+        launch_scale_copy<double>(h->x.p(), h->x.p(), 1.0 / sf, n, h->stream);
+        check_launch();
+    }
+    *theta_alpha = theta;
+    if (st) st->pressure_vcycles = h->pvcycles;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int lmm_stokes_solve_device(lmm_handle* h, const lmm_fields_in* in, lmm_fields_out* out, double* theta_alpha,
+                                       double* norm_pre_rhs, lmm_stats* st) {
+    if (!h || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
+    if (in->layout != LMM_LAYOUT_COMPACT || out->layout != LMM_LAYOUT_COMPACT) return LMM_ERR_INVALID;
+    g_last_error.clear();
+    try {
+        LMM_CK(cudaSetDevice(h->device));
+        if (st) std::memset(st, 0, sizeof(*st));
+        LMM_CK(cudaEventRecord(h->ev0, h->stream));
+        const double* x0u[3] = {out->x_u[0], out->x_u[1], out->x_u[2]};
+        int rc = solve_core(h, in, x0u, out->x_p, theta_alpha, norm_pre_rhs, st);
+        if (rc >= 0 || rc == LMM_ERR_BREAKDOWN || rc == LMM_ERR_NONFINITE) {
+            for (int d = 0; d < h->dm; ++d)
+                LMM_CK(cudaMemcpyAsync(out->x_u[d], h->x.c(d), h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+            LMM_CK(cudaMemcpyAsync(out->x_p, h->x.p(), h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        }
+        LMM_CK(cudaEventRecord(h->ev1, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        if (st) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+            st->solve_ms = ms;
+        }
+        return rc;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fields_out* out, double* theta_alpha,
+                                double* norm_pre_rhs, lmm_stats* st) {
+    if (!h || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
+    g_last_error.clear();
+    const int dm = h->dm;
+    const int64_t n = h->n;
+    const Dims& D = h->D0;
+    try {
+        LMM_CK(cudaSetDevice(h->device));
+        if (st) std::memset(st, 0, sizeof(*st));
+        auto t0 = std::chrono::steady_clock::now();
+        // host -> device: inputs land in the level-0 / Krylov buffers
+        LevelDev<double>& L0 = h->L64[0];
+        // staging targets: b -> r, x0 -> w, coefficients -> their level-0 homes
+        auto upload = [&](const double* src, double* dst, int layout, int ng, const int nodal[3]) {
+            if (layout == LMM_LAYOUT_COMPACT) {
+                LMM_CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            } else {
+                int64_t sz = boxlib_size(D, nodal, ng);
+                if (sz > h->stage_elems || ng > 4) {
+                    g_last_error = "ghost width above 4 is not supported";
+                    throw LmmError(LMM_ERR_INVALID);
+                }
+                LMM_CK(cudaMemcpyAsync(h->stage, src, sz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                launch_gather_boxlib(D, nodal, ng, h->stage, dst, h->stream);
+                check_launch();
+            }
+        };
+        int nod_face[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        int nod_cell[3] = {0, 0, 0};
+        int nod_edge[3][3] = {{1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+        if (dm == 2) nod_edge[0][2] = 0;
+        const int lay = in->layout;
+        for (int d = 0; d < dm; ++d) {
+            upload(in->b_u[d], h->r.c(d), lay, in->ng_b_u, nod_face[d]);
+            upload(in->alpha_fc[d], h->alpha_fc[d], lay, in->ng_alpha, nod_face[d]);
+            upload(out->x_u[d], h->w.c(d), out->layout, out->ng_x_u, nod_face[d]);
+        }
+        upload(in->b_p, h->r.p(), lay, in->ng_b_p, nod_cell);
+        upload(out->x_p, h->w.p(), out->layout, out->ng_x_p, nod_cell);
+        upload(in->beta, L0.beta, lay, in->ng_beta, nod_cell);
+        for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) upload(in->beta_ed[e], L0.bed[e], lay, in->ng_beta_ed, nod_edge[e]);
+        if (in->gamma) upload(in->gamma, L0.gamma, lay, in->ng_gamma, nod_cell);
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        auto t1 = std::chrono::steady_clock::now();
+        lmm_fields_in din{};
+        for (int d = 0; d < 3; ++d) {
+            din.b_u[d] = (d < dm) ? h->r.c(d) : nullptr;
+            din.alpha_fc[d] = (d < dm) ? h->alpha_fc[d] : nullptr;
+            din.beta_ed[d] = L0.bed[d];
+        }
+        din.b_p = h->r.p();
+        din.beta = L0.beta;
+        din.gamma = in->gamma ? L0.gamma : nullptr;
+        din.layout = LMM_LAYOUT_COMPACT;
+        const double* x0u[3] = {h->w.c(0), h->w.c(1), dm == 3 ? h->w.c(2) : nullptr};
+        LMM_CK(cudaEventRecord(h->ev0, h->stream));
+        int rc = solve_core(h, &din, x0u, h->w.p(), theta_alpha, norm_pre_rhs, st);
+        LMM_CK(cudaEventRecord(h->ev1, h->stream));
+        // device -> host
+        if (rc >= 0 || rc == LMM_ERR_BREAKDOWN || rc == LMM_ERR_NONFINITE) {
+            auto download = [&](const double* src, double* dst, int layout, int ng, const int nodal[3]) {
+                if (layout == LMM_LAYOUT_COMPACT) {
+                    LMM_CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                } else {
+                    int64_t sz = boxlib_size(D, nodal, ng);
+                    if (sz > h->stage_elems || ng > 4) throw LmmError(LMM_ERR_INVALID);
+                    launch_scatter_boxlib(D, nodal, ng, src, h->stage, h->stream);
+                    check_launch();
+                    LMM_CK(cudaMemcpyAsync(dst, h->stage, sz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                    LMM_CK(cudaStreamSynchronize(h->stream));
+                }
+            };
+            for (int d = 0; d < dm; ++d) download(h->x.c(d), out->x_u[d], out->layout, out->ng_x_u, nod_face[d]);
+            download(h->x.p(), out->x_p, out->layout, out->ng_x_p, nod_cell);
+        }
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        auto t2 = std::chrono::steady_clock::now();
+        if (st) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+            st->solve_ms = ms;
+            st->h2d_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+            st->d2h_ms = std::chrono::duration<double, std::milli>(t2 - t1).count() - ms;
+        }
+        return rc;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+// ------------------------------------------------------------ operator-level entry points
+extern "C" int64_t lmm_kernel_launches(void) { return lmm::launches_total(); }
+
+extern "C" int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_rep) {
+    if (!h || !h->coeffs_loaded || reps < 1 || !ms_per_rep) return LMM_ERR_INVALID;
+    if ((which == 1 || which == 5) && h->knobs.precision != LMM_PRECISION_FP32) return LMM_ERR_INVALID;
+    try {
+        LevelDev<double>& L = h->L64[0];
+        auto once = [&]() {
+            switch (which) {
+            case 0: smooth<double>(h, L, 1); break;
+            case 1: smooth<float>(h, h->L32[0], 1); break;
+            case 2:
+                launch_applyop<double>(L, h->knobs.visc_type, L.phi, L.tmp, h->stream, 0);
+                check_launch();
+                break;
+            case 3:
+                launch_apply_matrix(L, h->knobs.visc_type, h->x, h->tmp, h->stream);
+                check_launch();
+                break;
+            case 4: vcycle<double>(h, h->L64); break;
+            case 5: vcycle<float>(h, h->L32); break;
+            case 6: macproject<double>(h); break;
+            default: throw LmmError(LMM_ERR_INVALID);
+            }
+        };
+        once();  // warm
+        LMM_CK(cudaEventRecord(h->ev0, h->stream));
+        for (int r = 0; r < reps; ++r) once();
+        LMM_CK(cudaEventRecord(h->ev1, h->stream));
+        LMM_CK(cudaEventSynchronize(h->ev1));
+        float ms = 0;
+        LMM_CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        *ms_per_rep = (double)ms / reps;
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_load_coeffs(lmm_handle* h, const lmm_fields_in* c, double theta_alpha) {
+    if (!h || !c) return LMM_ERR_INVALID;
+    try {
+        const double* al[3] = {c->alpha_fc[0], c->alpha_fc[1], c->alpha_fc[2]};
+        const double* bed[3] = {c->beta_ed[0], c->beta_ed[1], c->beta_ed[2]};
+        load_coeffs(h, al, c->beta, bed, c->gamma, theta_alpha);
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_stag_applyop(lmm_handle* h, const double* const phi[3], double* const Lphi[3], int color) {
+    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    try {
+        if (color < 0 || color > 2 * h->dm) return LMM_ERR_INVALID;
+        launch_applyop<double>(h->L64[0], h->knobs.visc_type, phi, Lphi, h->stream, color);
+        check_launch();
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_apply_matrix(lmm_handle* h, const double* const x_u[3], const double* x_p, double* const b_u[3],
+                                   double* b_p) {
+    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    try {
+        const int dm = h->dm;
+        const int64_t n = h->n;
+        for (int d = 0; d < dm; ++d)
+            LMM_CK(cudaMemcpyAsync(h->r.c(d), x_u[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaMemcpyAsync(h->r.p(), x_p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->r, h->tmp, h->stream);
+        check_launch();
+        for (int d = 0; d < dm; ++d)
+            LMM_CK(cudaMemcpyAsync(b_u[d], h->tmp.c(d), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaMemcpyAsync(b_p, h->tmp.p(), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_apply_precon(lmm_handle* h, const double* const b_u[3], const double* b_p, double* const x_u[3],
+                                   double* x_p) {
+    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    try {
+        const int dm = h->dm;
+        const int64_t n = h->n;
+        for (int d = 0; d < dm; ++d)
+            LMM_CK(cudaMemcpyAsync(h->r.c(d), b_u[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaMemcpyAsync(h->r.p(), b_p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        if (h->knobs.precision == LMM_PRECISION_FP32) {
+            precon32(h, h->r, h->pout32);
+            launch_convert<float, double>(h->pout32, h->w.base, h->w.size(), h->stream);
+            check_launch();
+        } else {
+            precon64(h, h->r, h->w);
+        }
+        for (int d = 0; d < dm; ++d)
+            LMM_CK(cudaMemcpyAsync(x_u[d], h->w.c(d), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaMemcpyAsync(x_p, h->w.p(), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_stag_mg_solver(lmm_handle* h, const double* const rhs[3], double* const phi[3]) {
+    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    try {
+        LevelDev<double>& L0 = h->L64[0];
+        for (int d = 0; d < h->dm; ++d) {
+            LMM_CK(cudaMemcpyAsync(L0.rhs[d], rhs[d], h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+            LMM_CK(cudaMemcpyAsync(L0.phi[d], phi[d], h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        }
+        stag_mg_solver<double>(h);
+        for (int d = 0; d < h->dm; ++d)
+            LMM_CK(cudaMemcpyAsync(phi[d], L0.phi[d], h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_smooth(lmm_handle* h, int lev, const double* const rhs[3], double* const phi[3], int color) {
+    if (!h || !h->coeffs_loaded || lev < 0 || lev >= h->nlev) return LMM_ERR_INVALID;
+    try {
+        LevelDev<double>& L = h->L64[lev];
+        for (int d = 0; d < h->dm; ++d) {
+            LMM_CK(cudaMemcpyAsync(L.rhs[d], rhs[d], L.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+            LMM_CK(cudaMemcpyAsync(L.phi[d], phi[d], L.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        }
+        if (color == 0) {
+            launch_jacobi<double>(L, h->knobs.visc_type, L.rhs, L.phi, L.tmp, h->knobs.stag_mg_omega, h->stream);
+            check_launch();
+            for (int d = 0; d < h->dm; ++d)
+                LMM_CK(cudaMemcpyAsync(phi[d], L.tmp[d], L.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        } else {
+            launch_gs_colour<double>(L, h->knobs.visc_type, color, L.rhs, L.phi, h->knobs.stag_mg_omega, h->stream);
+            check_launch();
+            for (int d = 0; d < h->dm; ++d)
+                LMM_CK(cudaMemcpyAsync(phi[d], L.phi[d], L.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        }
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* const rhs[3], const double* const phi[3],
+                                        double* const rhs_coarse[3]) {
+    if (!h || !h->coeffs_loaded || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
+    try {
+        launch_residual_restrict<double>(h->L64[lev], h->L64[lev + 1], h->knobs.visc_type, rhs, phi, rhs_coarse, h->stream);
+        check_launch();
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_prolong_add(lmm_handle* h, int lev, const double* const phi_coarse[3], double* const phi_fine[3]) {
+    if (!h || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
+    try {
+        launch_prolong_add<double>(h->L64[lev], h->L64[lev + 1], phi_coarse, phi_fine, h->stream);
+        check_launch();
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_inner_prod(lmm_handle* h, const double* const a_u[3], const double* a_p, const double* const b_u[3],
+                                 const double* b_p, double* out_host) {
+    if (!h) return LMM_ERR_INVALID;
+    try {
+        const double* a[4] = {a_u[0], a_u[1], h->dm == 3 ? a_u[2] : nullptr, a_p};
+        const double* b[4] = {b_u[0], b_u[1], h->dm == 3 ? b_u[2] : nullptr, b_p};
+        stokes_reduce(h, 0, a, b, 2);
+        LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(2), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        for (int c = 0; c <= h->dm; ++c) out_host[c] = h->hscal[c];
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+extern "C" int lmm_op_sum_umac_press(lmm_handle* h, const double* const u[3], const double* p, double* out_host) {
+    if (!h) return LMM_ERR_INVALID;
+    try {
+        const double* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
+        const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
+        stokes_reduce(h, 1, a, b, 2);
+        LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(2), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        double tv = 1.0;
+        for (int d = 0; d < h->dm; ++d) tv *= (double)h->grid.n[d];
+        out_host[0] = h->hscal[h->dm] / tv;
+        for (int d = 0; d < h->dm; ++d) out_host[1 + d] = h->hscal[d] / tv;
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+namespace lmm {
+namespace {
+std::atomic<int64_t> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+int reduce_blocks(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    if (b > 1184) b = 1184;  // 8 blocks per SM on 148 SMs
+    if (b < 1) b = 1;
+    return (int)b;
+}
+}  // namespace lmm

@@ -1,0 +1,328 @@
+"""GPU parity: every CUDA kernel and the full solve against the CPU oracle.
+
+The FP64 stencil kernels are built with -fmad=false and keep the reference's
+operand order, so applyop, Gauss-Seidel colours, Jacobi, residual
+restriction, prolongation, apply_matrix and whole V-cycles must be
+bit-identical to the oracle.  Reductions (inner products, means) sum in a
+different order: tolerance 1e-13 relative.  Full solves: velocity and
+mean-removed pressure within 1e-10 relative, iteration count +-1 (the bar
+the solver is held to).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from lowmachmixtures_b200 import abi, synth  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+VISCS = (-1, 1, -2, 2, -3, 3)
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def random_problem(dm, n, seed, visc, theta=7.0):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shape = (n,) * dm
+    ne = 1 if dm == 2 else 3
+    const = visc > 0
+    p = synth.make_problem(dm, n, 10.0, seed, theta_alpha=theta)
+    if const:
+        p.beta = np.full(shape, 0.8)
+        p.beta_ed = [np.full(shape, 0.8) for _ in range(ne)]
+        p.gamma = np.full(shape, 0.3)
+    else:
+        p.beta = rng.uniform(0.5, 2.0, shape)
+        p.beta_ed = [rng.uniform(0.5, 2.0, shape) for _ in range(ne)]
+        p.gamma = rng.uniform(0.1, 0.5, shape)
+    p.alpha_fc = [rng.uniform(0.5, 1.5, shape) for _ in range(dm)]
+    return p, rng
+
+
+def make_solver(p, **kn):
+    from lowmachmixtures_b200.gmres import StokesSolver
+    k = abi.make_knobs(**kn)
+    s = StokesSolver(p.dm, p.n[: p.dm], p.dx, knobs=k)
+    s.load_coeffs([dev(a) for a in p.alpha_fc], dev(p.beta), [dev(b) for b in p.beta_ed], dev(p.gamma), p.theta_alpha)
+    return s
+
+
+@pytest.mark.parametrize("dm,n", [(2, 16), (3, 8)])
+@pytest.mark.parametrize("visc", VISCS)
+def test_applyop_bit_exact(oracle, dm, n, visc):
+    p, rng = random_problem(dm, n, 11, visc)
+    s = make_solver(p, visc_type=visc)
+    phi = [rng.standard_normal(p.shape) for _ in range(dm)]
+    for color in range(0, 2 * dm + 1):
+        init = [rng.standard_normal(p.shape) for _ in range(dm)]
+        ref = oracle.stag_applyop(p, visc, phi, color=color, Lphi=init)
+        out = [dev(a) for a in init]
+        s.stag_applyop([dev(a) for a in phi], out, color)
+        for c in range(dm):
+            np.testing.assert_array_equal(host(out[c]), ref[c], err_msg=f"colour {color} comp {c}")
+    s.close()
+
+
+@pytest.mark.parametrize("dm,n", [(2, 16), (3, 8)])
+@pytest.mark.parametrize("visc", VISCS)
+@pytest.mark.parametrize("lev", [0, 1])
+def test_smooth_colours_bit_exact(oracle, dm, n, visc, lev):
+    p, rng = random_problem(dm, n, 12, visc)
+    k = oracle.default_knobs(visc_type=visc, stag_mg_omega=0.9)
+    s = make_solver(p, visc_type=visc, stag_mg_omega=0.9)
+    shp = oracle.level_shape(p, lev)
+    for color in range(0, 2 * dm + 1):
+        phi = [rng.standard_normal(shp) for _ in range(dm)]
+        rhs = [rng.standard_normal(shp) for _ in range(dm)]
+        ref = oracle.smooth(p, k, lev, rhs, phi, color)
+        dphi = [dev(a) for a in phi]
+        s.smooth(lev, [dev(a) for a in rhs], dphi, color)
+        for c in range(dm):
+            np.testing.assert_array_equal(host(dphi[c]), ref[c], err_msg=f"lev {lev} colour {color} comp {c}")
+    s.close()
+
+
+@pytest.mark.parametrize("dm,n", [(2, 16), (3, 16)])
+@pytest.mark.parametrize("visc", [-1, -2, -3, 2])
+def test_residual_restrict_and_prolong_bit_exact(oracle, dm, n, visc):
+    p, rng = random_problem(dm, n, 13, visc)
+    k = oracle.default_knobs(visc_type=visc)
+    s = make_solver(p, visc_type=visc)
+    for lev in (0, 1):
+        shp = oracle.level_shape(p, lev)
+        shc = oracle.level_shape(p, lev + 1)
+        phi = [rng.standard_normal(shp) for _ in range(dm)]
+        rhs = [rng.standard_normal(shp) for _ in range(dm)]
+        ref = oracle.residual_restrict(p, k, lev, rhs, phi)
+        out = [dev(np.zeros(shc)) for _ in range(dm)]
+        s.residual_restrict(lev, [dev(a) for a in rhs], [dev(a) for a in phi], out)
+        for c in range(dm):
+            np.testing.assert_array_equal(host(out[c]), ref[c], err_msg=f"restrict lev {lev} comp {c}")
+        coarse = [rng.standard_normal(shc) for _ in range(dm)]
+        refp = oracle.prolong_add(p, lev, coarse, phi)
+        dphi = [dev(a) for a in phi]
+        s.prolong_add(lev, [dev(a) for a in coarse], dphi)
+        for c in range(dm):
+            np.testing.assert_array_equal(host(dphi[c]), refp[c], err_msg=f"prolong lev {lev} comp {c}")
+    s.close()
+
+
+@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
+@pytest.mark.parametrize("visc", [-1, -2, -3])
+@pytest.mark.parametrize("smoother", [1, 0])
+def test_vcycle_bit_exact(oracle, dm, n, visc, smoother):
+    p, rng = random_problem(dm, n, 14, visc, theta=3.0)
+    kn = dict(visc_type=visc, stag_mg_smoother=smoother, stag_mg_omega=1.0 if smoother else 0.7)
+    k = oracle.default_knobs(**kn)
+    s = make_solver(p, **kn)
+    rhs = [rng.standard_normal(p.shape) for _ in range(dm)]
+    ref = oracle.stag_mg_solver(p, k, rhs)
+    phi = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    s.stag_mg_solver([dev(a) for a in rhs], phi)
+    for c in range(dm):
+        np.testing.assert_array_equal(host(phi[c]), ref[c])
+    s.close()
+
+
+@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
+@pytest.mark.parametrize("visc", VISCS)
+def test_apply_matrix_bit_exact(oracle, dm, n, visc):
+    p, rng = random_problem(dm, n, 15, visc)
+    s = make_solver(p, visc_type=visc)
+    xu = [rng.standard_normal(p.shape) for _ in range(dm)]
+    xp = rng.standard_normal(p.shape)
+    ref_u, ref_p = oracle.apply_matrix(p, visc, xu, xp)
+    bu = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    bp = dev(np.zeros(p.shape))
+    s.apply_matrix([dev(a) for a in xu], dev(xp), bu, bp)
+    for c in range(dm):
+        np.testing.assert_array_equal(host(bu[c]), ref_u[c])
+    np.testing.assert_array_equal(host(bp), ref_p)
+    s.close()
+
+
+@pytest.mark.parametrize("dm,n", [(2, 16), (3, 16)])
+def test_inner_products_and_means(oracle, dm, n):
+    p, rng = random_problem(dm, n, 16, -2)
+    s = make_solver(p, visc_type=-2)
+    a = [rng.standard_normal(p.shape) for _ in range(dm)]
+    b = [rng.standard_normal(p.shape) for _ in range(dm)]
+    ap, bp = rng.standard_normal(p.shape), rng.standard_normal(p.shape)
+    ref = oracle.inner_prod(p, a, ap, b, bp)
+    got = s.inner_prod([dev(x) for x in a], dev(ap), [dev(x) for x in b], dev(bp))
+    np.testing.assert_allclose(got, ref, rtol=1e-13, atol=1e-13 * max(abs(x) for x in ref))
+    ref = oracle.sum_umac_press(p, a, ap)
+    got = s.sum_umac_press([dev(x) for x in a], dev(ap))
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-15)
+    s.close()
+
+
+PRECONS = [1, -1, 2, -2, 3, -3, 4, -4, 5, -5]
+
+
+@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
+@pytest.mark.parametrize("pt", PRECONS)
+@pytest.mark.parametrize("theta", [0.0, 50.0])
+def test_apply_precon(oracle, dm, n, pt, theta):
+    visc = -2 if pt % 2 else -3
+    p, rng = random_problem(dm, n, 17, visc, theta=theta)
+    k = oracle.default_knobs(visc_type=visc, precon_type=pt)
+    s = make_solver(p, visc_type=visc, precon_type=pt)
+    bu = [rng.standard_normal(p.shape) for _ in range(dm)]
+    bpp = rng.standard_normal(p.shape)
+    ref_u, ref_p = oracle.apply_precon(p, k, bu, bpp)
+    xu = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    xp = dev(np.zeros(p.shape))
+    s.apply_precon([dev(a) for a in bu], dev(bpp), xu, xp)
+    scale = max(np.abs(r).max() for r in ref_u + [ref_p])
+    for c in range(dm):
+        np.testing.assert_allclose(host(xu[c]), ref_u[c], rtol=0, atol=1e-12 * scale)
+    np.testing.assert_allclose(host(xp), ref_p, rtol=0, atol=1e-12 * scale)
+    s.close()
+
+
+def _solve_both(oracle, prob, **kn):
+    k = oracle.default_knobs(**kn)
+    rc_o, xu_o, xp_o, th_o, npr_o, st_o = oracle.solve(prob, k)
+    from lowmachmixtures_b200.gmres import StokesSolver
+    with StokesSolver(prob.dm, prob.n[: prob.dm], prob.dx, knobs=abi.make_knobs(**kn)) as s:
+        xu, xp = prob.zeros_like_solution()
+        th, npr, st = s.solve(prob.b_u, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma,
+                              prob.theta_alpha)
+    return (rc_o, xu_o, xp_o, th_o, npr_o, st_o), (st["status"], xu, xp, th, npr, st)
+
+
+def _assert_solution_parity(ref, got, tol=1e-10):
+    _, xu_o, xp_o, _, _, st_o = ref
+    _, xu, xp, _, _, st = got
+    for c in range(len(xu)):
+        err = np.abs(xu[c] - xu_o[c]).max() / np.abs(xu_o[c]).max()
+        assert err <= tol, f"velocity comp {c} rel err {err:.3e}"
+    po = xp_o - xp_o.mean()
+    pg = xp - xp.mean()
+    err = np.abs(pg - po).max() / max(np.abs(po).max(), 1e-300)
+    assert err <= tol, f"pressure rel err {err:.3e}"
+    assert abs(st["total_iter"] - st_o["total_iter"]) <= 1, (st["total_iter"], st_o["total_iter"])
+
+
+@pytest.mark.parametrize("pt", [2, 1])
+@pytest.mark.parametrize("seed", [0, 1])
+def test_gmres_parity_2d_64(oracle, pt, seed):
+    prob = synth.config_2d_64(seed)
+    ref, got = _solve_both(oracle, prob, precon_type=pt, visc_type=-2)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
+    assert abs(got[4] - ref[4]) <= 1e-12 * ref[4]  # norm_pre_rhs
+
+
+@pytest.mark.parametrize("pt", [2, 1])
+def test_gmres_parity_3d_inertial(oracle, pt):
+    prob = synth.config_3d_128(0, n=32)
+    ref, got = _solve_both(oracle, prob, precon_type=pt, visc_type=-2)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
+
+
+@pytest.mark.parametrize("visc", [-1, -3, 1])
+def test_gmres_parity_other_visc_types(oracle, visc):
+    prob = synth.make_problem(2, 32, 20.0, 3, theta_alpha=100.0, gamma_value=0.25)
+    if visc > 0:
+        prob.beta[:] = 1.3
+        for b in prob.beta_ed:
+            b[:] = 1.3
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=visc)
+    assert ref[0] == got[0]
+    _assert_solution_parity(ref, got)
+
+
+def test_gmres_scale_factor_and_jacobi(oracle):
+    prob = synth.make_problem(2, 32, 10.0, 4, theta_alpha=30.0)
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2, scale_factor=2.5, stag_mg_smoother=0,
+                           stag_mg_omega=0.6, gmres_max_inner=8)
+    assert ref[0] == got[0]
+    _assert_solution_parity(ref, got)
+    assert got[3] == ref[3]  # theta_alpha scaled and unscaled like the reference
+
+
+def test_fgmres_fp64_parity(oracle):
+    prob = synth.config_3d_128(1, n=32)
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
+    assert got[5]["norm_resid_true"] <= 1e-9 * got[5]["norm_b"]
+
+
+def test_fgmres_fp32_preconditioner_reaches_fp64_tolerance(oracle):
+    prob = synth.config_3d_128(2, n=32)
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES,
+                           precision=abi.LMM_PRECISION_FP32)
+    st = got[5]
+    assert got[0] == 0
+    assert st["norm_resid_true"] <= 1e-9 * st["norm_b"]
+    # solution error against the FP64 oracle solve (both converged to 1e-9)
+    xu_o, xu = ref[1], got[1]
+    err = max(np.abs(xu[c] - xu_o[c]).max() / np.abs(xu_o[c]).max() for c in range(3))
+    assert err < 1e-6, err
+    assert abs(st["total_iter"] - ref[5]["total_iter"]) <= 2
+
+
+def test_boxlib_layout_matches_compact(oracle):
+    """Host arrays laid out like BoxLib's dataptr(): ghosts, nodal hi+1 faces."""
+    prob = synth.make_problem(3, 16, 10.0, 5, theta_alpha=40.0)
+    from lowmachmixtures_b200.gmres import StokesSolver
+
+    def boxlib(a, nodal, ng):
+        # BoxLib single-box array: nodal directions hold n+1 entries (hi+1 is
+        # the periodic copy of face 0), plus ng periodic ghost layers
+        out = a
+        for ax, nod in enumerate(reversed(nodal)):
+            n = a.shape[ax]
+            out = np.take(out, [v % n for v in range(-ng, n + nod + ng)], axis=ax)
+        return np.ascontiguousarray(out)
+
+    faces = [(1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    edges = [(1, 1, 0), (1, 0, 1), (0, 1, 1)]
+    ng = 1
+    bu = [boxlib(prob.b_u[c], faces[c], 0) for c in range(3)]
+    al = [boxlib(prob.alpha_fc[c], faces[c], 0) for c in range(3)]
+    be = boxlib(prob.beta, (0, 0, 0), 1)
+    ga = boxlib(prob.gamma, (0, 0, 0), 1)
+    bed = [boxlib(prob.beta_ed[e], edges[e], 0) for e in range(3)]
+    bp = boxlib(prob.b_p, (0, 0, 0), 0)
+    xu = [np.zeros_like(boxlib(prob.b_u[c], faces[c], ng)) for c in range(3)]
+    xp = np.zeros_like(boxlib(prob.b_p, (0, 0, 0), ng))
+    kn = dict(precon_type=2, visc_type=-2)
+    with StokesSolver(3, (16, 16, 16), prob.dx, knobs=abi.make_knobs(**kn)) as s:
+        s.solve(bu, bp, xu, xp, al, be, bed, ga, prob.theta_alpha, layout=abi.LMM_LAYOUT_BOXLIB,
+                ng=dict(b_u=0, b_p=0, alpha_fc=0, beta=1, beta_ed=0, gamma=1, x_u=ng, x_p=ng))
+        xu_c, xp_c = prob.zeros_like_solution()
+        s.solve(prob.b_u, prob.b_p, xu_c, xp_c, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma, prob.theta_alpha)
+    for c in range(3):
+        np.testing.assert_array_equal(xu[c], boxlib(xu_c[c], faces[c], ng))
+    np.testing.assert_array_equal(xp, boxlib(xp_c, (0, 0, 0), ng))
+
+
+def test_zero_rhs_returns_zero_and_nan_is_an_error():
+    from lowmachmixtures_b200.gmres import StokesSolver
+    from lowmachmixtures_b200._native import LmmError
+    prob = synth.make_problem(2, 16, 10.0, 6, theta_alpha=5.0)
+    with StokesSolver(2, (16, 16), prob.dx, precon_type=2, visc_type=-2) as s:
+        xu = [np.ones(prob.shape) for _ in range(2)]
+        xp = np.ones(prob.shape)
+        zero = [np.zeros(prob.shape) for _ in range(2)]
+        _, npr, st = s.solve(zero, np.zeros(prob.shape), xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma,
+                             5.0)
+        assert st["status"] == 0 and st["total_iter"] == 0
+        assert all(np.all(a == 0) for a in xu) and np.all(xp == 0)
+        bad = [b.copy() for b in prob.b_u]
+        bad[0][3, 4] = np.nan
+        with pytest.raises(LmmError) as ei:
+            s.solve(bad, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma, 5.0)
+        assert ei.value.code == abi.LMM_ERR_NONFINITE
