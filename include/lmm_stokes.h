@@ -103,7 +103,10 @@ typedef struct lmm_knobs {
     int    method;                 /* LMM_METHOD_* */
     int    precision;              /* LMM_PRECISION_* */
     int    learned_stage;          /* 0 off, 1 network stage before the V-cycle (FGMRES only) */
-    int    reserved[8];
+    int    tail_cells;             /* multigrid levels with at most this many cells run in one
+                                      cluster launch; 0 = default (4096), -1 = never */
+    int    tail_cluster;           /* thread blocks in that cluster (1..16); 0 = default (8) */
+    int    reserved[6];
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -26,16 +26,25 @@ namespace lmm {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ void unflat(const Dims& D, int64_t t, int& i, int& j, int& k) {
-    i = (int)(t % D.nx);
-    int64_t r = t / D.nx;
-    j = (int)(r % D.ny);
-    k = (int)(r / D.ny);
-}
-
 static inline int nblocks_for(int64_t n, int threads = kThreads) {
     int64_t b = (n + threads - 1) / threads;
     return (int)(b < 1 ? 1 : b);
+}
+
+// 3D launch: x spans nx (i, or i/2 for a colour), y spans ny, z spans nz
+struct G3 {
+    dim3 grid, block;
+};
+static inline G3 geom3(int nx, int ny, int nz) {
+    int bx = nx < 64 ? nx : 64;
+    if (bx < 1) bx = 1;
+    int by = kThreads / bx;
+    if (by > ny) by = ny;
+    if (by < 1) by = 1;
+    G3 g;
+    g.block = dim3(bx, by, 1);
+    g.grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+    return g;
 }
 
 // --------------------------------------------------------------- applyop
@@ -43,12 +52,11 @@ template <class T, int DM, int VISC>
 __global__ void __launch_bounds__(kThreads) k_applyop(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
                                                       const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                       T* __restrict__ o2, T dxsqinv, int color) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(D, t, i, j, k);
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    const int i = q.i, j = q.j, k = q.k;
     Nb nb = make_nb(D, i, j, k);
+    const int t = nb.s;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
     // colour c >= 1 covers component (c-1)/2, faces with (i+j+k) even for odd c
@@ -68,15 +76,10 @@ __global__ void __launch_bounds__(kThreads) k_applyop(Dims D, Coef<T> C, const T
 template <class T, int DM, int VISC, int COMP>
 __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const T* __restrict__ rhs, T* p0, T* p1, T* p2,
                                                         int parity, T omega, T dxsqinv) {
-    const int hx = D.nx >> 1;
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)hx * D.ny * D.nz;
-    if (t >= n) return;
-    int ih = (int)(t % hx);
-    int64_t r = t / hx;
-    int j = (int)(r % D.ny);
-    int k = (int)(r / D.ny);
-    int i = 2 * ih + ((j + k + parity) & 1);
+    const Pos q = pos3(D.nx >> 1, D.ny);
+    if (!q.ok) return;
+    const int j = q.j, k = q.k;
+    const int i = 2 * q.i + ((j + k + parity) & 1);
     Nb nb = make_nb(D, i, j, k);
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
@@ -93,12 +96,10 @@ __global__ void __launch_bounds__(kThreads) k_jacobi(Dims D, Coef<T> C, const T*
                                                      const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
                                                      const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                      T* __restrict__ o2, T omega, T dxsqinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(D, t, i, j, k);
-    Nb nb = make_nb(D, i, j, k);
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
     {
@@ -120,15 +121,72 @@ __global__ void __launch_bounds__(kThreads) k_jacobi(Dims D, Coef<T> C, const T*
 
 // --------------------------------------------------------------- residual + restriction
 // residual of one fine face: (L phi - rhs) * -1  (stag_mg_solver.f90:414-415)
-template <class T, int DM, int VISC, int D_>
+template <class T, int DM, int VISC, int D_, int LD = 0>
 __device__ __forceinline__ T fine_resid(const Dims& F, const Coef<T>& C, const T* const phi[3], const T* rhs, int i, int j, int k,
                                         T dxsqinv, T b, T c) {
-    i = (i + F.nx) % F.nx;
-    j = (j + F.ny) % F.ny;
-    k = (DM == 3) ? (k + F.nz) % F.nz : 0;
+    i = wrapi(i, F.nx);
+    j = wrapi(j, F.ny);
+    k = (DM == 3) ? wrapi(k, F.nz) : 0;
     Nb nb = make_nb(F, i, j, k);
-    T v = face_L<T, DM, VISC, D_>(phi, C, nb, dxsqinv, b, c) - ld(rhs, nb.s);
+    T v = face_L<T, DM, VISC, D_, LD>(phi, C, nb, dxsqinv, b, c) - ldp<LD>(rhs, nb.s);
     return v * T(-1);
+}
+
+// coarse face of component COMP at coarse index (i, j, k): the fine-level
+// residual restricted with the 6-point (2D) / 12-point (3D) stencil.  The 12
+// (6) fine residuals are evaluated one at a time (keeps registers low) and
+// summed in the reference's order:
+//   3D: 1/8 (r0+r1+r2+r3) + 1/16 (r4+r5+r6+r7) + 1/16 (r8+r9+r10+r11)
+//   2D: 1/4 (r0+r1) + 1/8 (r2+r3+r4+r5)
+// with normal offsets 0, +1, -1 and the transverse offsets of
+// stag_mg_solver.f90:1063-1078, 1133-1171.
+template <class T, int DM, int VISC, int COMP, int LD = 0>
+__device__ __forceinline__ T restrict_face(const Dims& F, const Coef<T>& C, const T* const rhs[3], const T* const phi[3], int i,
+                                           int j, int k, T dxsqinv) {
+    const T b = ld(C.beta, 0), cc = ld(C.gamma, 0);
+    constexpr int NQ = (DM == 2) ? 2 : 4;
+    // transverse offsets (di, dj, dk) per component
+    int qi[4], qj[4], qk[4];
+    if constexpr (DM == 2) {
+        if (COMP == 0) { qi[0] = 0; qj[0] = 0; qi[1] = 0; qj[1] = 1; }
+        else { qi[0] = 0; qj[0] = 0; qi[1] = 1; qj[1] = 0; }
+        qk[0] = qk[1] = 0;
+    } else {
+        if (COMP == 0) { int a_[4] = {0, 0, 0, 0}, b_[4] = {0, 1, 0, 1}, c_[4] = {0, 0, 1, 1};
+            for (int q = 0; q < 4; ++q) { qi[q] = a_[q]; qj[q] = b_[q]; qk[q] = c_[q]; } }
+        else if (COMP == 1) { int a_[4] = {0, 1, 0, 1}, b_[4] = {0, 0, 0, 0}, c_[4] = {0, 0, 1, 1};
+            for (int q = 0; q < 4; ++q) { qi[q] = a_[q]; qj[q] = b_[q]; qk[q] = c_[q]; } }
+        else { int a_[4] = {0, 1, 0, 1}, b_[4] = {0, 0, 1, 1}, c_[4] = {0, 0, 0, 0};
+            for (int q = 0; q < 4; ++q) { qi[q] = a_[q]; qj[q] = b_[q]; qk[q] = c_[q]; } }
+    }
+    T r[3 * NQ];
+    const int I = 2 * i, J = 2 * j, K = 2 * k;
+#pragma unroll 1
+    for (int m = 0; m < 3 * NQ; ++m) {
+        const int nrm = (m < NQ) ? 0 : (m < 2 * NQ ? 1 : -1);
+        const int q = m % NQ;
+        int ii = I + qi[q], jj = J + qj[q], kk = K + qk[q];
+        if (COMP == 0) ii += nrm;
+        else if (COMP == 1) jj += nrm;
+        else kk += nrm;
+        r[m] = fine_resid<T, DM, VISC, COMP, LD>(F, C, phi, rhs[COMP], ii, jj, kk, dxsqinv, b, cc);
+    }
+    if constexpr (DM == 2)
+        return T(0.25) * (r[0] + r[1]) + T(0.125) * (r[2] + r[3] + r[4] + r[5]);
+    else
+        return T(0.125) * (r[0] + r[1] + r[2] + r[3]) + T(0.0625) * (r[4] + r[5] + r[6] + r[7]) +
+               T(0.0625) * (r[8] + r[9] + r[10] + r[11]);
+}
+
+template <class T, int DM, int VISC, int LD = 0>
+__device__ __forceinline__ void restrict_comp(int comp, const Dims& F, const Coef<T>& C, const T* const rhs[3],
+                                              const T* const phi[3], T* const out[3], int t, int i, int j, int k, T dxsqinv) {
+    if (comp == 0)
+        out[0][t] = restrict_face<T, DM, VISC, 0, LD>(F, C, rhs, phi, i, j, k, dxsqinv);
+    else if (comp == 1)
+        out[1][t] = restrict_face<T, DM, VISC, 1, LD>(F, C, rhs, phi, i, j, k, dxsqinv);
+    else if constexpr (DM == 3)
+        out[2][t] = restrict_face<T, DM, VISC, 2, LD>(F, C, rhs, phi, i, j, k, dxsqinv);
 }
 
 template <class T, int DM, int VISC>
@@ -137,133 +195,118 @@ __global__ void __launch_bounds__(kThreads) k_residual_restrict(Dims F, Coef<T> 
                                                                 const T* __restrict__ p0, const T* __restrict__ p1,
                                                                 const T* __restrict__ p2, Dims Dc, T* __restrict__ c0,
                                                                 T* __restrict__ c1, T* __restrict__ c2, T dxsqinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)Dc.nx * Dc.ny * Dc.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(Dc, t, i, j, k);
+    const Pos q = pos3(Dc.nx, Dc.ny);
+    if (!q.ok) return;
+    const int comp = q.k % DM, k = q.k / DM;  // grid.z covers nz * DM
+    const int t = q.i + Dc.nx * (q.j + Dc.ny * k);
     const T* phi[3] = {p0, p1, p2};
-    const T b = ld(C.beta, 0), cc = ld(C.gamma, 0);
-    const int I = 2 * i, J = 2 * j, K = 2 * k;
-#define RX(a, bb, ccc) fine_resid<T, DM, VISC, 0>(F, C, phi, r0, a, bb, ccc, dxsqinv, b, cc)
-#define RY(a, bb, ccc) fine_resid<T, DM, VISC, 1>(F, C, phi, r1, a, bb, ccc, dxsqinv, b, cc)
-#define RZ(a, bb, ccc) fine_resid<T, DM, VISC, 2>(F, C, phi, r2, a, bb, ccc, dxsqinv, b, cc)
-    if constexpr (DM == 2) {
-        c0[t] = T(0.25) * (RX(I, J, 0) + RX(I, J + 1, 0)) + T(0.125) * (RX(I + 1, J, 0) + RX(I + 1, J + 1, 0) + RX(I - 1, J, 0) + RX(I - 1, J + 1, 0));
-        c1[t] = T(0.25) * (RY(I, J, 0) + RY(I + 1, J, 0)) + T(0.125) * (RY(I, J + 1, 0) + RY(I + 1, J + 1, 0) + RY(I, J - 1, 0) + RY(I + 1, J - 1, 0));
-    } else {
-        c0[t] = T(0.125) * (RX(I, J, K) + RX(I, J + 1, K) + RX(I, J, K + 1) + RX(I, J + 1, K + 1)) +
-                T(0.0625) * (RX(I + 1, J, K) + RX(I + 1, J + 1, K) + RX(I + 1, J, K + 1) + RX(I + 1, J + 1, K + 1)) +
-                T(0.0625) * (RX(I - 1, J, K) + RX(I - 1, J + 1, K) + RX(I - 1, J, K + 1) + RX(I - 1, J + 1, K + 1));
-        c1[t] = T(0.125) * (RY(I, J, K) + RY(I + 1, J, K) + RY(I, J, K + 1) + RY(I + 1, J, K + 1)) +
-                T(0.0625) * (RY(I, J + 1, K) + RY(I + 1, J + 1, K) + RY(I, J + 1, K + 1) + RY(I + 1, J + 1, K + 1)) +
-                T(0.0625) * (RY(I, J - 1, K) + RY(I + 1, J - 1, K) + RY(I, J - 1, K + 1) + RY(I + 1, J - 1, K + 1));
-        c2[t] = T(0.125) * (RZ(I, J, K) + RZ(I + 1, J, K) + RZ(I, J + 1, K) + RZ(I + 1, J + 1, K)) +
-                T(0.0625) * (RZ(I, J, K + 1) + RZ(I + 1, J, K + 1) + RZ(I, J + 1, K + 1) + RZ(I + 1, J + 1, K + 1)) +
-                T(0.0625) * (RZ(I, J, K - 1) + RZ(I + 1, J, K - 1) + RZ(I, J + 1, K - 1) + RZ(I + 1, J + 1, K - 1));
-    }
-#undef RX
-#undef RY
-#undef RZ
+    const T* rhs[3] = {r0, r1, r2};
+    T* out[3] = {c0, c1, c2};
+    restrict_comp<T, DM, VISC, 0>(comp, F, C, rhs, phi, out, t, q.i, q.j, k, dxsqinv);
 }
 
 // --------------------------------------------------------------- prolongation
-template <class T>
+template <class T, int LD = 0>
 __device__ __forceinline__ T cat(const T* a, const Dims& Dc, int i, int j, int k) {
-    i = (i + Dc.nx) % Dc.nx;
-    j = (j + Dc.ny) % Dc.ny;
-    k = (Dc.dm == 3) ? (k + Dc.nz) % Dc.nz : 0;
-    return ld(a, i + (int64_t)Dc.nx * (j + (int64_t)Dc.ny * k));
+    i = wrapi(i, Dc.nx);
+    j = wrapi(j, Dc.ny);
+    k = (Dc.dm == 3) ? wrapi(k, Dc.nz) : 0;
+    return ldp<LD>(a, i + Dc.nx * (j + Dc.ny * k));
+}
+
+// add the interpolated coarse correction to the DM fine faces at (i, j, k)
+template <class T, int DM, int LD = 0>
+__device__ __forceinline__ void prolong_cell(const Dims& Dc, const T* q0, const T* q1, const T* q2, T* f0, T* f1, T* f2, int t,
+                                             int i, int j, int k) {
+    const int i2 = i >> 1, j2 = j >> 1, k2 = k >> 1;
+    if constexpr (DM == 2) {
+        {
+            int joff = ((j & 1) == 0) ? -1 : 1;
+            T v = (LD == 2) ? __ldcg(f0 + t) : f0[t];
+            if ((i & 1) == 0)
+                v = v + T(0.75) * cat<T, LD>(q0, Dc, i2, j2, 0) + T(0.25) * cat<T, LD>(q0, Dc, i2, j2 + joff, 0);
+            else
+                v = v + T(0.375) * cat<T, LD>(q0, Dc, i2, j2, 0) + T(0.125) * cat<T, LD>(q0, Dc, i2, j2 + joff, 0) + T(0.375) * cat<T, LD>(q0, Dc, i2 + 1, j2, 0) +
+                    T(0.125) * cat<T, LD>(q0, Dc, i2 + 1, j2 + joff, 0);
+            f0[t] = v;
+        }
+        {
+            int ioff = ((i & 1) == 0) ? -1 : 1;
+            T v = (LD == 2) ? __ldcg(f1 + t) : f1[t];
+            if ((j & 1) == 0)
+                v = v + T(0.75) * cat<T, LD>(q1, Dc, i2, j2, 0) + T(0.25) * cat<T, LD>(q1, Dc, i2 + ioff, j2, 0);
+            else
+                v = v + T(0.375) * cat<T, LD>(q1, Dc, i2, j2, 0) + T(0.125) * cat<T, LD>(q1, Dc, i2 + ioff, j2, 0) + T(0.375) * cat<T, LD>(q1, Dc, i2, j2 + 1, 0) +
+                    T(0.125) * cat<T, LD>(q1, Dc, i2 + ioff, j2 + 1, 0);
+            f1[t] = v;
+        }
+    } else {
+        const T n16 = T(9.0 / 16.0), t16 = T(3.0 / 16.0), o16 = T(1.0 / 16.0);
+        const T n32 = T(9.0 / 32.0), t32 = T(3.0 / 32.0), o32 = T(1.0 / 32.0);
+        const int ioff = ((i & 1) == 0) ? -1 : 1, joff = ((j & 1) == 0) ? -1 : 1, koff = ((k & 1) == 0) ? -1 : 1;
+        {
+            T v = (LD == 2) ? __ldcg(f0 + t) : f0[t];
+            if ((i & 1) == 0)
+                v = v + n16 * cat<T, LD>(q0, Dc, i2, j2, k2) + t16 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2) + t16 * cat<T, LD>(q0, Dc, i2, j2, k2 + koff) +
+                    o16 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2 + koff);
+            else
+                v = v + n32 * cat<T, LD>(q0, Dc, i2, j2, k2) + t32 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2) + t32 * cat<T, LD>(q0, Dc, i2, j2, k2 + koff) +
+                    o32 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2 + koff) + n32 * cat<T, LD>(q0, Dc, i2 + 1, j2, k2) +
+                    t32 * cat<T, LD>(q0, Dc, i2 + 1, j2 + joff, k2) + t32 * cat<T, LD>(q0, Dc, i2 + 1, j2, k2 + koff) +
+                    o32 * cat<T, LD>(q0, Dc, i2 + 1, j2 + joff, k2 + koff);
+            f0[t] = v;
+        }
+        {
+            T v = (LD == 2) ? __ldcg(f1 + t) : f1[t];
+            if ((j & 1) == 0)
+                v = v + n16 * cat<T, LD>(q1, Dc, i2, j2, k2) + t16 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2) + t16 * cat<T, LD>(q1, Dc, i2, j2, k2 + koff) +
+                    o16 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2 + koff);
+            else
+                v = v + n32 * cat<T, LD>(q1, Dc, i2, j2, k2) + t32 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2) + t32 * cat<T, LD>(q1, Dc, i2, j2, k2 + koff) +
+                    o32 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2 + koff) + n32 * cat<T, LD>(q1, Dc, i2, j2 + 1, k2) +
+                    t32 * cat<T, LD>(q1, Dc, i2 + ioff, j2 + 1, k2) + t32 * cat<T, LD>(q1, Dc, i2, j2 + 1, k2 + koff) +
+                    o32 * cat<T, LD>(q1, Dc, i2 + ioff, j2 + 1, k2 + koff);
+            f1[t] = v;
+        }
+        {
+            T v = (LD == 2) ? __ldcg(f2 + t) : f2[t];
+            if ((k & 1) == 0)
+                v = v + n16 * cat<T, LD>(q2, Dc, i2, j2, k2) + t16 * cat<T, LD>(q2, Dc, i2 + ioff, j2, k2) + t16 * cat<T, LD>(q2, Dc, i2, j2 + joff, k2) +
+                    o16 * cat<T, LD>(q2, Dc, i2 + ioff, j2 + joff, k2);
+            else
+                v = v + n32 * cat<T, LD>(q2, Dc, i2, j2, k2) + t32 * cat<T, LD>(q2, Dc, i2 + ioff, j2, k2) + t32 * cat<T, LD>(q2, Dc, i2, j2 + joff, k2) +
+                    o32 * cat<T, LD>(q2, Dc, i2 + ioff, j2 + joff, k2) + n32 * cat<T, LD>(q2, Dc, i2, j2, k2 + 1) +
+                    t32 * cat<T, LD>(q2, Dc, i2 + ioff, j2, k2 + 1) + t32 * cat<T, LD>(q2, Dc, i2, j2 + joff, k2 + 1) +
+                    o32 * cat<T, LD>(q2, Dc, i2 + ioff, j2 + joff, k2 + 1);
+            f2[t] = v;
+        }
+    }
 }
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_prolong_add(Dims F, Dims Dc, const T* __restrict__ q0, const T* __restrict__ q1,
                                                           const T* __restrict__ q2, T* __restrict__ f0, T* __restrict__ f1,
                                                           T* __restrict__ f2) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)F.nx * F.ny * F.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(F, t, i, j, k);
-    const int i2 = i / 2, j2 = j / 2, k2 = k / 2;
-    if constexpr (DM == 2) {
-        {
-            int joff = (j % 2 == 0) ? -1 : 1;
-            T v = f0[t];
-            if (i % 2 == 0)
-                v = v + T(0.75) * cat(q0, Dc, i2, j2, 0) + T(0.25) * cat(q0, Dc, i2, j2 + joff, 0);
-            else
-                v = v + T(0.375) * cat(q0, Dc, i2, j2, 0) + T(0.125) * cat(q0, Dc, i2, j2 + joff, 0) + T(0.375) * cat(q0, Dc, i2 + 1, j2, 0) +
-                    T(0.125) * cat(q0, Dc, i2 + 1, j2 + joff, 0);
-            f0[t] = v;
-        }
-        {
-            int ioff = (i % 2 == 0) ? -1 : 1;
-            T v = f1[t];
-            if (j % 2 == 0)
-                v = v + T(0.75) * cat(q1, Dc, i2, j2, 0) + T(0.25) * cat(q1, Dc, i2 + ioff, j2, 0);
-            else
-                v = v + T(0.375) * cat(q1, Dc, i2, j2, 0) + T(0.125) * cat(q1, Dc, i2 + ioff, j2, 0) + T(0.375) * cat(q1, Dc, i2, j2 + 1, 0) +
-                    T(0.125) * cat(q1, Dc, i2 + ioff, j2 + 1, 0);
-            f1[t] = v;
-        }
-    } else {
-        const T n16 = T(9.0 / 16.0), t16 = T(3.0 / 16.0), o16 = T(1.0 / 16.0);
-        const T n32 = T(9.0 / 32.0), t32 = T(3.0 / 32.0), o32 = T(1.0 / 32.0);
-        const int ioff = (i % 2 == 0) ? -1 : 1, joff = (j % 2 == 0) ? -1 : 1, koff = (k % 2 == 0) ? -1 : 1;
-        {
-            T v = f0[t];
-            if (i % 2 == 0)
-                v = v + n16 * cat(q0, Dc, i2, j2, k2) + t16 * cat(q0, Dc, i2, j2 + joff, k2) + t16 * cat(q0, Dc, i2, j2, k2 + koff) +
-                    o16 * cat(q0, Dc, i2, j2 + joff, k2 + koff);
-            else
-                v = v + n32 * cat(q0, Dc, i2, j2, k2) + t32 * cat(q0, Dc, i2, j2 + joff, k2) + t32 * cat(q0, Dc, i2, j2, k2 + koff) +
-                    o32 * cat(q0, Dc, i2, j2 + joff, k2 + koff) + n32 * cat(q0, Dc, i2 + 1, j2, k2) +
-                    t32 * cat(q0, Dc, i2 + 1, j2 + joff, k2) + t32 * cat(q0, Dc, i2 + 1, j2, k2 + koff) +
-                    o32 * cat(q0, Dc, i2 + 1, j2 + joff, k2 + koff);
-            f0[t] = v;
-        }
-        {
-            T v = f1[t];
-            if (j % 2 == 0)
-                v = v + n16 * cat(q1, Dc, i2, j2, k2) + t16 * cat(q1, Dc, i2 + ioff, j2, k2) + t16 * cat(q1, Dc, i2, j2, k2 + koff) +
-                    o16 * cat(q1, Dc, i2 + ioff, j2, k2 + koff);
-            else
-                v = v + n32 * cat(q1, Dc, i2, j2, k2) + t32 * cat(q1, Dc, i2 + ioff, j2, k2) + t32 * cat(q1, Dc, i2, j2, k2 + koff) +
-                    o32 * cat(q1, Dc, i2 + ioff, j2, k2 + koff) + n32 * cat(q1, Dc, i2, j2 + 1, k2) +
-                    t32 * cat(q1, Dc, i2 + ioff, j2 + 1, k2) + t32 * cat(q1, Dc, i2, j2 + 1, k2 + koff) +
-                    o32 * cat(q1, Dc, i2 + ioff, j2 + 1, k2 + koff);
-            f1[t] = v;
-        }
-        {
-            T v = f2[t];
-            if (k % 2 == 0)
-                v = v + n16 * cat(q2, Dc, i2, j2, k2) + t16 * cat(q2, Dc, i2 + ioff, j2, k2) + t16 * cat(q2, Dc, i2, j2 + joff, k2) +
-                    o16 * cat(q2, Dc, i2 + ioff, j2 + joff, k2);
-            else
-                v = v + n32 * cat(q2, Dc, i2, j2, k2) + t32 * cat(q2, Dc, i2 + ioff, j2, k2) + t32 * cat(q2, Dc, i2, j2 + joff, k2) +
-                    o32 * cat(q2, Dc, i2 + ioff, j2 + joff, k2) + n32 * cat(q2, Dc, i2, j2, k2 + 1) +
-                    t32 * cat(q2, Dc, i2 + ioff, j2, k2 + 1) + t32 * cat(q2, Dc, i2, j2 + joff, k2 + 1) +
-                    o32 * cat(q2, Dc, i2 + ioff, j2 + joff, k2 + 1);
-            f2[t] = v;
-        }
-    }
+    const Pos q = pos3(F.nx, F.ny);
+    if (!q.ok) return;
+    const int t = q.i + F.nx * (q.j + F.ny * q.k);
+    prolong_cell<T, DM, 0>(Dc, q0, q1, q2, f0, f1, f2, t, q.i, q.j, q.k);
 }
 
 // --------------------------------------------------------------- coefficient coarsening
+// fine-grid value at (i, j, k), all indices inside the fine box
 template <class T>
 __device__ __forceinline__ T fat(const T* a, const Dims& F, int i, int j, int k) {
-    return ld(a, (i % F.nx) + (int64_t)F.nx * ((j % F.ny) + (int64_t)F.ny * (F.dm == 3 ? (k % F.nz) : 0)));
+    return ld(a, i + F.nx * (j + F.ny * (F.dm == 3 ? k : 0)));
 }
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> Cf, T* a0, T* a1, T* a2, T* beta, T* gamma,
                                                       T* e0, T* e1, T* e2, int do_visc) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)Dc.nx * Dc.ny * Dc.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(Dc, t, i, j, k);
+    const Pos q = pos3(Dc.nx, Dc.ny);
+    if (!q.ok) return;
+    const int i = q.i, j = q.j, k = q.k;
+    const int t = i + Dc.nx * (j + Dc.ny * k);
     const int I = 2 * i, J = 2 * j, K = 2 * k;
     if constexpr (DM == 2) {
         a0[t] = T(0.5) * (fat(Cf.alpha[0], F, I, J, 0) + fat(Cf.alpha[0], F, I, J + 1, 0));
@@ -299,18 +342,19 @@ __global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> C
 }
 
 // --------------------------------------------------------------- pressure multigrid
-template <class T, int DM>
+template <class T, int DM, int LD = 0>
 __device__ __forceinline__ T cc_lap(const T* const a[3], const T* phi, const Nb& n, T dxsqinv) {
-    const int64_t s = n.s;
-    const T p = ld(phi, s);
-    T v = (ld(a[0], s + n.op[0]) * (ld(phi, s + n.op[0]) - p) - ld(a[0], s) * (p - ld(phi, s + n.om[0]))) +
-          (ld(a[1], s + n.op[1]) * (ld(phi, s + n.op[1]) - p) - ld(a[1], s) * (p - ld(phi, s + n.om[1])));
-    if constexpr (DM == 3) v = v + (ld(a[2], s + n.op[2]) * (ld(phi, s + n.op[2]) - p) - ld(a[2], s) * (p - ld(phi, s + n.om[2])));
+    const int s = n.s;
+    const T p = ldp<LD>(phi, s);
+    T v = (ld(a[0], s + n.op[0]) * (ldp<LD>(phi, s + n.op[0]) - p) - ld(a[0], s) * (p - ldp<LD>(phi, s + n.om[0]))) +
+          (ld(a[1], s + n.op[1]) * (ldp<LD>(phi, s + n.op[1]) - p) - ld(a[1], s) * (p - ldp<LD>(phi, s + n.om[1])));
+    if constexpr (DM == 3)
+        v = v + (ld(a[2], s + n.op[2]) * (ldp<LD>(phi, s + n.op[2]) - p) - ld(a[2], s) * (p - ldp<LD>(phi, s + n.om[2])));
     return v * dxsqinv;
 }
 template <class T, int DM>
 __device__ __forceinline__ T cc_diag(const T* const a[3], const Nb& n, T dxsqinv) {
-    const int64_t s = n.s;
+    const int s = n.s;
     T sum = ld(a[0], s) + ld(a[0], s + n.op[0]) + ld(a[1], s) + ld(a[1], s + n.op[1]);
     if constexpr (DM == 3) sum = sum + ld(a[2], s) + ld(a[2], s + n.op[2]);
     return -(sum * dxsqinv);
@@ -319,15 +363,10 @@ __device__ __forceinline__ T cc_diag(const T* const a[3], const Nb& n, T dxsqinv
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ rhs,
                                                         T* phi, int parity, T dxsqinv) {
-    const int hx = D.nx >> 1;
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)hx * D.ny * D.nz;
-    if (t >= n) return;
-    int ih = (int)(t % hx);
-    int64_t r = t / hx;
-    int j = (int)(r % D.ny);
-    int k = (int)(r / D.ny);
-    int i = 2 * ih + ((j + k + parity) & 1);
+    const Pos q = pos3(D.nx >> 1, D.ny);
+    if (!q.ok) return;
+    const int j = q.j, k = q.k;
+    const int i = 2 * q.i + ((j + k + parity) & 1);
     Nb nb = make_nb(D, i, j, k);
     const T* a[3] = {a0, a1, a2};
     T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
@@ -335,22 +374,21 @@ __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, con
     phi[nb.s] = cur + res / cc_diag<T, DM>(a, nb, dxsqinv);
 }
 
-template <class T, int DM>
+template <class T, int DM, int LD = 0>
 __device__ __forceinline__ T cc_res_at(const Dims& F, const T* const a[3], const T* phi, const T* rhs, int i, int j, int k,
                                        T dxsqinv) {
-    Nb nb = make_nb(F, i, j, k);
-    return ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
+    Nb nb = make_nb(F, i, j, (DM == 3) ? k : 0);
+    return ldp<LD>(rhs, nb.s) - cc_lap<T, DM, LD>(a, phi, nb, dxsqinv);
 }
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const T* a0, const T* a1, const T* a2,
                                                                    const T* __restrict__ rhs, const T* __restrict__ phi, Dims Dc,
                                                                    T* __restrict__ rc, T dxsqinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)Dc.nx * Dc.ny * Dc.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(Dc, t, i, j, k);
+    const Pos q = pos3(Dc.nx, Dc.ny);
+    if (!q.ok) return;
+    const int i = q.i, j = q.j, k = q.k;
+    const int t = i + Dc.nx * (j + Dc.ny * k);
     const T* a[3] = {a0, a1, a2};
     const int I = 2 * i, J = 2 * j, K = 2 * k;
 #define R(ii, jj, kk) cc_res_at<T, DM>(F, a, phi, rhs, ii, jj, kk, dxsqinv)
@@ -364,25 +402,20 @@ __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_prolong_add(Dims F, Dims Dc, const T* __restrict__ pc, T* __restrict__ pf) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)F.nx * F.ny * F.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(F, t, i, j, k);
-    pf[t] = pf[t] + ld(pc, (i / 2) + (int64_t)Dc.nx * ((j / 2) + (int64_t)Dc.ny * (k / 2)));
+    const Pos q = pos3(F.nx, F.ny);
+    if (!q.ok) return;
+    const int t = q.i + F.nx * (q.j + F.ny * q.k);
+    pf[t] = pf[t] + ld(pc, (q.i >> 1) + Dc.nx * ((q.j >> 1) + Dc.ny * (q.k >> 1)));
 }
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_neg_cc_lap(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ phi,
                                                          T* __restrict__ out, T dxsqinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(D, t, i, j, k);
-    Nb nb = make_nb(D, i, j, k);
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
     const T* a[3] = {a0, a1, a2};
-    out[t] = -cc_lap<T, DM>(a, phi, nb, dxsqinv);
+    out[nb.s] = -cc_lap<T, DM>(a, phi, nb, dxsqinv);
 }
 
 // --------------------------------------------------------------- div / grad pieces
@@ -390,12 +423,10 @@ template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_div_plus(Dims D, const T* __restrict__ u0, const T* __restrict__ u1,
                                                        const T* __restrict__ u2, const T* __restrict__ bp, T* __restrict__ out,
                                                        T dxinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(D, t, i, j, k);
-    Nb nb = make_nb(D, i, j, k);
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
     T v = (ld(u0, t + nb.op[0]) - ld(u0, t)) * dxinv + (ld(u1, t + nb.op[1]) - ld(u1, t)) * dxinv;
     if constexpr (DM == 3) v = v + (ld(u2, t + nb.op[2]) - ld(u2, t)) * dxinv;
     out[t] = v + ld(bp, t);
@@ -404,12 +435,10 @@ __global__ void __launch_bounds__(kThreads) k_div_plus(Dims D, const T* __restri
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_sub_weighted_grad(Dims D, const T* c0, const T* c1, const T* c2,
                                                                 const T* __restrict__ phi, T* u0, T* u1, T* u2, T dxinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat(D, t, i, j, k);
-    Nb nb = make_nb(D, i, j, k);
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
     const T p = ld(phi, t);
     T* u[3] = {u0, u1, u2};
     const T* c[3] = {c0, c1, c2};
@@ -448,7 +477,11 @@ __global__ void k_fill(T* __restrict__ out, T v, int64_t n) {
 // a fixed tree, writes its partials; the last block to finish sums all
 // partials in block order.  The result depends only on n and the launch
 // shape, never on scheduling.
+//
 // MODE 0: weighted dot, MODE 1: weighted sum, MODE 2: max |a - b| (inf norm).
+// Seam weights: the main loop gives every face weight 1; a second loop over
+// the periodic seam plane of face component c (index_c == 0) adds
+// (w_c - 1) a b, so the seam face ends with weight w_c.
 // out[0..dm] per component; out[4] = sum_d out[d] + pw^2 out[dm] (the
 // Hessenberg entry of gmres.f90:344), out[5] = sqrt(|u|^2 + (pw |p|)^2)
 // (the Stokes norm of gmres.f90:127-130).
@@ -463,26 +496,46 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
     double acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-    const int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) {
-        int i, j, k;
-        unflat(D, t, i, j, k);
-        const int idx[3] = {i, j, k};
+    const int n = D.nx * D.ny * D.nz;
+    const int stride = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const T* a = (c < DM) ? A[c] : A[3];
-            const T* b = (c < DM) ? B[c] : B[3];
-            if (!a) continue;
-            double v = (double)ld(a, t);
+    for (int c = 0; c < NC; ++c) {
+        const T* a = (c < DM) ? A[c] : A[3];
+        const T* b = (c < DM) ? B[c] : B[3];
+        if (!a) continue;
+        double v = 0.0;
+        for (int t = tid; t < n; t += stride) {
+            double x = (double)ld(a, t);
             if (MODE == 2) {
-                v = fabs(v - (b ? (double)ld(b, t) : 0.0));
-                acc[c] = fmax(acc[c], v);
-                continue;
+                v = fmax(v, fabs(x - (b ? (double)ld(b, t) : 0.0)));
+            } else {
+                if (MODE == 0) x = x * (double)ld(b, t);
+                v += x;
             }
-            if (MODE == 0) v = v * (double)ld(b, t);
-            if (c < DM && idx[c] == 0) v = v * W[c];
-            acc[c] += v;
+        }
+        acc[c] = v;
+    }
+    if (MODE != 2) {
+        // seam planes: x faces i == 0 (ny*nz of them), y faces j == 0 (nx*nz),
+        // z faces k == 0 (nx*ny)
+#pragma unroll
+        for (int c = 0; c < DM; ++c) {
+            const T* a = A[c];
+            const T* b = B[c];
+            if (!a || W[c] == 1.0) continue;
+            const int m = (c == 0) ? D.ny * D.nz : (c == 1 ? D.nx * D.nz : D.nx * D.ny);
+            double v = 0.0;
+            for (int q = tid; q < m; q += stride) {
+                int t;
+                if (c == 0) t = D.nx * q;                                     // (0, j, k)
+                else if (c == 1) t = (q % D.nx) + D.nx * D.ny * (q / D.nx);   // (i, 0, k)
+                else t = q;                                                   // (i, j, 0)
+                double x = (double)ld(a, t);
+                if (MODE == 0) x = x * (double)ld(b, t);
+                v += x;
+            }
+            acc[c] += (W[c] - 1.0) * v;
         }
     }
     __shared__ double sh[NC][kThreads / 32];
@@ -501,7 +554,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
         for (int c = 0; c < NC; ++c) {
             double v = 0.0;
             for (int w = 0; w < kThreads / 32; ++w) v = (MODE == 2) ? fmax(v, sh[c][w]) : v + sh[c][w];
-            partials[(int64_t)blockIdx.x * NC + c] = v;
+            partials[blockIdx.x * NC + c] = v;
         }
         __threadfence();
     }
@@ -519,7 +572,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
         const int c = threadIdx.x;
         double v = 0.0;
         for (unsigned bidx = 0; bidx < gridDim.x; ++bidx) {
-            double q = ((volatile double*)partials)[(int64_t)bidx * NC + c];
+            double q = ((volatile double*)partials)[bidx * NC + c];
             v = (MODE == 2) ? fmax(v, q) : v + q;
         }
         fin[c] = v;
@@ -552,11 +605,11 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
 template <class T>
 void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
-    const int nb = nblocks_for(L.n);
+    const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_applyop<T, 2, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+        LMM_VISC_DISPATCH(visc, (k_applyop<T, 2, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_applyop<T, 3, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+        LMM_VISC_DISPATCH(visc, (k_applyop<T, 3, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
     }
 }
 
@@ -566,9 +619,9 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const int comp = (color - 1) / 2;
     const int parity = (color % 2 == 1) ? 0 : 1;
-    const int nb = nblocks_for(L.n / 2);
+    const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
     const T om = (T)omega;
-#define GS(DM_, COMP_) k_gs_colour<T, DM_, V, COMP_><<<nb, kThreads, 0, s>>>(L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
+#define GS(DM_, COMP_) k_gs_colour<T, DM_, V, COMP_><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
         else { LMM_VISC_DISPATCH(visc, GS(2, 1)) }
@@ -584,12 +637,12 @@ template <class T>
 void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const pin[3], T* const pout[3],
                    double omega, cudaStream_t s) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
-    const int nb = nblocks_for(L.n);
+    const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     const T om = (T)omega;
     if (L.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 2, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 2, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 3, V><<<nb, kThreads, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 3, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
     }
 }
 
@@ -597,102 +650,102 @@ template <class T>
 void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
                               const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s) {
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
-    const int nb = nblocks_for(Cc.n);
+    const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz * F.D.dm);
     if (F.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 2, V><<<nb, kThreads, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 2, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 3, V><<<nb, kThreads, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 3, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
     }
 }
 
 template <class T>
 void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3],
                         cudaStream_t s) {
-    const int nb = nblocks_for(F.n);
+    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
-        k_prolong_add<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+        k_prolong_add<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
     else
-        k_prolong_add<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+        k_prolong_add<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
 }
 
 template <class T>
 void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s) {
-    const int nb = nblocks_for(Cc.n);
+    const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
     Coef<T> cf = F.coef();
     if (pressure_faces) {
         for (int d = 0; d < 3; ++d) cf.alpha[d] = F.pa[d];
         if (F.D.dm == 2)
-            k_coarsen<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+            k_coarsen<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
         else
-            k_coarsen<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+            k_coarsen<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
         return;
     }
     if (F.D.dm == 2)
-        k_coarsen<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
+        k_coarsen<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
     else
-        k_coarsen<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
+        k_coarsen<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
 }
 
 template <class T>
 void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
-    const int nb = nblocks_for(L.n / 2);
+    const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
     if (L.D.dm == 2)
-        k_cc_smooth<T, 2><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+        k_cc_smooth<T, 2><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
     else
-        k_cc_smooth<T, 3><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+        k_cc_smooth<T, 3><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
 }
 
 template <class T>
 void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s) {
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
-    const int nb = nblocks_for(Cc.n);
+    const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
     if (F.D.dm == 2)
-        k_cc_residual_restrict<T, 2><<<nb, kThreads, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+        k_cc_residual_restrict<T, 2><<<g.grid, g.block, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
     else
-        k_cc_residual_restrict<T, 3><<<nb, kThreads, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+        k_cc_residual_restrict<T, 3><<<g.grid, g.block, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
 }
 
 template <class T>
 void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s) {
-    const int nb = nblocks_for(F.n);
+    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
-        k_cc_prolong_add<T, 2><<<nb, kThreads, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
+        k_cc_prolong_add<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
     else
-        k_cc_prolong_add<T, 3><<<nb, kThreads, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
+        k_cc_prolong_add<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
 }
 
 template <class T>
 void launch_neg_cc_lap(const LevelDev<T>& L, const T* phi, T* out, cudaStream_t s) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
-    const int nb = nblocks_for(L.n);
+    const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2)
-        k_neg_cc_lap<T, 2><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
+        k_neg_cc_lap<T, 2><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
     else
-        k_neg_cc_lap<T, 3><<<nb, kThreads, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
+        k_neg_cc_lap<T, 3><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
 }
 
 template <class T>
 void launch_div_plus(const LevelDev<T>& L, const T* const u[3], const T* bp, T* out, cudaStream_t s) {
     const T dxinv = T(1.0 / L.dx);
-    const int nb = nblocks_for(L.n);
+    const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2)
-        k_div_plus<T, 2><<<nb, kThreads, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+        k_div_plus<T, 2><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
     else
-        k_div_plus<T, 3><<<nb, kThreads, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+        k_div_plus<T, 3><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
 }
 
 template <class T>
 void launch_sub_weighted_grad(const LevelDev<T>& L, const T* const coef[3], const T* phi, T* const u[3], cudaStream_t s) {
     const T dxinv = T(1.0 / L.dx);
-    const int nb = nblocks_for(L.n);
+    const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     const T* c0 = coef ? coef[0] : nullptr;
     const T* c1 = coef ? coef[1] : nullptr;
     const T* c2 = coef ? coef[2] : nullptr;
     if (L.D.dm == 2)
-        k_sub_weighted_grad<T, 2><<<nb, kThreads, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+        k_sub_weighted_grad<T, 2><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
     else
-        k_sub_weighted_grad<T, 3><<<nb, kThreads, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+        k_sub_weighted_grad<T, 3><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
 }
 
 template <class Tin, class Tout>

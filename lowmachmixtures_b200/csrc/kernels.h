@@ -59,6 +59,14 @@ void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* co
 template <class T>
 void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s);
 
+// The coarse end of a V-cycle (levels L[0..nl-1], L[0] already holding its
+// rhs) in one thread-block-cluster launch of csize blocks (tail.cuh).
+template <class T>
+cudaError_t launch_vcycle_tail(const LevelDev<T>* L, int nl, int visc, int nu1, int nu2, int nub, int smoother, double omega,
+                               int csize, cudaStream_t s);
+template <class T>
+cudaError_t launch_ccmg_tail(const LevelDev<T>* L, int nl, int nu1, int nu2, int nub, int csize, cudaStream_t s);
+
 // ---- pressure multigrid (this library's cell-centred V-cycle) ----
 template <class T>
 void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s);

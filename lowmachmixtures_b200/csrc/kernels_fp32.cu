@@ -2,7 +2,9 @@
 // by the mixed-precision preconditioner inside FP64 flexible GMRES.  Built
 // with FMA contraction enabled (the FP32 V-cycle needs no bit parity).
 #include "kernels.cuh"
+#include "tail.cuh"
 
 namespace lmm {
 LMM_INSTANTIATE(float)
+LMM_INSTANTIATE_TAIL(float)
 }  // namespace lmm

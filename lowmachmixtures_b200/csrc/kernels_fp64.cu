@@ -3,9 +3,11 @@
 // the operand order of the reference Fortran, so face values match the
 // reference arithmetic (and the CPU oracle) bit for bit.
 #include "kernels.cuh"
+#include "tail.cuh"
 
 namespace lmm {
 LMM_INSTANTIATE(double)
+LMM_INSTANTIATE_TAIL(double)
 template void launch_convert<double, float>(const double*, float*, int64_t, cudaStream_t);
 template void launch_convert<float, double>(const float*, double*, int64_t, cudaStream_t);
 }  // namespace lmm

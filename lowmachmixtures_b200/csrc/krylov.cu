@@ -9,11 +9,11 @@ namespace {
 constexpr int kT = 256;
 inline int nb(int64_t n) { return (int)((n + kT - 1) / kT < 1 ? 1 : (n + kT - 1) / kT); }
 
-__device__ __forceinline__ void unflat3(const Dims& D, int64_t t, int& i, int& j, int& k) {
-    i = (int)(t % D.nx);
-    int64_t r = t / D.nx;
-    j = (int)(r % D.ny);
-    k = (int)(r / D.ny);
+__device__ __forceinline__ void unflat3(const Dims& D, int t, int& i, int& j, int& k) {
+    i = t % D.nx;
+    int r = t / D.nx;
+    j = r % D.ny;
+    k = r / D.ny;
 }
 }  // namespace
 
@@ -24,12 +24,10 @@ __global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, con
                                                      const double* __restrict__ p, double* __restrict__ o0,
                                                      double* __restrict__ o1, double* __restrict__ o2, double* __restrict__ op,
                                                      double dxsqinv, double dxinv) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
-    if (t >= n) return;
-    int i, j, k;
-    unflat3(D, t, i, j, k);
-    Nb nbr = make_nb(D, i, j, k);
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nbr = make_nb(D, q.i, q.j, q.k);
+    const int t = nbr.s;
     const double* phi[3] = {u0, u1, u2};
     const double b = ld(C.beta, 0), c = ld(C.gamma, 0);
     const double pc = ld(p, t);
@@ -56,10 +54,13 @@ __global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, con
 void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s) {
     const double dxsqinv = 1.0 / (L0.dx * L0.dx);
     const double dxinv = 1.0 / L0.dx;
-    const int g = nb(L0.n);
+    int bx = L0.D.nx < 64 ? L0.D.nx : 64;
+    int by = 256 / bx;
+    if (by > L0.D.ny) by = L0.D.ny;
+    const dim3 blk(bx, by, 1), grd((L0.D.nx + bx - 1) / bx, (L0.D.ny + by - 1) / by, L0.D.nz);
     const double* x2 = (x.dm == 3) ? x.c(2) : x.c(0);
     double* b2 = (b.dm == 3) ? b.c(2) : b.c(0);
-#define AM(DM_, V_) k_apply_matrix<DM_, V_><<<g, kT, 0, s>>>(L0.D, L0.coef(), x.c(0), x.c(1), x2, x.p(), b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
+#define AM(DM_, V_) k_apply_matrix<DM_, V_><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x.c(0), x.c(1), x2, x.p(), b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
 #define AMV(DM_)                    \
     switch (visc) {                 \
     case -1: AM(DM_, -1); break;    \
@@ -243,8 +244,8 @@ int64_t boxlib_size(const Dims& D, const int nodal[3], int ng) {
 }
 
 __global__ void k_gather_boxlib(Dims D, int ex, int ey, int ng, const double* __restrict__ in, double* __restrict__ out) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)D.nx * D.ny * D.nz;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = D.nx * D.ny * D.nz;
     if (t >= n) return;
     int i, j, k;
     unflat3(D, t, i, j, k);
@@ -253,13 +254,13 @@ __global__ void k_gather_boxlib(Dims D, int ex, int ey, int ng, const double* __
 }
 
 __global__ void k_scatter_boxlib(Dims D, int ex, int ey, int ez, int ng, const double* __restrict__ in, double* __restrict__ out) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t n = (int64_t)ex * ey * ez;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = ex * ey * ez;
     if (t >= n) return;
-    int I = (int)(t % ex);
-    int64_t r = t / ex;
-    int J = (int)(r % ey);
-    int K = (int)(r / ey);
+    int I = t % ex;
+    int r = t / ex;
+    int J = r % ey;
+    int K = r / ey;
     const int kg = (D.dm == 3) ? ng : 0;
     int i = ((I - ng) % D.nx + D.nx) % D.nx;
     int j = ((J - ng) % D.ny + D.ny) % D.ny;

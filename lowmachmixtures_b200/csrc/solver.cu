@@ -348,19 +348,44 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
     }
 }
 
+// first level handled by the cluster tail kernel (nl: no tail)
+template <class T>
+int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl) {
+    const int cells = h->knobs.tail_cells == 0 ? 4096 : h->knobs.tail_cells;
+    if (cells < 0) return nl;
+    int lc = nl;
+    while (lc > 0 && L[lc - 1].n <= cells) --lc;
+    if (nl - lc > 12) lc = nl - 12;  // kMaxTail levels at most
+    return lc;
+}
+
+int tail_cluster(lmm_handle* h) {
+    int c = h->knobs.tail_cluster == 0 ? 8 : h->knobs.tail_cluster;
+    return std::max(1, std::min(16, c));
+}
+
 template <class T>
 void vcycle(lmm_handle* h, std::vector<LevelDev<T>>& L) {
     const lmm_knobs& K = h->knobs;
     const int nl = h->nlev;
-    for (int l = 1; l < nl; ++l)
+    const int lc = tail_start<T>(h, L, nl);
+    // coarse-level initial guesses are zero; the tail zeroes the levels below its first
+    for (int l = 1; l <= std::min(lc, nl - 1); ++l)
         for (int d = 0; d < h->dm; ++d) LMM_CK(cudaMemsetAsync(L[l].phi[d], 0, L[l].n * sizeof(T), h->stream));
-    for (int l = 0; l < nl - 1; ++l) {
+    for (int l = 0; l < lc && l < nl - 1; ++l) {
         smooth<T>(h, L[l], K.stag_mg_nsmooths_down);
         launch_residual_restrict<T>(L[l], L[l + 1], K.visc_type, L[l].rhs, L[l].phi, L[l + 1].rhs, h->stream);
         check_launch();
     }
-    smooth<T>(h, L[nl - 1], K.stag_mg_nsmooths_bottom);
-    for (int l = nl - 2; l >= 0; --l) {
+    if (lc < nl) {
+        LMM_CK(launch_vcycle_tail<T>(&L[lc], nl - lc, K.visc_type, K.stag_mg_nsmooths_down, K.stag_mg_nsmooths_up,
+                                     K.stag_mg_nsmooths_bottom, K.stag_mg_smoother, K.stag_mg_omega, tail_cluster(h),
+                                     h->stream));
+        check_launch();
+    } else {
+        smooth<T>(h, L[nl - 1], K.stag_mg_nsmooths_bottom);
+    }
+    for (int l = std::min(lc, nl - 1) - 1; l >= 0; --l) {
         launch_prolong_add<T>(L[l], L[l + 1], L[l + 1].phi, L[l].phi, h->stream);
         check_launch();
         smooth<T>(h, L[l], K.stag_mg_nsmooths_up);
@@ -448,16 +473,23 @@ void macproject(lmm_handle* h) {
     auto& L = levels<T>(h);
     const lmm_knobs& K = h->knobs;
     const int nl = h->nlev_p;
+    const int lc = tail_start<T>(h, L, nl);
     LMM_CK(cudaMemsetAsync(L[0].pphi, 0, L[0].n * sizeof(T), h->stream));
     for (int vc = 0; vc < K.mg_max_vcycles; ++vc) {
-        for (int l = 1; l < nl; ++l) LMM_CK(cudaMemsetAsync(L[l].pphi, 0, L[l].n * sizeof(T), h->stream));
-        for (int l = 0; l < nl - 1; ++l) {
+        for (int l = 1; l <= std::min(lc, nl - 1); ++l) LMM_CK(cudaMemsetAsync(L[l].pphi, 0, L[l].n * sizeof(T), h->stream));
+        for (int l = 0; l < lc && l < nl - 1; ++l) {
             cc_smooth<T>(h, L[l], K.mg_nsmooths_down);
             launch_cc_residual_restrict<T>(L[l], L[l + 1], h->stream);
             check_launch();
         }
-        cc_smooth<T>(h, L[nl - 1], K.mg_nsmooths_bottom);
-        for (int l = nl - 2; l >= 0; --l) {
+        if (lc < nl) {
+            LMM_CK(launch_ccmg_tail<T>(&L[lc], nl - lc, K.mg_nsmooths_down, K.mg_nsmooths_up, K.mg_nsmooths_bottom,
+                                       tail_cluster(h), h->stream));
+            check_launch();
+        } else {
+            cc_smooth<T>(h, L[nl - 1], K.mg_nsmooths_bottom);
+        }
+        for (int l = std::min(lc, nl - 1) - 1; l >= 0; --l) {
             launch_cc_prolong_add<T>(L[l], L[l + 1], h->stream);
             check_launch();
             cc_smooth<T>(h, L[l], K.mg_nsmooths_up);

@@ -18,11 +18,12 @@
 
 namespace lmm {
 
-// neighbour offsets (with periodic wrap) of one index
+// neighbour offsets (with periodic wrap) of one index; 32-bit indices
+// (a field holds at most 2^31 - 1 entries)
 struct Nb {
-    int64_t s;       // linear index
-    int64_t op[3];   // offset to +1 in direction d
-    int64_t om[3];   // offset to -1 in direction d
+    int s;       // linear index
+    int op[3];   // offset to +1 in direction d
+    int om[3];   // offset to -1 in direction d
 };
 
 struct Dims {
@@ -32,15 +33,15 @@ struct Dims {
 
 __device__ __forceinline__ Nb make_nb(const Dims& D, int i, int j, int k) {
     Nb b;
-    const int64_t sx = 1, sy = D.nx, sz = (int64_t)D.nx * D.ny;
+    const int sx = 1, sy = D.nx, sz = D.nx * D.ny;
     b.s = i + sy * j + sz * k;
-    b.op[0] = (i == D.nx - 1) ? -(int64_t)(D.nx - 1) * sx : sx;
-    b.om[0] = (i == 0) ? (int64_t)(D.nx - 1) * sx : -sx;
-    b.op[1] = (j == D.ny - 1) ? -(int64_t)(D.ny - 1) * sy : sy;
-    b.om[1] = (j == 0) ? (int64_t)(D.ny - 1) * sy : -sy;
+    b.op[0] = (i == D.nx - 1) ? -(D.nx - 1) * sx : sx;
+    b.om[0] = (i == 0) ? (D.nx - 1) * sx : -sx;
+    b.op[1] = (j == D.ny - 1) ? -(D.ny - 1) * sy : sy;
+    b.om[1] = (j == 0) ? (D.ny - 1) * sy : -sy;
     if (D.dm == 3) {
-        b.op[2] = (k == D.nz - 1) ? -(int64_t)(D.nz - 1) * sz : sz;
-        b.om[2] = (k == 0) ? (int64_t)(D.nz - 1) * sz : -sz;
+        b.op[2] = (k == D.nz - 1) ? -(D.nz - 1) * sz : sz;
+        b.om[2] = (k == 0) ? (D.nz - 1) * sz : -sz;
     } else {
         b.op[2] = 0;
         b.om[2] = 0;
@@ -57,8 +58,41 @@ struct Coef {
 };
 
 template <class T>
-__device__ __forceinline__ T ld(const T* p, int64_t i) {
+__device__ __forceinline__ T ld(const T* p, int i) {
     return __ldg(p + i);
+}
+
+// loads of arrays a kernel may also write (phi, rhs):
+//   LD 0  read-only path (__ldg): the array is not written by this kernel;
+//   LD 1  plain load: written by other threads of the same block between
+//         __syncthreads();
+//   LD 2  L2 load (ld.global.cg): written by other blocks of the same
+//         thread-block cluster between cluster barriers.
+template <int LD, class T>
+__device__ __forceinline__ T ldp(const T* p, int i) {
+    if constexpr (LD == 0)
+        return __ldg(p + i);
+    else if constexpr (LD == 1)
+        return p[i];
+    else
+        return __ldcg(p + i);
+}
+
+// periodic wrap of an index known to lie in [-n, 2n)
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// 3D launch geometry: x covers i (or i/2 for one colour), y covers j, z covers k
+struct Pos {
+    int i, j, k;
+    bool ok;
+};
+__device__ __forceinline__ Pos pos3(int nx, int ny) {
+    Pos p;
+    p.i = blockIdx.x * blockDim.x + threadIdx.x;
+    p.j = blockIdx.y * blockDim.y + threadIdx.y;
+    p.k = blockIdx.z;
+    p.ok = (p.i < nx) && (p.j < ny);
+    return p;
 }
 
 // compile-time direction bookkeeping of a 3D face component
@@ -68,27 +102,27 @@ template <> struct Perm3<1> { static constexpr int t1 = 0, t2 = 2, e1 = 0, e2 = 
 template <> struct Perm3<2> { static constexpr int t1 = 0, t2 = 1, e1 = 1, e2 = 2; };
 
 // ------------------------------------------------------------------ 3D
-template <class T, int VISC, int D>
+template <class T, int VISC, int D, int LD = 0>
 __device__ __forceinline__ T face_L3(const T* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
     const T* p = phi[D];
-    const int64_t s = n.s;
-    const T p0 = ld(p, s);
+    const int s = n.s;
+    const T p0 = ldp<LD>(p, s);
     const T a = ld(C.alpha[D], s);
     if (VISC == 1) {
-        T nbs = ld(p, s + n.op[0]) + ld(p, s + n.om[0]) + ld(p, s + n.op[1]) + ld(p, s + n.om[1]) + ld(p, s + n.op[2]) +
-                ld(p, s + n.om[2]);
+        T nbs = ldp<LD>(p, s + n.op[0]) + ldp<LD>(p, s + n.om[0]) + ldp<LD>(p, s + n.op[1]) + ldp<LD>(p, s + n.om[1]) + ldp<LD>(p, s + n.op[2]) +
+                ldp<LD>(p, s + n.om[2]);
         return p0 * (a + T(6) * b * dxsqinv) - nbs * b * dxsqinv;
     }
     const T* q1 = phi[t1];
     const T* q2 = phi[t2];
-    const T ppd = ld(p, s + n.op[D]), pmd = ld(p, s + n.om[D]);
-    const T pp1 = ld(p, s + n.op[t1]), pm1 = ld(p, s + n.om[t1]);
-    const T pp2 = ld(p, s + n.op[t2]), pm2 = ld(p, s + n.om[t2]);
+    const T ppd = ldp<LD>(p, s + n.op[D]), pmd = ldp<LD>(p, s + n.om[D]);
+    const T pp1 = ldp<LD>(p, s + n.op[t1]), pm1 = ldp<LD>(p, s + n.om[t1]);
+    const T pp2 = ldp<LD>(p, s + n.op[t2]), pm2 = ldp<LD>(p, s + n.om[t2]);
     // cross terms q(i,+t) , q(i) , q(i-d,+t) , q(i-d)
-    const T c10 = ld(q1, s + n.op[t1]), c11 = ld(q1, s), c12 = ld(q1, s + n.om[D] + n.op[t1]), c13 = ld(q1, s + n.om[D]);
-    const T c20 = ld(q2, s + n.op[t2]), c21 = ld(q2, s), c22 = ld(q2, s + n.om[D] + n.op[t2]), c23 = ld(q2, s + n.om[D]);
+    const T c10 = ldp<LD>(q1, s + n.op[t1]), c11 = ldp<LD>(q1, s), c12 = ldp<LD>(q1, s + n.om[D] + n.op[t1]), c13 = ldp<LD>(q1, s + n.om[D]);
+    const T c20 = ldp<LD>(q2, s + n.op[t2]), c21 = ldp<LD>(q2, s), c22 = ldp<LD>(q2, s + n.om[D] + n.op[t2]), c23 = ldp<LD>(q2, s + n.om[D]);
     if (VISC == 2) {
         return p0 * (a + T(8) * b * dxsqinv) -
                (T(2) * ppd + T(2) * pmd + pp1 + pm1 + pp2 + pm2 + c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * b * dxsqinv;
@@ -126,7 +160,7 @@ __device__ __forceinline__ T face_L3(const T* const phi[3], const Coef<T>& C, co
 template <class T, int VISC, int D>
 __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
-    const int64_t s = n.s;
+    const int s = n.s;
     const T a = ld(C.alpha[D], s);
     if (VISC == 1) return a + T(6) * b * dxsqinv;
     if (VISC == 2) return a + T(8) * b * dxsqinv;
@@ -142,22 +176,22 @@ __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv
 }
 
 // ------------------------------------------------------------------ 2D
-template <class T, int VISC, int D>
+template <class T, int VISC, int D, int LD = 0>
 __device__ __forceinline__ T face_L2(const T* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t = 1 - D;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
     const T* p = phi[D];
     const T* q = phi[t];
-    const int64_t s = n.s;
-    const T p0 = ld(p, s);
+    const int s = n.s;
+    const T p0 = ldp<LD>(p, s);
     const T a = ld(C.alpha[D], s);
-    const T ppd = ld(p, s + n.op[D]), pmd = ld(p, s + n.om[D]);
-    const T ppt = ld(p, s + n.op[t]), pmt = ld(p, s + n.om[t]);
+    const T ppd = ldp<LD>(p, s + n.op[D]), pmd = ldp<LD>(p, s + n.om[D]);
+    const T ppt = ldp<LD>(p, s + n.op[t]), pmt = ldp<LD>(p, s + n.om[t]);
     if (VISC == 1) {
         // x: i+1, i-1, j+1, j-1 ; y: j+1, j-1, i+1, i-1  (own direction first)
         return p0 * (a + T(4) * b * dxsqinv) - (ppd + pmd + ppt + pmt) * b * dxsqinv;
     }
-    const T c0 = ld(q, s + n.op[t]), c1 = ld(q, s), c2 = ld(q, s + n.om[D] + n.op[t]), c3 = ld(q, s + n.om[D]);
+    const T c0 = ldp<LD>(q, s + n.op[t]), c1 = ldp<LD>(q, s), c2 = ldp<LD>(q, s + n.om[D] + n.op[t]), c3 = ldp<LD>(q, s + n.om[D]);
     if (VISC == 2) {
         return p0 * (a + T(6) * b * dxsqinv) - (T(2) * ppd + T(2) * pmd + ppt + pmt + c0 - c1 - c2 + c3) * b * dxsqinv;
     }
@@ -183,7 +217,7 @@ __device__ __forceinline__ T face_L2(const T* const phi[3], const Coef<T>& C, co
 template <class T, int VISC, int D>
 __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t = 1 - D;
-    const int64_t s = n.s;
+    const int s = n.s;
     const T a = ld(C.alpha[D], s);
     if (VISC == 1) return a + T(4) * b * dxsqinv;
     if (VISC == 2) return a + T(6) * b * dxsqinv;
@@ -197,12 +231,12 @@ __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv
     return a + (fourthirds * be + g + fourthirds * bm + gm + E + Ep) * dxsqinv;
 }
 
-template <class T, int DM, int VISC, int D>
+template <class T, int DM, int VISC, int D, int LD = 0>
 __device__ __forceinline__ T face_L(const T* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     if constexpr (DM == 2)
-        return face_L2<T, VISC, D>(phi, C, n, dxsqinv, b, c);
+        return face_L2<T, VISC, D, LD>(phi, C, n, dxsqinv, b, c);
     else
-        return face_L3<T, VISC, D>(phi, C, n, dxsqinv, b, c);
+        return face_L3<T, VISC, D, LD>(phi, C, n, dxsqinv, b, c);
 }
 template <class T, int DM, int VISC, int D>
 __device__ __forceinline__ T face_diag(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {

@@ -1,0 +1,59 @@
+"""Run a fixed number of device-resident Stokes solves (profiling driver).
+
+    python -m lowmachmixtures_b200.profile_solve --n 128 --method mixed --solves 1
+
+Used under ncu to list every kernel launch of a solve, and to capture the
+hot kernels on the benchmark workload (3D n^3, contrast 100, inertial
+theta*alpha*dx^2 = 0.1, precon_type 2, visc_type -2).  --warm solves run
+first so that a capture can skip them with ncu's -s.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--method", default="mixed", choices=["mixed", "plain", "reference"])
+    ap.add_argument("--solves", type=int, default=1)
+    ap.add_argument("--warm", type=int, default=1)
+    a = ap.parse_args()
+
+    import numpy as np
+    import torch
+
+    from lowmachmixtures_b200 import abi, synth
+    from lowmachmixtures_b200.gmres import StokesSolver
+
+    prob = synth.config_3d_128(0, n=a.n)
+    kn = dict(precon_type=2, visc_type=-2)
+    if a.method == "mixed":
+        kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
+    elif a.method == "plain":
+        kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP64)
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
+    bu, bp = [dev(x) for x in prob.b_u], dev(prob.b_p)
+    al, be, bed, ga = [dev(x) for x in prob.alpha_fc], dev(prob.beta), [dev(x) for x in prob.beta_ed], dev(prob.gamma)
+    xu, xp = [torch.zeros_like(bu[0]) for _ in range(3)], torch.zeros_like(bp)
+    with StokesSolver(3, (a.n,) * 3, prob.dx, knobs=abi.make_knobs(**kn)) as s:
+        out = []
+        for i in range(a.warm + a.solves):
+            for t in xu:
+                t.zero_()
+            xp.zero_()
+            l0 = s.lib.lmm_kernel_launches()
+            _, _, st = s.solve_device(bu, bp, xu, xp, al, be, bed, ga, prob.theta_alpha)
+            out.append({"solve": i, "iters": st["total_iter"], "ms": st["solve_ms"],
+                        "launches": s.lib.lmm_kernel_launches() - l0,
+                        "rel_res": st["norm_resid_true"] / st["norm_b"]})
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

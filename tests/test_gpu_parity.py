@@ -48,7 +48,7 @@ def random_problem(dm, n, seed, visc, theta=7.0):
 
 def make_solver(p, **kn):
     from lowmachmixtures_b200.gmres import StokesSolver
-    k = abi.make_knobs(**kn)
+    k = abi.make_knobs(**kn)  # knobs the oracle does not know are the library's own
     s = StokesSolver(p.dm, p.n[: p.dm], p.dx, knobs=k)
     s.load_coeffs([dev(a) for a in p.alpha_fc], dev(p.beta), [dev(b) for b in p.beta_ed], dev(p.gamma), p.theta_alpha)
     return s
@@ -114,14 +114,20 @@ def test_residual_restrict_and_prolong_bit_exact(oracle, dm, n, visc):
     s.close()
 
 
-@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
+# tail: (tail_cells, tail_cluster): -1 = every level by per-level kernels;
+# otherwise the coarse levels run in one thread-block-cluster launch
+TAILS = [(-1, 0), (0, 1), (0, 8), (0, 16), (64, 4)]
+
+
+@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16), (3, 32)])
 @pytest.mark.parametrize("visc", [-1, -2, -3])
 @pytest.mark.parametrize("smoother", [1, 0])
-def test_vcycle_bit_exact(oracle, dm, n, visc, smoother):
+@pytest.mark.parametrize("tail", TAILS)
+def test_vcycle_bit_exact(oracle, dm, n, visc, smoother, tail):
     p, rng = random_problem(dm, n, 14, visc, theta=3.0)
     kn = dict(visc_type=visc, stag_mg_smoother=smoother, stag_mg_omega=1.0 if smoother else 0.7)
     k = oracle.default_knobs(**kn)
-    s = make_solver(p, **kn)
+    s = make_solver(p, **kn, tail_cells=tail[0], tail_cluster=tail[1])
     rhs = [rng.standard_normal(p.shape) for _ in range(dm)]
     ref = oracle.stag_mg_solver(p, k, rhs)
     phi = [dev(np.zeros(p.shape)) for _ in range(dm)]
@@ -170,11 +176,12 @@ PRECONS = [1, -1, 2, -2, 3, -3, 4, -4, 5, -5]
 @pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
 @pytest.mark.parametrize("pt", PRECONS)
 @pytest.mark.parametrize("theta", [0.0, 50.0])
-def test_apply_precon(oracle, dm, n, pt, theta):
+@pytest.mark.parametrize("tail_cells", [-1, 0])
+def test_apply_precon(oracle, dm, n, pt, theta, tail_cells):
     visc = -2 if pt % 2 else -3
     p, rng = random_problem(dm, n, 17, visc, theta=theta)
     k = oracle.default_knobs(visc_type=visc, precon_type=pt)
-    s = make_solver(p, visc_type=visc, precon_type=pt)
+    s = make_solver(p, visc_type=visc, precon_type=pt, tail_cells=tail_cells)
     bu = [rng.standard_normal(p.shape) for _ in range(dm)]
     bpp = rng.standard_normal(p.shape)
     ref_u, ref_p = oracle.apply_precon(p, k, bu, bpp)
