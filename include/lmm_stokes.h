@@ -103,10 +103,12 @@ typedef struct lmm_knobs {
     int    method;                 /* LMM_METHOD_* */
     int    precision;              /* LMM_PRECISION_* */
     int    learned_stage;          /* 0 off, 1 network stage before the V-cycle (FGMRES only) */
-    int    tail_cells;             /* multigrid levels with at most this many cells run in one
-                                      cluster launch; 0 = default (4096), -1 = never */
-    int    tail_cluster;           /* thread blocks in that cluster (1..16); 0 = default (8) */
-    int    reserved[6];
+    int    tail_cells;             /* coarse multigrid levels with at most this many cells run in
+                                      one single-block launch; 0 = default (4096), -1 = never */
+    int    tail_smem_kb;           /* shared-memory budget of that launch in KiB; 0 = 200 */
+    int    use_graphs;             /* replay each preconditioner application from a captured
+                                      CUDA graph: 0 = default (on), -1 = off */
+    int    reserved[5];
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -79,8 +79,9 @@ _KNOB_FIELDS = [
     ("precision", C.c_int),
     ("learned_stage", C.c_int),
     ("tail_cells", C.c_int),
-    ("tail_cluster", C.c_int),
-    ("reserved", C.c_int * 6),
+    ("tail_smem_kb", C.c_int),
+    ("use_graphs", C.c_int),
+    ("reserved", C.c_int * 5),
 ]
 
 
@@ -103,7 +104,7 @@ KNOB_DEFAULTS = dict(
     gmres_rel_tol=1e-9, gmres_abs_tol=0.0, gmres_verbose=1, gmres_max_outer=20,
     gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1,
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
-    tail_cells=0, tail_cluster=0,
+    tail_cells=0, tail_smem_kb=0, use_graphs=0,
 )
 
 

@@ -189,6 +189,66 @@ __device__ __forceinline__ void restrict_comp(int comp, const Dims& F, const Coe
         out[2][t] = restrict_face<T, DM, VISC, 2, LD>(F, C, rhs, phi, i, j, k, dxsqinv);
 }
 
+// r = (L phi - rhs) * -1 on every face of one level (stag_mg_solver.f90:406-415)
+template <class T, int DM, int VISC>
+__global__ void __launch_bounds__(kThreads) k_residual(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
+                                                       const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
+                                                       const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
+                                                       T* __restrict__ o2, T dxsqinv) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    {
+        T v = face_L<T, DM, VISC, 0>(phi, C, nb, dxsqinv, b, c) - ld(r0, t);
+        o0[t] = v * T(-1);
+    }
+    {
+        T v = face_L<T, DM, VISC, 1>(phi, C, nb, dxsqinv, b, c) - ld(r1, t);
+        o1[t] = v * T(-1);
+    }
+    if constexpr (DM == 3) {
+        T v = face_L<T, DM, VISC, 2>(phi, C, nb, dxsqinv, b, c) - ld(r2, t);
+        o2[t] = v * T(-1);
+    }
+}
+
+// 6-point (2D) / 12-point (3D) restriction of precomputed fine residuals,
+// same summation order as restrict_face
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restrict__ f0, const T* __restrict__ f1,
+                                                       const T* __restrict__ f2, Dims Dc, T* __restrict__ c0, T* __restrict__ c1,
+                                                       T* __restrict__ c2) {
+    const Pos q = pos3(Dc.nx, Dc.ny);
+    if (!q.ok) return;
+    const int t = q.i + Dc.nx * (q.j + Dc.ny * q.k);
+    const int I = 2 * q.i, J = 2 * q.j, K = 2 * q.k;
+    auto R = [&](const T* f, int i, int j, int k) {
+        i = wrapi(i, F.nx);
+        j = wrapi(j, F.ny);
+        k = (DM == 3) ? wrapi(k, F.nz) : 0;
+        return ld(f, i + F.nx * (j + F.ny * k));
+    };
+    if constexpr (DM == 2) {
+        c0[t] = T(0.25) * (R(f0, I, J, 0) + R(f0, I, J + 1, 0)) +
+                T(0.125) * (R(f0, I + 1, J, 0) + R(f0, I + 1, J + 1, 0) + R(f0, I - 1, J, 0) + R(f0, I - 1, J + 1, 0));
+        c1[t] = T(0.25) * (R(f1, I, J, 0) + R(f1, I + 1, J, 0)) +
+                T(0.125) * (R(f1, I, J + 1, 0) + R(f1, I + 1, J + 1, 0) + R(f1, I, J - 1, 0) + R(f1, I + 1, J - 1, 0));
+    } else {
+        c0[t] = T(0.125) * (R(f0, I, J, K) + R(f0, I, J + 1, K) + R(f0, I, J, K + 1) + R(f0, I, J + 1, K + 1)) +
+                T(0.0625) * (R(f0, I + 1, J, K) + R(f0, I + 1, J + 1, K) + R(f0, I + 1, J, K + 1) + R(f0, I + 1, J + 1, K + 1)) +
+                T(0.0625) * (R(f0, I - 1, J, K) + R(f0, I - 1, J + 1, K) + R(f0, I - 1, J, K + 1) + R(f0, I - 1, J + 1, K + 1));
+        c1[t] = T(0.125) * (R(f1, I, J, K) + R(f1, I + 1, J, K) + R(f1, I, J, K + 1) + R(f1, I + 1, J, K + 1)) +
+                T(0.0625) * (R(f1, I, J + 1, K) + R(f1, I + 1, J + 1, K) + R(f1, I, J + 1, K + 1) + R(f1, I + 1, J + 1, K + 1)) +
+                T(0.0625) * (R(f1, I, J - 1, K) + R(f1, I + 1, J - 1, K) + R(f1, I, J - 1, K + 1) + R(f1, I + 1, J - 1, K + 1));
+        c2[t] = T(0.125) * (R(f2, I, J, K) + R(f2, I + 1, J, K) + R(f2, I, J + 1, K) + R(f2, I + 1, J + 1, K)) +
+                T(0.0625) * (R(f2, I, J, K + 1) + R(f2, I + 1, J, K + 1) + R(f2, I, J + 1, K + 1) + R(f2, I + 1, J + 1, K + 1)) +
+                T(0.0625) * (R(f2, I, J, K - 1) + R(f2, I + 1, J, K - 1) + R(f2, I, J + 1, K - 1) + R(f2, I + 1, J + 1, K - 1));
+    }
+}
+
 template <class T, int DM, int VISC>
 __global__ void __launch_bounds__(kThreads) k_residual_restrict(Dims F, Coef<T> C, const T* __restrict__ r0,
                                                                 const T* __restrict__ r1, const T* __restrict__ r2,
@@ -499,22 +559,25 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
     const int n = D.nx * D.ny * D.nz;
     const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const T* AA[NC];
+    const T* BB[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-        const T* a = (c < DM) ? A[c] : A[3];
-        const T* b = (c < DM) ? B[c] : B[3];
-        if (!a) continue;
-        double v = 0.0;
-        for (int t = tid; t < n; t += stride) {
-            double x = (double)ld(a, t);
+        AA[c] = (c < DM) ? A[c] : A[3];
+        BB[c] = (c < DM) ? B[c] : B[3];
+    }
+    for (int t = tid; t < n; t += stride) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (!AA[c]) continue;
+            double x = (double)ld(AA[c], t);
             if (MODE == 2) {
-                v = fmax(v, fabs(x - (b ? (double)ld(b, t) : 0.0)));
+                acc[c] = fmax(acc[c], fabs(x - (BB[c] ? (double)ld(BB[c], t) : 0.0)));
             } else {
-                if (MODE == 0) x = x * (double)ld(b, t);
-                v += x;
+                if (MODE == 0) x = x * (double)ld(BB[c], t);
+                acc[c] += x;
             }
         }
-        acc[c] = v;
     }
     if (MODE != 2) {
         // seam planes: x faces i == 0 (ny*nz of them), y faces j == 0 (nx*nz),
@@ -566,17 +629,29 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // fixed-order final sum: thread c handles component c over all blocks
+    // final sum in a fixed order: thread t adds partials t, t + 256, ... of
+    // each component, then the same fixed warp/block tree as above
     __shared__ double fin[4];
-    if (threadIdx.x < NC) {
-        const int c = threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
         double v = 0.0;
-        for (unsigned bidx = 0; bidx < gridDim.x; ++bidx) {
+        for (unsigned bidx = threadIdx.x; bidx < gridDim.x; bidx += blockDim.x) {
             double q = ((volatile double*)partials)[bidx * NC + c];
             v = (MODE == 2) ? fmax(v, q) : v + q;
         }
-        fin[c] = v;
-        out[c] = v;
+        for (int o = 16; o > 0; o >>= 1) {
+            double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = (MODE == 2) ? fmax(v, u) : v + u;
+        }
+        __syncthreads();
+        if (lane == 0) sh[c][warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double r = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) r = (MODE == 2) ? fmax(r, sh[c][w]) : r + sh[c][w];
+            fin[c] = r;
+            out[c] = r;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -649,13 +724,20 @@ void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const 
 template <class T>
 void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
                               const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s) {
+    // residual on every fine face into F.tmp, then the pure restriction
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
-    const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz * F.D.dm);
+    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 2, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (k_residual<T, 2, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_residual_restrict<T, 3, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (k_residual<T, 3, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     }
+    count_launch();
+    const G3 gc = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
+    if (F.D.dm == 2)
+        k_restrict<T, 2><<<gc.grid, gc.block, 0, s>>>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
+    else
+        k_restrict<T, 3><<<gc.grid, gc.block, 0, s>>>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
 }
 
 template <class T>

@@ -60,12 +60,14 @@ template <class T>
 void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s);
 
 // The coarse end of a V-cycle (levels L[0..nl-1], L[0] already holding its
-// rhs) in one thread-block-cluster launch of csize blocks (tail.cuh).
+// rhs) in one single-block launch with every level in shared memory (tail.cuh).
 template <class T>
 cudaError_t launch_vcycle_tail(const LevelDev<T>* L, int nl, int visc, int nu1, int nu2, int nub, int smoother, double omega,
-                               int csize, cudaStream_t s);
+                               cudaStream_t s);
 template <class T>
-cudaError_t launch_ccmg_tail(const LevelDev<T>* L, int nl, int nu1, int nu2, int nub, int csize, cudaStream_t s);
+cudaError_t launch_ccmg_tail(const LevelDev<T>* L, int nl, int nu1, int nu2, int nub, cudaStream_t s);
+template <class T>
+size_t tail_smem_bytes(const LevelDev<T>* L, int nl, bool stag, bool jacobi);
 
 // ---- pressure multigrid (this library's cell-centred V-cycle) ----
 template <class T>

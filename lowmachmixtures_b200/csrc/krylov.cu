@@ -18,49 +18,55 @@ __device__ __forceinline__ void unflat3(const Dims& D, int t, int& i, int& j, in
 }  // namespace
 
 // b_u = stag_applyop(x_u) + grad(x_p);  b_p = -div(x_u)   (apply_matrix.f90:96-112)
-template <int DM, int VISC>
-__global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, const double* __restrict__ u0,
-                                                     const double* __restrict__ u1, const double* __restrict__ u2,
-                                                     const double* __restrict__ p, double* __restrict__ o0,
+template <int DM, int VISC, class TX>
+__global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, const TX* __restrict__ u0,
+                                                     const TX* __restrict__ u1, const TX* __restrict__ u2,
+                                                     const TX* __restrict__ p, double* __restrict__ o0,
                                                      double* __restrict__ o1, double* __restrict__ o2, double* __restrict__ op,
                                                      double dxsqinv, double dxinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nbr = make_nb(D, q.i, q.j, q.k);
     const int t = nbr.s;
-    const double* phi[3] = {u0, u1, u2};
+    const TX* phi[3] = {u0, u1, u2};
     const double b = ld(C.beta, 0), c = ld(C.gamma, 0);
-    const double pc = ld(p, t);
+    auto X = [](const TX* a, int i) { return (double)__ldg(a + i); };
+    const double pc = X(p, t);
     {
-        double L = face_L<double, DM, VISC, 0>(phi, C, nbr, dxsqinv, b, c);
-        double g = (pc - ld(p, t + nbr.om[0])) * dxinv;
+        double L = face_L<double, DM, VISC, 0, 0, TX>(phi, C, nbr, dxsqinv, b, c);
+        double g = (pc - X(p, t + nbr.om[0])) * dxinv;
         o0[t] = L + g;
     }
     {
-        double L = face_L<double, DM, VISC, 1>(phi, C, nbr, dxsqinv, b, c);
-        double g = (pc - ld(p, t + nbr.om[1])) * dxinv;
+        double L = face_L<double, DM, VISC, 1, 0, TX>(phi, C, nbr, dxsqinv, b, c);
+        double g = (pc - X(p, t + nbr.om[1])) * dxinv;
         o1[t] = L + g;
     }
-    double dv = (ld(u0, t + nbr.op[0]) - ld(u0, t)) * dxinv + (ld(u1, t + nbr.op[1]) - ld(u1, t)) * dxinv;
+    double dv = (X(u0, t + nbr.op[0]) - X(u0, t)) * dxinv + (X(u1, t + nbr.op[1]) - X(u1, t)) * dxinv;
     if constexpr (DM == 3) {
-        double L = face_L<double, DM, VISC, 2>(phi, C, nbr, dxsqinv, b, c);
-        double g = (pc - ld(p, t + nbr.om[2])) * dxinv;
+        double L = face_L<double, DM, VISC, 2, 0, TX>(phi, C, nbr, dxsqinv, b, c);
+        double g = (pc - X(p, t + nbr.om[2])) * dxinv;
         o2[t] = L + g;
-        dv = dv + (ld(u2, t + nbr.op[2]) - ld(u2, t)) * dxinv;
+        dv = dv + (X(u2, t + nbr.op[2]) - X(u2, t)) * dxinv;
     }
     op[t] = dv * -1.0;
 }
 
-void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s) {
+template <class TX>
+static void apply_matrix_impl(const LevelDev<double>& L0, int visc, const TX* xb, int64_t n, int dm, const SVec& b,
+                              cudaStream_t s) {
     const double dxsqinv = 1.0 / (L0.dx * L0.dx);
     const double dxinv = 1.0 / L0.dx;
     int bx = L0.D.nx < 64 ? L0.D.nx : 64;
     int by = 256 / bx;
     if (by > L0.D.ny) by = L0.D.ny;
     const dim3 blk(bx, by, 1), grd((L0.D.nx + bx - 1) / bx, (L0.D.ny + by - 1) / by, L0.D.nz);
-    const double* x2 = (x.dm == 3) ? x.c(2) : x.c(0);
+    const TX* x0 = xb;
+    const TX* x1 = xb + n;
+    const TX* x2 = (dm == 3) ? xb + 2 * n : xb;
+    const TX* xp = xb + (int64_t)dm * n;
     double* b2 = (b.dm == 3) ? b.c(2) : b.c(0);
-#define AM(DM_, V_) k_apply_matrix<DM_, V_><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x.c(0), x.c(1), x2, x.p(), b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
+#define AM(DM_, V_) k_apply_matrix<DM_, V_, TX><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
 #define AMV(DM_)                    \
     switch (visc) {                 \
     case -1: AM(DM_, -1); break;    \
@@ -70,13 +76,21 @@ void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, co
     case -3: AM(DM_, -3); break;    \
     case 3: AM(DM_, 3); break;      \
     }
-    if (x.dm == 2) {
+    if (dm == 2) {
         AMV(2)
     } else {
         AMV(3)
     }
 #undef AMV
 #undef AM
+}
+
+void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s) {
+    apply_matrix_impl<double>(L0, visc, x.base, x.n, x.dm, b, s);
+}
+void launch_apply_matrix_f32(const LevelDev<double>& L0, int visc, const float* x, int64_t n, int dm, const SVec& b,
+                             cudaStream_t s) {
+    apply_matrix_impl<float>(L0, visc, x, n, dm, b, s);
 }
 
 __global__ void k_neg_resid(double* __restrict__ out, const double* __restrict__ b, int64_t n) {

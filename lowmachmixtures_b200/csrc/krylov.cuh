@@ -30,6 +30,9 @@ struct SVec {
 };
 
 void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s);
+// the same operator applied to an FP32 Stokes vector (FGMRES Z storage), FP64 arithmetic
+void launch_apply_matrix_f32(const LevelDev<double>& L0, int visc, const float* x, int64_t n, int dm, const SVec& b,
+                             cudaStream_t s);
 // out = (out - b) * -1  (gmres.f90:186-194)
 void launch_neg_resid(double* out, const double* b, int64_t n, cudaStream_t s);
 // v = w / (*den)   (multifab_div_div_s_c)

@@ -21,7 +21,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/lmm_stokes.h"
@@ -118,6 +120,14 @@ struct lmm_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool coeffs_loaded = false;
     double theta_loaded = 0.0;
+    // captured preconditioner applications: (input, output, theta, precision)
+    struct Graph {
+        int seen = 0;
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+        int vcycles = 0, pvcycles = 0;
+    };
+    std::map<std::tuple<const void*, const void*, double, int>, Graph> graphs;
 
     template <class T>
     T* alloc(int64_t count) {
@@ -348,27 +358,27 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
     }
 }
 
-// first level handled by the cluster tail kernel (nl: no tail)
+// first level handled by the shared-memory tail kernel (nl: no tail): the
+// largest run of coarse levels with at most tail_cells cells each whose
+// phi/rhs fit the shared-memory budget
 template <class T>
-int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl) {
+int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool stag) {
     const int cells = h->knobs.tail_cells == 0 ? 4096 : h->knobs.tail_cells;
     if (cells < 0) return nl;
+    const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
+    const bool jacobi = stag && h->knobs.stag_mg_smoother == 0;
     int lc = nl;
-    while (lc > 0 && L[lc - 1].n <= cells) --lc;
-    if (nl - lc > 12) lc = nl - 12;  // kMaxTail levels at most
+    while (lc > 0 && nl - (lc - 1) <= 12 && L[lc - 1].n <= cells &&
+           tail_smem_bytes<T>(&L[lc - 1], nl - (lc - 1), stag, jacobi) <= budget)
+        --lc;
     return lc;
-}
-
-int tail_cluster(lmm_handle* h) {
-    int c = h->knobs.tail_cluster == 0 ? 8 : h->knobs.tail_cluster;
-    return std::max(1, std::min(16, c));
 }
 
 template <class T>
 void vcycle(lmm_handle* h, std::vector<LevelDev<T>>& L) {
     const lmm_knobs& K = h->knobs;
     const int nl = h->nlev;
-    const int lc = tail_start<T>(h, L, nl);
+    const int lc = tail_start<T>(h, L, nl, true);
     // coarse-level initial guesses are zero; the tail zeroes the levels below its first
     for (int l = 1; l <= std::min(lc, nl - 1); ++l)
         for (int d = 0; d < h->dm; ++d) LMM_CK(cudaMemsetAsync(L[l].phi[d], 0, L[l].n * sizeof(T), h->stream));
@@ -379,8 +389,7 @@ void vcycle(lmm_handle* h, std::vector<LevelDev<T>>& L) {
     }
     if (lc < nl) {
         LMM_CK(launch_vcycle_tail<T>(&L[lc], nl - lc, K.visc_type, K.stag_mg_nsmooths_down, K.stag_mg_nsmooths_up,
-                                     K.stag_mg_nsmooths_bottom, K.stag_mg_smoother, K.stag_mg_omega, tail_cluster(h),
-                                     h->stream));
+                                     K.stag_mg_nsmooths_bottom, K.stag_mg_smoother, K.stag_mg_omega, h->stream));
         check_launch();
     } else {
         smooth<T>(h, L[nl - 1], K.stag_mg_nsmooths_bottom);
@@ -473,7 +482,7 @@ void macproject(lmm_handle* h) {
     auto& L = levels<T>(h);
     const lmm_knobs& K = h->knobs;
     const int nl = h->nlev_p;
-    const int lc = tail_start<T>(h, L, nl);
+    const int lc = tail_start<T>(h, L, nl, false);
     LMM_CK(cudaMemsetAsync(L[0].pphi, 0, L[0].n * sizeof(T), h->stream));
     for (int vc = 0; vc < K.mg_max_vcycles; ++vc) {
         for (int l = 1; l <= std::min(lc, nl - 1); ++l) LMM_CK(cudaMemsetAsync(L[l].pphi, 0, L[l].n * sizeof(T), h->stream));
@@ -484,7 +493,7 @@ void macproject(lmm_handle* h) {
         }
         if (lc < nl) {
             LMM_CK(launch_ccmg_tail<T>(&L[lc], nl - lc, K.mg_nsmooths_down, K.mg_nsmooths_up, K.mg_nsmooths_bottom,
-                                       tail_cluster(h), h->stream));
+                                       h->stream));
             check_launch();
         } else {
             cc_smooth<T>(h, L[nl - 1], K.mg_nsmooths_bottom);
@@ -654,22 +663,72 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
     check_launch();
 }
 
+// Run `body` (a fixed sequence of launches on h->stream) through a CUDA graph
+// keyed by (in, out, theta, precision): the first call runs eagerly (kernel
+// attributes get set), the second captures and instantiates, later calls
+// replay.  Launch and V-cycle counters advance as if launched eagerly.
+template <class F>
+void run_graphed(lmm_handle* h, const void* in, const void* out, int prec, F body) {
+    // stag_mg_max_vcycles > 1 reads residual norms on the host between cycles
+    if (h->knobs.use_graphs < 0 || h->knobs.stag_mg_max_vcycles > 1) {
+        body();
+        return;
+    }
+    auto key = std::make_tuple(in, out, h->theta_loaded, prec);
+    lmm_handle::Graph& g = h->graphs[key];
+    if (g.exec) {
+        LMM_CK(cudaGraphLaunch(g.exec, h->stream));
+        for (int64_t q = 0; q < g.launches; ++q) count_launch();
+        h->vcycles += g.vcycles;
+        h->pvcycles += g.pvcycles;
+        return;
+    }
+    if (g.seen++ == 0) {
+        body();
+        return;
+    }
+    const int64_t l0 = launches_total();
+    const int v0 = h->vcycles, p0 = h->pvcycles;
+    cudaGraph_t graph = nullptr;
+    LMM_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        body();
+    } catch (...) {
+        cudaStreamEndCapture(h->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    LMM_CK(cudaStreamEndCapture(h->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+        throw LmmError(LMM_ERR_CUDA);
+    }
+    g.launches = launches_total() - l0;
+    g.vcycles = h->vcycles - v0;
+    g.pvcycles = h->pvcycles - p0;
+    LMM_CK(cudaGraphLaunch(g.exec, h->stream));
+}
+
 // FP64 Stokes vector in, FP64 Stokes vector out
 void precon64(lmm_handle* h, const SVec& bin, const SVec& xout) {
     const double* bu[3] = {bin.c(0), bin.c(1), h->dm == 3 ? bin.c(2) : nullptr};
     double* xu[3] = {xout.c(0), xout.c(1), h->dm == 3 ? xout.c(2) : nullptr};
-    apply_precon<double>(h, bu, bin.p(), xu, xout.p());
+    run_graphed(h, bin.base, xout.base, 0, [&]() { apply_precon<double>(h, bu, bin.p(), xu, xout.p()); });
 }
 
 // FP64 Stokes vector in, FP32 Stokes vector out (Z storage)
 void precon32(lmm_handle* h, const SVec& bin, float* zout) {
     const int dm = h->dm;
     const int64_t n = h->n;
-    launch_convert<double, float>(bin.base, h->pin32, (int64_t)(dm + 1) * n, h->stream);
-    check_launch();
-    const float* bu[3] = {h->pin32, h->pin32 + n, dm == 3 ? h->pin32 + 2 * n : nullptr};
-    float* xu[3] = {zout, zout + n, dm == 3 ? zout + 2 * n : nullptr};
-    apply_precon<float>(h, bu, h->pin32 + (int64_t)dm * n, xu, zout + (int64_t)dm * n);
+    run_graphed(h, bin.base, zout, 1, [&]() {
+        launch_convert<double, float>(bin.base, h->pin32, (int64_t)(dm + 1) * n, h->stream);
+        check_launch();
+        const float* bu[3] = {h->pin32, h->pin32 + n, dm == 3 ? h->pin32 + 2 * n : nullptr};
+        float* xu[3] = {zout, zout + n, dm == 3 ? zout + 2 * n : nullptr};
+        apply_precon<float>(h, bu, h->pin32 + (int64_t)dm * n, xu, zout + (int64_t)dm * n);
+    });
 }
 
 // ------------------------------------------------------------ Givens (host, gmres.f90:517-605)
@@ -908,9 +967,7 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             i_copy = i;
             if (fp32) {
                 precon32(h, h->V[i - 1], h->Z32[i - 1]);
-                launch_convert<float, double>(h->Z32[i - 1], h->zt.base, len, h->stream);
-                check_launch();
-                launch_apply_matrix(h->L64[0], K.visc_type, h->zt, h->w, h->stream);
+                launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[i - 1], h->n, h->dm, h->w, h->stream);
             } else {
                 precon64(h, h->V[i - 1], h->Z64[i - 1]);
                 launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[i - 1], h->w, h->stream);
@@ -1139,6 +1196,8 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
 int lmm_stokes_destroy(lmm_handle* h) {
     if (!h) return LMM_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& kv : h->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (h->arena) cudaFree(h->arena);
     if (h->hscal) cudaFreeHost(h->hscal);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1558,8 +1617,8 @@ std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 int reduce_blocks(int64_t n) {
-    int64_t b = (n + 255) / 256;
-    if (b > 1184) b = 1184;  // 8 blocks per SM on 148 SMs
+    int64_t b = (n + 2047) / 2048;  // at least 8 elements per thread
+    if (b > 592) b = 592;           // 4 blocks per SM on 148 SMs
     if (b < 1) b = 1;
     return (int)b;
 }

@@ -102,27 +102,27 @@ template <> struct Perm3<1> { static constexpr int t1 = 0, t2 = 2, e1 = 0, e2 = 
 template <> struct Perm3<2> { static constexpr int t1 = 0, t2 = 1, e1 = 1, e2 = 2; };
 
 // ------------------------------------------------------------------ 3D
-template <class T, int VISC, int D, int LD = 0>
-__device__ __forceinline__ T face_L3(const T* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
+template <class T, int VISC, int D, int LD = 0, class TP = T>
+__device__ __forceinline__ T face_L3(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
-    const T* p = phi[D];
+    const TP* p = phi[D];
     const int s = n.s;
-    const T p0 = ldp<LD>(p, s);
+    const T p0 = (T)ldp<LD>(p, s);
     const T a = ld(C.alpha[D], s);
     if (VISC == 1) {
-        T nbs = ldp<LD>(p, s + n.op[0]) + ldp<LD>(p, s + n.om[0]) + ldp<LD>(p, s + n.op[1]) + ldp<LD>(p, s + n.om[1]) + ldp<LD>(p, s + n.op[2]) +
-                ldp<LD>(p, s + n.om[2]);
+        T nbs = (T)ldp<LD>(p, s + n.op[0]) + (T)ldp<LD>(p, s + n.om[0]) + (T)ldp<LD>(p, s + n.op[1]) + (T)ldp<LD>(p, s + n.om[1]) + (T)ldp<LD>(p, s + n.op[2]) +
+                (T)ldp<LD>(p, s + n.om[2]);
         return p0 * (a + T(6) * b * dxsqinv) - nbs * b * dxsqinv;
     }
-    const T* q1 = phi[t1];
-    const T* q2 = phi[t2];
-    const T ppd = ldp<LD>(p, s + n.op[D]), pmd = ldp<LD>(p, s + n.om[D]);
-    const T pp1 = ldp<LD>(p, s + n.op[t1]), pm1 = ldp<LD>(p, s + n.om[t1]);
-    const T pp2 = ldp<LD>(p, s + n.op[t2]), pm2 = ldp<LD>(p, s + n.om[t2]);
+    const TP* q1 = phi[t1];
+    const TP* q2 = phi[t2];
+    const T ppd = (T)ldp<LD>(p, s + n.op[D]), pmd = (T)ldp<LD>(p, s + n.om[D]);
+    const T pp1 = (T)ldp<LD>(p, s + n.op[t1]), pm1 = (T)ldp<LD>(p, s + n.om[t1]);
+    const T pp2 = (T)ldp<LD>(p, s + n.op[t2]), pm2 = (T)ldp<LD>(p, s + n.om[t2]);
     // cross terms q(i,+t) , q(i) , q(i-d,+t) , q(i-d)
-    const T c10 = ldp<LD>(q1, s + n.op[t1]), c11 = ldp<LD>(q1, s), c12 = ldp<LD>(q1, s + n.om[D] + n.op[t1]), c13 = ldp<LD>(q1, s + n.om[D]);
-    const T c20 = ldp<LD>(q2, s + n.op[t2]), c21 = ldp<LD>(q2, s), c22 = ldp<LD>(q2, s + n.om[D] + n.op[t2]), c23 = ldp<LD>(q2, s + n.om[D]);
+    const T c10 = (T)ldp<LD>(q1, s + n.op[t1]), c11 = (T)ldp<LD>(q1, s), c12 = (T)ldp<LD>(q1, s + n.om[D] + n.op[t1]), c13 = (T)ldp<LD>(q1, s + n.om[D]);
+    const T c20 = (T)ldp<LD>(q2, s + n.op[t2]), c21 = (T)ldp<LD>(q2, s), c22 = (T)ldp<LD>(q2, s + n.om[D] + n.op[t2]), c23 = (T)ldp<LD>(q2, s + n.om[D]);
     if (VISC == 2) {
         return p0 * (a + T(8) * b * dxsqinv) -
                (T(2) * ppd + T(2) * pmd + pp1 + pm1 + pp2 + pm2 + c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * b * dxsqinv;
@@ -176,22 +176,22 @@ __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv
 }
 
 // ------------------------------------------------------------------ 2D
-template <class T, int VISC, int D, int LD = 0>
-__device__ __forceinline__ T face_L2(const T* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
+template <class T, int VISC, int D, int LD = 0, class TP = T>
+__device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t = 1 - D;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
-    const T* p = phi[D];
-    const T* q = phi[t];
+    const TP* p = phi[D];
+    const TP* q = phi[t];
     const int s = n.s;
-    const T p0 = ldp<LD>(p, s);
+    const T p0 = (T)ldp<LD>(p, s);
     const T a = ld(C.alpha[D], s);
-    const T ppd = ldp<LD>(p, s + n.op[D]), pmd = ldp<LD>(p, s + n.om[D]);
-    const T ppt = ldp<LD>(p, s + n.op[t]), pmt = ldp<LD>(p, s + n.om[t]);
+    const T ppd = (T)ldp<LD>(p, s + n.op[D]), pmd = (T)ldp<LD>(p, s + n.om[D]);
+    const T ppt = (T)ldp<LD>(p, s + n.op[t]), pmt = (T)ldp<LD>(p, s + n.om[t]);
     if (VISC == 1) {
         // x: i+1, i-1, j+1, j-1 ; y: j+1, j-1, i+1, i-1  (own direction first)
         return p0 * (a + T(4) * b * dxsqinv) - (ppd + pmd + ppt + pmt) * b * dxsqinv;
     }
-    const T c0 = ldp<LD>(q, s + n.op[t]), c1 = ldp<LD>(q, s), c2 = ldp<LD>(q, s + n.om[D] + n.op[t]), c3 = ldp<LD>(q, s + n.om[D]);
+    const T c0 = (T)ldp<LD>(q, s + n.op[t]), c1 = (T)ldp<LD>(q, s), c2 = (T)ldp<LD>(q, s + n.om[D] + n.op[t]), c3 = (T)ldp<LD>(q, s + n.om[D]);
     if (VISC == 2) {
         return p0 * (a + T(6) * b * dxsqinv) - (T(2) * ppd + T(2) * pmd + ppt + pmt + c0 - c1 - c2 + c3) * b * dxsqinv;
     }
@@ -231,12 +231,12 @@ __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv
     return a + (fourthirds * be + g + fourthirds * bm + gm + E + Ep) * dxsqinv;
 }
 
-template <class T, int DM, int VISC, int D, int LD = 0>
-__device__ __forceinline__ T face_L(const T* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
+template <class T, int DM, int VISC, int D, int LD = 0, class TP = T>
+__device__ __forceinline__ T face_L(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     if constexpr (DM == 2)
-        return face_L2<T, VISC, D, LD>(phi, C, n, dxsqinv, b, c);
+        return face_L2<T, VISC, D, LD, TP>(phi, C, n, dxsqinv, b, c);
     else
-        return face_L3<T, VISC, D, LD>(phi, C, n, dxsqinv, b, c);
+        return face_L3<T, VISC, D, LD, TP>(phi, C, n, dxsqinv, b, c);
 }
 template <class T, int DM, int VISC, int D>
 __device__ __forceinline__ T face_diag(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {

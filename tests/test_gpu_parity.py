@@ -114,9 +114,9 @@ def test_residual_restrict_and_prolong_bit_exact(oracle, dm, n, visc):
     s.close()
 
 
-# tail: (tail_cells, tail_cluster): -1 = every level by per-level kernels;
-# otherwise the coarse levels run in one thread-block-cluster launch
-TAILS = [(-1, 0), (0, 1), (0, 8), (0, 16), (64, 4)]
+# tail: (tail_cells, tail_smem_kb): -1 = every level by per-level kernels;
+# otherwise the coarse levels run in one single-block shared-memory launch
+TAILS = [(-1, 0), (0, 0), (64, 0), (0, 24)]
 
 
 @pytest.mark.parametrize("dm,n", [(2, 32), (3, 16), (3, 32)])
@@ -127,7 +127,7 @@ def test_vcycle_bit_exact(oracle, dm, n, visc, smoother, tail):
     p, rng = random_problem(dm, n, 14, visc, theta=3.0)
     kn = dict(visc_type=visc, stag_mg_smoother=smoother, stag_mg_omega=1.0 if smoother else 0.7)
     k = oracle.default_knobs(**kn)
-    s = make_solver(p, **kn, tail_cells=tail[0], tail_cluster=tail[1])
+    s = make_solver(p, **kn, tail_cells=tail[0], tail_smem_kb=tail[1])
     rhs = [rng.standard_normal(p.shape) for _ in range(dm)]
     ref = oracle.stag_mg_solver(p, k, rhs)
     phi = [dev(np.zeros(p.shape)) for _ in range(dm)]
@@ -333,3 +333,23 @@ def test_zero_rhs_returns_zero_and_nan_is_an_error():
         with pytest.raises(LmmError) as ei:
             s.solve(bad, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma, 5.0)
         assert ei.value.code == abi.LMM_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("method,precision", [(0, 0), (1, 0), (1, 1)])
+def test_graphs_and_tail_are_bitwise_neutral(method, precision):
+    """Captured CUDA graphs and the single-block coarse tail reorder nothing:
+    repeated solves with them on or off give bit-identical solutions."""
+    from lowmachmixtures_b200.gmres import StokesSolver
+    prob = synth.config_3d_128(3, n=32)
+    outs = []
+    for extra in (dict(use_graphs=-1, tail_cells=-1), dict(), dict(use_graphs=-1)):
+        kn = abi.make_knobs(precon_type=2, visc_type=-2, method=method, precision=precision, **extra)
+        with StokesSolver(3, (32, 32, 32), prob.dx, knobs=kn) as s:
+            for _ in range(3):
+                xu, xp = prob.zeros_like_solution()
+                s.solve(prob.b_u, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma, prob.theta_alpha)
+                outs.append((xu, xp))
+    for xu, xp in outs[1:]:
+        for c in range(3):
+            np.testing.assert_array_equal(xu[c], outs[0][0][c])
+        np.testing.assert_array_equal(xp, outs[0][1])
