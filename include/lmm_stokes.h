@@ -108,7 +108,11 @@ typedef struct lmm_knobs {
     int    tail_smem_kb;           /* shared-memory budget of that launch in KiB; 0 = 200 */
     int    use_graphs;             /* replay each preconditioner application from a captured
                                       CUDA graph: 0 = default (on), -1 = off */
-    int    reserved[5];
+    int    smoother_fusion;        /* Gauss-Seidel on 3D levels: 0 = one launch per colour (default),
+                                      1 = both colours of a component in one out-of-place launch
+                                      where the level allows it, k > 1 = the same with k planes
+                                      per block */
+    int    reserved[4];
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.
@@ -238,7 +242,8 @@ int64_t lmm_kernel_launches(void);
 /* Average device time (CUDA events on the handle's stream) of `reps`
  * repetitions of one hot operation on the finest level, using the
  * coefficients and level-0 buffers of the last solve:
- *   0 one Gauss-Seidel smooth, all 2*dm colours, FP64
+ *   0 one Gauss-Seidel smooth, all 2*dm colours, FP64 (timed as pairs of
+ *     smooths and halved)
  *   1 the same in FP32
  *   2 stag_applyop (all faces), FP64
  *   3 apply_matrix, FP64

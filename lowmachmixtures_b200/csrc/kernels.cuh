@@ -90,6 +90,80 @@ __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const
     p[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
 }
 
+// --------------------------------------------------------------- GS red/black pair (3D)
+// Both colours of one component in one launch (colours 2*COMP+1 and
+// 2*COMP+2 of the sweep above, same arithmetic).  The block owns a
+// TX x TY x TZ tile.  Phase 1 updates the faces of parity par0 ("red") on the
+// tile, on the one-face rings around each of its planes and on the planes
+// just below and above it, into shared memory; phase 2, after one barrier,
+// updates the other parity ("black"), whose six same-component neighbours are
+// all red and all in shared memory.  Red values depend only on the input
+// buffers, so a face computed by two blocks has the same bits in both.
+//
+// The update is out of place: every input (p0, p1, p2) is read-only and the
+// new values of component COMP (both parities) go to `out`, so one pair
+// reads each array once instead of once per colour.
+template <class T, int VISC, int COMP>
+__global__ void __launch_bounds__(kThreads) k_gs_pair(Dims D, Coef<T> C, const T* __restrict__ rhs, const T* __restrict__ p0,
+                                                      const T* __restrict__ p1, const T* __restrict__ p2, T* __restrict__ out,
+                                                      int TX, int TY, int TZ, int par0, T omega, T dxsqinv) {
+    extern __shared__ __align__(16) unsigned char pair_smem[];
+    T* red = reinterpret_cast<T*>(pair_smem);   // (TZ+2) planes of (TY+2) x (TX+2)
+    const int W = TX + 2, PL = (TY + 2) * W;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * blockDim.x + tx;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * TZ;
+    const T* phi[3] = {p0, p1, p2};
+    const T* pc = phi[COMP];
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    const int j = j0 + ty;
+    // phase 1: red faces
+    for (int kk = 0; kk < TZ + 2; ++kk) {
+        const int k = wrapi(k0 - 1 + kk, D.nz);
+        T* slot = red + kk * PL;
+        {
+            const int x = 2 * tx + ((par0 + j + k) & 1);
+            const Nb nb = make_nb(D, i0 + x, j, k);
+            const T Lp = face_L3<T, VISC, COMP>(phi, C, nb, dxsqinv, b, c);
+            const T fac = face_diag3<T, VISC, COMP>(C, nb, dxsqinv, b, c);
+            const T v = ld(pc, nb.s) + omega * (ld(rhs, nb.s) - Lp) / fac;
+            slot[(ty + 1) * W + x + 1] = v;
+            if (kk >= 1 && kk <= TZ) out[nb.s] = v;
+        }
+        if (kk >= 1 && kk <= TZ && tid < TX + TY) {   // rings y = -1, y = TY, x = -1, x = TX
+            int x, y;
+            if (tid < TX) {
+                const bool lo = tid < TX / 2;
+                y = lo ? -1 : TY;
+                x = 2 * (lo ? tid : tid - TX / 2) + ((par0 + j0 + y + k) & 1);
+            } else {
+                const int r = tid - TX;
+                const bool lo = r < TY / 2;
+                x = lo ? -1 : TX;
+                y = 2 * (lo ? r : r - TY / 2) + ((par0 + i0 + x + j0 + k) & 1);
+            }
+            const Nb nb = make_nb(D, wrapi(i0 + x, D.nx), wrapi(j0 + y, D.ny), k);
+            const T Lp = face_L3<T, VISC, COMP>(phi, C, nb, dxsqinv, b, c);
+            const T fac = face_diag3<T, VISC, COMP>(C, nb, dxsqinv, b, c);
+            slot[(y + 1) * W + x + 1] = ld(pc, nb.s) + omega * (ld(rhs, nb.s) - Lp) / fac;
+        }
+    }
+    __syncthreads();
+    // phase 2: black faces of the TZ planes
+    for (int kk = 1; kk <= TZ; ++kk) {
+        const int k = wrapi(k0 - 1 + kk, D.nz);
+        const int x = 2 * tx + ((par0 + 1 + j + k) & 1);
+        const T* sc = red + kk * PL;
+        const int o = (ty + 1) * W + x + 1;
+        const Nb nb = make_nb(D, i0 + x, j, k);
+        const T nbv[6] = {sc[o + 1], sc[o - 1], sc[o + W], sc[o - W], sc[o + PL], sc[o - PL]};
+        const T cur = ld(pc, nb.s);
+        const T Lp = face_L3_own<T, VISC, COMP>(cur, nbv, phi, C, nb, dxsqinv, b, c);
+        const T fac = face_diag3<T, VISC, COMP>(C, nb, dxsqinv, b, c);
+        out[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
+    }
+}
+
 // --------------------------------------------------------------- Jacobi
 template <class T, int DM, int VISC>
 __global__ void __launch_bounds__(kThreads) k_jacobi(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
@@ -708,6 +782,60 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
 #undef GS
 }
 
+// tile of the fused pair on one level (ok == false: use the per-colour
+// kernels); tz_req > 1 forces the planes per block
+struct PairGeom {
+    bool ok = false;
+    int TX = 0, TY = 0, TZ = 0;
+};
+static inline PairGeom pair_geom(const Dims& D, int tz_req) {
+    PairGeom g;
+    if (D.dm != 3) return g;
+    if ((D.nx & 1) || (D.ny & 1) || (D.nz & 1) || D.nx < 8 || D.ny < 4 || D.nz < 2) return g;
+    g.TX = D.nx < 64 ? D.nx : 64;
+    if (D.nx % g.TX) return g;
+    auto blocks = [&](int ty, int tz) { return (int64_t)(D.nx / g.TX) * (D.ny / ty) * (D.nz / tz); };
+    g.TY = (D.ny % 8 == 0 && D.nz % 8 == 0 && blocks(8, 8) >= 444) ? 8 : 4;
+    if (D.ny % g.TY) return g;
+    if (tz_req > 1) {
+        if (D.nz % tz_req) return g;
+        g.TZ = tz_req;
+    } else {
+        g.TZ = (D.nz % 8 == 0 && blocks(g.TY, 8) >= 444) ? 8 : (D.nz % 4 == 0 ? 4 : 2);
+    }
+    g.ok = (g.TX / 2) * g.TY >= g.TX + g.TY;
+    return g;
+}
+
+template <class T>
+bool gs_pair_supported(const LevelDev<T>& L, int tz) {
+    return pair_geom(L.D, tz).ok;
+}
+
+template <class T>
+void launch_gs_pair(const LevelDev<T>& L, int visc, int comp, const T* const rhs[3], const T* const cur[3], T* out, double omega,
+                    int tz, cudaStream_t s) {
+    const PairGeom pg = pair_geom(L.D, tz);
+    const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    const T om = (T)omega;
+    const dim3 grid(L.D.nx / pg.TX, L.D.ny / pg.TY, L.D.nz / pg.TZ), block(pg.TX / 2, pg.TY, 1);
+    const size_t smem = (size_t)(pg.TZ + 2) * (pg.TY + 2) * (pg.TX + 2) * sizeof(T);
+#define GSP(COMP_)                                                                                                       \
+    {                                                                                                                    \
+        static bool attr_set = false;                                                                                    \
+        if (!attr_set) {                                                                                                 \
+            cudaFuncSetAttribute(k_gs_pair<T, V, COMP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);      \
+            attr_set = true;                                                                                             \
+        }                                                                                                                \
+        k_gs_pair<T, V, COMP_><<<grid, block, smem, s>>>(L.D, L.coef(), rhs[COMP_], cur[0], cur[1], cur[2], out, pg.TX, \
+                                                          pg.TY, pg.TZ, 0, om, dxsqinv);                                 \
+    }
+    if (comp == 0) { LMM_VISC_DISPATCH(visc, GSP(0)) }
+    else if (comp == 1) { LMM_VISC_DISPATCH(visc, GSP(1)) }
+    else { LMM_VISC_DISPATCH(visc, GSP(2)) }
+#undef GSP
+}
+
 template <class T>
 void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const pin[3], T* const pout[3],
                    double omega, cudaStream_t s) {
@@ -864,6 +992,9 @@ void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const 
     template void launch_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t);     \
     template void launch_jacobi<T>(const LevelDev<T>&, int, const T* const[3], const T* const[3], T* const[3], double,         \
                                    cudaStream_t);                                                                              \
+    template bool gs_pair_supported<T>(const LevelDev<T>&, int);                                                               \
+    template void launch_gs_pair<T>(const LevelDev<T>&, int, int, const T* const[3], const T* const[3], T*, double, int,        \
+                                    cudaStream_t);                                                                             \
     template void launch_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, int, const T* const[3],                  \
                                               const T* const[3], T* const[3], cudaStream_t);                                   \
     template void launch_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, const T* const[3], T* const[3], cudaStream_t); \

@@ -47,6 +47,15 @@ void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* co
 template <class T>
 void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega,
                       cudaStream_t s);
+// Both Gauss-Seidel colours of component comp in one launch, out of place:
+// cur[] are read, the new values of component comp go to out (3D levels with
+// even sizes; gs_pair_supported says whether the level qualifies).  kc > 0
+// forces the k-chunk per block, 0 picks it from the level size.
+template <class T>
+bool gs_pair_supported(const LevelDev<T>& L, int kc);
+template <class T>
+void launch_gs_pair(const LevelDev<T>& L, int visc, int comp, const T* const rhs[3], const T* const cur[3], T* out, double omega,
+                    int kc, cudaStream_t s);
 template <class T>
 void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const phi_in[3], T* const phi_out[3],
                    double omega, cudaStream_t s);

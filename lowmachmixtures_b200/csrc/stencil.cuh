@@ -102,24 +102,26 @@ template <> struct Perm3<1> { static constexpr int t1 = 0, t2 = 2, e1 = 0, e2 = 
 template <> struct Perm3<2> { static constexpr int t1 = 0, t2 = 1, e1 = 1, e2 = 2; };
 
 // ------------------------------------------------------------------ 3D
+// The face value with the own component's centre p0 and its six neighbours
+// nb = {+x, -x, +y, -y, +z, -z} supplied by the caller (global memory for the
+// plain kernels, shared memory for the fused red/black pair); the other two
+// components and the coefficients are read through phi / C.
 template <class T, int VISC, int D, int LD = 0, class TP = T>
-__device__ __forceinline__ T face_L3(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
+__device__ __forceinline__ T face_L3_own(const T p0, const T (&nb)[6], const TP* const phi[3], const Coef<T>& C, const Nb& n,
+                                         T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
-    const TP* p = phi[D];
     const int s = n.s;
-    const T p0 = (T)ldp<LD>(p, s);
     const T a = ld(C.alpha[D], s);
     if (VISC == 1) {
-        T nbs = (T)ldp<LD>(p, s + n.op[0]) + (T)ldp<LD>(p, s + n.om[0]) + (T)ldp<LD>(p, s + n.op[1]) + (T)ldp<LD>(p, s + n.om[1]) + (T)ldp<LD>(p, s + n.op[2]) +
-                (T)ldp<LD>(p, s + n.om[2]);
+        T nbs = nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5];
         return p0 * (a + T(6) * b * dxsqinv) - nbs * b * dxsqinv;
     }
     const TP* q1 = phi[t1];
     const TP* q2 = phi[t2];
-    const T ppd = (T)ldp<LD>(p, s + n.op[D]), pmd = (T)ldp<LD>(p, s + n.om[D]);
-    const T pp1 = (T)ldp<LD>(p, s + n.op[t1]), pm1 = (T)ldp<LD>(p, s + n.om[t1]);
-    const T pp2 = (T)ldp<LD>(p, s + n.op[t2]), pm2 = (T)ldp<LD>(p, s + n.om[t2]);
+    const T ppd = nb[2 * D], pmd = nb[2 * D + 1];
+    const T pp1 = nb[2 * t1], pm1 = nb[2 * t1 + 1];
+    const T pp2 = nb[2 * t2], pm2 = nb[2 * t2 + 1];
     // cross terms q(i,+t) , q(i) , q(i-d,+t) , q(i-d)
     const T c10 = (T)ldp<LD>(q1, s + n.op[t1]), c11 = (T)ldp<LD>(q1, s), c12 = (T)ldp<LD>(q1, s + n.om[D] + n.op[t1]), c13 = (T)ldp<LD>(q1, s + n.om[D]);
     const T c20 = (T)ldp<LD>(q2, s + n.op[t2]), c21 = (T)ldp<LD>(q2, s), c22 = (T)ldp<LD>(q2, s + n.om[D] + n.op[t2]), c23 = (T)ldp<LD>(q2, s + n.om[D]);
@@ -155,6 +157,16 @@ __device__ __forceinline__ T face_L3(const TP* const phi[3], const Coef<T>& C, c
             c10 * (E1p - twothirds * be + g) - c11 * (E1 - twothirds * be + g) - c12 * (E1p - twothirds * bm + gm) +
             c13 * (E1 - twothirds * bm + gm) + c20 * (E2p - twothirds * be + g) - c21 * (E2 - twothirds * be + g) -
             c22 * (E2p - twothirds * bm + gm) + c23 * (E2 - twothirds * bm + gm)) * dxsqinv;
+}
+
+template <class T, int VISC, int D, int LD = 0, class TP = T>
+__device__ __forceinline__ T face_L3(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
+    const TP* p = phi[D];
+    const int s = n.s;
+    const T p0 = (T)ldp<LD>(p, s);
+    const T nb[6] = {(T)ldp<LD>(p, s + n.op[0]), (T)ldp<LD>(p, s + n.om[0]), (T)ldp<LD>(p, s + n.op[1]),
+                     (T)ldp<LD>(p, s + n.om[1]), (T)ldp<LD>(p, s + n.op[2]), (T)ldp<LD>(p, s + n.om[2])};
+    return face_L3_own<T, VISC, D, LD, TP>(p0, nb, phi, C, n, dxsqinv, b, c);
 }
 
 template <class T, int VISC, int D>

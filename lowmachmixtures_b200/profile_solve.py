@@ -23,6 +23,8 @@ def main():
     ap.add_argument("--method", default="mixed", choices=["mixed", "plain", "reference"])
     ap.add_argument("--solves", type=int, default=1)
     ap.add_argument("--warm", type=int, default=1)
+    ap.add_argument("--knob", action="append", default=[], metavar="NAME=INT",
+                    help="extra lmm_knobs integer field (repeatable), e.g. --knob tail_cells=512")
     a = ap.parse_args()
 
     import numpy as np
@@ -37,6 +39,9 @@ def main():
         kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
     elif a.method == "plain":
         kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP64)
+    for kv in a.knob:
+        name, val = kv.split("=")
+        kn[name] = int(val)
     dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
     bu, bp = [dev(x) for x in prob.b_u], dev(prob.b_p)
     al, be, bed, ga = [dev(x) for x in prob.alpha_fc], dev(prob.beta), [dev(x) for x in prob.beta_ed], dev(prob.gamma)
