@@ -1,5 +1,5 @@
 """CPU-side checks of the C ABI: the library loads and exports every symbol
-declared in include/lmm_stokes.h, the ctypes structs match the C layout, the
+declared in include/*.h, the ctypes structs match the C layout, the
 knob defaults mirror probin_gmres.f90, and create() fails cleanly without a
 GPU (no compute calls are made here)."""
 import ctypes as C
@@ -11,11 +11,11 @@ import pytest
 from lowmachmixtures_b200 import abi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "lmm_stokes.h")
+HEADERS = sorted(os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
 
 
 def declared_functions():
-    src = open(HEADER).read()
+    src = "".join(open(h).read() for h in HEADERS)
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     names = re.findall(r"\b(lmm_[a-z0-9_]+)\s*\(", src)
     return sorted(set(names))
