@@ -18,6 +18,7 @@ LMM_ERR_NONFINITE = -3
 LMM_ERR_CUDA = -4
 LMM_ERR_WATCHDOG = -5
 LMM_ERR_NO_DEVICE = -6
+LMM_ERR_TOO_LARGE = -7
 
 LMM_BC_PERIODIC = -1
 LMM_LAYOUT_COMPACT = 0

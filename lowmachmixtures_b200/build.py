@@ -26,6 +26,7 @@ UNITS = [
     ("kernels_fp32.cu", ["-fmad=true"]),
     ("krylov.cu", ["-fmad=false"]),
     ("solver.cu", ["-fmad=false"]),
+    ("noalloc.cu", ["-fmad=false"]),
     ("nn.cu", ["-fmad=true"]),
 ]
 

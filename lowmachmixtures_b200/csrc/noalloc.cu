@@ -1,0 +1,92 @@
+// noalloc.cu - lmm_inner_prod_noalloc: the weighted Stokes inner product with
+// its reduction scratch in a static __device__ array (include/lmm_noalloc.h).
+//
+// Callers that cannot allocate device memory at the point where they need an
+// inner product (their device memory is held by their own pool, or they have
+// no solver handle and creating one would allocate a full solve workspace)
+// get the same deterministic reduction as lmm_op_inner_prod, with the block
+// partials, the last-block counter and the result in a fixed 19 KB array.
+// Built with -fmad=false like the FP64 kernels, so both entry points return
+// the same bits.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "kernels.cuh"
+#include "../../include/lmm_noalloc.h"
+
+namespace {
+
+struct NoallocScratch {
+    double partials[LMM_NOALLOC_MAX_BLOCKS * 4];  // block partial sums, 4 components
+    double out[8];                                // result slot (6 used)
+    unsigned counter;                             // finished blocks; must be 0 at launch
+};
+
+static __device__ __align__(256) NoallocScratch g_scratch;
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+NoallocScratch* g_addr[kMaxDevices] = {};
+
+// Set-up, once per device with that device current: the address of the
+// static scratch in this device's copy of the module.
+int scratch_address(NoallocScratch** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LMM_ERR_NO_DEVICE;
+    if (dev < 0 || dev >= kMaxDevices) return LMM_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return LMM_ERR_CUDA;
+        g_addr[dev] = static_cast<NoallocScratch*>(p);
+    }
+    *out = g_addr[dev];
+    return LMM_OK;
+}
+
+}  // namespace
+
+extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* const a_u[3], const double* a_p,
+                                      const double* const b_u[3], const double* b_p, double p_norm_weight, void* stream,
+                                      double* out_host) {
+    using namespace lmm;
+    if ((dm != 2 && dm != 3) || !n || !a_u || !b_u || !a_p || !b_p || !out_host) return LMM_ERR_INVALID;
+    int64_t cells = 1;
+    for (int d = 0; d < dm; ++d) {
+        if (n[d] < 1) return LMM_ERR_INVALID;
+        cells *= n[d];
+        if (cells > LMM_NOALLOC_MAX_CELLS) return LMM_ERR_TOO_LARGE;
+    }
+    for (int d = 0; d < dm; ++d)
+        if (!a_u[d] || !b_u[d]) return LMM_ERR_INVALID;
+    const int nblocks = reduce_blocks(cells);
+    if (nblocks > LMM_NOALLOC_MAX_BLOCKS) return LMM_ERR_TOO_LARGE;
+
+    NoallocScratch* scr = nullptr;
+    const int rc = scratch_address(&scr);
+    if (rc != LMM_OK) return rc;
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Dims D;
+    D.nx = n[0];
+    D.ny = n[1];
+    D.nz = dm == 3 ? n[2] : 1;
+    D.dm = dm;
+    // each periodic seam face is stored once and weighed 1.5 per stored copy
+    // in the reference's two copies (as lmm_op_inner_prod)
+    const double w = 3.0;
+    if (cudaMemsetAsync(&scr->counter, 0, sizeof(unsigned), s) != cudaSuccess) return LMM_ERR_CUDA;
+    if (dm == 2)
+        k_reduce<double, 2, 0><<<nblocks, kThreads, 0, s>>>(D, a_u[0], a_u[1], nullptr, a_p, b_u[0], b_u[1], nullptr, b_p, w, w, w,
+                                                             p_norm_weight, scr->partials, &scr->counter, scr->out);
+    else
+        k_reduce<double, 3, 0><<<nblocks, kThreads, 0, s>>>(D, a_u[0], a_u[1], a_u[2], a_p, b_u[0], b_u[1], b_u[2], b_p, w, w, w,
+                                                             p_norm_weight, scr->partials, &scr->counter, scr->out);
+    if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+    count_launch();
+    if (cudaMemcpyAsync(out_host, scr->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return LMM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return LMM_ERR_CUDA;
+    return LMM_OK;
+}

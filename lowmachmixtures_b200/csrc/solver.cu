@@ -26,6 +26,7 @@
 #include <tuple>
 #include <vector>
 
+#include "../../include/lmm_noalloc.h"
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
 #include "krylov.cuh"
@@ -1082,6 +1083,7 @@ const char* lmm_strerror(int code) {
     case LMM_ERR_CUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
     case LMM_ERR_WATCHDOG: return "a bounded device wait gave up";
     case LMM_ERR_NO_DEVICE: return "no CUDA device";
+    case LMM_ERR_TOO_LARGE: return "grid larger than this fixed-size entry point accepts";
     default: return "unknown status";
     }
 }
