@@ -50,6 +50,10 @@ def load() -> C.CDLL:
     lib.lmm_op_inner_prod.argtypes = [C.c_void_p, _dpp, _dp, _dpp, _dp, _dp]
     lib.lmm_op_sum_umac_press.argtypes = [C.c_void_p, _dpp, _dp, _dp]
     lib.lmm_nn_gemm_bf16.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    vp, ci = C.c_void_p, C.c_int
+    lib.lmm_nn_conv3d.argtypes = [vp, vp, vp, vp, vp, vp, vp] + [ci] * 9 + [vp, vp]
+    lib.lmm_nn_conv3d_wgrad.argtypes = [vp, vp, vp] + [ci] * 8 + [vp, vp]
+    lib.lmm_nn_pack_weights.argtypes = [vp, vp, vp, ci, ci, vp]
     lib.lmm_inner_prod_noalloc.argtypes = [C.c_int, P(C.c_int), _dpp, _dp, _dpp, _dp, C.c_double, C.c_void_p, _dp]
     lib.lmm_op_num_levels.argtypes = [C.c_void_p]
     lib.lmm_kernel_launches.restype = C.c_int64

@@ -7,6 +7,7 @@
 #include "../../include/lmm_learned.h"
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
+#include "nn_layers.cuh"
 #include "tc.cuh"
 
 namespace lmm {
@@ -72,4 +73,109 @@ extern "C" int lmm_nn_gemm_bf16(const void* A, const void* B, float* D, int M, i
     if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
     count_launch();
     return LMM_OK;
+}
+
+// ------------------------------------------------------------ layer launchers
+namespace lmm {
+namespace nn {
+
+static inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+template <class K>
+static cudaError_t raise_smem(K kern) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+int conv3d(const bf16* x, const bf16* w, const float* bias, const bf16* skip, const bf16* mask, bf16* out, float* out32, int B,
+           int nx, int ny, int nz, int up, int Cin, int Cout, int Cs, int relu, int* err, cudaStream_t s) {
+    if (!x || !w || !err || (!out && !out32) || B < 1 || nx < 1 || ny < 1 || nz < 1 || Cin < 8 || (Cin % 8) || Cout < 1 ||
+        Cout > 256 || Cs < Cout || (out && (Cs % 8)) || (up && ((nx | ny | nz) & 1)))
+        return LMM_ERR_INVALID;
+    static bool attr = false;
+    if (!attr) {
+        if (raise_smem(k_conv3d) != cudaSuccess) return LMM_ERR_CUDA;
+        attr = true;
+    }
+    ConvGather G;
+    G.x = x;
+    G.w = w;
+    G.g = Grid3{nx, ny, nz, nx * ny * nz};
+    G.up = up;
+    G.Cin = Cin;
+    G.Mtot = B * nx * ny * nz;
+    G.N = round_up(Cout, 16);
+    G.K = 27 * Cin;
+    ConvEpi E{bias, skip, mask, out, out32, G.Mtot, Cout, Cs, relu};
+    k_conv3d<<<(G.Mtot + tc::kM - 1) / tc::kM, tc::kThreadsTC, tc::smem_bytes(G.N), s>>>(G, E, err);
+    if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+    count_launch();
+    return LMM_OK;
+}
+
+int conv3d_wgrad(const bf16* x, const bf16* g, float* dw, int B, int nx, int ny, int nz, int up, int Cin, int Cg, int Cout, int* err,
+                 cudaStream_t s) {
+    if (!x || !g || !dw || !err || B < 1 || Cin < 8 || (Cin % 8) || Cg < Cout || (Cg % 8) || Cout < 1 || Cout > 256 ||
+        (up && ((nx | ny | nz) & 1)))
+        return LMM_ERR_INVALID;
+    static bool attr = false;
+    if (!attr) {
+        if (raise_smem(k_conv3d_wgrad) != cudaSuccess) return LMM_ERR_CUDA;
+        attr = true;
+    }
+    WgradGather G;
+    G.x = x;
+    G.gr = g;
+    G.g = Grid3{nx, ny, nz, nx * ny * nz};
+    G.up = up;
+    G.Cin = Cin;
+    G.Cg = Cg;
+    G.Mtot = B * nx * ny * nz;
+    G.N = round_up(Cout, 16);
+    G.kbeg = 0;
+    const int rows = 27 * Cin;
+    WgradEpi E{dw, rows, Cout};
+    // split the voxels so that about 4 CTAs per SM run
+    const int mt = (rows + tc::kM - 1) / tc::kM;
+    int splits = (148 * 4 + mt - 1) / mt;
+    int kspan = round_up((G.Mtot + splits - 1) / splits, tc::kKC);
+    if (kspan < 8 * tc::kKC) kspan = 8 * tc::kKC;
+    splits = (G.Mtot + kspan - 1) / kspan;
+    k_conv3d_wgrad<<<dim3(mt, splits), tc::kThreadsTC, tc::smem_bytes(G.N), s>>>(G, E, kspan, err);
+    if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+    count_launch();
+    return LMM_OK;
+}
+
+int pack_weights(const float* w, bf16* wf, bf16* wt, int Cout, int Cin, cudaStream_t s) {
+    if (!w || !wf || Cin < 1 || Cout < 1) return LMM_ERR_INVALID;
+    const int Npad = round_up(Cout, 16), Coutp = round_up(Cout, 8), Cinpad = round_up(Cin, 16);
+    const int n = Npad * 27 * Cin + (wt ? Cinpad * 27 * Coutp : 0);
+    k_pack_weights<<<(n + 255) / 256, 256, 0, s>>>(w, wf, wt, Cout, Cin, Npad, Coutp, Cinpad);
+    if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+    count_launch();
+    return LMM_OK;
+}
+
+}  // namespace nn
+}  // namespace lmm
+
+extern "C" int lmm_nn_conv3d(const void* x, const void* w, const float* bias, const void* skip, const void* mask, void* out,
+                             float* out32, int B, int nx, int ny, int nz, int up, int Cin, int Cout, int Cs, int relu, int* err_dev,
+                             void* stream) {
+    using lmm::nn::bf16;
+    return lmm::nn::conv3d(static_cast<const bf16*>(x), static_cast<const bf16*>(w), bias, static_cast<const bf16*>(skip),
+                           static_cast<const bf16*>(mask), static_cast<bf16*>(out), out32, B, nx, ny, nz, up, Cin, Cout, Cs, relu,
+                           err_dev, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int lmm_nn_conv3d_wgrad(const void* x, const void* g, float* dw, int B, int nx, int ny, int nz, int up, int Cin, int Cg,
+                                   int Cout, int* err_dev, void* stream) {
+    using lmm::nn::bf16;
+    return lmm::nn::conv3d_wgrad(static_cast<const bf16*>(x), static_cast<const bf16*>(g), dw, B, nx, ny, nz, up, Cin, Cg, Cout,
+                                 err_dev, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int lmm_nn_pack_weights(const float* w, void* wf, void* wt, int Cout, int Cin, void* stream) {
+    using lmm::nn::bf16;
+    return lmm::nn::pack_weights(w, static_cast<bf16*>(wf), static_cast<bf16*>(wt), Cout, Cin, static_cast<cudaStream_t>(stream));
 }

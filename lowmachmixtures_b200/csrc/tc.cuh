@@ -44,9 +44,18 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return d;                                     // base offset 0, no swizzle
 }
 
-// kind::f16 instruction descriptor: D FP32, A and B BF16, both K-major
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// byte offset of the 16-byte unit holding rows mn0..mn0+7 (mn0 % 8 == 0) at
+// one k, for an MN-major operand chunk of R rows (same core-matrix grid as
+// chunk_off: the 8 contiguous elements run along MN instead of k)
+__device__ __forceinline__ uint32_t chunk_off_mn(int R, int mn0, int k) {
+    return (uint32_t)((k >> 4) * R * 32 + (mn0 >> 3) * 256 + ((k >> 3) & 1) * 128 + (k & 7) * 16);
+}
+
+// kind::f16 instruction descriptor: D FP32, A and B BF16; amn / bmn select
+// the MN-major operand layout (0 = K-major)
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int amn = 0, int bmn = 0) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)amn << 15) | ((uint32_t)bmn << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -121,7 +130,7 @@ __host__ __device__ constexpr size_t smem_bytes(int N) {
 // Epi: __device__ void operator()(int row, int col0, const float (&v)[16])
 // for row = m0 + 32*warp + lane, columns col0..col0+15.
 // Returns false (and sets *err) when a bounded wait gave up.
-template <class Gather, class Epi>
+template <class Gather, class Epi, int AMN = 0, int BMN = 0>
 __device__ bool gemm_tile(const Gather& G, const Epi& E, int m0, int N, int K, uint8_t* smem, int* err) {
     uint8_t* sA[2];
     uint8_t* sB[2];
@@ -143,7 +152,7 @@ __device__ bool gemm_tile(const Gather& G, const Epi& E, int m0, int N, int K, u
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *holder;
-    const uint32_t idesc = idesc_bf16(kM, N);
+    const uint32_t idesc = idesc_bf16(kM, N, AMN, BMN);
     const int nchunks = (K + kKC - 1) / kKC;
     bool ok = true;
     int issued = 0;  // chunks whose MMAs were committed

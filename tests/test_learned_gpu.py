@@ -34,3 +34,128 @@ def test_gemm_bf16_matches_fp32_product(M, N, K):
     D = _gemm(A, B)
     ref = A.float() @ B.float().t()
     np.testing.assert_allclose(D.cpu().numpy(), ref.cpu().numpy(), rtol=1e-4, atol=1e-3 * np.sqrt(K))
+
+
+# ---------------------------------------------------------------- conv layers
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ref_conv(x_cl, w, up):
+    """circular 3x3x3 conv of channels-last x [B,z,y,x,C] with w [Cout][27][Cin]"""
+    import torch
+    import torch.nn.functional as F
+    x = x_cl.float().permute(0, 4, 1, 2, 3)
+    if up:
+        x = F.interpolate(x, scale_factor=2, mode="nearest")
+    co, _, cin = w.shape
+    wt = w.float().reshape(co, 3, 3, 3, cin).permute(0, 4, 1, 2, 3)
+    return F.conv3d(F.pad(x, (1, 1, 1, 1, 1, 1), mode="circular"), wt).permute(0, 2, 3, 4, 1)
+
+
+def _packed(w, with_t=False):
+    import torch
+    from lowmachmixtures_b200 import _native
+    lib = _native.load()
+    co, _, cin = w.shape
+    r16 = lambda v: (v + 15) // 16 * 16  # noqa: E731
+    wf = torch.zeros(r16(co), 27 * cin, dtype=torch.bfloat16, device="cuda")
+    wt = torch.zeros(r16(cin), 27 * ((co + 7) // 8 * 8), dtype=torch.bfloat16, device="cuda") if with_t else None
+    assert lib.lmm_nn_pack_weights(_p(w), _p(wf), _p(wt), co, cin, _stream()) == 0
+    return wf, wt
+
+
+@pytest.mark.parametrize("B,n,cin,cout,up,relu", [(2, (16, 8, 8), 16, 32, 0, 1), (1, (16, 16, 8), 32, 16, 1, 1),
+                                                  (1, (8, 8, 8), 64, 64, 0, 0), (1, (32, 16, 16), 8, 16, 0, 1)])
+def test_conv3d_matches_torch(B, n, cin, cout, up, relu):
+    import torch
+    from lowmachmixtures_b200 import _native
+    lib = _native.load()
+    nx, ny, nz = n
+    g = torch.Generator().manual_seed(cin * cout + up)
+    sh = (B, nz >> up, ny >> up, nx >> up, cin)
+    x = torch.randn(sh, generator=g).to(torch.bfloat16).cuda()
+    w = (torch.randn(cout, 27, cin, generator=g) / np.sqrt(27 * cin)).cuda()
+    bias = torch.randn(cout, generator=g).cuda() * 0.1
+    skip = torch.randn(B, nz, ny, nx, cout, generator=g).to(torch.bfloat16).cuda()
+    wf, _ = _packed(w)
+    out = torch.empty(B, nz, ny, nx, cout, dtype=torch.bfloat16, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.lmm_nn_conv3d(_p(x), _p(wf), _p(bias), _p(skip), None, _p(out), None, B, nx, ny, nz, up, cin, cout, cout, relu,
+                           _p(err), _stream())
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = _ref_conv(x, w.to(torch.bfloat16), up) + bias + skip.float()
+    if relu:
+        ref = torch.relu(ref)
+    scale = ref.abs().max().item()
+    np.testing.assert_allclose(out.float().cpu().numpy(), ref.cpu().numpy(), rtol=1e-2, atol=1e-2 * scale)
+
+
+def test_conv3d_fp32_output_and_mask():
+    import torch
+    from lowmachmixtures_b200 import _native
+    lib = _native.load()
+    B, nx, ny, nz, cin, cout = 1, 16, 16, 16, 16, 4
+    g = torch.Generator().manual_seed(5)
+    x = torch.randn(B, nz, ny, nx, cin, generator=g).to(torch.bfloat16).cuda()
+    w = (torch.randn(cout, 27, cin, generator=g) / 20).cuda()
+    wf, _ = _packed(w)
+    out32 = torch.empty(B, nz, ny, nx, cout, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.lmm_nn_conv3d(_p(x), _p(wf), None, None, None, None, _p(out32), B, nx, ny, nz, 0, cin, cout, cout, 0, _p(err),
+                             _stream()) == 0
+    torch.cuda.synchronize()
+    ref = _ref_conv(x, w.to(torch.bfloat16), 0)
+    np.testing.assert_allclose(out32.cpu().numpy(), ref.cpu().numpy(), rtol=1e-4, atol=1e-4)
+    # masked BF16 output with padded channel rows (Cs = 8 > Cout = 4)
+    mask = torch.randn(B, nz, ny, nx, 8, generator=g).to(torch.bfloat16).cuda()
+    out = torch.full((B, nz, ny, nx, 8), 7.0, dtype=torch.bfloat16, device="cuda")
+    assert lib.lmm_nn_conv3d(_p(x), _p(wf), None, None, _p(mask), _p(out), None, B, nx, ny, nz, 0, cin, cout, 8, 0, _p(err),
+                             _stream()) == 0
+    torch.cuda.synchronize()
+    exp = torch.where(mask[..., :4].float() > 0, ref, torch.zeros_like(ref))
+    np.testing.assert_allclose(out[..., :4].float().cpu().numpy(), exp.cpu().numpy(), rtol=1e-2, atol=1e-2)
+    assert (out[..., 4:].float() == 0).all()
+
+
+@pytest.mark.parametrize("B,n,cin,cout,up", [(2, (16, 8, 8), 16, 32, 0), (1, (16, 16, 16), 32, 16, 1), (1, (32, 32, 32), 8, 16, 0),
+                                             (1, (16, 16, 16), 16, 4, 0)])
+def test_conv3d_gradients_match_torch_autograd(B, n, cin, cout, up):
+    import torch
+    from lowmachmixtures_b200 import _native
+    lib = _native.load()
+    nx, ny, nz = n
+    g = torch.Generator().manual_seed(cin + 3 * cout + up)
+    x = torch.randn(B, nz >> up, ny >> up, nx >> up, cin, generator=g).to(torch.bfloat16).cuda()
+    w = (torch.randn(cout, 27, cin, generator=g) / np.sqrt(27 * cin)).cuda()
+    coutp = (cout + 7) // 8 * 8
+    gy = torch.zeros(B, nz, ny, nx, coutp, dtype=torch.bfloat16, device="cuda")
+    gy[..., :cout] = torch.randn(B, nz, ny, nx, cout, generator=g).to(torch.bfloat16).cuda()
+    # torch reference gradients of sum(conv(x, w) * gy)
+    xr = x.float().clone().requires_grad_(True)
+    wr = w.to(torch.bfloat16).float().clone().requires_grad_(True)
+    y = _ref_conv(xr, wr, up)
+    (y * gy[..., :cout].float()).sum().backward()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dw = torch.zeros(cout, 27, cin, dtype=torch.float32, device="cuda")
+    assert lib.lmm_nn_conv3d_wgrad(_p(x), _p(gy), _p(dw), B, nx, ny, nz, up, cin, coutp, cout, _p(err), _stream()) == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref_dw = wr.grad
+    np.testing.assert_allclose(dw.cpu().numpy(), ref_dw.cpu().numpy(), rtol=2e-3, atol=2e-3 * ref_dw.abs().max().item())
+    if up == 0:
+        # data gradient: the same convolution kernel with the flipped, transposed weights
+        _, wt = _packed(w, with_t=True)
+        dx = torch.empty(B, nz, ny, nx, cin, dtype=torch.float32, device="cuda")
+        assert lib.lmm_nn_conv3d(_p(gy), _p(wt), None, None, None, None, _p(dx), B, nx, ny, nz, 0, coutp, cin, cin, 0, _p(err),
+                                 _stream()) == 0
+        torch.cuda.synchronize()
+        ref_dx = xr.grad
+        np.testing.assert_allclose(dx.cpu().numpy(), ref_dx.cpu().numpy(), rtol=2e-3, atol=2e-3 * ref_dx.abs().max().item())
