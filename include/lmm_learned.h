@@ -5,9 +5,54 @@
 #ifndef LMM_LEARNED_H
 #define LMM_LEARNED_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+/* The network of the learned stage: a 3-level periodic convolutional
+ * encoder-decoder (3x3x3 kernels, 16/32/64 channels, BF16 weights and
+ * activations, FP32 accumulation), E0a E0b | pool | E1a E1b | pool | E2a E2b
+ * | up D1a (+E1b) D1b | up D0a (+E0b) D0b | Out.  Inputs: BF16 [batch][nz]
+ * [ny][nx][8] (5 channels used); output FP32 [batch][nz][ny][nx][4].
+ * Parameters: per layer the weights [Cout][27][Cin] then the biases [Cout],
+ * in layer order, FP32 (lmm_net_num_params floats). */
+typedef struct lmm_net lmm_net;
+
+int lmm_net_create(int nx, int ny, int nz, int batch, unsigned long long seed, lmm_net** out);
+int lmm_net_destroy(lmm_net* net);
+int64_t lmm_net_num_params(lmm_net* net);
+/* the network's CUDA stream */
+int lmm_net_stream(lmm_net* net, void** stream);
+/* copy the FP32 parameters to (set = 0) or from (set = 1) host memory */
+int lmm_net_params(lmm_net* net, float* host, int set);
+/* y (device, may be NULL) = network(x), x device BF16 */
+int lmm_net_forward(lmm_net* net, const void* x, float* y);
+/* gradients of sum(gy * network(x)) with respect to every parameter
+ * (gy device FP32 [M][4]) copied to grads_host (lmm_net_num_params floats) */
+int lmm_net_gradients(lmm_net* net, const void* x, const float* gy, float* grads_host);
+/* one Adam step on the mean squared error against target (device FP32
+ * [M][4]); *loss_host (may be NULL) = the loss before the step */
+int lmm_net_train_step(lmm_net* net, const void* x, const float* target, float lr, float* loss_host);
+
+/* ---- the stage inside the solver (include lmm_stokes.h for lmm_handle) ----
+ * A 3D solver handle can carry a network on its own grid (batch 1 is
+ * enough).  With knobs.learned_stage = 1, FGMRES with the FP32
+ * preconditioner adds the network's correction after every V-cycle
+ * application when it reduces the residual, and keeps the plain V-cycle
+ * result otherwise.  set_net(h, NULL) detaches. */
+struct lmm_handle;
+int lmm_stokes_set_net(struct lmm_handle* h, lmm_net* net);
+/* count training pairs from the handle's loaded coefficients (see
+ * lmm_op_load_coeffs): inputs into x_out (BF16 [count][n][8]) and targets
+ * into t_out (FP32 [count][n][4]), device pointers.  Needs set_net first. */
+int lmm_learned_make_pairs(struct lmm_handle* h, unsigned long long seed, int count, void* x_out, float* t_out);
+/* ratios[0] = |r1| / |r0| after the preconditioner, ratios[1] = |r1 - A c| / |r1|
+ * after the network's correction, on one fresh random pair */
+int lmm_learned_eval(struct lmm_handle* h, unsigned long long seed, double* ratios);
+/* corrections accepted / tried in the last solve */
+int lmm_learned_stats(struct lmm_handle* h, int* accepted, int* tried);
 
 /* D[M x N] (FP32, row-major) = A[M x K] * B[N x K]^T with BF16 row-major A
  * and B on the device, FP32 accumulation in tensor memory.  K % 8 == 0,

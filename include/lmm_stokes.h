@@ -102,7 +102,8 @@ typedef struct lmm_knobs {
     /* additions of this library */
     int    method;                 /* LMM_METHOD_* */
     int    precision;              /* LMM_PRECISION_* */
-    int    learned_stage;          /* 0 off, 1 network stage before the V-cycle (FGMRES only) */
+    int    learned_stage;          /* 0 off, 1 network correction after each FP32 V-cycle application
+                                      (3D FGMRES; needs lmm_stokes_set_net) */
     int    tail_cells;             /* coarse multigrid levels with at most this many cells run in
                                       one single-block launch; 0 = default (4096), -1 = never */
     int    tail_smem_kb;           /* shared-memory budget of that launch in KiB; 0 = 200 */

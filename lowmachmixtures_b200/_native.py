@@ -54,6 +54,19 @@ def load() -> C.CDLL:
     lib.lmm_nn_conv3d.argtypes = [vp, vp, vp, vp, vp, vp, vp] + [ci] * 9 + [vp, vp]
     lib.lmm_nn_conv3d_wgrad.argtypes = [vp, vp, vp] + [ci] * 8 + [vp, vp]
     lib.lmm_nn_pack_weights.argtypes = [vp, vp, vp, ci, ci, vp]
+    lib.lmm_net_create.argtypes = [ci, ci, ci, ci, C.c_ulonglong, P(vp)]
+    lib.lmm_net_destroy.argtypes = [vp]
+    lib.lmm_net_num_params.argtypes = [vp]
+    lib.lmm_net_num_params.restype = C.c_int64
+    lib.lmm_net_stream.argtypes = [vp, P(vp)]
+    lib.lmm_net_params.argtypes = [vp, vp, ci]
+    lib.lmm_net_forward.argtypes = [vp, vp, vp]
+    lib.lmm_net_gradients.argtypes = [vp, vp, vp, vp]
+    lib.lmm_net_train_step.argtypes = [vp, vp, vp, C.c_float, vp]
+    lib.lmm_stokes_set_net.argtypes = [vp, vp]
+    lib.lmm_learned_make_pairs.argtypes = [vp, C.c_ulonglong, ci, vp, vp]
+    lib.lmm_learned_eval.argtypes = [vp, C.c_ulonglong, P(C.c_double)]
+    lib.lmm_learned_stats.argtypes = [vp, P(ci), P(ci)]
     lib.lmm_inner_prod_noalloc.argtypes = [C.c_int, P(C.c_int), _dpp, _dp, _dpp, _dp, C.c_double, C.c_void_p, _dp]
     lib.lmm_op_num_levels.argtypes = [C.c_void_p]
     lib.lmm_kernel_launches.restype = C.c_int64

@@ -28,6 +28,8 @@ UNITS = [
     ("solver.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
     ("nn.cu", ["-fmad=true"]),
+    ("net.cu", ["-fmad=true"]),
+    ("learned.cu", ["-fmad=true"]),
 ]
 
 

@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(kThreads) k_gs_pair(Dims D, Coef<T> C, const T
     const T* pc = phi[COMP];
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
     const int j = j0 + ty;
-    // phase 1: red faces
+    // phase 1: red faces (two planes in flight per thread)
+#pragma unroll 2
     for (int kk = 0; kk < TZ + 2; ++kk) {
         const int k = wrapi(k0 - 1 + kk, D.nz);
         T* slot = red + kk * PL;
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(kThreads) k_gs_pair(Dims D, Coef<T> C, const T
     }
     __syncthreads();
     // phase 2: black faces of the TZ planes
+#pragma unroll 2
     for (int kk = 1; kk <= TZ; ++kk) {
         const int k = wrapi(k0 - 1 + kk, D.nz);
         const int x = 2 * tx + ((par0 + 1 + j + k) & 1);

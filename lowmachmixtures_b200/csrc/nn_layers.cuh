@@ -124,7 +124,7 @@ struct ConvEpi {
     }
 };
 
-__global__ void __launch_bounds__(tc::kThreadsTC) k_conv3d(ConvGather G, ConvEpi E, int* err) {
+static __global__ void __launch_bounds__(tc::kThreadsTC) k_conv3d(ConvGather G, ConvEpi E, int* err) {
     extern __shared__ __align__(1024) uint8_t conv_smem[];
     tc::gemm_tile(G, E, blockIdx.x * tc::kM, G.N, G.K, conv_smem, err);
 }
@@ -175,7 +175,7 @@ struct WgradEpi {
     }
 };
 
-__global__ void __launch_bounds__(tc::kThreadsTC) k_conv3d_wgrad(WgradGather G, WgradEpi E, int kspan, int* err) {
+static __global__ void __launch_bounds__(tc::kThreadsTC) k_conv3d_wgrad(WgradGather G, WgradEpi E, int kspan, int* err) {
     extern __shared__ __align__(1024) uint8_t wg_smem[];
     WgradGather g = G;
     g.kbeg = blockIdx.y * kspan;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(tc::kThreadsTC) k_conv3d_wgrad(WgradGather G, 
 
 // ------------------------------------------------------------ elementwise
 // 2x2x2 average (fine [B][2nz][2ny][2nx][C] -> coarse), FP32 sum
-__global__ void k_pool2(const bf16* __restrict__ f, bf16* __restrict__ c, int B, int nx, int ny, int nz, int C) {
+static __global__ void k_pool2(const bf16* __restrict__ f, bf16* __restrict__ c, int B, int nx, int ny, int nz, int C) {
     const int64_t n = (int64_t)B * nx * ny * nz * C;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const int ch = (int)(e % C);
@@ -207,7 +207,7 @@ __global__ void k_pool2(const bf16* __restrict__ f, bf16* __restrict__ c, int B,
 }
 
 // adjoint of nearest upsampling: coarse[v][c] = sum of the 8 fine children
-__global__ void k_downsum(const bf16* __restrict__ f, bf16* __restrict__ c, int B, int nx, int ny, int nz, int C) {
+static __global__ void k_downsum(const bf16* __restrict__ f, bf16* __restrict__ c, int B, int nx, int ny, int nz, int C) {
     const int64_t n = (int64_t)B * nx * ny * nz * C;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const int ch = (int)(e % C);
@@ -229,7 +229,7 @@ __global__ void k_downsum(const bf16* __restrict__ f, bf16* __restrict__ c, int 
 
 // g = (a + pool_adjoint(p)) * (act > 0) on the fine grid [B][nz][ny][nx][C];
 // p (coarse, may be null) contributes p[parent] / 8
-__global__ void k_grad_combine(const bf16* __restrict__ a, const bf16* __restrict__ p, const bf16* __restrict__ act,
+static __global__ void k_grad_combine(const bf16* __restrict__ a, const bf16* __restrict__ p, const bf16* __restrict__ act,
                                bf16* __restrict__ g, int B, int nx, int ny, int nz, int C) {
     const int64_t n = (int64_t)B * nx * ny * nz * C;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -252,7 +252,7 @@ __global__ void k_grad_combine(const bf16* __restrict__ a, const bf16* __restric
 }
 
 // db[c] += sum_m g[m][c]  (Cs channels per row, the first C summed)
-__global__ void k_bias_grad(const bf16* __restrict__ g, float* __restrict__ db, int64_t M, int C, int Cs) {
+static __global__ void k_bias_grad(const bf16* __restrict__ g, float* __restrict__ db, int64_t M, int C, int Cs) {
     __shared__ float acc[64];
     for (int c = threadIdx.x; c < 64; c += blockDim.x) acc[c] = 0.f;
     __syncthreads();
@@ -268,7 +268,7 @@ __global__ void k_bias_grad(const bf16* __restrict__ g, float* __restrict__ db, 
 }
 
 // Adam on FP32 master parameters
-__global__ void k_adam(float* __restrict__ w, float* __restrict__ m1, float* __restrict__ m2, const float* __restrict__ gr,
+static __global__ void k_adam(float* __restrict__ w, float* __restrict__ m1, float* __restrict__ m2, const float* __restrict__ gr,
                        int64_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const float g = gr[e];
@@ -282,7 +282,7 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m1, float* __r
 
 // FP32 master [Cout][27][Cin] -> forward GEMM rows wf[Npad][27*Cin] and the
 // data-gradient rows wt[Cinpad][27*Coutp]: wt[ci][s][co] = w[co][26-s][ci]
-__global__ void k_pack_weights(const float* __restrict__ w, bf16* __restrict__ wf, bf16* __restrict__ wt, int Cout, int Cin,
+static __global__ void k_pack_weights(const float* __restrict__ w, bf16* __restrict__ wf, bf16* __restrict__ wt, int Cout, int Cin,
                                int Npad, int Coutp, int Cinpad) {
     const int K = 27 * Cin, Kt = 27 * Coutp;
     const int nf = Npad * K, nt = wt ? Cinpad * Kt : 0;

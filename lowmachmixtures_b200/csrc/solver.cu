@@ -30,6 +30,7 @@
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
 #include "krylov.cuh"
+#include "learned.cuh"
 
 using namespace lmm;
 
@@ -129,6 +130,15 @@ struct lmm_handle {
         int vcycles = 0, pvcycles = 0;
     };
     std::map<std::tuple<const void*, const void*, double, int>, Graph> graphs;
+    // learned stage (3D, FGMRES with the FP32 preconditioner): network and
+    // its buffers, allocated by lmm_stokes_set_net outside the arena
+    lmm_net* net = nullptr;
+    void* lrn_block = nullptr;
+    SVec lr1, lc, lAc, le;
+    std::vector<SVec> Zc;  // FP64 corrections added to the FP32 Z basis
+    float* lz32 = nullptr;
+    int* luses = nullptr;  // [accepted, tried] of the current solve
+    static constexpr int kLrnSlot = 250;
 
     template <class T>
     T* alloc(int64_t count) {
@@ -929,11 +939,50 @@ int run_gmres(lmm_handle* h, double* theta_alpha, double* norm_pre_rhs, lmm_stat
 }
 
 // ------------------------------------------------------------ flexible GMRES
+// ------------------------------------------------------------ learned stage
+// After z1 = M v (FP32 V-cycles) and w = A z1: r1 = v - w, c = network(r1)
+// with its means removed (the constant modes of the periodic operator, as
+// apply_precon.f90:433-460 removes them from z1), and, when
+// |r1 - A c| < |r1| (decided on the device, no host synchronisation),
+// z = z1 + c (c kept in FP64 beside the FP32 basis) and w = A z1 + A c;
+// otherwise c = 0 and the plain V-cycle result stands.  Mode 2 computes the
+// correction but never accepts it (the stage's cost without its effect).
+void learned_stage(lmm_handle* h, const SVec& c, const SVec& v, int mode) {
+    const int64_t len = v.size();
+    const int S1 = lmm_handle::kLrnSlot, S2 = S1 + 1, S3 = S1 + 2;
+    launch_lin(h->lr1.base, v.base, -1.0, h->w.base, len, h->stream);
+    check_launch();
+    stokes_norm(h, h->lr1, S1);
+    launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx, nn::net_input(h->net), h->stream);
+    check_launch();
+    if (nn::net_forward_on(h->net, h->stream) != LMM_OK) throw LmmError(LMM_ERR_CUDA);
+    launch_correction(h->D0, nn::net_output(h->net), h->slot(S1), h->grid.dx, c.base, h->stream);
+    check_launch();
+    {
+        double* cu[3] = {c.c(0), c.c(1), c.c(2)};
+        reduce_means<double>(h, cu, c.p(), S3);
+        double tv = 1.0;
+        for (int d = 0; d < h->dm; ++d) tv *= (double)h->grid.n[d];
+        launch_sub_means<double>(h->D0, cu, c.p(), h->slot(S3), tv, h->theta_loaded == 0.0 ? 1 : 0, h->stream);
+        check_launch();
+    }
+    launch_apply_matrix(h->L64[0], h->knobs.visc_type, c, h->lAc, h->stream);
+    check_launch();
+    launch_lin(h->le.base, h->lr1.base, -1.0, h->lAc.base, len, h->stream);
+    check_launch();
+    stokes_norm(h, h->le, S2);
+    launch_accept(c.base, h->w.base, h->lAc.base, h->slot(S1) + 5, h->slot(S2) + 5, mode == 2 ? 0.0 : 1.0, h->luses, len,
+                  h->stream);
+    check_launch();
+}
+
 int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
     const lmm_knobs& K = h->knobs;
     const int m = K.gmres_max_inner;
     const int64_t len = h->b.size();
     const bool fp32 = (K.precision == LMM_PRECISION_FP32);
+    const bool learned = fp32 && K.learned_stage > 0 && h->net != nullptr;
+    if (learned) LMM_CK(cudaMemsetAsync(h->luses, 0, 2 * sizeof(int), h->stream));
     std::vector<double> cs(m + 2), sn(m + 2), y(m + 2), s(m + 3), col;
     Hess H{m + 1, std::vector<double>((size_t)(m + 1) * m, 0.0)};
     h->vcycles = 0;
@@ -984,6 +1033,7 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             if (fp32) {
                 precon32(h, h->V[i - 1], h->Z32[i - 1]);
                 launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[i - 1], h->n, h->dm, h->w, h->stream);
+                if (learned) learned_stage(h, h->Zc[i - 1], h->V[i - 1], K.learned_stage);
             } else {
                 precon64(h, h->V[i - 1], h->Z64[i - 1]);
                 launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[i - 1], h->w, h->stream);
@@ -1007,9 +1057,13 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
         }
         solve_utri(i_copy - 1, H, s, y);
         for (int it = 1; it <= i_copy; ++it) {
-            if (fp32)
+            if (fp32) {
                 launch_add_scaled_f32(h->x.base, h->Z32[it - 1], y[it], len, h->stream);
-            else
+                if (learned) {
+                    check_launch();
+                    launch_add_scaled(h->x.base, h->Zc[it - 1].base, y[it], len, h->stream);
+                }
+            } else
                 launch_add_scaled(h->x.base, h->Z64[it - 1].base, y[it], len, h->stream);
             check_launch();
         }
@@ -1216,6 +1270,7 @@ int lmm_stokes_destroy(lmm_handle* h) {
     for (auto& kv : h->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (h->arena) cudaFree(h->arena);
+    if (h->lrn_block) cudaFree(h->lrn_block);
     if (h->hscal) cudaFreeHost(h->hscal);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -1642,3 +1697,141 @@ int reduce_blocks(int64_t n) {
     return (int)b;
 }
 }  // namespace lmm
+
+// ------------------------------------------------------------ learned stage entry points
+extern "C" int lmm_stokes_set_net(lmm_handle* h, lmm_net* net) {
+    if (!h) return LMM_ERR_INVALID;
+    try {
+        if (net) {
+            int nx, ny, nz, B;
+            nn::net_dims(net, &nx, &ny, &nz, &B);
+            if (h->dm != 3 || nx != h->grid.n[0] || ny != h->grid.n[1] || nz != h->grid.n[2]) {
+                g_last_error = "the network's grid differs from the solver's (3D only)";
+                return LMM_ERR_INVALID;
+            }
+            if (!h->lrn_block) {
+                const int64_t len = (int64_t)(h->dm + 1) * h->n;
+                const int nv = 4 + h->m;
+                const size_t bytes = (size_t)nv * len * sizeof(double) + (size_t)len * sizeof(float) + 256;
+                LMM_CK(cudaMalloc(&h->lrn_block, bytes));
+                double* p = static_cast<double*>(h->lrn_block);
+                h->Zc.assign(h->m, SVec());
+                SVec* v[4] = {&h->lr1, &h->lc, &h->lAc, &h->le};
+                for (int q = 0; q < nv; ++q) {
+                    SVec& t = q < 4 ? *v[q] : h->Zc[q - 4];
+                    t.base = p + (int64_t)q * len;
+                    t.n = h->n;
+                    t.dm = h->dm;
+                }
+                h->lz32 = reinterpret_cast<float*>(p + (int64_t)nv * len);
+                h->luses = reinterpret_cast<int*>(h->lz32 + len);
+                LMM_CK(cudaMemsetAsync(h->luses, 0, 2 * sizeof(int), h->stream));
+            }
+        }
+        h->net = net;
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+// Training pairs from the solver's own operators on the loaded coefficients:
+// e0 ~ N(0,1) on every face and cell, r0 = A e0, z1 = M r0 (the configured
+// preconditioner), e1 = e0 - z1, r1 = A e1; pair q gets the network input
+// rows of r1 and the target rows of e1.
+extern "C" int lmm_learned_make_pairs(lmm_handle* h, unsigned long long seed, int count, void* x_out, float* t_out) {
+    if (!h || !h->coeffs_loaded || !h->lrn_block || count < 1 || !x_out || !t_out) return LMM_ERR_INVALID;
+    try {
+        const int64_t len = (int64_t)(h->dm + 1) * h->n;
+        const int S1 = lmm_handle::kLrnSlot, S3 = S1 + 2;
+        for (int q = 0; q < count; ++q) {
+            launch_randn(h->le.base, len, seed * 7919ull + (unsigned long long)q, h->stream);
+            check_launch();
+            launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->le, h->lAc, h->stream);
+            check_launch();
+            if (h->knobs.precision == LMM_PRECISION_FP32) {
+                precon32(h, h->lAc, h->lz32);
+                launch_convert<float, double>(h->lz32, h->lc.base, len, h->stream);
+                check_launch();
+            } else {
+                precon64(h, h->lAc, h->lc);
+            }
+            launch_lin(h->le.base, h->le.base, -1.0, h->lc.base, len, h->stream);
+            check_launch();
+            launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->le, h->lr1, h->stream);
+            check_launch();
+            stokes_norm(h, h->lr1, S1);
+            const double* a[4] = {h->le.c(0), h->le.c(1), h->le.c(2), h->le.p()};
+            const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
+            stokes_reduce(h, 1, a, b, S3);
+            launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx,
+                            static_cast<__nv_bfloat16*>(x_out) + (int64_t)q * h->n * 8, h->stream);
+            check_launch();
+            launch_target(h->D0, h->le.base, h->slot(S1), h->slot(S3), h->grid.dx, t_out + (int64_t)q * h->n * 4, h->stream);
+            check_launch();
+        }
+        LMM_CK(cudaStreamSynchronize(h->stream));
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+// One fresh pair through the attached network: ratios[0] = |r1| / |r0|
+// (what the preconditioner alone leaves), ratios[1] = |r1 - A c| / |r1|
+// (what the network's correction leaves of that).
+extern "C" int lmm_learned_eval(lmm_handle* h, unsigned long long seed, double* ratios) {
+    if (!h || !h->net || !h->coeffs_loaded || !ratios) return LMM_ERR_INVALID;
+    try {
+        const int64_t len = (int64_t)(h->dm + 1) * h->n;
+        const int S1 = lmm_handle::kLrnSlot, S2 = S1 + 1, S3 = S1 + 2;
+        launch_randn(h->le.base, len, seed * 7919ull, h->stream);
+        check_launch();
+        launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->le, h->lAc, h->stream);
+        check_launch();
+        stokes_norm(h, h->lAc, S3);
+        if (h->knobs.precision == LMM_PRECISION_FP32) {
+            precon32(h, h->lAc, h->lz32);
+            launch_convert<float, double>(h->lz32, h->lc.base, len, h->stream);
+            check_launch();
+        } else {
+            precon64(h, h->lAc, h->lc);
+        }
+        launch_lin(h->le.base, h->le.base, -1.0, h->lc.base, len, h->stream);
+        check_launch();
+        launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->le, h->lr1, h->stream);
+        check_launch();
+        stokes_norm(h, h->lr1, S1);
+        launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx, nn::net_input(h->net), h->stream);
+        check_launch();
+        if (nn::net_forward_on(h->net, h->stream) != LMM_OK) throw LmmError(LMM_ERR_CUDA);
+        launch_correction(h->D0, nn::net_output(h->net), h->slot(S1), h->grid.dx, h->lc.base, h->stream);
+        check_launch();
+        launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->lc, h->lAc, h->stream);
+        check_launch();
+        launch_lin(h->le.base, h->lr1.base, -1.0, h->lAc.base, len, h->stream);
+        check_launch();
+        stokes_norm(h, h->le, S2);
+        const double n0 = read_slot(h, S3, 5), n1 = read_slot(h, S1, 5), n2 = read_slot(h, S2, 5);
+        ratios[0] = n0 > 0 ? n1 / n0 : 0.0;
+        ratios[1] = n1 > 0 ? n2 / n1 : 0.0;
+        return LMM_OK;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
+// accepted / tried corrections of the last solve
+extern "C" int lmm_learned_stats(lmm_handle* h, int* accepted, int* tried) {
+    if (!h || !accepted || !tried) return LMM_ERR_INVALID;
+    if (!h->luses) {
+        *accepted = *tried = 0;
+        return LMM_OK;
+    }
+    int u[2] = {0, 0};
+    if (cudaMemcpyAsync(u, h->luses, sizeof(u), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess) return LMM_ERR_CUDA;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return LMM_ERR_CUDA;
+    *accepted = u[0];
+    *tried = u[1];
+    return LMM_OK;
+}
