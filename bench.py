@@ -18,7 +18,12 @@ A step is one full solve.  Reported:
   roofline of the dominant kernel (one Gauss-Seidel smooth of the finest
           level), measured live with CUDA events on the solver's stream;
   cpu_baseline  the CPU oracle (C++ restatement of the reference algorithm)
-          on a bounded sample of the same solve, rank 0 only.
+          on a bounded sample of the same solve, rank 0 only;
+  learned_stage  the same mixed method with the learned correction stage
+          (network trained on the GPU before the timed region, on 64^3
+          problems of this workload's family) -- measured beside `value`,
+          which is the faster mixed configuration without it;
+  mixed_vs_fp64  relative L2 error of the mixed solution against the FP64 one.
 
 N > 1 GPUs: replicas only (one independent solve per GPU, a different seed
 per rank, no collective on the data path); value = total solves / max time.
@@ -28,6 +33,7 @@ built on this machine) on the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -49,6 +55,9 @@ def parse():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-stage leg")
+    ap.add_argument("--learned-steps", type=int, default=1000, help="training steps (4 pairs each) of the learned stage")
+    ap.add_argument("--learned-fields", type=int, default=100)
     return ap.parse_args()
 
 
@@ -123,24 +132,26 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(world, v):
+def _reduce(world, v, op):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(world, v):
+    """the slowest rank's time (every rank calls it, in the same order)"""
+    import torch.distributed as dist
+    return _reduce(world, v, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(world, v):
-    if world == 1:
-        return v
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(world, v, dist.ReduceOp.SUM if world > 1 else None)
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
@@ -367,10 +378,80 @@ def run_product(args, world, rank, local):
             "value": 1.0 / solve_s, "unit": "solves/s", "cores": omp_threads(), "kind": "port",
             "sample": (f"oracle reference GMRES: 2 inner iterations ({apps} preconditioner applications, "
                        f"{dt:.1f} s) of the same {n}^3 solve, scaled to the full solve's {full_apps} applications")}
+    # error of the mixed-precision solution against the FP64 one (same inputs;
+    # the FP64 path is bit-for-bit the oracle's arithmetic)
+    solve_dev(mixed)
+    xu_m, xp_m = [t.clone() for t in d_xu], d_xp.clone()
+    solve_dev(plain)
+    num = sum(float(((a - b) ** 2).sum()) for a, b in zip(xu_m, d_xu))
+    den = sum(float((b ** 2).sum()) for b in d_xu)
+    pm, pp = xp_m - xp_m.mean(), d_xp - d_xp.mean()
+    line["mixed_vs_fp64"] = {"velocity_rel_l2": (num / den) ** 0.5,
+                             "pressure_rel_l2_mean_removed": float(((pm - pp) ** 2).sum().sqrt() / (pp ** 2).sum().sqrt())}
+    if not args.no_learned:
+        line["learned_stage"] = learned_leg(args, prob, n, local, solve_dev, d_in, d_xu, d_xp, world)
+    traffic = profiled_traffic("gs_colour_fp32_128")
+    if traffic is not None and n == 128:
+        line["roofline"]["traffic"] = traffic * 6  # six colour launches per smooth
     for s in (mixed, plain, refg):
         s.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def profiled_traffic(key):
+    """DRAM bytes per launch of a kernel from the committed ncu summary
+    (profiles/traffic.txt: `key bytes_per_launch` lines), or None."""
+    try:
+        for ln in open(os.path.join(ROOT, "profiles", "traffic.txt")):
+            parts = ln.split()
+            if len(parts) >= 2 and parts[0] == key:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+def learned_leg(args, prob, n, local, solve_dev, d_in, d_xu, d_xp, world):
+    """Train the learned stage (untimed) on 64^3 problems of this workload's
+    family (theta alpha dx^2 = 0.1, contrast log-uniform in [10, 1000]), load
+    the weights into a network on the bench grid, and time the mixed method
+    with the stage switched on."""
+    import torch
+
+    from lowmachmixtures_b200 import learned
+    from lowmachmixtures_b200.gmres import StokesSolver
+    t0 = time.perf_counter()
+    net64, hist, _ = learned.train(n=64, fields=args.learned_fields, steps=args.learned_steps, batch=4, theta_alpha=0.1)
+    train_s = time.perf_counter() - t0
+    params = net64.params()
+    net64.close()
+    net = learned.Net((n, n, n), 1, 0)
+    net.set_params(params)
+    kn = learned.mixed_knobs(learned_stage=1)
+    with StokesSolver(3, (n, n, n), prob.dx, knobs=kn, device=local) as s:
+        assert s.lib.lmm_stokes_set_net(s._h, net.h) == 0
+        solve_dev(s)
+        ext = torch.cuda.ExternalStream(s.stream_ptr())
+        steps = max(1, args.steps // 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(ext)
+        iters = []
+        for _ in range(steps):
+            _, _, st = solve_dev(s)
+            iters.append(st["total_iter"])
+        e1.record(ext)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        acc, tried = ctypes.c_int(), ctypes.c_int()
+        s.lib.lmm_learned_stats(s._h, ctypes.byref(acc), ctypes.byref(tried))
+        rel = st["norm_resid_true"] / st["norm_b"]
+    net.close()
+    return {"value": steps / (ms / 1e3), "unit": "solves/s", "ms_per_step": ms / steps, "iterations": iters,
+            "true_rel_residual": rel, "accepted": acc.value, "tried": tried.value,
+            "train_seconds": train_s, "train_pairs": args.learned_steps * 4, "train_fields": args.learned_fields,
+            "train_grid": "64^3", "loss_first": hist[0], "loss_last": sum(hist[-20:]) / 20}
 
 
 def main():

@@ -1,0 +1,44 @@
+/* lmm_ensemble.h - ensembles of independent Stokes solves (no counterpart in
+ * the reference, which solves one problem per time step).
+ *
+ * lmm_ensemble_solve solves `count` independent problems of the same
+ * dimension and knobs but with their own grid sizes, spacing, coefficients
+ * and right-hand sides, concurrently on one device: `workers` host threads
+ * each own a solver handle per grid shape (own CUDA stream) and take the
+ * instances largest first.  Every array is a device array in the compact
+ * layout (lmm_fields_in / lmm_fields_out), already written when the call
+ * starts.  Per instance: status (as lmm_stokes_solve) and stats.  Returns
+ * the most negative instance status, or LMM_OK.  Several GPUs: call it once
+ * per device with that device's share of the instances. */
+#ifndef LMM_ENSEMBLE_H
+#define LMM_ENSEMBLE_H
+
+#include "lmm_stokes.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lmm_ensemble_item {
+    int n[3];                      /* cells per direction (n[2] ignored in 2D) */
+    double dx;
+    double theta_alpha;
+    const double* b_u[3];
+    const double* b_p;
+    const double* alpha_fc[3];
+    const double* beta;
+    const double* beta_ed[3];
+    const double* gamma;
+    double* x_u[3];                /* initial guess in, solution out */
+    double* x_p;
+    int status;                    /* out */
+    lmm_stats stats;               /* out */
+} lmm_ensemble_item;
+
+int lmm_ensemble_solve(int dm, const lmm_knobs* knobs, int device, lmm_ensemble_item* items, int count, int workers);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LMM_ENSEMBLE_H */

@@ -113,7 +113,10 @@ typedef struct lmm_knobs {
                                       1 = both colours of a component in one out-of-place launch
                                       where the level allows it, k > 1 = the same with k planes
                                       per block */
-    int    reserved[4];
+    int    l2_persist;             /* FP32 preconditioner: keep the finest level's coefficients
+                                      resident in L2 (access-policy window): 0 = default (on when
+                                      they fit), -1 = off */
+    int    reserved[3];
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -83,7 +83,8 @@ _KNOB_FIELDS = [
     ("tail_smem_kb", C.c_int),
     ("use_graphs", C.c_int),
     ("smoother_fusion", C.c_int),
-    ("reserved", C.c_int * 4),
+    ("l2_persist", C.c_int),
+    ("reserved", C.c_int * 3),
 ]
 
 
@@ -106,7 +107,7 @@ KNOB_DEFAULTS = dict(
     gmres_rel_tol=1e-9, gmres_abs_tol=0.0, gmres_verbose=1, gmres_max_outer=20,
     gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1,
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
-    tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0,
+    tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0,
 )
 
 
@@ -173,6 +174,25 @@ class Stats(C.Structure):
         d = {name: getattr(self, name) for name, _ in self._fields_ if name != "history"}
         d["history"] = list(self.history[: self.n_history])
         return d
+
+
+class EnsembleItem(C.Structure):
+    """lmm_ensemble_item (include/lmm_ensemble.h)"""
+    _fields_ = [
+        ("n", C.c_int * 3),
+        ("dx", C.c_double),
+        ("theta_alpha", C.c_double),
+        ("b_u", _dp * 3),
+        ("b_p", _dp),
+        ("alpha_fc", _dp * 3),
+        ("beta", _dp),
+        ("beta_ed", _dp * 3),
+        ("gamma", _dp),
+        ("x_u", _dp * 3),
+        ("x_p", _dp),
+        ("status", C.c_int),
+        ("stats", Stats),
+    ]
 
 
 def make_grid(dm: int, n, dx: float) -> Grid:

@@ -30,6 +30,7 @@ UNITS = [
     ("nn.cu", ["-fmad=true"]),
     ("net.cu", ["-fmad=true"]),
     ("learned.cu", ["-fmad=true"]),
+    ("ensemble.cu", ["-fmad=false"]),
 ]
 
 

@@ -90,6 +90,28 @@ __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const
     p[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
 }
 
+// --------------------------------------------------------------- odd levels
+// A level with an odd cell count (only a coarsest level can have one) lets
+// two faces of the same colour be periodic neighbours, so a colour is
+// applied as the reference writes it: L phi of the colour's faces first
+// (stag_applyop_level with the colour), then every update from those values
+// (stag_mg_update).
+__host__ __device__ __forceinline__ bool odd_level(const Dims& D) {
+    return (D.nx & 1) || (D.ny & 1) || (D.dm == 3 && (D.nz & 1));
+}
+
+template <class T, int DM, int VISC, int COMP>
+__global__ void __launch_bounds__(kThreads) k_colour_update(Dims D, Coef<T> C, const T* __restrict__ rhs, const T* __restrict__ Lp,
+                                                            T* p, int parity, T omega, T dxsqinv) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    T fac = face_diag<T, DM, VISC, COMP>(C, nb, dxsqinv, b, c);
+    T cur = p[nb.s];
+    p[nb.s] = cur + omega * (ld(rhs, nb.s) - ld(Lp, nb.s)) / fac;
+}
+
 // --------------------------------------------------------------- GS red/black pair (3D)
 // Both colours of one component in one launch (colours 2*COMP+1 and
 // 2*COMP+2 of the sweep above, same arithmetic).  The block owns a
@@ -510,6 +532,28 @@ __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, con
     phi[nb.s] = cur + res / cc_diag<T, DM>(a, nb, dxsqinv);
 }
 
+// one colour of the pressure smoother on an odd level: new values from the
+// values before the colour's pass (out), then copied back
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_cc_smooth_odd(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ rhs,
+                                                            const T* __restrict__ phi, T* __restrict__ out, int parity, T dxsqinv) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const T* a[3] = {a0, a1, a2};
+    T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
+    T cur = phi[nb.s];
+    out[nb.s] = cur + res / cc_diag<T, DM>(a, nb, dxsqinv);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_copy_parity(Dims D, const T* __restrict__ in, T* __restrict__ out, int parity) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
+    const int s = q.i + D.nx * (q.j + D.ny * q.k);
+    out[s] = in[s];
+}
+
 template <class T, int DM, int LD = 0>
 __device__ __forceinline__ T cc_res_at(const Dims& F, const T* const a[3], const T* phi, const T* rhs, int i, int j, int k,
                                        T dxsqinv) {
@@ -770,8 +814,26 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const int comp = (color - 1) / 2;
     const int parity = (color % 2 == 1) ? 0 : 1;
-    const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
     const T om = (T)omega;
+    if (odd_level(L.D)) {
+        const T* pin[3] = {phi[0], phi[1], phi[2]};
+        T* lp[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
+        launch_applyop<T>(L, visc, pin, lp, s, color);
+        count_launch();
+        const G3 go = geom3(L.D.nx, L.D.ny, L.D.nz);
+#define CU(DM_, COMP_) k_colour_update<T, DM_, V, COMP_><<<go.grid, go.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], L.tmp[COMP_], phi[COMP_], parity, om, dxsqinv)
+        if (L.D.dm == 2) {
+            if (comp == 0) { LMM_VISC_DISPATCH(visc, CU(2, 0)) }
+            else { LMM_VISC_DISPATCH(visc, CU(2, 1)) }
+        } else {
+            if (comp == 0) { LMM_VISC_DISPATCH(visc, CU(3, 0)) }
+            else if (comp == 1) { LMM_VISC_DISPATCH(visc, CU(3, 1)) }
+            else { LMM_VISC_DISPATCH(visc, CU(3, 2)) }
+        }
+#undef CU
+        return;
+    }
+    const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
 #define GS(DM_, COMP_) k_gs_colour<T, DM_, V, COMP_><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
@@ -824,11 +886,7 @@ void launch_gs_pair(const LevelDev<T>& L, int visc, int comp, const T* const rhs
     const size_t smem = (size_t)(pg.TZ + 2) * (pg.TY + 2) * (pg.TX + 2) * sizeof(T);
 #define GSP(COMP_)                                                                                                       \
     {                                                                                                                    \
-        static bool attr_set = false;                                                                                    \
-        if (!attr_set) {                                                                                                 \
-            cudaFuncSetAttribute(k_gs_pair<T, V, COMP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);      \
-            attr_set = true;                                                                                             \
-        }                                                                                                                \
+        raise_smem_limit((const void*)k_gs_pair<T, V, COMP_>, smem);                                                     \
         k_gs_pair<T, V, COMP_><<<grid, block, smem, s>>>(L.D, L.coef(), rhs[COMP_], cur[0], cur[1], cur[2], out, pg.TX, \
                                                           pg.TY, pg.TZ, 0, om, dxsqinv);                                 \
     }
@@ -901,6 +959,16 @@ void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pre
 template <class T>
 void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    if (odd_level(L.D)) {
+        const G3 go = geom3(L.D.nx, L.D.ny, L.D.nz);
+        if (L.D.dm == 2)
+            k_cc_smooth_odd<T, 2><<<go.grid, go.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, L.ptmp, parity, dxsqinv);
+        else
+            k_cc_smooth_odd<T, 3><<<go.grid, go.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, L.ptmp, parity, dxsqinv);
+        count_launch();
+        k_copy_parity<T><<<go.grid, go.block, 0, s>>>(L.D, L.ptmp, L.pphi, parity);
+        return;
+    }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
     if (L.D.dm == 2)
         k_cc_smooth<T, 2><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);

@@ -118,6 +118,9 @@ void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const 
                    double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s);
 
 int reduce_blocks(int64_t n);
+// raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device, once per (device, kernel); safe from several host threads
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
 // one kernel launch issued (counted by check_launch after every launch site)
 void count_launch();
 int64_t launches_total();

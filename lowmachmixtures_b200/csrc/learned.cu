@@ -4,9 +4,9 @@
 //
 // Scales: with s the RMS of the velocity residual, the network sees
 // r_u / s (velocity residual averaged to cells), r_p / (s dx) (divergence
-// residual) and log beta, and predicts e_u / (s dx^2), e_p / (s dx) at
-// cells, so its inputs and outputs are O(1) whatever the grid spacing and
-// the residual's size.
+// residual) and log beta, and predicts beta e_u / (s dx^2) and e_p / (s dx)
+// at cells, so its inputs and outputs are O(1) whatever the grid spacing,
+// the viscosity contrast and the residual's size.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -75,8 +75,8 @@ __global__ void k_features(Dims D, const double* __restrict__ r, const double* _
 }
 
 // psum[3]: sum of e_p (its mean is removed: the pressure is defined up to a constant)
-__global__ void k_target(Dims D, const double* __restrict__ ev, const double* __restrict__ sums, const double* __restrict__ psum,
-                         double dx, float* __restrict__ t) {
+__global__ void k_target(Dims D, const double* __restrict__ ev, const double* __restrict__ beta, const double* __restrict__ sums,
+                         const double* __restrict__ psum, double dx, float* __restrict__ t) {
     const int64_t n = (int64_t)D.nx * D.ny * D.nz;
     const double s = vel_scale(sums, n);
     const double iu = 1.0 / (s * dx * dx), ip = 1.0 / (s * dx);
@@ -87,15 +87,17 @@ __global__ void k_target(Dims D, const double* __restrict__ ev, const double* __
         const int64_t ex = (i == D.nx - 1) ? e - (D.nx - 1) : e + 1;
         const int64_t ey = (j == D.ny - 1) ? e - (int64_t)(D.ny - 1) * D.nx : e + D.nx;
         const int64_t ez = (k == D.nz - 1) ? e - (int64_t)(D.nz - 1) * D.nx * D.ny : e + (int64_t)D.nx * D.ny;
-        t[e * 4 + 0] = (float)(0.5 * (ev[e] + ev[ex]) * iu);
-        t[e * 4 + 1] = (float)(0.5 * (ev[n + e] + ev[n + ey]) * iu);
-        t[e * 4 + 2] = (float)(0.5 * (ev[2 * n + e] + ev[2 * n + ez]) * iu);
+        const double bu = beta[e] * iu;
+        t[e * 4 + 0] = (float)(0.5 * (ev[e] + ev[ex]) * bu);
+        t[e * 4 + 1] = (float)(0.5 * (ev[n + e] + ev[n + ey]) * bu);
+        t[e * 4 + 2] = (float)(0.5 * (ev[2 * n + e] + ev[2 * n + ez]) * bu);
         t[e * 4 + 3] = (float)((ev[3 * n + e] - pmean) * ip);
     }
 }
 
-// c_u(face i) = (y_u(cell i-1) + y_u(cell i)) / 2 * s dx^2, c_p = y_p s dx
-__global__ void k_correction(Dims D, const float* __restrict__ y, const double* __restrict__ sums, double dx, double* __restrict__ c) {
+// c_u(face i) = (y_u/beta (cell i-1) + y_u/beta (cell i)) / 2 * s dx^2, c_p = y_p s dx
+__global__ void k_correction(Dims D, const float* __restrict__ y, const double* __restrict__ beta, const double* __restrict__ sums,
+                             double dx, double* __restrict__ c) {
     const int64_t n = (int64_t)D.nx * D.ny * D.nz;
     const double s = vel_scale(sums, n);
     const double su = s * dx * dx, sp = s * dx;
@@ -105,9 +107,10 @@ __global__ void k_correction(Dims D, const float* __restrict__ y, const double* 
         const int64_t mx = (i == 0) ? e + (D.nx - 1) : e - 1;
         const int64_t my = (j == 0) ? e + (int64_t)(D.ny - 1) * D.nx : e - D.nx;
         const int64_t mz = (k == 0) ? e + (int64_t)(D.nz - 1) * D.nx * D.ny : e - (int64_t)D.nx * D.ny;
-        c[e] = 0.5 * ((double)y[mx * 4 + 0] + (double)y[e * 4 + 0]) * su;
-        c[n + e] = 0.5 * ((double)y[my * 4 + 1] + (double)y[e * 4 + 1]) * su;
-        c[2 * n + e] = 0.5 * ((double)y[mz * 4 + 2] + (double)y[e * 4 + 2]) * su;
+        const double ib = 1.0 / beta[e];
+        c[e] = 0.5 * ((double)y[mx * 4 + 0] / beta[mx] + (double)y[e * 4 + 0] * ib) * su;
+        c[n + e] = 0.5 * ((double)y[my * 4 + 1] / beta[my] + (double)y[e * 4 + 1] * ib) * su;
+        c[2 * n + e] = 0.5 * ((double)y[mz * 4 + 2] / beta[mz] + (double)y[e * 4 + 2] * ib) * su;
         c[3 * n + e] = (double)y[e * 4 + 3] * sp;
     }
 }
@@ -144,11 +147,12 @@ void launch_features(const Dims& D, const double* r, const double* beta, const d
                      cudaStream_t s) {
     k_features<<<grid_for((int64_t)D.nx * D.ny * D.nz), 256, 0, s>>>(D, r, beta, sums, dx, x);
 }
-void launch_target(const Dims& D, const double* e, const double* sums, const double* psum, double dx, float* t, cudaStream_t s) {
-    k_target<<<grid_for((int64_t)D.nx * D.ny * D.nz), 256, 0, s>>>(D, e, sums, psum, dx, t);
+void launch_target(const Dims& D, const double* e, const double* beta, const double* sums, const double* psum, double dx, float* t,
+                   cudaStream_t s) {
+    k_target<<<grid_for((int64_t)D.nx * D.ny * D.nz), 256, 0, s>>>(D, e, beta, sums, psum, dx, t);
 }
-void launch_correction(const Dims& D, const float* y, const double* sums, double dx, double* c, cudaStream_t s) {
-    k_correction<<<grid_for((int64_t)D.nx * D.ny * D.nz), 256, 0, s>>>(D, y, sums, dx, c);
+void launch_correction(const Dims& D, const float* y, const double* beta, const double* sums, double dx, double* c, cudaStream_t s) {
+    k_correction<<<grid_for((int64_t)D.nx * D.ny * D.nz), 256, 0, s>>>(D, y, beta, sums, dx, c);
 }
 void launch_accept(double* c, double* w, const double* Ac, const double* n1, const double* n2, double factor, int* uses, int64_t len,
                    cudaStream_t s) {

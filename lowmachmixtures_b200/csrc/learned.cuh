@@ -19,9 +19,10 @@ void launch_lin(double* out, const double* a, double alpha, const double* b, int
 void launch_features(const Dims& D, const double* r, const double* beta, const double* sums, double dx, __nv_bfloat16* x,
                      cudaStream_t s);
 // training target rows (4 FP32 per cell) from an error e; psum[3] = sum of e_p
-void launch_target(const Dims& D, const double* e, const double* sums, const double* psum, double dx, float* t, cudaStream_t s);
+void launch_target(const Dims& D, const double* e, const double* beta, const double* sums, const double* psum, double dx, float* t,
+                   cudaStream_t s);
 // Stokes correction c from the network output y
-void launch_correction(const Dims& D, const float* y, const double* sums, double dx, double* c, cudaStream_t s);
+void launch_correction(const Dims& D, const float* y, const double* beta, const double* sums, double dx, double* c, cudaStream_t s);
 // w += Ac when *n2 < factor * *n1, else c = 0; uses[0] counts acceptances, uses[1] tries
 void launch_accept(double* c, double* w, const double* Ac, const double* n1, const double* n2, double factor, int* uses, int64_t len,
                    cudaStream_t s);

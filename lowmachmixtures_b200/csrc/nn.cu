@@ -61,12 +61,7 @@ extern "C" int lmm_nn_gemm_bf16(const void* A, const void* B, float* D, int M, i
     using namespace lmm;
     if (!A || !B || !D || !err_dev || M < 1 || K < 8 || (K % 8) || N < 16 || N > 256 || (N % 16)) return LMM_ERR_INVALID;
     const size_t smem = tc::smem_bytes(N);
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
-            return LMM_ERR_CUDA;
-        attr = true;
-    }
+    if (raise_smem_limit((const void*)k_gemm_bf16, smem) != cudaSuccess) return LMM_ERR_CUDA;
     GatherRowMajor G{static_cast<const __nv_bfloat16*>(A), static_cast<const __nv_bfloat16*>(B), M, N, K};
     EpiStore E{D, M, N};
     k_gemm_bf16<<<(M + tc::kM - 1) / tc::kM, tc::kThreadsTC, smem, static_cast<cudaStream_t>(stream)>>>(G, E, err_dev);
@@ -81,21 +76,11 @@ namespace nn {
 
 static inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-template <class K>
-static cudaError_t raise_smem(K kern) {
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-}
-
 int conv3d(const bf16* x, const bf16* w, const float* bias, const bf16* skip, const bf16* mask, bf16* out, float* out32, int B,
            int nx, int ny, int nz, int up, int Cin, int Cout, int Cs, int relu, int* err, cudaStream_t s) {
     if (!x || !w || !err || (!out && !out32) || B < 1 || nx < 1 || ny < 1 || nz < 1 || Cin < 8 || (Cin % 8) || Cout < 1 ||
         Cout > 256 || Cs < Cout || (out && (Cs % 8)) || (up && ((nx | ny | nz) & 1)))
         return LMM_ERR_INVALID;
-    static bool attr = false;
-    if (!attr) {
-        if (raise_smem(k_conv3d) != cudaSuccess) return LMM_ERR_CUDA;
-        attr = true;
-    }
     ConvGather G;
     G.x = x;
     G.w = w;
@@ -106,6 +91,7 @@ int conv3d(const bf16* x, const bf16* w, const float* bias, const bf16* skip, co
     G.N = round_up(Cout, 16);
     G.K = 27 * Cin;
     ConvEpi E{bias, skip, mask, out, out32, G.Mtot, Cout, Cs, relu};
+    if (raise_smem_limit((const void*)k_conv3d, tc::smem_bytes(G.N)) != cudaSuccess) return LMM_ERR_CUDA;
     k_conv3d<<<(G.Mtot + tc::kM - 1) / tc::kM, tc::kThreadsTC, tc::smem_bytes(G.N), s>>>(G, E, err);
     if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
     count_launch();
@@ -117,11 +103,6 @@ int conv3d_wgrad(const bf16* x, const bf16* g, float* dw, int B, int nx, int ny,
     if (!x || !g || !dw || !err || B < 1 || Cin < 8 || (Cin % 8) || Cg < Cout || (Cg % 8) || Cout < 1 || Cout > 256 ||
         (up && ((nx | ny | nz) & 1)))
         return LMM_ERR_INVALID;
-    static bool attr = false;
-    if (!attr) {
-        if (raise_smem(k_conv3d_wgrad) != cudaSuccess) return LMM_ERR_CUDA;
-        attr = true;
-    }
     WgradGather G;
     G.x = x;
     G.gr = g;
@@ -140,6 +121,7 @@ int conv3d_wgrad(const bf16* x, const bf16* g, float* dw, int B, int nx, int ny,
     int kspan = round_up((G.Mtot + splits - 1) / splits, tc::kKC);
     if (kspan < 8 * tc::kKC) kspan = 8 * tc::kKC;
     splits = (G.Mtot + kspan - 1) / kspan;
+    if (raise_smem_limit((const void*)k_conv3d_wgrad, tc::smem_bytes(G.N)) != cudaSuccess) return LMM_ERR_CUDA;
     k_conv3d_wgrad<<<dim3(mt, splits), tc::kThreadsTC, tc::smem_bytes(G.N), s>>>(G, E, kspan, err);
     if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
     count_launch();

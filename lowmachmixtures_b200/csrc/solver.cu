@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -225,15 +226,17 @@ void build_levels(lmm_handle* h) {
         v.dx = h->grid.dx * (double)(1 << l);
         v.n = (int64_t)v.D.nx * v.D.ny * v.D.nz;
         if (l < h->nlev) {
+            // the coefficients first and contiguous (one L2 persistence window
+            // can cover them), then the fields
+            for (int d = 0; d < dm; ++d) v.alpha[d] = h->alloc<T>(v.n);
+            for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) v.bed[e] = h->alloc<T>(v.n);
+            v.beta = h->alloc<T>(v.n);
+            v.gamma = h->alloc<T>(v.n);
             for (int d = 0; d < dm; ++d) {
-                v.alpha[d] = h->alloc<T>(v.n);
                 v.phi[d] = h->alloc<T>(v.n);
                 v.rhs[d] = h->alloc<T>(v.n);
                 v.tmp[d] = h->alloc<T>(v.n);
             }
-            for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) v.bed[e] = h->alloc<T>(v.n);
-            v.beta = h->alloc<T>(v.n);
-            v.gamma = h->alloc<T>(v.n);
         }
         if (l < h->nlev_p) {
             for (int d = 0; d < dm; ++d) v.pa[d] = h->alloc<T>(v.n);
@@ -242,6 +245,34 @@ void build_levels(lmm_handle* h) {
             v.ptmp = h->alloc<T>(v.n);
         }
     }
+}
+
+// Keep the finest FP32 level's coefficients (theta alpha, beta_ed, beta,
+// gamma: read by every colour pass, residual and operator application of
+// the V-cycle) resident in L2 for kernels on the handle's stream: an access
+// policy window marks them persisting.  The persisting carve-out is a
+// limit of this process's context (it ends with the context).  Skipped
+// when the arrays do not fit the device's window or carve-out.
+void set_l2_window(lmm_handle* h) {
+    const LevelDev<float>& v = h->L32[0];
+    const int ne = (h->dm == 2) ? 1 : 3;
+    const size_t bytes = (size_t)(h->dm + ne + 2) * (((size_t)v.n * sizeof(float) + 255) & ~(size_t)255);
+    int max_window = 0, max_persist = 0;
+    if (cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, h->device) != cudaSuccess) return;
+    if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, h->device) != cudaSuccess) return;
+    if (max_window <= 0 || max_persist <= 0 || bytes > (size_t)max_window) return;
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t want = std::min(bytes, (size_t)max_persist);
+    if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) return;
+    cudaStreamAttrValue a{};
+    a.accessPolicyWindow.base_ptr = v.alpha[0];
+    a.accessPolicyWindow.num_bytes = bytes;
+    a.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)want / (double)bytes);
+    a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cudaStreamSetAttribute(h->stream, cudaStreamAttributeAccessPolicyWindow, &a);
+    cudaGetLastError();
 }
 
 SVec make_svec(lmm_handle* h) {
@@ -956,7 +987,7 @@ void learned_stage(lmm_handle* h, const SVec& c, const SVec& v, int mode) {
     launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx, nn::net_input(h->net), h->stream);
     check_launch();
     if (nn::net_forward_on(h->net, h->stream) != LMM_OK) throw LmmError(LMM_ERR_CUDA);
-    launch_correction(h->D0, nn::net_output(h->net), h->slot(S1), h->grid.dx, c.base, h->stream);
+    launch_correction(h->D0, nn::net_output(h->net), h->L64[0].beta, h->slot(S1), h->grid.dx, c.base, h->stream);
     check_launch();
     {
         double* cu[3] = {c.c(0), c.c(1), c.c(2)};
@@ -1105,16 +1136,11 @@ int validate(const lmm_grid* g, const lmm_knobs* k) {
         return LMM_ERR_INVALID;
     }
     if (k->stag_mg_smoother != 0 && k->stag_mg_smoother != 1) return LMM_ERR_INVALID;
-    // every multigrid level the colour kernels touch needs even cell counts
+    // levels halve exactly down to the coarsest (which may have an odd cell
+    // count: its colours are then applied in the reference's two steps)
     int nl = compute_nlevs(g->n, g->dm, k->stag_mg_minwidth);
-    int nlp = compute_nlevs(g->n, g->dm, k->mg_minwidth);
-    for (int d = 0; d < g->dm; ++d) {
-        if (((g->n[d] >> (nl - 1)) % 2) != 0 || ((g->n[d] >> (nlp - 1)) % 2) != 0) {
-            g_last_error = "a multigrid level with an odd cell count is not supported";
-            return LMM_ERR_INVALID;
-        }
+    for (int d = 0; d < g->dm; ++d)
         if ((g->n[d] >> (nl - 1)) << (nl - 1) != g->n[d]) return LMM_ERR_INVALID;
-    }
     return LMM_OK;
 }
 
@@ -1214,7 +1240,10 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         LMM_CK(cudaMalloc(&h->arena, h->arena_bytes));
         LMM_CK(cudaMemset(h->arena, 0, h->arena_bytes));
         build_levels<double>(h);
-        if (k->precision == LMM_PRECISION_FP32) build_levels<float>(h);
+        if (k->precision == LMM_PRECISION_FP32) {
+            build_levels<float>(h);
+            if (k->l2_persist >= 0) set_l2_window(h);
+        }
         const int dm = h->dm;
         for (int d = 0; d < dm; ++d) {
             h->alpha_fc[d] = h->alloc<double>(h->n);
@@ -1689,6 +1718,19 @@ namespace {
 std::atomic<int64_t> g_launches{0};
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> raised;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = raised[{dev, kernel}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 int reduce_blocks(int64_t n) {
     int64_t b = (n + 2047) / 2048;  // at least 8 elements per thread
@@ -1767,7 +1809,7 @@ extern "C" int lmm_learned_make_pairs(lmm_handle* h, unsigned long long seed, in
             launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx,
                             static_cast<__nv_bfloat16*>(x_out) + (int64_t)q * h->n * 8, h->stream);
             check_launch();
-            launch_target(h->D0, h->le.base, h->slot(S1), h->slot(S3), h->grid.dx, t_out + (int64_t)q * h->n * 4, h->stream);
+            launch_target(h->D0, h->le.base, h->L64[0].beta, h->slot(S1), h->slot(S3), h->grid.dx, t_out + (int64_t)q * h->n * 4, h->stream);
             check_launch();
         }
         LMM_CK(cudaStreamSynchronize(h->stream));
@@ -1805,7 +1847,7 @@ extern "C" int lmm_learned_eval(lmm_handle* h, unsigned long long seed, double* 
         launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx, nn::net_input(h->net), h->stream);
         check_launch();
         if (nn::net_forward_on(h->net, h->stream) != LMM_OK) throw LmmError(LMM_ERR_CUDA);
-        launch_correction(h->D0, nn::net_output(h->net), h->slot(S1), h->grid.dx, h->lc.base, h->stream);
+        launch_correction(h->D0, nn::net_output(h->net), h->L64[0].beta, h->slot(S1), h->grid.dx, h->lc.base, h->stream);
         check_launch();
         launch_apply_matrix(h->L64[0], h->knobs.visc_type, h->lc, h->lAc, h->stream);
         check_launch();

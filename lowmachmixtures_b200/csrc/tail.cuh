@@ -12,7 +12,6 @@
 // so results are bit-identical.
 #pragma once
 #include <cstring>
-#include <map>
 
 #include "kernels.cuh"
 
@@ -53,6 +52,7 @@ struct TailView {
     const T* pa[3];
     T* pphi;
     T* prhs;
+    T* ptmp;   // odd levels: the pressure colour's new values
 };
 
 __device__ __forceinline__ int ncells(const Dims& D) { return D.nx * D.ny * D.nz; }
@@ -82,6 +82,33 @@ __device__ __forceinline__ void tail_colour(const TailView<T>& L, int parity, T 
         T fac = face_diag<T, DM, VISC, COMP>(L.C, nb, L.dxsqinv, b, c);
         T cur = p[nb.s];
         p[nb.s] = cur + omega * (r[nb.s] - Lp) / fac;
+    }
+}
+
+// a colour on an odd level (as k_colour_update): every new value from the
+// values before the colour's pass, staged in L.tmp[COMP]
+template <class T, int DM, int VISC, int COMP>
+__device__ __forceinline__ void tail_colour_odd(const TailView<T>& L, int parity, T omega) {
+    const T b = ld(L.C.beta, 0), c = ld(L.C.gamma, 0);
+    const int n = ncells(L.D);
+    const T* phi[3] = {L.phi[0], L.phi[1], L.phi[2]};
+    T* p = L.phi[COMP];
+    const T* r = L.rhs[COMP];
+    for (int w = threadIdx.x; w < n; w += blockDim.x) {
+        int i, j, k;
+        unflat3d(L.D, w, i, j, k);
+        if (((i + j + k) & 1) != parity) continue;
+        Nb nb = make_nb(L.D, i, j, k);
+        T Lp = face_L<T, DM, VISC, COMP, 1>(phi, L.C, nb, L.dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, COMP>(L.C, nb, L.dxsqinv, b, c);
+        T cur = p[nb.s];
+        L.tmp[COMP][w] = cur + omega * (r[nb.s] - Lp) / fac;
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < n; w += blockDim.x) {
+        int i, j, k;
+        unflat3d(L.D, w, i, j, k);
+        if (((i + j + k) & 1) == parity) p[w] = L.tmp[COMP][w];
     }
 }
 
@@ -120,12 +147,21 @@ __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega
             for (int color = 1; color <= 2 * DM; ++color) {
                 const int comp = (color - 1) / 2;
                 const int parity = (color % 2 == 1) ? 0 : 1;
-                if (comp == 0)
-                    tail_colour<T, DM, VISC, 0>(L, parity, omega);
-                else if (comp == 1)
-                    tail_colour<T, DM, VISC, 1>(L, parity, omega);
-                else if constexpr (DM == 3)
-                    tail_colour<T, DM, VISC, 2>(L, parity, omega);
+                if (odd_level(L.D)) {
+                    if (comp == 0)
+                        tail_colour_odd<T, DM, VISC, 0>(L, parity, omega);
+                    else if (comp == 1)
+                        tail_colour_odd<T, DM, VISC, 1>(L, parity, omega);
+                    else if constexpr (DM == 3)
+                        tail_colour_odd<T, DM, VISC, 2>(L, parity, omega);
+                } else {
+                    if (comp == 0)
+                        tail_colour<T, DM, VISC, 0>(L, parity, omega);
+                    else if (comp == 1)
+                        tail_colour<T, DM, VISC, 1>(L, parity, omega);
+                    else if constexpr (DM == 3)
+                        tail_colour<T, DM, VISC, 2>(L, parity, omega);
+                }
                 __syncthreads();
             }
         }
@@ -146,15 +182,17 @@ __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool sta
             v.pa[d] = A.L[l].pa[d];
             v.phi[d] = v.rhs[d] = v.tmp[d] = nullptr;
         }
-        v.pphi = v.prhs = nullptr;
+        v.pphi = v.prhs = v.ptmp = nullptr;
+        const bool odd = odd_level(v.D);
         if (stag) {
             for (int d = 0; d < DM; ++d) { v.phi[d] = sm + off; off += n; }
             for (int d = 0; d < DM; ++d) { v.rhs[d] = sm + off; off += n; }
-            if (jacobi)
+            if (jacobi || odd)
                 for (int d = 0; d < DM; ++d) { v.tmp[d] = sm + off; off += n; }
         } else {
             v.pphi = sm + off; off += n;
             v.prhs = sm + off; off += n;
+            if (odd) { v.ptmp = sm + off; off += n; }
         }
     }
 }
@@ -221,6 +259,30 @@ template <class T, int DM>
 __device__ void tail_cc_smooth(const TailView<T>& L, int nsweeps) {
     const int half = L.D.nx >> 1;
     const int count = half * L.D.ny * L.D.nz;
+    if (odd_level(L.D)) {
+        // odd level: each colour from the values before its pass
+        const int n = ncells(L.D);
+        for (int s = 0; s < nsweeps; ++s)
+            for (int parity = 0; parity < 2; ++parity) {
+                for (int w = threadIdx.x; w < n; w += blockDim.x) {
+                    int i, j, k;
+                    unflat3d(L.D, w, i, j, k);
+                    if (((i + j + k) & 1) != parity) continue;
+                    Nb nb = make_nb(L.D, i, j, k);
+                    T res = L.prhs[nb.s] - cc_lap<T, DM, 1>(L.pa, L.pphi, nb, L.dxsqinv);
+                    T cur = L.pphi[nb.s];
+                    L.ptmp[w] = cur + res / cc_diag<T, DM>(L.pa, nb, L.dxsqinv);
+                }
+                __syncthreads();
+                for (int w = threadIdx.x; w < n; w += blockDim.x) {
+                    int i, j, k;
+                    unflat3d(L.D, w, i, j, k);
+                    if (((i + j + k) & 1) == parity) L.pphi[w] = L.ptmp[w];
+                }
+                __syncthreads();
+            }
+        return;
+    }
     for (int s = 0; s < nsweeps; ++s)
         for (int parity = 0; parity < 2; ++parity) {
             for (int w = threadIdx.x; w < count; w += blockDim.x) {
@@ -323,7 +385,10 @@ static TailArgs<T> tail_args(const LevelDev<T>* L, int nl, int nu1, int nu2, int
 template <class T>
 size_t tail_smem_bytes(const LevelDev<T>* L, int nl, bool stag, bool jacobi) {
     size_t e = 0;
-    for (int l = 0; l < nl; ++l) e += (size_t)L[l].n * (stag ? (size_t)L[l].D.dm * (jacobi ? 3 : 2) : 2);
+    for (int l = 0; l < nl; ++l) {
+        const bool odd = odd_level(L[l].D);
+        e += (size_t)L[l].n * (stag ? (size_t)L[l].D.dm * ((jacobi || odd) ? 3 : 2) : (odd ? 3 : 2));
+    }
     return e * sizeof(T);
 }
 
@@ -331,13 +396,8 @@ size_t tail_smem_bytes(const LevelDev<T>* L, int nl, bool stag, bool jacobi) {
 // stream is being captured into a graph: the first call always runs eagerly)
 template <class K, class A>
 static cudaError_t launch_tail(K kernel, const A& args, size_t smem, cudaStream_t s) {
-    static std::map<const void*, size_t> raised;
-    size_t& cur = raised[(const void*)kernel];
-    if (smem > cur) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        cur = smem;
-    }
+    cudaError_t e = raise_smem_limit((const void*)kernel, smem);
+    if (e != cudaSuccess) return e;
     kernel<<<1, kTailThreads, smem, s>>>(args);
     return cudaGetLastError();
 }

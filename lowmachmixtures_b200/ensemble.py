@@ -1,0 +1,133 @@
+"""Ensembles of independent Stokes problems (uneven grid sizes, different
+seeds and viscosity fields): the units of work that shard across GPUs.
+
+Instances are independent, so a multi-GPU run gives every rank a disjoint
+set of whole instances -- no collective on the data path, only a final
+gather of per-instance statistics.  `shard` balances the ranks by the cost
+of an instance (its cell count).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+SIZES_2D = (64, 96, 128, 192, 256)
+
+
+def instance_sizes(count: int, seed: int = 0, sizes=SIZES_2D):
+    """grid size of each instance, drawn per seed from `sizes`"""
+    rng = np.random.Generator(np.random.PCG64(424242 + seed))
+    return [int(v) for v in rng.choice(np.asarray(sizes), size=count)]
+
+
+def instance_contrast(i: int, seed: int = 0) -> float:
+    """viscosity contrast of instance i: log-uniform in [10, 1000]"""
+    u = np.random.Generator(np.random.PCG64(777 + 1000003 * seed + i)).uniform()
+    return float(10.0 ** (1.0 + 2.0 * u))
+
+
+def shard(costs, world: int):
+    """Partition instance indices over `world` ranks, largest first onto the
+    least-loaded rank (longest-processing-time rule).  Returns one sorted
+    index list per rank; every index appears exactly once."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def make_instances(count: int, seed: int = 0, dm: int = 2, sizes=SIZES_2D, theta_alpha: float = 0.0):
+    """The config-3 ensemble: instance i has grid size instance_sizes()[i],
+    its own seeded log-viscosity field with contrast instance_contrast(i)
+    and an N(0,1) mean-removed face rhs."""
+    from . import synth
+    ns = instance_sizes(count, seed, sizes)
+    return [synth.make_problem(dm, n, instance_contrast(i, seed), 100000 * (seed + 1) + i, theta_alpha=theta_alpha)
+            for i, n in enumerate(ns)]
+
+
+def solve(problems, knobs, workers: int = 16, device: int = 0):
+    """Solve a list of StokesProblem concurrently on one GPU
+    (lmm_ensemble_solve).  Returns (statuses, stats dicts, solutions as
+    (x_u, x_p) torch tensors, wall seconds of the call)."""
+    import ctypes as C
+    import time
+
+    import torch
+
+    from . import _native, abi
+    lib = _native.load()
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda(device)  # noqa: E731
+    keep, sols = [], []
+    items = (abi.EnsembleItem * len(problems))()
+    for it, p in zip(items, problems):
+        dm = p.dm
+        arrs = dict(b_u=[dev(a) for a in p.b_u], b_p=dev(p.b_p), al=[dev(a) for a in p.alpha_fc], be=dev(p.beta),
+                    bed=[dev(a) for a in p.beta_ed], ga=dev(p.gamma))
+        xu = [torch.zeros_like(arrs["b_p"]) for _ in range(dm)]
+        xp = torch.zeros_like(arrs["b_p"])
+        keep.append(arrs)
+        sols.append((xu, xp))
+        for d in range(3):
+            it.n[d] = p.n[d]
+        it.dx = p.dx
+        it.theta_alpha = p.theta_alpha
+        for d in range(dm):
+            it.b_u[d] = abi.ptr(arrs["b_u"][d])
+            it.alpha_fc[d] = abi.ptr(arrs["al"][d])
+            it.x_u[d] = abi.ptr(xu[d])
+        for d, b in enumerate(arrs["bed"]):
+            it.beta_ed[d] = abi.ptr(b)
+        it.b_p, it.beta, it.gamma, it.x_p = abi.ptr(arrs["b_p"]), abi.ptr(arrs["be"]), abi.ptr(arrs["ga"]), abi.ptr(xp)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    lib.lmm_ensemble_solve(problems[0].dm, C.byref(knobs), device, items, len(problems), workers)
+    secs = time.perf_counter() - t0
+    return [it.status for it in items], [it.stats.as_dict() for it in items], sols, secs
+
+
+def main():
+    import argparse
+    import json
+    import os
+
+    from . import abi
+    ap = argparse.ArgumentParser(description="config-3 ensemble: independent 2D periodic Stokes problems of uneven sizes")
+    ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--rel-tol", type=float, default=1e-8)
+    ap.add_argument("--repeats", type=int, default=2)
+    a = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    sizes = instance_sizes(a.count)
+    mine = shard([n * n for n in sizes], world)[rank]
+    allp = make_instances(a.count)
+    probs = [allp[i] for i in mine]
+    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                        gmres_rel_tol=a.rel_tol)
+    from . import _native
+    lib = _native.load()
+    best = None
+    for _ in range(a.repeats):
+        st, stats, _, secs = solve(probs, kn, a.workers, local)
+        best = secs if best is None else min(best, secs)
+    ok = [s for s, c in zip(stats, st) if c >= 0]
+    errors = {}
+    for c, p in zip(st, probs):
+        if c < 0:
+            errors.setdefault(lib.lmm_strerror(c).decode(), []).append(p.n[0])
+    out = dict(rank=rank, instances=len(probs), seconds=best, instances_per_s=len(probs) / best,
+               failed=int(sum(1 for c in st if c < 0)), unconverged=int(sum(1 for c in st if c > 0)), errors=errors,
+               iterations_mean=float(np.mean([s["total_iter"] for s in ok])) if ok else None,
+               max_true_rel_residual=float(max(s["norm_resid_true"] / s["norm_b"] for s in ok)) if ok else None,
+               sizes={int(n): int(sum(1 for p in probs if p.n[0] == n)) for n in sorted(set(p.n[0] for p in probs))})
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -45,8 +45,8 @@ module lmm_stokes_iface
      integer(c_int) :: gmres_verbose, gmres_max_outer, gmres_max_inner, gmres_max_iter, gmres_min_iter
      integer(c_int) :: visc_type
      integer(c_int) :: method, precision, learned_stage
-     integer(c_int) :: tail_cells, tail_smem_kb, use_graphs, smoother_fusion
-     integer(c_int) :: reserved(4)
+     integer(c_int) :: tail_cells, tail_smem_kb, use_graphs, smoother_fusion, l2_persist
+     integer(c_int) :: reserved(3)
   end type lmm_knobs
 
   type, bind(c) :: lmm_fields_in

@@ -86,7 +86,7 @@ def _load(solver, prob):
                        prob.theta_alpha)
 
 
-def train(n: int = 64, fields: int = 200, steps: int = 2000, batch: int = 4, lr: float = 2e-3, seed: int = 0,
+def train(n: int = 64, fields: int = 200, steps: int = 2000, batch: int = 4, lr: float = 1e-3, seed: int = 0,
           theta_alpha: float = 0.0, field_seed0: int = 1000, log=None):
     """Train a network on pairs from `fields` seeded viscosity fields
     (steps // fields consecutive steps per field, `batch` fresh pairs per
@@ -188,7 +188,7 @@ def main():
     ap.add_argument("--fields", type=int, default=200)
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-seeds", type=int, default=50)
     ap.add_argument("--out", default="")
     a = ap.parse_args()

@@ -439,6 +439,21 @@ void stag_mg_update(const Level& L, Fab* phi, const Fab* rhs, const Fab* Lphi, i
                     ph(i, j, k) = ph(i, j, k) + omega * (r(i, j, k) - Lp(i, j, k)) / fac;
                 }
             }
+        // The periodic seam face is stored twice (lo and hi+1).  With an even
+        // cell count both copies are in the same colour and get the same
+        // update; with an odd count (a coarsest level such as 3) they fall in
+        // different colours, and the reference's two copies would diverge.
+        // Keep one face: the hi+1 copy follows the lo face, as a single
+        // stored face does (even counts need nothing: the copies agree).
+        if (L.geo.n[comp] % 2 == 0) continue;
+        const int n = L.geo.n[comp];
+        for (int k = ph.vlo[2]; k <= ph.vhi[2]; ++k)
+            for (int j = ph.vlo[1]; j <= ph.vhi[1]; ++j)
+                for (int i = ph.vlo[0]; i <= ph.vhi[0]; ++i) {
+                    if (comp == 0 && i == n) ph(i, j, k) = ph(0, j, k);
+                    if (comp == 1 && j == n) ph(i, j, k) = ph(i, 0, k);
+                    if (comp == 2 && k == n) ph(i, j, k) = ph(i, j, 0);
+                }
     }
 }
 

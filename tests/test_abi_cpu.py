@@ -39,9 +39,10 @@ def test_struct_layout_matches_c(lib):
     # sizes of the C structs, computed by the C compiler
     src = r'''
 #include "lmm_stokes.h"
+#include "lmm_ensemble.h"
 #include <stdio.h>
-int main(){printf("%zu %zu %zu %zu %zu\n", sizeof(lmm_grid), sizeof(lmm_knobs), sizeof(lmm_fields_in),
- sizeof(lmm_fields_out), sizeof(lmm_stats)); return 0;}
+int main(){printf("%zu %zu %zu %zu %zu %zu\n", sizeof(lmm_grid), sizeof(lmm_knobs), sizeof(lmm_fields_in),
+ sizeof(lmm_fields_out), sizeof(lmm_stats), sizeof(lmm_ensemble_item)); return 0;}
 '''
     import subprocess
     import tempfile
@@ -53,7 +54,7 @@ int main(){printf("%zu %zu %zu %zu %zu\n", sizeof(lmm_grid), sizeof(lmm_knobs), 
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     sizes = [int(v) for v in out]
     assert sizes == [C.sizeof(abi.Grid), C.sizeof(abi.Knobs), C.sizeof(abi.FieldsIn), C.sizeof(abi.FieldsOut),
-                     C.sizeof(abi.Stats)]
+                     C.sizeof(abi.Stats), C.sizeof(abi.EnsembleItem)]
 
 
 def test_default_knobs_mirror_probin_gmres(lib):
@@ -87,6 +88,7 @@ def test_create_rejects_bad_arguments_without_gpu(lib):
     k = abi.make_knobs(visc_type=-2)
     g.bc_lo[0] = 0  # not periodic
     assert lib.lmm_stokes_create(C.byref(g), C.byref(k), 0, C.byref(h)) == abi.LMM_ERR_INVALID
-    g = abi.make_grid(2, (96, 96), 1.0 / 96)  # coarsest multigrid level 3x3 (odd)
+    g = abi.make_grid(2, (96, 96), 1.0 / 96)
+    k = abi.make_knobs(visc_schur_approx=1)  # BFBt Schur approximation: not built
     assert lib.lmm_stokes_create(C.byref(g), C.byref(k), 0, C.byref(h)) == abi.LMM_ERR_INVALID
     assert lib.lmm_strerror(abi.LMM_ERR_BREAKDOWN) == b"gmres: error in orthogonalization"

@@ -376,3 +376,54 @@ def test_graphs_and_tail_are_bitwise_neutral(method, precision):
         for c in range(3):
             np.testing.assert_array_equal(xu[c], outs[0][0][c])
         np.testing.assert_array_equal(xp, outs[0][1])
+
+
+# ---------------------------------------------------------------- odd coarsest levels
+# 96 -> 48 -> 24 -> 12 -> 6 -> 3 and 24 -> 12 -> 6 -> 3: the coarsest level has
+# an odd cell count, where a colour's faces can be periodic neighbours and the
+# colour is applied in the reference's two steps (applyop of the colour, then
+# the update).
+@pytest.mark.parametrize("dm,n", [(2, 96), (2, 48), (3, 24)])
+@pytest.mark.parametrize("visc", [-1, -2, 2])
+@pytest.mark.parametrize("tail", [(-1, 0), (0, 0)])
+def test_vcycle_odd_coarsest_bit_exact(oracle, dm, n, visc, tail):
+    p, rng = random_problem(dm, n, 23, visc, theta=2.0)
+    kn = dict(visc_type=visc)
+    k = oracle.default_knobs(**kn)
+    s = make_solver(p, **kn, tail_cells=tail[0], tail_smem_kb=tail[1])
+    assert oracle.level_shape(p, s.num_levels() - 1)[0] == 3
+    rhs = [rng.standard_normal(p.shape) for _ in range(dm)]
+    ref = oracle.stag_mg_solver(p, k, rhs)
+    phi = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    s.stag_mg_solver([dev(a) for a in rhs], phi)
+    for c in range(dm):
+        np.testing.assert_array_equal(host(phi[c]), ref[c])
+    s.close()
+
+
+@pytest.mark.parametrize("dm,n", [(2, 96), (3, 24)])
+@pytest.mark.parametrize("pt", [1, 2])
+@pytest.mark.parametrize("tail_cells", [-1, 0])
+def test_apply_precon_odd_coarsest(oracle, dm, n, pt, tail_cells):
+    p, rng = random_problem(dm, n, 29, -2, theta=40.0)
+    k = oracle.default_knobs(visc_type=-2, precon_type=pt)
+    s = make_solver(p, visc_type=-2, precon_type=pt, tail_cells=tail_cells)
+    bu = [rng.standard_normal(p.shape) for _ in range(dm)]
+    bpp = rng.standard_normal(p.shape)
+    ref_u, ref_p = oracle.apply_precon(p, k, bu, bpp)
+    xu = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    xp = dev(np.zeros(p.shape))
+    s.apply_precon([dev(a) for a in bu], dev(bpp), xu, xp)
+    scale = max(np.abs(ref_p).max(), max(np.abs(r).max() for r in ref_u))
+    for c in range(dm):
+        np.testing.assert_allclose(host(xu[c]), ref_u[c], rtol=0, atol=1e-12 * scale)
+    np.testing.assert_allclose(host(xp), ref_p, rtol=0, atol=1e-12 * scale)
+    s.close()
+
+
+@pytest.mark.parametrize("n", [96, 192])
+def test_gmres_parity_2d_odd_coarsest(oracle, n):
+    prob = synth.make_problem(2, n, 50.0, 31)
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
