@@ -37,6 +37,17 @@ typedef struct lmm_ensemble_item {
 
 int lmm_ensemble_solve(int dm, const lmm_knobs* knobs, int device, lmm_ensemble_item* items, int count, int workers);
 
+/* The same with the worker pool kept between calls: create makes every
+ * handle (one per worker and distinct (n, dx) of `shapes`, which only needs
+ * n and dx filled) before any solve -- creation and destruction allocate and
+ * free memory, which must not overlap a worker's graph capture -- and run
+ * solves items whose shapes are among them. */
+typedef struct lmm_ensemble lmm_ensemble;
+int lmm_ensemble_create(int dm, const lmm_knobs* knobs, int device, const lmm_ensemble_item* shapes, int nshapes,
+                        int workers, lmm_ensemble** out);
+int lmm_ensemble_run(lmm_ensemble* ens, lmm_ensemble_item* items, int count);
+int lmm_ensemble_destroy(lmm_ensemble* ens);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,10 +113,13 @@ typedef struct lmm_knobs {
                                       1 = both colours of a component in one out-of-place launch
                                       where the level allows it, k > 1 = the same with k planes
                                       per block */
-    int    l2_persist;             /* FP32 preconditioner: keep the finest level's coefficients
-                                      resident in L2 (access-policy window): 0 = default (on when
-                                      they fit), -1 = off */
-    int    reserved[3];
+    int    l2_persist;             /* FP32 preconditioner: 1 = keep the finest level's coefficients
+                                      resident in L2 (access-policy window, when they fit);
+                                      0 = default (off: the carve-out costs the Krylov kernels more
+                                      than the V-cycle gains at 128^3) */
+    int    orthogonalization;      /* FGMRES: 0 = modified Gram-Schmidt (the reference's), 1 =
+                                      classical Gram-Schmidt, all projections in one pass */
+    int    reserved[2];
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -68,6 +68,10 @@ def load() -> C.CDLL:
     lib.lmm_learned_eval.argtypes = [vp, C.c_ulonglong, P(C.c_double)]
     lib.lmm_learned_stats.argtypes = [vp, P(ci), P(ci)]
     lib.lmm_ensemble_solve.argtypes = [ci, P(abi.Knobs), ci, P(abi.EnsembleItem), ci, ci]
+    lib.lmm_ensemble_create.argtypes = [ci, P(abi.Knobs), ci, P(abi.EnsembleItem), ci, ci, P(vp)]
+    lib.lmm_ensemble_run.argtypes = [vp, P(abi.EnsembleItem), ci]
+    lib.lmm_ensemble_destroy.argtypes = [vp]
+    lib.lmm_stochastic_rhs.argtypes = [ci, P(ci), C.c_double, C.c_double, C.c_double, _dp, _dpp, C.c_ulonglong, _dpp, vp]
     lib.lmm_inner_prod_noalloc.argtypes = [C.c_int, P(C.c_int), _dpp, _dp, _dpp, _dp, C.c_double, C.c_void_p, _dp]
     lib.lmm_op_num_levels.argtypes = [C.c_void_p]
     lib.lmm_kernel_launches.restype = C.c_int64

@@ -84,7 +84,8 @@ _KNOB_FIELDS = [
     ("use_graphs", C.c_int),
     ("smoother_fusion", C.c_int),
     ("l2_persist", C.c_int),
-    ("reserved", C.c_int * 3),
+    ("orthogonalization", C.c_int),
+    ("reserved", C.c_int * 2),
 ]
 
 
@@ -107,7 +108,7 @@ KNOB_DEFAULTS = dict(
     gmres_rel_tol=1e-9, gmres_abs_tol=0.0, gmres_verbose=1, gmres_max_outer=20,
     gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1,
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
-    tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0,
+    tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0, orthogonalization=0,
 )
 
 

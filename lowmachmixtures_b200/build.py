@@ -31,6 +31,7 @@ UNITS = [
     ("net.cu", ["-fmad=true"]),
     ("learned.cu", ["-fmad=true"]),
     ("ensemble.cu", ["-fmad=false"]),
+    ("stochastic.cu", ["-fmad=false"]),
 ]
 
 

@@ -296,3 +296,150 @@ void launch_scatter_boxlib(const Dims& D, const int nodal[3], int ng, const doub
 }
 
 }  // namespace lmm
+
+// ---------------------------------------------------------------- classical Gram-Schmidt (FGMRES option)
+namespace lmm {
+namespace {
+
+constexpr int kMdotThreads = 256;
+
+// Stokes inner products <w, V_k>, k < J, in one pass over w: per component
+// the plain sum plus (seam weight - 1) x the seam-plane sum, as k_reduce
+// weighs them; out[k*8 + 4] = sum_d <w_d, V_k,d> + pw^2 <w_p, V_k,p>.
+template <int DM, int J>
+__global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __restrict__ w, MVecs V, double wseam, double pw,
+                                                       double* __restrict__ partials, unsigned* __restrict__ counter,
+                                                       double* __restrict__ out) {
+    constexpr int NC = DM + 1;
+    const int n = D.nx * D.ny * D.nz;
+    double acc[J][NC];
+#pragma unroll
+    for (int k = 0; k < J; ++k)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[k][c] = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int t = tid; t < n; t += stride) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double x = __ldg(w + (int64_t)c * n + t);
+#pragma unroll
+            for (int k = 0; k < J; ++k) acc[k][c] += x * __ldg(V.p[k] + (int64_t)c * n + t);
+        }
+    }
+    // seam planes of the face components (x: i == 0, y: j == 0, z: k == 0)
+#pragma unroll
+    for (int c = 0; c < DM; ++c) {
+        const int m = (c == 0) ? D.ny * D.nz : (c == 1 ? D.nx * D.nz : D.nx * D.ny);
+        double v[J];
+#pragma unroll
+        for (int k = 0; k < J; ++k) v[k] = 0.0;
+        for (int q = tid; q < m; q += stride) {
+            int t;
+            if (c == 0) t = D.nx * q;
+            else if (c == 1) t = (q % D.nx) + D.nx * D.ny * (q / D.nx);
+            else t = q;
+            const double x = __ldg(w + (int64_t)c * n + t);
+#pragma unroll
+            for (int k = 0; k < J; ++k) v[k] += x * __ldg(V.p[k] + (int64_t)c * n + t);
+        }
+#pragma unroll
+        for (int k = 0; k < J; ++k) acc[k][c] += (wseam - 1.0) * v[k];
+    }
+    __shared__ double sh[J * NC][kMdotThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < J; ++k)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            double v = acc[k][c];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) sh[k * NC + c][warp] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < J * NC) {
+        double v = 0.0;
+        for (int q = 0; q < kMdotThreads / 32; ++q) v += sh[threadIdx.x][q];
+        partials[blockIdx.x * J * NC + threadIdx.x] = v;
+    }
+    __threadfence();
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < J * NC) {
+        // fixed order over the blocks
+        double v = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) v += ((volatile double*)partials)[b * J * NC + threadIdx.x];
+        sh[threadIdx.x][0] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < J) {
+        const int k = threadIdx.x;
+        double su = 0.0;
+        for (int c = 0; c < DM; ++c) su = su + sh[k * NC + c][0];
+        out[k * 8 + 4] = su + (pw * pw) * sh[k * NC + DM][0];
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
+// w -= sum_k h_k V_k, h_k = hs[k * 8 + 4]
+template <int J>
+__global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restrict__ hs, int64_t len) {
+    double h[J];
+#pragma unroll
+    for (int k = 0; k < J; ++k) h[k] = hs[k * 8 + 4];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x) {
+        double x = w[t];
+#pragma unroll
+        for (int k = 0; k < J; ++k) x = x - V.p[k][t] * h[k];
+        w[t] = x;
+    }
+}
+
+}  // namespace
+
+int mdot_blocks(int64_t n) {
+    int64_t b = (n + 2047) / 2048;
+    if (b > 444) b = 444;
+    return (int)(b < 1 ? 1 : b);
+}
+
+void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
+                 double* out, cudaStream_t s) {
+    const int nb = mdot_blocks((int64_t)D.nx * D.ny * D.nz);
+#define MD(DM_, J_) k_mdot<DM_, J_><<<nb, kMdotThreads, 0, s>>>(D, w, V, wseam, pw, partials, counter, out)
+#define MDJ(DM_)                               \
+    switch (J) {                               \
+    case 1: MD(DM_, 1); break;                 \
+    case 2: MD(DM_, 2); break;                 \
+    case 3: MD(DM_, 3); break;                 \
+    case 4: MD(DM_, 4); break;                 \
+    case 5: MD(DM_, 5); break;                 \
+    case 6: MD(DM_, 6); break;                 \
+    case 7: MD(DM_, 7); break;                 \
+    default: MD(DM_, 8); break;                \
+    }
+    if (D.dm == 2) { MDJ(2) } else { MDJ(3) }
+#undef MDJ
+#undef MD
+}
+
+void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s) {
+    int64_t b = (len + kT - 1) / kT;
+    const int nb = (int)(b > 8192 ? 8192 : b);
+    switch (J) {
+    case 1: k_maxpy<1><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 2: k_maxpy<2><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 3: k_maxpy<3><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 4: k_maxpy<4><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 5: k_maxpy<5><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 6: k_maxpy<6><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 7: k_maxpy<7><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    default: k_maxpy<8><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    }
+}
+
+}  // namespace lmm

@@ -29,6 +29,17 @@ struct SVec {
     int64_t size() const { return (int64_t)(dm + 1) * n; }
 };
 
+// up to 8 Stokes vectors (their bases; components at c * n)
+struct MVecs {
+    const double* p[8];
+};
+// classical Gram-Schmidt pieces: out[k*8+4] = <w, V_k> (Stokes inner product
+// with the seam weight), then w -= sum_k out[k*8+4] V_k; J <= 8
+int mdot_blocks(int64_t n);
+void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
+                 double* out, cudaStream_t s);
+void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s);
+
 void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s);
 // the same operator applied to an FP32 Stokes vector (FGMRES Z storage), FP64 arithmetic
 void launch_apply_matrix_f32(const LevelDev<double>& L0, int visc, const float* x, int64_t n, int dm, const SVec& b,

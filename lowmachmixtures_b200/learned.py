@@ -74,7 +74,8 @@ class Net:
 
 
 def mixed_knobs(**extra) -> abi.Knobs:
-    kw = dict(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
+    kw = dict(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+              orthogonalization=1)
     kw.update(extra)
     return abi.make_knobs(**kw)
 

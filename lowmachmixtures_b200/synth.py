@@ -133,3 +133,59 @@ def config_3d_128(seed: int = 0, n: int = 128) -> StokesProblem:
 def config_3d_64_learned(seed: int = 0, contrast: float = 1000.0) -> StokesProblem:
     """3D 64^3 steady problems of the learned-preconditioner workload."""
     return make_problem(3, 64, contrast, seed, theta_alpha=0.0)
+
+
+SPECIES_VISCOSITY = (1.0, 2.0, 5.0, 10.0)
+
+
+def mixture_viscosity(dm: int, n: int, seed: int, eta_s=SPECIES_VISCOSITY):
+    """Viscosity of a 4-species mixture: seeded smooth mass fractions (6
+    Fourier modes |k| <= 4 per species, shifted positive and normalised to sum
+    to 1) and the log-linear rule ln eta = sum_s w_s ln eta_s (not a rule of
+    the reference, whose compute_mixture_properties.f90:315-346 offers
+    constant, water-glycerol and linear forms).  Returns (eta_cc, eta_ed)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    offs_cc = [0.5] * dm
+    offs_ed = [[0.0, 0.0]] if dm == 2 else [[0.0, 0.0, 0.5], [0.0, 0.5, 0.0], [0.5, 0.0, 0.0]]
+
+    def field(ks, ph, offs):
+        # sum of cos(2 pi k.x + phase), separable: products of 1D complex exponentials
+        axes = [(np.arange(n) + offs[d]) / n for d in range(dm)]
+        g = 0.0
+        for k, p in zip(ks, ph):
+            e = [np.exp(2j * math.pi * k[d] * axes[d]) for d in range(dm)]
+            if dm == 2:
+                term = e[1][:, None] * e[0][None, :]
+            else:
+                term = e[2][:, None, None] * e[1][None, :, None] * e[0][None, None, :]
+            g = g + (np.exp(1j * p) * term).real
+        return g
+
+    fields = []
+    for _ in eta_s:
+        ks = _wave_vectors(rng, dm)
+        ph = rng.uniform(0.0, 2.0 * math.pi, size=len(ks))
+        cc = field(ks, ph, offs_cc)
+        eds = [field(ks, ph, o) for o in offs_ed]
+        gmax = max(np.abs(cc).max(), *[np.abs(e).max() for e in eds])
+        fields.append((cc / gmax, [e / gmax for e in eds]))
+
+    def mix(parts):
+        w = [1.0 + 0.9 * p for p in parts]   # positive: g in [-1, 1]
+        tot = sum(w)
+        return np.exp(sum((wi / tot) * math.log(es) for wi, es in zip(w, eta_s)))
+
+    eta_cc = mix([f[0] for f in fields])
+    eta_ed = [mix([f[1][e] for f in fields]) for e in range(len(offs_ed))]
+    return eta_cc, eta_ed
+
+
+def config_3d_256_mixture(n: int = 256, seed: int = 0) -> StokesProblem:
+    """3D n^3 periodic, 4-species mixture viscosity, overdamped (theta = 0).
+    b_u is left zero: the stochastic-stress divergence is generated on the
+    GPU (lmm_stochastic_rhs, kT = 1, dt = 1e-3, dV = dx^3)."""
+    eta_cc, eta_ed = mixture_viscosity(3, n, seed)
+    shape = (n, n, n)
+    return StokesProblem(dm=3, n=(n, n, n), dx=1.0 / n, theta_alpha=0.0, alpha_fc=[np.ones(shape) for _ in range(3)],
+                         beta=eta_cc, beta_ed=eta_ed, gamma=np.zeros(shape), b_u=[np.zeros(shape) for _ in range(3)],
+                         b_p=np.zeros(shape), contrast=float(eta_cc.max() / eta_cc.min()), seed=int(seed))

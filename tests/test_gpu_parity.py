@@ -427,3 +427,25 @@ def test_gmres_parity_2d_odd_coarsest(oracle, n):
     ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2)
     assert ref[0] == got[0] == 0
     _assert_solution_parity(ref, got)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fgmres_classical_gram_schmidt(oracle, precision):
+    """FGMRES with all projections in one pass (orthogonalization = 1):
+    same iteration count within one and the same solution within the
+    parity bar as modified Gram-Schmidt."""
+    from lowmachmixtures_b200.gmres import StokesSolver
+    prob = synth.config_3d_128(4, n=32)
+    outs = []
+    for orth in (0, 1):
+        kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=precision,
+                            orthogonalization=orth)
+        xu, xp = prob.zeros_like_solution()
+        with StokesSolver(3, (32, 32, 32), prob.dx, knobs=kn) as s:
+            _, _, st = s.solve(prob.b_u, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma,
+                               prob.theta_alpha)
+        assert st["norm_resid_true"] <= 1e-9 * st["norm_b"]
+        outs.append((st["total_iter"], xu, xp))
+    assert abs(outs[0][0] - outs[1][0]) <= 1
+    for c in range(3):
+        assert np.linalg.norm(outs[1][1][c] - outs[0][1][c]) <= 1e-8 * np.linalg.norm(outs[0][1][c])
