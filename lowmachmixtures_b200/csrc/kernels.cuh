@@ -49,7 +49,7 @@ static inline G3 geom3(int nx, int ny, int nz) {
 
 // --------------------------------------------------------------- applyop
 template <class T, int DM, int VISC>
-__global__ void __launch_bounds__(kThreads) k_applyop(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
                                                       const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                       T* __restrict__ o2, T dxsqinv, int color) {
     const Pos q = pos3(D.nx, D.ny);
@@ -289,7 +289,7 @@ __device__ __forceinline__ void restrict_comp(int comp, const Dims& F, const Coe
 
 // r = (L phi - rhs) * -1 on every face of one level (stag_mg_solver.f90:406-415)
 template <class T, int DM, int VISC>
-__global__ void __launch_bounds__(kThreads) k_residual(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_residual(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
                                                        const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
                                                        const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                        T* __restrict__ o2, T dxsqinv) {
@@ -642,6 +642,11 @@ __global__ void k_scale_copy(const T* __restrict__ in, T* __restrict__ out, T s,
     if (t < n) out[t] = in[t] * s;
 }
 template <class T>
+__global__ void k_add_to(T* __restrict__ x, const T* __restrict__ y, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) x[t] = x[t] + y[t];
+}
+template <class T>
 __global__ void k_recip(const T* __restrict__ in, T* __restrict__ out, int64_t n) {
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) out[t] = T(1) / in[t];
@@ -783,6 +788,76 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
         out[5] = sqrt(nu * nu + np * np);
         *counter = 0u;
     }
+}
+
+// --------------------------------------------------------------- BFBt Schur approximation pieces
+// inverse_diag_lap (src_gmres/inverse_diag_lap.f90:17-250): per face the
+// reciprocal of the viscous operator's diagonal without theta*alpha and dx^2
+template <class T, int DM, int VISC>
+__global__ void __launch_bounds__(kThreads) k_inverse_diag_lap(Dims D, Coef<T> C, T* m0, T* m1, T* m2) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int s = nb.s;
+    T* m[3] = {m0, m1, m2};
+    const T b = ld(C.beta, 0);
+#pragma unroll
+    for (int d = 0; d < DM; ++d) {
+        T v;
+        if (VISC == 1) {
+            v = T(1) / ((DM == 3 ? T(6) : T(4)) * b);
+        } else if (VISC == 2) {
+            v = T(1) / ((DM == 3 ? T(8) : T(6)) * b);
+        } else if constexpr (DM == 2) {
+            const int t = 1 - d;
+            const T be = ld(C.beta, s), bm = ld(C.beta, s + nb.om[d]);
+            const T E = ld(C.bed[0], s), Ep = ld(C.bed[0], s + nb.op[t]);
+            v = (VISC == -1) ? T(1) / (be + bm + Ep + E) : T(1) / (T(2) * be + T(2) * bm + Ep + E);
+        } else {
+            // (e1, t1), (e2, t2) of the face component as in Perm3
+            const int e1 = d == 2 ? 1 : 0, t1 = d == 0 ? 1 : 0;
+            const int e2 = d == 0 ? 1 : 2, t2 = d == 2 ? 1 : 2;
+            const T be = ld(C.beta, s), bm = ld(C.beta, s + nb.om[d]);
+            const T A = ld(C.bed[e1], s), Ap = ld(C.bed[e1], s + nb.op[t1]);
+            const T B = ld(C.bed[e2], s), Bp = ld(C.bed[e2], s + nb.op[t2]);
+            v = (VISC == -1) ? T(1) / (be + bm + A + Ap + B + Bp) : T(1) / (T(2) * be + T(2) * bm + A + Ap + B + Bp);
+        }
+        m[d][s] = v;
+    }
+}
+
+// g_d = ((phi - phi(-e_d)) / dx) * m_d   (compute_grad, then multifab_mult_mult_c)
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_grad_mul(Dims D, const T* __restrict__ phi, const T* m0, const T* m1, const T* m2, T* g0,
+                                                      T* g1, T* g2, T dxinv) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
+    const T p = ld(phi, t);
+    const T* m[3] = {m0, m1, m2};
+    T* g[3] = {g0, g1, g2};
+#pragma unroll
+    for (int d = 0; d < DM; ++d) g[d][t] = ((p - ld(phi, t + nb.om[d])) * dxinv) * ld(m[d], t);
+}
+
+// out = div(m * L): each face product first (multifab_mult_mult_c), then
+// compute_div's differences in its order
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_div_mul(Dims D, const T* l0, const T* l1, const T* l2, const T* m0, const T* m1,
+                                                     const T* m2, T* __restrict__ out, T dxinv) {
+    const Pos q = pos3(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
+    const T x1 = ld(l0, t + nb.op[0]) * ld(m0, t + nb.op[0]), x0 = ld(l0, t) * ld(m0, t);
+    const T y1 = ld(l1, t + nb.op[1]) * ld(m1, t + nb.op[1]), y0 = ld(l1, t) * ld(m1, t);
+    T v = (x1 - x0) * dxinv + (y1 - y0) * dxinv;
+    if constexpr (DM == 3) {
+        const T z1 = ld(l2, t + nb.op[2]) * ld(m2, t + nb.op[2]), z0 = ld(l2, t) * ld(m2, t);
+        v = v + (z1 - z0) * dxinv;
+    }
+    out[t] = v;
 }
 
 // =============================================================== launchers
@@ -1033,6 +1108,11 @@ void launch_convert(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
     k_convert<Tin, Tout><<<nblocks_for(n), kThreads, 0, s>>>(in, out, n);
 }
 template <class T>
+void launch_add_to(T* x, const T* y, int64_t n, cudaStream_t s) {
+    k_add_to<T><<<nblocks_for(n), kThreads, 0, s>>>(x, y, n);
+}
+
+template <class T>
 void launch_scale_copy(const T* in, T* out, double scale, int64_t n, cudaStream_t s) {
     k_scale_copy<T><<<nblocks_for(n), kThreads, 0, s>>>(in, out, (T)scale, n);
 }
@@ -1057,12 +1137,47 @@ void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const 
 #undef RED
 }
 
+template <class T>
+void launch_inverse_diag_lap(const LevelDev<T>& L, int visc, T* const m[3], cudaStream_t s) {
+    const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
+#define IDL(DM_, V_) k_inverse_diag_lap<T, DM_, V_><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), m[0], m[1], m[2])
+    if (L.D.dm == 2) {
+        if (visc == -1) IDL(2, -1); else if (visc == 1) IDL(2, 1); else if (visc == -2) IDL(2, -2); else IDL(2, 2);
+    } else {
+        if (visc == -1) IDL(3, -1); else if (visc == 1) IDL(3, 1); else if (visc == -2) IDL(3, -2); else IDL(3, 2);
+    }
+#undef IDL
+}
+
+template <class T>
+void launch_grad_mul(const LevelDev<T>& L, const T* phi, const T* const m[3], T* const g[3], cudaStream_t s) {
+    const T dxinv = T(1.0 / L.dx);
+    const G3 gg = geom3(L.D.nx, L.D.ny, L.D.nz);
+    if (L.D.dm == 2)
+        k_grad_mul<T, 2><<<gg.grid, gg.block, 0, s>>>(L.D, phi, m[0], m[1], m[2], g[0], g[1], g[2], dxinv);
+    else
+        k_grad_mul<T, 3><<<gg.grid, gg.block, 0, s>>>(L.D, phi, m[0], m[1], m[2], g[0], g[1], g[2], dxinv);
+}
+
+template <class T>
+void launch_div_mul(const LevelDev<T>& L, const T* const l[3], const T* const m[3], T* out, cudaStream_t s) {
+    const T dxinv = T(1.0 / L.dx);
+    const G3 gg = geom3(L.D.nx, L.D.ny, L.D.nz);
+    if (L.D.dm == 2)
+        k_div_mul<T, 2><<<gg.grid, gg.block, 0, s>>>(L.D, l[0], l[1], l[2], m[0], m[1], m[2], out, dxinv);
+    else
+        k_div_mul<T, 3><<<gg.grid, gg.block, 0, s>>>(L.D, l[0], l[1], l[2], m[0], m[1], m[2], out, dxinv);
+}
+
 #define LMM_INSTANTIATE(T)                                                                                                     \
     template void launch_applyop<T>(const LevelDev<T>&, int, const T* const[3], T* const[3], cudaStream_t, int);              \
     template void launch_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t);     \
     template void launch_jacobi<T>(const LevelDev<T>&, int, const T* const[3], const T* const[3], T* const[3], double,         \
                                    cudaStream_t);                                                                              \
     template bool gs_pair_supported<T>(const LevelDev<T>&, int);                                                               \
+    template void launch_inverse_diag_lap<T>(const LevelDev<T>&, int, T* const[3], cudaStream_t);                                \
+    template void launch_grad_mul<T>(const LevelDev<T>&, const T*, const T* const[3], T* const[3], cudaStream_t);                \
+    template void launch_div_mul<T>(const LevelDev<T>&, const T* const[3], const T* const[3], T*, cudaStream_t);                 \
     template void launch_gs_pair<T>(const LevelDev<T>&, int, int, const T* const[3], const T* const[3], T*, double, int,        \
                                     cudaStream_t);                                                                             \
     template void launch_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, int, const T* const[3],                  \
@@ -1076,6 +1191,7 @@ void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const 
     template void launch_div_plus<T>(const LevelDev<T>&, const T* const[3], const T*, T*, cudaStream_t);                        \
     template void launch_sub_weighted_grad<T>(const LevelDev<T>&, const T* const[3], const T*, T* const[3], cudaStream_t);     \
     template void launch_scale_copy<T>(const T*, T*, double, int64_t, cudaStream_t);                                           \
+    template void launch_add_to<T>(T*, const T*, int64_t, cudaStream_t);                                                      \
     template void launch_recip<T>(const T*, T*, int64_t, cudaStream_t);                                                        \
     template void launch_fill<T>(T*, double, int64_t, cudaStream_t);                                                           \
     template void launch_reduce<T>(const Dims&, int, const T* const[4], const T* const[4], const double[3], double,            \

@@ -28,6 +28,7 @@ struct LevelDev {
     T* tmp[3];          // Jacobi output / scratch
     // pressure (cell-centred) multigrid level
     T* pa[3];           // face coefficient 1/alpha (coarsened)
+    T* pmu[3];          // BFBt: face coefficient 1/diag(viscous operator) (coarsened)
     T* pphi;
     T* prhs;
     T* ptmp;
@@ -88,6 +89,17 @@ void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStre
 template <class T>
 void launch_neg_cc_lap(const LevelDev<T>& L, const T* phi, T* out, cudaStream_t s);
 
+// ---- BFBt Schur approximation (visc_schur_approx = 1) ----
+// m = 1 / diag of the viscous operator per face (|visc| 1 or 2)
+template <class T>
+void launch_inverse_diag_lap(const LevelDev<T>& L, int visc, T* const m[3], cudaStream_t s);
+// g = m * grad(phi)
+template <class T>
+void launch_grad_mul(const LevelDev<T>& L, const T* phi, const T* const m[3], T* const g[3], cudaStream_t s);
+// out = div(m * l)
+template <class T>
+void launch_div_mul(const LevelDev<T>& L, const T* const l[3], const T* const m[3], T* out, cudaStream_t s);
+
 // ---- elementwise pieces of apply_precon (level-0 geometry) ----
 // mac_rhs = div(u) + b_p
 template <class T>
@@ -101,6 +113,9 @@ template <class Tin, class Tout>
 void launch_convert(const Tin* in, Tout* out, int64_t n, cudaStream_t s);
 template <class T>
 void launch_scale_copy(const T* in, T* out, double scale, int64_t n, cudaStream_t s);
+// x = x + y
+template <class T>
+void launch_add_to(T* x, const T* y, int64_t n, cudaStream_t s);
 template <class T>
 void launch_recip(const T* in, T* out, int64_t n, cudaStream_t s);
 template <class T>

@@ -403,7 +403,7 @@ __global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restric
 
 int mdot_blocks(int64_t n) {
     int64_t b = (n + 2047) / 2048;
-    if (b > 444) b = 444;
+    if (b > 592) b = 592;  // 4 CTAs per SM; partials hold 592 x 8 x 4
     return (int)(b < 1 ? 1 : b);
 }
 

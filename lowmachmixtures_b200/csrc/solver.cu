@@ -106,6 +106,9 @@ struct lmm_handle {
     // apply_precon scratch (FP64 and FP32)
     double *mac64 = nullptr, *src64 = nullptr, *xptmp64 = nullptr, *butmp64[3] = {nullptr, nullptr, nullptr};
     float *mac32 = nullptr, *src32 = nullptr, *xptmp32 = nullptr, *butmp32[3] = {nullptr, nullptr, nullptr};
+    // BFBt scratch per precision: [0] zero, [1] kept phi, [2..4] m grad phi, [5..7] L(m grad phi)
+    double* bf64[8] = {};
+    float* bf32[8] = {};
     float* pin32 = nullptr;   // FP32 copy of a Stokes vector (precon input)
     float* pout32 = nullptr;  // FP32 precon output
     // reductions
@@ -174,6 +177,8 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
             }
             if (l < nlev_p) {
                 for (int q = 0; q < dm + 3; ++q) add(c, sz);
+                if (k.visc_schur_approx == 1)
+                    for (int q = 0; q < dm; ++q) add(c, sz);  // pmu
             }
         }
     }
@@ -193,13 +198,16 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
     for (int q = 0; q < 3 + dm; ++q) add(n, sizeof(float));
     add(vec, sizeof(float));
     add(vec, sizeof(float));
-    add(4096 * 4, sizeof(double));
+    add(4096 * 8, sizeof(double));  // reduction partials (k_mdot: 592 blocks x 8 vectors x 4 components)
     add(64, sizeof(unsigned));
     add(8 * lmm_handle::kSlots, sizeof(double));
     // BoxLib staging: the largest field with up to 4 ghost layers
     int64_t st = 1;
     for (int d = 0; d < dm; ++d) st *= (g.n[d] + 1 + 8);
     add(st, sizeof(double));
+    if (k.visc_schur_approx == 1)
+        for (int prec = 0; prec < 2; ++prec)
+            for (int q = 0; q < 8; ++q) add(n, prec ? sizeof(float) : sizeof(double));  // BFBt scratch
     return tot + (1 << 20);
 }
 
@@ -240,6 +248,8 @@ void build_levels(lmm_handle* h) {
         }
         if (l < h->nlev_p) {
             for (int d = 0; d < dm; ++d) v.pa[d] = h->alloc<T>(v.n);
+            if (h->knobs.visc_schur_approx == 1)
+                for (int d = 0; d < dm; ++d) v.pmu[d] = h->alloc<T>(v.n);
             v.pphi = h->alloc<T>(v.n);
             v.prhs = h->alloc<T>(v.n);
             v.ptmp = h->alloc<T>(v.n);
@@ -360,6 +370,20 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
             check_launch();
         }
     }
+    // BFBt: 1/diag(viscous operator) on faces, coarsened like 1/alpha
+    if (h->knobs.visc_schur_approx == 1 && h->nlev_p > 0) {
+        launch_inverse_diag_lap<double>(h->L64[0], h->knobs.visc_type, h->L64[0].pmu, h->stream);
+        check_launch();
+        for (int l = 1; l < h->nlev_p; ++l) {
+            LevelDev<double> F = h->L64[l - 1], C = h->L64[l];
+            for (int d = 0; d < 3; ++d) {
+                F.pa[d] = F.pmu[d];
+                C.pa[d] = C.pmu[d];
+            }
+            launch_coarsen_coeffs<double>(F, C, true, h->stream);
+            check_launch();
+        }
+    }
     if (h->knobs.precision == LMM_PRECISION_FP32) {
         for (int l = 0; l < (int)h->L64.size(); ++l) {
             LevelDev<double>& a = h->L64[l];
@@ -372,6 +396,8 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
             }
             if (l < h->nlev_p)
                 for (int d = 0; d < dm; ++d) launch_convert<double, float>(a.pa[d], b.pa[d], a.n, h->stream);
+            if (l < h->nlev_p && h->knobs.visc_schur_approx == 1)
+                for (int d = 0; d < dm; ++d) launch_convert<double, float>(a.pmu[d], b.pmu[d], a.n, h->stream);
             check_launch();
         }
         for (int d = 0; d < dm; ++d) launch_convert<double, float>(h->alphainv[d], h->alphainv32[d], n, h->stream);
@@ -572,18 +598,21 @@ struct PrecScratch {
     T* xptmp;
     T* butmp[3];
     T* alphainv[3];
+    T* bf[8];
 };
 template <class T>
 PrecScratch<T> prec_scratch(lmm_handle* h);
 template <>
 PrecScratch<double> prec_scratch<double>(lmm_handle* h) {
     return {h->mac64, h->src64, h->xptmp64, {h->butmp64[0], h->butmp64[1], h->butmp64[2]},
-            {h->alphainv[0], h->alphainv[1], h->alphainv[2]}};
+            {h->alphainv[0], h->alphainv[1], h->alphainv[2]},
+            {h->bf64[0], h->bf64[1], h->bf64[2], h->bf64[3], h->bf64[4], h->bf64[5], h->bf64[6], h->bf64[7]}};
 }
 template <>
 PrecScratch<float> prec_scratch<float>(lmm_handle* h) {
     return {h->mac32, h->src32, h->xptmp32, {h->butmp32[0], h->butmp32[1], h->butmp32[2]},
-            {h->alphainv32[0], h->alphainv32[1], h->alphainv32[2]}};
+            {h->alphainv32[0], h->alphainv32[1], h->alphainv32[2]},
+            {h->bf32[0], h->bf32[1], h->bf32[2], h->bf32[3], h->bf32[4], h->bf32[5], h->bf32[6], h->bf32[7]}};
 }
 
 template <class T>
@@ -606,6 +635,63 @@ void reduce_means<float>(lmm_handle* h, float* const u[3], const float* p, int s
     }
     launch_reduce<float>(h->D0, 1, a, b, w, 0.0, h->partials, h->counter, h->slot(slot), h->red_blocks, h->stream);
     check_launch();
+}
+
+// visc_schur_complement (apply_precon.f90:538-685), the BFBt Schur
+// approximation: with M = 1/diag(viscous operator) on faces,
+//   x_p = (D M G)^-1 D M L M G (D M G)^-1 rhs  [+ theta alpha phi]
+// where phi is the 1/alpha pressure solution already in L0.pphi; both
+// Poisson solves use this library's pressure V-cycle with face coefficient
+// M.  rhs (mac) is overwritten as in the reference.
+template <class T>
+void visc_schur(lmm_handle* h, T* mac, T* x_p) {
+    auto& L = levels<T>(h);
+    LevelDev<T>& L0 = L[0];
+    const int dm = h->dm;
+    const int64_t n = h->n;
+    const double theta = h->theta_loaded;
+    PrecScratch<T> S = prec_scratch<T>(h);
+    T* zero = S.bf[0];
+    T* keep = S.bf[1];
+    T* g[3] = {S.bf[2], S.bf[3], S.bf[4]};
+    T* lg[3] = {S.bf[5], S.bf[6], S.bf[7]};
+    const T* m[3] = {L0.pmu[0], L0.pmu[1], L0.pmu[2]};
+    if (std::fabs(theta) > 0.0) LMM_CK(cudaMemcpyAsync(keep, L0.pphi, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+    auto swap_coefficients = [&]() {
+        for (int l = 0; l < h->nlev_p; ++l)
+            for (int d = 0; d < dm; ++d) std::swap(L[l].pa[d], L[l].pmu[d]);
+    };
+    swap_coefficients();
+    // STEP 1: phi_mu = (D M G)^-1 rhs
+    LMM_CK(cudaMemcpyAsync(L0.prhs, mac, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+    macproject<T>(h);
+    // STEP 2: rhs = D M L (M G phi_mu), L the viscous operator without theta alpha and gamma
+    launch_grad_mul<T>(L0, L0.pphi, m, g, h->stream);
+    check_launch();
+    LMM_CK(cudaMemsetAsync(zero, 0, n * sizeof(T), h->stream));
+    {
+        LevelDev<T> Lv = L0;
+        for (int d = 0; d < 3; ++d) Lv.alpha[d] = zero;
+        Lv.gamma = zero;
+        const T* gc[3] = {g[0], g[1], g[2]};
+        launch_applyop<T>(Lv, h->knobs.visc_type, gc, lg, h->stream, 0);
+        check_launch();
+    }
+    const T* lgc[3] = {lg[0], lg[1], lg[2]};
+    launch_div_mul<T>(L0, lgc, m, mac, h->stream);
+    check_launch();
+    // STEP 3: x_p = (D M G)^-1 rhs
+    LMM_CK(cudaMemcpyAsync(L0.prhs, mac, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+    macproject<T>(h);
+    swap_coefficients();
+    LMM_CK(cudaMemcpyAsync(x_p, L0.pphi, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+    // STEP 4: x_p += theta alpha phi
+    if (std::fabs(theta) > 0.0) {
+        launch_scale_copy<T>(keep, keep, theta, n, h->stream);
+        check_launch();
+        launch_add_to<T>(x_p, keep, n, h->stream);
+        check_launch();
+    }
 }
 
 // x = M^-1 b.  b_u / b_p and x_u / x_p are level-0 arrays of type T (they
@@ -651,8 +737,12 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
             launch_neg_cc_lap<T>(L0, L0.pphi, S.src, h->stream);
             check_launch();
         }
-        launch_schur<T>(1, pt, av, theta, S.mac, S.src, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
-        check_launch();
+        if (K.visc_schur_approx == 1) {
+            visc_schur<T>(h, S.mac, x_p);
+        } else {
+            launch_schur<T>(1, pt, av, theta, S.mac, S.src, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+            check_launch();
+        }
         break;
     }
     case 2:
@@ -664,8 +754,16 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
             pres_solve(S.mac);
         else
             LMM_CK(cudaMemsetAsync(L0.pphi, 0, n * sizeof(T), h->stream));
-        launch_schur<T>(0, pt, av, theta, S.mac, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
-        check_launch();
+        if (K.visc_schur_approx == 1) {
+            visc_schur<T>(h, S.mac, x_p);
+            if (pt == -2 || pt == -5) {
+                launch_scale_copy<T>(x_p, x_p, -1.0, n, h->stream);
+                check_launch();
+            }
+        } else {
+            launch_schur<T>(0, pt, av, theta, S.mac, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+            check_launch();
+        }
         if (std::abs(pt) == 5) {
             for (int d = 0; d < dm; ++d)
                 LMM_CK(cudaMemcpyAsync(S.butmp[d], b_u[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
@@ -690,8 +788,12 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
             pres_solve(S.mac);
         else
             LMM_CK(cudaMemsetAsync(L0.pphi, 0, n * sizeof(T), h->stream));
-        launch_schur<T>(0, 3, av, theta, S.mac, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
-        check_launch();
+        if (K.visc_schur_approx == 1) {
+            visc_schur<T>(h, S.mac, x_p);
+        } else {
+            launch_schur<T>(0, 3, av, theta, S.mac, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+            check_launch();
+        }
         for (int d = 0; d < dm; ++d) LMM_CK(cudaMemcpyAsync(S.butmp[d], b_u[d], n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
         launch_sub_weighted_grad<T>(L0, nullptr, x_p, S.butmp, h->stream);
         check_launch();
@@ -705,8 +807,15 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
             pres_solve(b_p);
         else
             LMM_CK(cudaMemsetAsync(L0.pphi, 0, n * sizeof(T), h->stream));
-        launch_schur<T>(2, pt, av, theta, nullptr, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
-        check_launch();
+        if (K.visc_schur_approx == 1) {
+            // the reference leaves mac_rhs unset here when theta = 0; b_p is
+            // what it holds whenever it is set (apply_precon.f90:362-366)
+            LMM_CK(cudaMemcpyAsync(S.mac, b_p, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+            visc_schur<T>(h, S.mac, x_p);
+        } else {
+            launch_schur<T>(2, pt, av, theta, nullptr, nullptr, L0.beta, L0.gamma, L0.pphi, b_p, x_p, n, h->stream);
+            check_launch();
+        }
         break;
     }
     default:
@@ -1156,8 +1265,10 @@ int validate(const lmm_grid* g, const lmm_knobs* k) {
         g_last_error = "unsupported precon_type";
         return LMM_ERR_INVALID;
     }
-    if (k->visc_schur_approx != 0) {
-        g_last_error = "visc_schur_approx /= 0 (BFBt) is not built";
+    if (k->visc_schur_approx != 0 && k->visc_schur_approx != 1) return LMM_ERR_INVALID;
+    if (k->visc_schur_approx == 1 && av == 3) {
+        // inverse_diag_lap.f90:135,246
+        g_last_error = "inverse_diag_lap does not support abs(visc_type) = 3";
         return LMM_ERR_INVALID;
     }
     if (k->gmres_max_inner < 1 || k->gmres_max_inner > 120) return LMM_ERR_INVALID;
@@ -1307,11 +1418,16 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         h->mac32 = h->alloc<float>(h->n);
         h->src32 = h->alloc<float>(h->n);
         h->xptmp32 = h->alloc<float>(h->n);
+        if (k->visc_schur_approx == 1)
+            for (int q = 0; q < 8; ++q) {
+                h->bf64[q] = h->alloc<double>(h->n);
+                h->bf32[q] = h->alloc<float>(h->n);
+            }
         for (int d = 0; d < dm; ++d) h->butmp32[d] = h->alloc<float>(h->n);
         h->pin32 = h->alloc<float>((int64_t)(dm + 1) * h->n);
         h->pout32 = h->alloc<float>((int64_t)(dm + 1) * h->n);
         h->red_blocks = reduce_blocks(h->n);
-        h->partials = h->alloc<double>(4096 * 4);
+        h->partials = h->alloc<double>(4096 * 8);
         h->counter = h->alloc<unsigned>(64);
         h->scal = h->alloc<double>(8 * lmm_handle::kSlots);
         int64_t st = 1;

@@ -177,7 +177,8 @@ int orc_num_levels(const lmm_grid* g, int minwidth) { return compute_nlevs_mg(ge
 int orc_stokes_solve(const lmm_grid* g, const lmm_knobs* k, const lmm_fields_in* in, lmm_fields_out* out,
                      double* theta_alpha, double* norm_pre_rhs, lmm_stats* st) {
     if (!valid_grid(g) || !k || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
-    if (k->visc_schur_approx != 0) return LMM_ERR_INVALID;
+    if (k->visc_schur_approx != 0 && k->visc_schur_approx != 1) return LMM_ERR_INVALID;
+    if (k->visc_schur_approx == 1 && std::abs(k->visc_type) == 3) return LMM_ERR_INVALID;  // inverse_diag_lap.f90:135,246
     int apt = std::abs(k->precon_type);
     if (apt < 1 || apt > 5) return LMM_ERR_INVALID;
     if (st) std::memset(st, 0, sizeof(*st));

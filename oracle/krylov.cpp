@@ -86,8 +86,73 @@ static void neg_cc_lap(const Problem& P, const Fab* a, const Fab& phi, Fab& out)
     });
 }
 
+// inverse_diag_lap (inverse_diag_lap.f90:17-250): 1 / diag of the viscous
+// operator per face, without theta*alpha and dx^2 (|visc_type| 1, 2)
+static void inverse_diag_lap(const Problem& P, Fab* m) {
+    const int dm = P.geo.dm, visc = P.visc_type;
+    const Fab& b = P.beta;
+    const double b0 = P.beta(0, 0, 0);
+    for (int d = 0; d < dm; ++d) {
+        m[d] = make_face(P.geo, d, 0);
+        for_valid(m[d], [&](double& v, int i, int j, int k) {
+            if (visc == 1) { v = 1.0 / ((dm == 3 ? 6.0 : 4.0) * b0); return; }
+            if (visc == 2) { v = 1.0 / ((dm == 3 ? 8.0 : 6.0) * b0); return; }
+            const double c = (visc == -2) ? 2.0 : 1.0;
+            if (dm == 2) {
+                const Fab& e = P.beta_ed[0];
+                if (d == 0) v = 1.0 / (c * b(i, j, 0) + c * b(i - 1, j, 0) + e(i, j + 1, 0) + e(i, j, 0));
+                else v = 1.0 / (c * b(i, j, 0) + c * b(i, j - 1, 0) + e(i + 1, j, 0) + e(i, j, 0));
+                return;
+            }
+            const Fab &xy = P.beta_ed[0], &xz = P.beta_ed[1], &yz = P.beta_ed[2];
+            if (d == 0)
+                v = 1.0 / (c * b(i, j, k) + c * b(i - 1, j, k) + xy(i, j, k) + xy(i, j + 1, k) + xz(i, j, k) + xz(i, j, k + 1));
+            else if (d == 1)
+                v = 1.0 / (c * b(i, j, k) + c * b(i, j - 1, k) + xy(i, j, k) + xy(i + 1, j, k) + yz(i, j, k) + yz(i, j, k + 1));
+            else
+                v = 1.0 / (c * b(i, j, k) + c * b(i, j, k - 1) + xz(i, j, k) + xz(i + 1, j, k) + yz(i, j, k) + yz(i, j + 1, k));
+        });
+    }
+}
+
+// visc_schur_complement (apply_precon.f90:538-685), the BFBt approximation
+static void visc_schur(const Problem& P, const lmm_knobs& K, Fab& rhs, Fab& x_out, double theta_alpha, const Fab& phi, int* pvc) {
+    const int dm = P.geo.dm;
+    Fab muinv[3], gphi[3], Lgphi[3];
+    inverse_diag_lap(P, muinv);
+    Fab phi_mu = make_cc(P.geo, 1);
+    phi_mu.setval(0.0);
+    macproject(P, K, phi_mu, muinv, rhs, pvc);
+    for (int d = 0; d < dm; ++d) {
+        gphi[d] = make_face(P.geo, d, 1);
+        Lgphi[d] = make_face(P.geo, d, 1);
+    }
+    compute_grad(P.geo, P.dx, phi_mu, gphi);
+    for (int d = 0; d < dm; ++d) {
+        for_valid(gphi[d], [&](double& v, int a, int b, int c) { v = v * muinv[d](a, b, c); });
+        fill_boundary(gphi[d]);
+    }
+    Level L0 = make_level0(P, 0.0);  // zero alpha
+    L0.gamma_cc.setval(0.0);
+    stag_applyop_level(L0, gphi, Lgphi, 0, P.visc_type);
+    for (int d = 0; d < dm; ++d) {
+        for_valid(Lgphi[d], [&](double& v, int a, int b, int c) { v = v * muinv[d](a, b, c); });
+        fill_boundary(Lgphi[d]);
+    }
+    compute_div(P.geo, P.dx, Lgphi, rhs);
+    phi_mu.setval(0.0);
+    macproject(P, K, phi_mu, muinv, rhs, pvc);
+    copy_valid(x_out, phi_mu);
+    if (std::fabs(theta_alpha) > 0.0) {
+        Fab phi_rho = phi;
+        scale_valid(phi_rho, theta_alpha);
+        for_valid(x_out, [&](double& v, int a, int b, int c) { v = v + phi_rho(a, b, c); });
+    }
+}
+
 void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, const Fab* b_u, const Fab& b_p,
                   Fab* x_u, Fab& x_p, int* vc, int* pvc) {
+    const bool bfbt = K.visc_schur_approx == 1;
     const int dm = P.geo.dm;
     const int pt = K.precon_type;
     const int av = std::abs(P.visc_type);
@@ -131,6 +196,10 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         for_valid(mac_rhs, [&](double& d, int a, int b, int c) { d = d + b_p(a, b, c); });
         macproject(P, K, phi, alphainv, mac_rhs, pvc);
         subtract_weighted_gradp(P, x_u, alphainv, phi);
+        if (bfbt) {
+            visc_schur(P, K, mac_rhs, x_p, theta_alpha, phi, pvc);
+            break;
+        }
         if (pt == 1 || theta_alpha == 0.0) {
             copy_valid(x_p, mac_rhs);
             scale_valid(x_p, -1.0);
@@ -157,7 +226,10 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         compute_div(P.geo, P.dx, x_u, mac_rhs);
         for_valid(mac_rhs, [&](double& d, int a, int b, int c) { d = d + b_p(a, b, c); });
         if (std::fabs(theta_alpha) > 0.0) macproject(P, K, phi, alphainv, mac_rhs, pvc);
-        simple_schur();
+        if (bfbt)
+            visc_schur(P, K, mac_rhs, x_p, theta_alpha, phi, pvc);
+        else
+            simple_schur();
         if (pt == -2 || pt == -5) scale_valid(x_p, -1.0);
         if (std::abs(pt) == 5) {
             copy_valid(x_p_tmp, x_p);
@@ -172,7 +244,10 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         copy_valid(mac_rhs, b_p);
         if (pt == -3) scale_valid(mac_rhs, -1.0);
         if (std::fabs(theta_alpha) > 0.0) macproject(P, K, phi, alphainv, mac_rhs, pvc);
-        simple_schur();
+        if (bfbt)
+            visc_schur(P, K, mac_rhs, x_p, theta_alpha, phi, pvc);
+        else
+            simple_schur();
         copy_valid(x_p_tmp, x_p);
         fill_boundary(x_p_tmp);
         for (int i = 0; i < dm; ++i) copy_valid(b_u_tmp[i], b_u[i]);
@@ -185,6 +260,12 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         if (std::fabs(theta_alpha) > 0.0) {
             copy_valid(mac_rhs, b_p);
             macproject(P, K, phi, alphainv, mac_rhs, pvc);
+        }
+        if (bfbt) {
+            // mac_rhs holds b_p whenever the reference sets it (apply_precon.f90:362-366)
+            copy_valid(mac_rhs, b_p);
+            visc_schur(P, K, mac_rhs, x_p, theta_alpha, phi, pvc);
+            break;
         }
         if (std::fabs(theta_alpha) > 0.0) scale_valid(phi, theta_alpha);
         copy_valid(x_p, b_p);

@@ -89,6 +89,6 @@ def test_create_rejects_bad_arguments_without_gpu(lib):
     g.bc_lo[0] = 0  # not periodic
     assert lib.lmm_stokes_create(C.byref(g), C.byref(k), 0, C.byref(h)) == abi.LMM_ERR_INVALID
     g = abi.make_grid(2, (96, 96), 1.0 / 96)
-    k = abi.make_knobs(visc_schur_approx=1)  # BFBt Schur approximation: not built
+    k = abi.make_knobs(visc_schur_approx=1, visc_type=3)  # inverse_diag_lap has no |visc_type| = 3
     assert lib.lmm_stokes_create(C.byref(g), C.byref(k), 0, C.byref(h)) == abi.LMM_ERR_INVALID
     assert lib.lmm_strerror(abi.LMM_ERR_BREAKDOWN) == b"gmres: error in orthogonalization"

@@ -449,3 +449,36 @@ def test_fgmres_classical_gram_schmidt(oracle, precision):
     assert abs(outs[0][0] - outs[1][0]) <= 1
     for c in range(3):
         assert np.linalg.norm(outs[1][1][c] - outs[0][1][c]) <= 1e-8 * np.linalg.norm(outs[0][1][c])
+
+
+# ---------------------------------------------------------------- BFBt Schur approximation
+@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
+@pytest.mark.parametrize("pt", [1, 2, -2, 3, 4, 5])
+@pytest.mark.parametrize("theta", [0.0, 30.0])
+@pytest.mark.parametrize("visc", [-1, -2, 2])
+def test_apply_precon_bfbt(oracle, dm, n, pt, theta, visc):
+    """visc_schur_approx = 1: the BFBt Schur approximation of
+    visc_schur_complement (two inverse-viscosity-weighted pressure solves
+    around D M L M G) against the oracle."""
+    p, rng = random_problem(dm, n, 37, visc, theta=theta)
+    k = oracle.default_knobs(visc_type=visc, precon_type=pt, visc_schur_approx=1)
+    s = make_solver(p, visc_type=visc, precon_type=pt, visc_schur_approx=1)
+    bu = [rng.standard_normal(p.shape) for _ in range(dm)]
+    bpp = rng.standard_normal(p.shape)
+    ref_u, ref_p = oracle.apply_precon(p, k, bu, bpp)
+    xu = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    xp = dev(np.zeros(p.shape))
+    s.apply_precon([dev(a) for a in bu], dev(bpp), xu, xp)
+    scale = max(np.abs(r).max() for r in ref_u + [ref_p])
+    for c in range(dm):
+        np.testing.assert_allclose(host(xu[c]), ref_u[c], rtol=0, atol=1e-12 * scale)
+    np.testing.assert_allclose(host(xp), ref_p, rtol=0, atol=1e-12 * scale)
+    s.close()
+
+
+@pytest.mark.parametrize("pt", [1, 2])
+def test_gmres_parity_bfbt(oracle, pt):
+    prob = synth.make_problem(2, 32, 100.0, 41, theta_alpha=50.0)
+    ref, got = _solve_both(oracle, prob, precon_type=pt, visc_type=-2, visc_schur_approx=1)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
