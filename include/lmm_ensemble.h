@@ -9,7 +9,9 @@
  * layout (lmm_fields_in / lmm_fields_out), already written when the call
  * starts.  Per instance: status (as lmm_stokes_solve) and stats.  Returns
  * the most negative instance status, or LMM_OK.  Several GPUs: call it once
- * per device with that device's share of the instances. */
+ * per device with that device's share of the instances.  Four workers with
+ * spinning host waits (knobs->host_wait = 0) measured fastest on B200 for
+ * 2D grids of 32^2..256^2; blocking waits and more workers were slower. */
 #ifndef LMM_ENSEMBLE_H
 #define LMM_ENSEMBLE_H
 

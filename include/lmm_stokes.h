@@ -119,7 +119,9 @@ typedef struct lmm_knobs {
                                       than the V-cycle gains at 128^3) */
     int    orthogonalization;      /* FGMRES: 0 = modified Gram-Schmidt (the reference's), 1 =
                                       classical Gram-Schmidt, all projections in one pass */
-    int    reserved[2];
+    int    host_wait;              /* 0 = the host spins on the stream when it reads a scalar (lowest
+                                      latency), 1 = it blocks (many host threads driving solvers) */
+    int    reserved[1];
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

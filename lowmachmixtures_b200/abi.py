@@ -85,7 +85,8 @@ _KNOB_FIELDS = [
     ("smoother_fusion", C.c_int),
     ("l2_persist", C.c_int),
     ("orthogonalization", C.c_int),
-    ("reserved", C.c_int * 2),
+    ("host_wait", C.c_int),
+    ("reserved", C.c_int * 1),
 ]
 
 
@@ -108,7 +109,7 @@ KNOB_DEFAULTS = dict(
     gmres_rel_tol=1e-9, gmres_abs_tol=0.0, gmres_verbose=1, gmres_max_outer=20,
     gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1,
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
-    tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0, orthogonalization=0,
+    tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0, orthogonalization=0, host_wait=0,
 )
 
 

@@ -124,6 +124,7 @@ struct lmm_handle {
     // statistics
     int vcycles = 0, pvcycles = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t wait_ev = nullptr;  // knobs.host_wait = 1: host waits block instead of spinning
     bool coeffs_loaded = false;
     double theta_loaded = 0.0;
     // captured preconditioner applications: (input, output, theta, precision)
@@ -156,6 +157,15 @@ struct lmm_handle {
 };
 
 namespace {
+
+// wait for the handle's stream: spin (default, lowest latency) or block the
+// thread (knobs.host_wait = 1; many host threads driving solvers at once)
+cudaError_t host_wait(lmm_handle* h) {
+    if (!h->wait_ev) return cudaStreamSynchronize(h->stream);
+    cudaError_t e = cudaEventRecord(h->wait_ev, h->stream);
+    if (e != cudaSuccess) return e;
+    return cudaEventSynchronize(h->wait_ev);
+}
 
 int64_t level_cells(const int n[3], int dm, int lev) {
     int64_t c = 1;
@@ -329,7 +339,7 @@ void stokes_norm(lmm_handle* h, const SVec& a, int slot) { stokes_dot(h, a, a, s
 
 double read_slot(lmm_handle* h, int slot, int idx) {
     LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(slot), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    LMM_CK(cudaStreamSynchronize(h->stream));
+    LMM_CK(host_wait(h));
     return h->hscal[idx];
 }
 
@@ -522,7 +532,7 @@ void stag_mg_solver(lmm_handle* h) {
         mg_resid_inf<T>(h, L[0], s0);
         double r0[3] = {0, 0, 0};
         LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(s0), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         bool all_zero = true, any_zero = false;
         for (int d = 0; d < dm; ++d) {
             r0[d] = h->hscal[d];
@@ -539,7 +549,7 @@ void stag_mg_solver(lmm_handle* h) {
                 vcycle<T>(h, L);
                 mg_resid_inf<T>(h, L[0], s1);
                 LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(s1), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-                LMM_CK(cudaStreamSynchronize(h->stream));
+                LMM_CK(host_wait(h));
                 bool done = true;
                 for (int d = 0; d < dm; ++d) done = done && (h->hscal[d] / r0[d] < K.stag_mg_rel_tol);
                 if (done) break;
@@ -957,7 +967,7 @@ void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
     }
     stokes_norm(h, h->w, i + 1);
     LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
-    LMM_CK(cudaStreamSynchronize(h->stream));
+    LMM_CK(host_wait(h));
     col.assign(i + 2, 0.0);
     for (int k = 1; k <= i; ++k) col[k] = h->hscal[8 * k + 4];
     col[i + 1] = h->hscal[8 * (i + 1) + 5];
@@ -985,7 +995,7 @@ void arnoldi_column_cgs(lmm_handle* h, int i, std::vector<double>& col) {
     }
     stokes_norm(h, h->w, i + 1);
     LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
-    LMM_CK(cudaStreamSynchronize(h->stream));
+    LMM_CK(host_wait(h));
     col.assign(i + 2, 0.0);
     for (int k = 1; k <= i; ++k) col[k] = h->hscal[8 * k + 4];
     col[i + 1] = h->hscal[8 * (i + 1) + 5];
@@ -1030,7 +1040,7 @@ int run_gmres(lmm_handle* h, double* theta_alpha, double* norm_pre_rhs, lmm_stat
         h->vcycles = vtemp;
         stokes_norm(h, h->r, 1);
         LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         const double norm_resid_Stokes = h->hscal[5];
         const double norm_resid = h->hscal[8 + 5];
         if (!std::isfinite(norm_resid) || !std::isfinite(norm_resid_Stokes)) return LMM_ERR_NONFINITE;
@@ -1382,6 +1392,7 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         LMM_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         LMM_CK(cudaEventCreate(&h->ev0));
         LMM_CK(cudaEventCreate(&h->ev1));
+        if (k->host_wait == 1) LMM_CK(cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming));
         h->arena_bytes = plan_bytes(*g, *k, h->nlev, h->nlev_p);
         LMM_CK(cudaMalloc(&h->arena, h->arena_bytes));
         LMM_CK(cudaMemset(h->arena, 0, h->arena_bytes));
@@ -1435,7 +1446,7 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         h->stage_elems = st;
         h->stage = h->alloc<double>(st);
         LMM_CK(cudaMallocHost(&h->hscal, 8 * sizeof(double) * lmm_handle::kSlots));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
     } catch (const LmmError& e) {
         lmm_stokes_destroy(h);
         return e.code;
@@ -1454,6 +1465,7 @@ int lmm_stokes_destroy(lmm_handle* h) {
     if (h->hscal) cudaFreeHost(h->hscal);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->wait_ev) cudaEventDestroy(h->wait_ev);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LMM_OK;
@@ -1543,7 +1555,7 @@ extern "C" int lmm_stokes_solve_device(lmm_handle* h, const lmm_fields_in* in, l
             LMM_CK(cudaMemcpyAsync(out->x_p, h->x.p(), h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         }
         LMM_CK(cudaEventRecord(h->ev1, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         if (st) {
             float ms = 0;
             cudaEventElapsedTime(&ms, h->ev0, h->ev1);
@@ -1598,7 +1610,7 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
         upload(in->beta, L0.beta, lay, in->ng_beta, nod_cell);
         for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) upload(in->beta_ed[e], L0.bed[e], lay, in->ng_beta_ed, nod_edge[e]);
         if (in->gamma) upload(in->gamma, L0.gamma, lay, in->ng_gamma, nod_cell);
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         auto t1 = std::chrono::steady_clock::now();
         lmm_fields_in din{};
         for (int d = 0; d < 3; ++d) {
@@ -1625,13 +1637,13 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
                     launch_scatter_boxlib(D, nodal, ng, src, h->stage, h->stream);
                     check_launch();
                     LMM_CK(cudaMemcpyAsync(dst, h->stage, sz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-                    LMM_CK(cudaStreamSynchronize(h->stream));
+                    LMM_CK(host_wait(h));
                 }
             };
             for (int d = 0; d < dm; ++d) download(h->x.c(d), out->x_u[d], out->layout, out->ng_x_u, nod_face[d]);
             download(h->x.p(), out->x_p, out->layout, out->ng_x_p, nod_cell);
         }
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         auto t2 = std::chrono::steady_clock::now();
         if (st) {
             float ms = 0;
@@ -1694,7 +1706,7 @@ extern "C" int lmm_op_load_coeffs(lmm_handle* h, const lmm_fields_in* c, double 
         const double* al[3] = {c->alpha_fc[0], c->alpha_fc[1], c->alpha_fc[2]};
         const double* bed[3] = {c->beta_ed[0], c->beta_ed[1], c->beta_ed[2]};
         load_coeffs(h, al, c->beta, bed, c->gamma, theta_alpha);
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1707,7 +1719,7 @@ extern "C" int lmm_op_stag_applyop(lmm_handle* h, const double* const phi[3], do
         if (color < 0 || color > 2 * h->dm) return LMM_ERR_INVALID;
         launch_applyop<double>(h->L64[0], h->knobs.visc_type, phi, Lphi, h->stream, color);
         check_launch();
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1728,7 +1740,7 @@ extern "C" int lmm_op_apply_matrix(lmm_handle* h, const double* const x_u[3], co
         for (int d = 0; d < dm; ++d)
             LMM_CK(cudaMemcpyAsync(b_u[d], h->tmp.c(d), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(cudaMemcpyAsync(b_p, h->tmp.p(), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1754,7 +1766,7 @@ extern "C" int lmm_op_apply_precon(lmm_handle* h, const double* const b_u[3], co
         for (int d = 0; d < dm; ++d)
             LMM_CK(cudaMemcpyAsync(x_u[d], h->w.c(d), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(cudaMemcpyAsync(x_p, h->w.p(), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1772,7 +1784,7 @@ extern "C" int lmm_op_stag_mg_solver(lmm_handle* h, const double* const rhs[3], 
         stag_mg_solver<double>(h);
         for (int d = 0; d < h->dm; ++d)
             LMM_CK(cudaMemcpyAsync(phi[d], L0.phi[d], h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1798,7 +1810,7 @@ extern "C" int lmm_op_smooth(lmm_handle* h, int lev, const double* const rhs[3],
             for (int d = 0; d < h->dm; ++d)
                 LMM_CK(cudaMemcpyAsync(phi[d], L.phi[d], L.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         }
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1811,7 +1823,7 @@ extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* co
     try {
         launch_residual_restrict<double>(h->L64[lev], h->L64[lev + 1], h->knobs.visc_type, rhs, phi, rhs_coarse, h->stream);
         check_launch();
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1823,7 +1835,7 @@ extern "C" int lmm_op_prolong_add(lmm_handle* h, int lev, const double* const ph
     try {
         launch_prolong_add<double>(h->L64[lev], h->L64[lev + 1], phi_coarse, phi_fine, h->stream);
         check_launch();
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;
@@ -1838,7 +1850,7 @@ extern "C" int lmm_op_inner_prod(lmm_handle* h, const double* const a_u[3], cons
         const double* b[4] = {b_u[0], b_u[1], h->dm == 3 ? b_u[2] : nullptr, b_p};
         stokes_reduce(h, 0, a, b, 2);
         LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(2), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         for (int c = 0; c <= h->dm; ++c) out_host[c] = h->hscal[c];
         return LMM_OK;
     } catch (const LmmError& e) {
@@ -1853,7 +1865,7 @@ extern "C" int lmm_op_sum_umac_press(lmm_handle* h, const double* const u[3], co
         const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
         stokes_reduce(h, 1, a, b, 2);
         LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(2), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         double tv = 1.0;
         for (int d = 0; d < h->dm; ++d) tv *= (double)h->grid.n[d];
         out_host[0] = h->hscal[h->dm] / tv;
@@ -1963,7 +1975,7 @@ extern "C" int lmm_learned_make_pairs(lmm_handle* h, unsigned long long seed, in
             launch_target(h->D0, h->le.base, h->L64[0].beta, h->slot(S1), h->slot(S3), h->grid.dx, t_out + (int64_t)q * h->n * 4, h->stream);
             check_launch();
         }
-        LMM_CK(cudaStreamSynchronize(h->stream));
+        LMM_CK(host_wait(h));
         return LMM_OK;
     } catch (const LmmError& e) {
         return e.code;

@@ -140,16 +140,27 @@ def main():
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--rel-tol", type=float, default=1e-8)
     ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--host-wait", type=int, default=0, help="0: worker threads spin on their streams (1: block)")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        # whole instances per rank (no collective on the data path); only the
+        # per-rank results are gathered at the end
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     sizes = instance_sizes(a.count)
     mine = shard([n * n for n in sizes], world)[rank]
     allp = make_instances(a.count)
     probs = [allp[i] for i in mine]
     kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
-                        gmres_rel_tol=a.rel_tol)
+                        orthogonalization=1, gmres_rel_tol=a.rel_tol, host_wait=a.host_wait)
     from . import _native
     lib = _native.load()
     import time
@@ -158,6 +169,8 @@ def main():
     create_s = time.perf_counter() - t0
     best = None
     for _ in range(a.repeats):
+        if dist is not None:
+            dist.barrier()
         st, stats, _, secs = ens.run(probs)
         best = secs if best is None else min(best, secs)
     ens.close()
@@ -172,7 +185,17 @@ def main():
                iterations_mean=float(np.mean([s["total_iter"] for s in ok])) if ok else None,
                max_true_rel_residual=float(max(s["norm_resid_true"] / s["norm_b"] for s in ok)) if ok else None,
                sizes={int(n): int(sum(1 for p in probs if p.n[0] == n)) for n in sorted(set(p.n[0] for p in probs))})
-    print(json.dumps(out), flush=True)
+    if dist is None:
+        print(json.dumps(out), flush=True)
+        return
+    outs = [None] * world
+    dist.all_gather_object(outs, out)
+    if rank == 0:
+        slowest = max(o["seconds"] for o in outs)
+        print(json.dumps(dict(ranks=world, instances=sum(o["instances"] for o in outs), seconds=slowest,
+                              instances_per_s=sum(o["instances"] for o in outs) / slowest,
+                              failed=sum(o["failed"] for o in outs), per_rank=outs)), flush=True)
+    dist.destroy_process_group()
 
 
 if __name__ == "__main__":
