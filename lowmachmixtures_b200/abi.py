@@ -21,6 +21,8 @@ LMM_ERR_NO_DEVICE = -6
 LMM_ERR_TOO_LARGE = -7
 
 LMM_BC_PERIODIC = -1
+LMM_BC_NO_SLIP_WALL = 100
+LMM_BC_SLIP_WALL = 200
 LMM_LAYOUT_COMPACT = 0
 LMM_LAYOUT_BOXLIB = 1
 LMM_METHOD_GMRES = 0
@@ -197,16 +199,46 @@ class EnsembleItem(C.Structure):
     ]
 
 
-def make_grid(dm: int, n, dx: float) -> Grid:
+def make_grid(dm: int, n, dx: float, bc=None) -> Grid:
+    """bc: None (periodic box) or one entry per direction, either a code
+    (both sides) or a (lo, hi) pair of codes (LMM_BC_PERIODIC,
+    100-103 no-slip walls, 200-203 slip walls)."""
     g = Grid()
     g.dm = dm
     nn = list(n) + [1] * (3 - len(n))
     for d in range(3):
         g.n[d] = int(nn[d]) if d < dm else 1
-        g.bc_lo[d] = LMM_BC_PERIODIC
-        g.bc_hi[d] = LMM_BC_PERIODIC
+        lo = hi = LMM_BC_PERIODIC
+        if bc is not None and d < dm:
+            b = bc[d]
+            lo, hi = (b, b) if isinstance(b, int) else (int(b[0]), int(b[1]))
+        g.bc_lo[d] = lo
+        g.bc_hi[d] = hi
     g.dx = float(dx)
     return g
+
+
+def walled(bc, d: int) -> bool:
+    """True when direction d of a make_grid-style bc spec has walls."""
+    if bc is None:
+        return False
+    b = bc[d]
+    lo = b if isinstance(b, int) else b[0]
+    return lo != LMM_BC_PERIODIC
+
+
+def edge_nodal(dm: int, e: int):
+    """Directions in which edge array e is nodal: 2D (x, y); 3D xy, xz, yz."""
+    if dm == 2:
+        return (0, 1)
+    return ((0, 1), (0, 2), (1, 2))[e]
+
+
+def edge_shape(dm: int, n, bc, e: int):
+    """Compact (z, y, x) shape of edge array e: n+1 nodes along a
+    wall-bounded direction in which the edge is nodal, n otherwise."""
+    ext = [int(n[d]) + (1 if (d in edge_nodal(dm, e) and walled(bc, d)) else 0) for d in range(dm)]
+    return tuple(reversed(ext))
 
 
 def ptr(a) -> "C.POINTER(C.c_double) | None":

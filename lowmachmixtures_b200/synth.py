@@ -1,7 +1,7 @@
 """Seeded synthetic Stokes problems with the shapes of the benchmark workloads.
 
 The reference benchmarks nothing and ships no input data, so every workload
-is synthetic (periodic box, one grid, isotropic dx = 1/n):
+is synthetic (one grid, isotropic dx = 1/n, periodic unless walls are asked for):
 
 * log-viscosity field g(x) = sum_{m=1..6} cos(2 pi k_m . x + phi_m) with integer
   wave vectors 0 < |k_m| <= 4 and phases phi_m ~ U[0, 2 pi), normalised to
@@ -16,7 +16,10 @@ is synthetic (periodic box, one grid, isotropic dx = 1/n):
   b_p = 0, zero initial guess.
 
 Arrays are numpy float64 in the compact layout: shape (ny, nx) in 2D or
-(nz, ny, nx) in 3D, i fastest, periodic seam stored once.
+(nz, ny, nx) in 3D, i fastest, periodic seam stored once.  Along a
+wall-bounded direction the wall-normal face array keeps faces lo..hi (face
+lo is the wall, zero in every rhs; hi+1 is implied zero) and an edge array
+nodal in that direction keeps all n+1 nodes.
 """
 from __future__ import annotations
 
@@ -40,6 +43,7 @@ class StokesProblem:
     b_p: np.ndarray
     contrast: float
     seed: int
+    bc: tuple = None
 
     @property
     def shape(self):
@@ -67,13 +71,14 @@ def _logfield(ks, phases, coords):
     return g
 
 
-def _grids(n, dm, offsets):
+def _grids(n, dm, offsets, extra=(0, 0, 0)):
     """Coordinates (x, y[, z]) broadcast to the compact array shape, with
-    per-direction offsets in units of dx (0 = nodal, 0.5 = cell centred)."""
+    per-direction offsets in units of dx (0 = nodal, 0.5 = cell centred) and
+    `extra` points past the last (the hi wall node of a wall-bounded edge)."""
     dx = 1.0 / n[0]
     axes = []
     for d in range(dm):
-        axes.append((np.arange(n[d]) + offsets[d]) * dx)
+        axes.append((np.arange(n[d] + extra[d]) + offsets[d]) * dx)
     if dm == 2:
         y, x = np.meshgrid(axes[1], axes[0], indexing="ij")
         return [x, y]
@@ -81,19 +86,24 @@ def _grids(n, dm, offsets):
     return [x, y, z]
 
 
-def viscosity_fields(dm, n, contrast, seed):
-    """beta at cells and beta_ed at nodes (2D) / edges xy, xz, yz (3D)."""
+def viscosity_fields(dm, n, contrast, seed, bc=None):
+    """beta at cells and beta_ed at nodes (2D) / edges xy, xz, yz (3D);
+    edges keep the hi wall node along wall-bounded directions."""
+    from .abi import edge_nodal, walled
     rng = np.random.Generator(np.random.PCG64(seed))
     ks = _wave_vectors(rng, dm)
     phases = rng.uniform(0.0, 2.0 * math.pi, size=len(ks))
     cc = _logfield(ks, phases, _grids(n, dm, [0.5] * dm))
+
+    def extra(e):
+        return tuple(1 if (d < dm and d in edge_nodal(dm, e) and walled(bc, d)) else 0 for d in range(3))
     if dm == 2:
-        eds = [_logfield(ks, phases, _grids(n, dm, [0.0, 0.0]))]
+        eds = [_logfield(ks, phases, _grids(n, dm, [0.0, 0.0], extra(0)))]
     else:
         eds = [
-            _logfield(ks, phases, _grids(n, dm, [0.0, 0.0, 0.5])),  # xy edges
-            _logfield(ks, phases, _grids(n, dm, [0.0, 0.5, 0.0])),  # xz edges
-            _logfield(ks, phases, _grids(n, dm, [0.5, 0.0, 0.0])),  # yz edges
+            _logfield(ks, phases, _grids(n, dm, [0.0, 0.0, 0.5], extra(0))),  # xy edges
+            _logfield(ks, phases, _grids(n, dm, [0.0, 0.5, 0.0], extra(1))),  # xz edges
+            _logfield(ks, phases, _grids(n, dm, [0.5, 0.0, 0.0], extra(2))),  # yz edges
         ]
     gmax = max(np.abs(cc).max(), *[np.abs(e).max() for e in eds])
     s = math.log(contrast) / 2.0 / gmax
@@ -102,20 +112,37 @@ def viscosity_fields(dm, n, contrast, seed):
     return beta, beta_ed, rng
 
 
+def zero_wall_faces(dm: int, bc, u):
+    """Zero face lo of each wall-normal component along its wall-bounded
+    direction (in place; u in the compact (z, y, x) layout)."""
+    from .abi import walled
+    for c in range(dm):
+        if walled(bc, c):
+            idx = [slice(None)] * dm
+            idx[dm - 1 - c] = 0
+            u[c][tuple(idx)] = 0.0
+    return u
+
+
 def make_problem(dm: int, n: int, contrast: float, seed: int, theta_alpha: float = 0.0,
-                 gamma_value: float = 0.0) -> StokesProblem:
+                 gamma_value: float = 0.0, bc=None) -> StokesProblem:
+    """bc: None (periodic) or per direction a code / (lo, hi) pair as in
+    abi.make_grid; the rhs is zero on the wall faces."""
     nn = (n,) * dm
-    beta, beta_ed, rng = viscosity_fields(dm, nn, contrast, seed)
+    beta, beta_ed, rng = viscosity_fields(dm, nn, contrast, seed, bc)
     shape = tuple(reversed(nn))
     b_u = []
     for _ in range(dm):
         r = rng.standard_normal(size=shape)
         b_u.append(np.ascontiguousarray(r - r.mean()))
+    if bc is not None:
+        bc = tuple(bc)
+        zero_wall_faces(dm, bc, b_u)
     return StokesProblem(
         dm=dm, n=nn + (1,) * (3 - dm), dx=1.0 / n, theta_alpha=float(theta_alpha),
         alpha_fc=[np.ones(shape) for _ in range(dm)], beta=beta, beta_ed=beta_ed,
         gamma=np.full(shape, float(gamma_value)), b_u=b_u, b_p=np.zeros(shape),
-        contrast=float(contrast), seed=int(seed))
+        contrast=float(contrast), seed=int(seed), bc=bc)
 
 
 # Named workloads (the parity and benchmark configurations).

@@ -29,7 +29,55 @@ Geo geo_of(const lmm_grid* g) {
     G.n[0] = g->n[0];
     G.n[1] = g->n[1];
     G.n[2] = (g->dm == 3) ? g->n[2] : 1;
+    for (int d = 0; d < 3; ++d) {
+        G.bc_lo[d] = (d < g->dm) ? g->bc_lo[d] : LMM_BC_PERIODIC;
+        G.bc_hi[d] = (d < g->dm) ? g->bc_hi[d] : LMM_BC_PERIODIC;
+    }
     return G;
+}
+
+// BoxLib-layout output of a wall-bounded problem: the valid region, then
+// every ghost index mapped direction by direction -- periodic: its image;
+// wall, face component normal to it: zero (the wall face hi+1 too); wall,
+// otherwise: the nearest valid entry, negated for a transverse velocity at a
+// no-slip wall.  kind: face component c (0..2) or -1 for cells.
+void boxlib_from_fab_walls(double* dst, int dst_ng, const Fab& f, const Geo& G, int kind) {
+    int slo[3], shi[3];
+    for (int d = 0; d < 3; ++d) {
+        int g = (d < f.dm) ? dst_ng : 0;
+        slo[d] = f.vlo[d] - g;
+        shi[d] = f.vhi[d] + g;
+    }
+    long sy = shi[0] - slo[0] + 1, sz = sy * (shi[1] - slo[1] + 1);
+    for (int k = slo[2]; k <= shi[2]; ++k)
+        for (int j = slo[1]; j <= shi[1]; ++j)
+            for (int i = slo[0]; i <= shi[0]; ++i) {
+                int idx[3] = {i, j, k};
+                double sgn = 1.0;
+                for (int d = 0; d < f.dm; ++d) {
+                    const int n = f.n[d];
+                    int& v = idx[d];
+                    if (f.per[d]) {
+                        v = wrap_to_valid(v, n, f.nodal[d]);
+                        continue;
+                    }
+                    if (kind == d) {
+                        if (v <= 0 || v >= n) sgn = 0.0;
+                        v = (v < 0) ? 0 : (v > n - 1 ? n - 1 : v);
+                        continue;
+                    }
+                    const bool slip_lo = bc_is_slip(G.bc_lo[d]), slip_hi = bc_is_slip(G.bc_hi[d]);
+                    if (v < 0) {
+                        v = 0;
+                        if (kind >= 0 && !slip_lo) sgn = -sgn;
+                    } else if (v > n - 1 + f.nodal[d]) {
+                        v = n - 1 + f.nodal[d];
+                        if (kind >= 0 && !slip_hi) sgn = -sgn;
+                    }
+                }
+                double v = (sgn == 0.0) ? 0.0 : f(idx[0], idx[1], idx[2]);
+                dst[(i - slo[0]) + sy * (j - slo[1]) + sz * (k - slo[2])] = (sgn < 0.0) ? -v : v;
+            }
 }
 
 // copy a BoxLib array (ghost width src_ng, same nodality) into f (any ng):
@@ -98,11 +146,32 @@ bool build_problem(const lmm_grid* g, int visc_type, const lmm_fields_in* in, Pr
     return true;
 }
 
+// per direction: both sides periodic, or both walls (no-slip 100-103 or
+// slip 200-203, bc.f90:23-35)
 bool valid_grid(const lmm_grid* g) {
     if (!g || (g->dm != 2 && g->dm != 3)) return false;
-    for (int d = 0; d < g->dm; ++d)
-        if (g->n[d] < 2 || g->bc_lo[d] != LMM_BC_PERIODIC || g->bc_hi[d] != LMM_BC_PERIODIC) return false;
+    auto wall = [](int c) { return bc_is_noslip(c) || bc_is_slip(c); };
+    for (int d = 0; d < g->dm; ++d) {
+        if (g->n[d] < 2) return false;
+        const bool per = g->bc_lo[d] == LMM_BC_PERIODIC && g->bc_hi[d] == LMM_BC_PERIODIC;
+        if (!per && !(wall(g->bc_lo[d]) && wall(g->bc_hi[d]))) return false;
+    }
     return g->dx > 0.0;
+}
+
+// zero the wall faces of a face array (the wall-normal component on its
+// wall-bounded direction: faces lo and hi+1)
+void zero_wall_faces(const Geo& G, Fab* u) {
+    for (int c = 0; c < G.dm; ++c) {
+        if (G.periodic(c)) continue;
+        Fab& f = u[c];
+        for (int k = f.vlo[2]; k <= f.vhi[2]; ++k)
+            for (int j = f.vlo[1]; j <= f.vhi[1]; ++j)
+                for (int i = f.vlo[0]; i <= f.vhi[0]; ++i) {
+                    const int idx[3] = {i, j, k};
+                    if (idx[c] == 0 || idx[c] == G.n[c]) f(i, j, k) = 0.0;
+                }
+    }
 }
 
 void faces_from_compact(const Geo& G, Fab* f, const double* const* src, int ng) {
@@ -179,6 +248,7 @@ int orc_stokes_solve(const lmm_grid* g, const lmm_knobs* k, const lmm_fields_in*
     if (!valid_grid(g) || !k || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
     if (k->visc_schur_approx != 0 && k->visc_schur_approx != 1) return LMM_ERR_INVALID;
     if (k->visc_schur_approx == 1 && std::abs(k->visc_type) == 3) return LMM_ERR_INVALID;  // inverse_diag_lap.f90:135,246
+    if (k->visc_schur_approx == 1 && geo_of(g).any_wall()) return LMM_ERR_INVALID;  // BFBt: periodic only here
     int apt = std::abs(k->precon_type);
     if (apt < 1 || apt > 5) return LMM_ERR_INVALID;
     if (st) std::memset(st, 0, sizeof(*st));
@@ -196,21 +266,35 @@ int orc_stokes_solve(const lmm_grid* g, const lmm_knobs* k, const lmm_fields_in*
     load(b.p, in->b_p, in->layout, in->ng_b_p);
     x.p = make_cc(G, 1);
     load(x.p, out->x_p, out->layout, out->ng_x_p);
+    // wall-normal velocities on the walls are not unknowns: the rhs there is
+    // taken as zero (the reference's preconditioner zeroes them in every
+    // correction, so they only ever enter its true-residual check)
+    zero_wall_faces(G, b.u);
     auto t0 = std::chrono::steady_clock::now();
     int status = (k->method == LMM_METHOD_FGMRES) ? fgmres(P, *k, b, x, theta_alpha, norm_pre_rhs, st)
                                                   : gmres(P, *k, b, x, theta_alpha, norm_pre_rhs, st);
     auto t1 = std::chrono::steady_clock::now();
     if (st) st->solve_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    const bool walls = G.any_wall();
+    if (walls) zero_wall_faces(G, x.u);
     for (int i = 0; i < G.dm; ++i) {
-        if (out->layout == LMM_LAYOUT_BOXLIB)
-            boxlib_from_fab(out->x_u[i], out->ng_x_u, x.u[i]);
-        else
+        if (out->layout == LMM_LAYOUT_BOXLIB) {
+            if (walls)
+                boxlib_from_fab_walls(out->x_u[i], out->ng_x_u, x.u[i], G, i);
+            else
+                boxlib_from_fab(out->x_u[i], out->ng_x_u, x.u[i]);
+        } else {
             compact_from_fab(out->x_u[i], x.u[i]);
+        }
     }
-    if (out->layout == LMM_LAYOUT_BOXLIB)
-        boxlib_from_fab(out->x_p, out->ng_x_p, x.p);
-    else
+    if (out->layout == LMM_LAYOUT_BOXLIB) {
+        if (walls)
+            boxlib_from_fab_walls(out->x_p, out->ng_x_p, x.p, G, -1);
+        else
+            boxlib_from_fab(out->x_p, out->ng_x_p, x.p);
+    } else {
         compact_from_fab(out->x_p, x.p);
+    }
     return status;
 }
 
@@ -223,6 +307,7 @@ int orc_stag_applyop(const lmm_grid* g, int visc_type, const lmm_fields_in* c, d
     Level L0 = make_level0(P, theta_alpha);
     Fab ph[3], L[3];
     faces_from_compact(P.geo, ph, phi, 1);
+    fill_vel(P.geo, ph);
     for (int i = 0; i < P.geo.dm; ++i) {
         L[i] = make_face(P.geo, i, 1);
         fab_from_compact(L[i], Lphi[i]);  // untouched colours keep their input
@@ -260,9 +345,11 @@ int orc_smooth(const lmm_grid* g, const lmm_knobs* k, const lmm_fields_in* c, do
     Fab ph[3], r[3], Lp[3];
     faces_from_compact(G, ph, phi, 1);
     faces_from_compact(G, r, rhs, 0);
+    fill_vel(G, ph);
     for (int i = 0; i < G.dm; ++i) Lp[i] = make_face(G, i, 1);
     stag_applyop_level(lev[l], ph, Lp, color, k->visc_type);
     stag_mg_update(lev[l], ph, r, Lp, color, k->visc_type, k->stag_mg_omega);
+    fill_vel(G, ph);
     compact_from_faces(G, phi, ph);
     return 0;
 }
@@ -279,6 +366,7 @@ int orc_residual_restrict(const lmm_grid* g, const lmm_knobs* k, const lmm_field
     Fab ph[3], r[3], Lp[3], rc[3];
     faces_from_compact(G, ph, phi, 1);
     faces_from_compact(G, r, rhs, 0);
+    fill_vel(G, ph);
     for (int i = 0; i < G.dm; ++i) {
         Lp[i] = make_face(G, i, 1);
         rc[i] = make_face(Gc, i, 0);
@@ -292,9 +380,10 @@ int orc_residual_restrict(const lmm_grid* g, const lmm_knobs* k, const lmm_field
                     double v = L(i, jj, kk) - r[j](i, jj, kk);
                     L(i, jj, kk) = v * -1.0;
                 }
-        fill_boundary(L);
     }
+    fill_vel(G, Lp);
     stag_restriction(Gc, Lp, rc, false);
+    for (int j = 0; j < G.dm; ++j) physbc_domainvel(Gc, rc[j], j);
     compact_from_faces(Gc, rhs_c, rc);
     return 0;
 }
@@ -305,7 +394,9 @@ int orc_prolong_add(const lmm_grid* g, int l, const double* const phi_c[3], doub
     Fab pf[3], pc[3];
     faces_from_compact(G, pf, phi_f, 1);
     faces_from_compact(Gc, pc, phi_c, 1);
+    fill_vel(Gc, pc);
     stag_prolongation(G, pf, pc);
+    fill_vel(G, pf);
     compact_from_faces(G, phi_f, pf);
     return 0;
 }

@@ -16,7 +16,10 @@
 //     ((i+j+k) even) first, mg_nsmooths_down / _up sweeps, mg_nsmooths_bottom
 //     sweeps at the coarsest level;
 //   * piecewise-constant prolongation;
-//   * mg_max_vcycles V-cycles from phi = 0.
+//   * mg_max_vcycles V-cycles from phi = 0;
+//   * walls: homogeneous Neumann (the reference's BC_NEU for the pressure,
+//     define_bc_tower.f90:285-294) as a zero face coefficient on the wall
+//     faces, so no flux crosses them on any level.
 #include "oracle_internal.hpp"
 
 #include <vector>
@@ -114,7 +117,17 @@ void macproject(const Problem& P, const lmm_knobs& K, Fab& phi, const Fab* alpha
         L.rhs = make_cc(L.geo, 0);
         L.res = make_cc(L.geo, 0);
     }
-    for (int d = 0; d < dm; ++d) lev[0].a[d].a = alphainv_fc[d].a;
+    for (int d = 0; d < dm; ++d) {
+        lev[0].a[d].a = alphainv_fc[d].a;
+        if (P.geo.periodic(d)) continue;
+        Fab& a = lev[0].a[d];
+        for (int k = a.vlo[2]; k <= a.vhi[2]; ++k)
+            for (int j = a.vlo[1]; j <= a.vhi[1]; ++j)
+                for (int i = a.vlo[0]; i <= a.vhi[0]; ++i) {
+                    const int idx[3] = {i, j, k};
+                    if (idx[d] == 0 || idx[d] == P.geo.n[d]) a(i, j, k) = 0.0;
+                }
+    }
     for (int l = 1; l < nlev; ++l) {
         Fab tmpc[3], tmpf[3];
         for (int d = 0; d < dm; ++d) { tmpf[d] = lev[l - 1].a[d]; tmpc[d] = lev[l].a[d]; }
@@ -148,7 +161,7 @@ void macproject(const Problem& P, const lmm_knobs& K, Fab& phi, const Fab* alpha
     for (int k = phi.vlo[2]; k <= phi.vhi[2]; ++k)
         for (int j = phi.vlo[1]; j <= phi.vhi[1]; ++j)
             for (int i = phi.vlo[0]; i <= phi.vhi[0]; ++i) phi(i, j, k) = lev[0].phi(i, j, k);
-    fill_boundary(phi);
+    fill_pres(P.geo, phi);  // macproject.f90:302-306
     if (pressure_vcycles) *pressure_vcycles += K.mg_max_vcycles;
 }
 

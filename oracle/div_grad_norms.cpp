@@ -3,7 +3,8 @@
 //
 // TEST INFRASTRUCTURE ONLY (the oracle).  Restates
 //   src_common/div_and_grad.f90:16-455       (compute_grad, compute_div;
-//       periodic faces never take the 2/dx boundary stencil of :139-182)
+//       periodic faces never take the 2/dx boundary stencil of :139-182,
+//       wall faces -- pressure FOEXTRAP -- always do)
 //   src_gmres/norm_inner_product.f90:16-418  (stag_inner_prod, cc_inner_prod,
 //       stag_l2_norm, cc_l2_norm)
 //   src_gmres/norm_inner_product.f90:579-794 (sum_umac_press)
@@ -70,6 +71,18 @@ void compute_grad(const Geo& g, double dx, const Fab& phi, Fab* gradp) {
             for (int j = gp.vlo[1]; j <= gp.vhi[1]; ++j)
                 for (int i = gp.vlo[0]; i <= gp.vhi[0]; ++i)
                     gp(i, j, k) = (phi(i, j, k) - phi(i - o[0], j - o[1], k - o[2])) * dxinv;
+        if (g.periodic(d)) continue;
+        // the ghost value represents the boundary value (div_and_grad.f90:139-182)
+        const double twodxinv = 2.0 * dxinv;
+        for (int side = 0; side < 2; ++side) {
+            const int f = (side == 0) ? 0 : g.n[d];
+            int r0[3] = {gp.vlo[0], gp.vlo[1], gp.vlo[2]}, r1[3] = {gp.vhi[0], gp.vhi[1], gp.vhi[2]};
+            r0[d] = r1[d] = f;
+            for (int k = r0[2]; k <= r1[2]; ++k)
+                for (int j = r0[1]; j <= r1[1]; ++j)
+                    for (int i = r0[0]; i <= r1[0]; ++i)
+                        gp(i, j, k) = (phi(i, j, k) - phi(i - o[0], j - o[1], k - o[2])) * twodxinv;
+        }
     }
 }
 

@@ -9,7 +9,9 @@
 // (multifab_build_edge, n+1 valid faces), 3D edge arrays nodal in two
 // directions (stag_mg_solver.f90:181-193), periodic ghost filling
 // (multifab_fill_boundary) and the periodic nodal seam (valid faces lo and
-// hi+1 are periodic images of each other).
+// hi+1 are periodic images of each other).  A direction bounded by walls
+// (bc.f90:23-35: no-slip 100-103, slip 200-203) is not periodic: its ghost
+// cells are left to the physical-boundary fills (physbc.cpp).
 #pragma once
 #include <cstddef>
 #include <cstring>
@@ -20,7 +22,18 @@ namespace orc {
 struct Geo {
     int dm;
     int n[3];  // cells per direction; n[2] == 1 in 2D
+    // domain BC per direction and side (bc.f90 codes; -1 = periodic)
+    int bc_lo[3] = {-1, -1, -1};
+    int bc_hi[3] = {-1, -1, -1};
+    bool periodic(int d) const { return d >= dm || bc_lo[d] == -1; }
+    bool any_wall() const {
+        for (int d = 0; d < dm; ++d)
+            if (!periodic(d)) return true;
+        return false;
+    }
 };
+inline bool bc_is_noslip(int c) { return c >= 100 && c <= 103; }  // NO_SLIP_START..NO_SLIP_END
+inline bool bc_is_slip(int c) { return c >= 200 && c <= 203; }    // SLIP_START..SLIP_END
 
 struct Fab {
     int dm = 0;
@@ -29,6 +42,10 @@ struct Fab {
     int vlo[3] = {0, 0, 0}, vhi[3] = {0, 0, 0};  // valid index range (inclusive)
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};    // allocated range incl. ghosts
     int n[3] = {1, 1, 1};                        // cells per direction (period)
+    int per[3] = {1, 1, 1};                      // periodic directions
+    // compact storage of a wall-bounded nodal direction: edge arrays keep all
+    // n+1 nodes, face arrays keep lo..hi (the hi+1 wall face is zero)
+    bool edge = false;
     long sx = 1, sy = 1, sz = 1;
     std::vector<double> a;
 
@@ -41,6 +58,7 @@ struct Fab {
         for (int d = 0; d < 3; ++d) {
             nodal[d] = (d < dm) ? nod[d] : 0;
             n[d] = (d < dm) ? g.n[d] : 1;
+            per[d] = g.periodic(d) ? 1 : 0;
             vlo[d] = 0;
             vhi[d] = n[d] - 1 + nodal[d];
             int gd = (d < dm) ? ng : 0;
@@ -77,7 +95,9 @@ inline Fab make_edge(const Geo& g, int e, int ng) {
         if (e == 1) { nod[0] = 1; nod[1] = 0; nod[2] = 1; }
         if (e == 2) { nod[0] = 0; nod[1] = 1; nod[2] = 1; }
     }
-    return Fab(g, nod, ng);
+    Fab f(g, nod, ng);
+    f.edge = true;
+    return f;
 }
 
 // periodic image of index v in a direction with period n; nodal directions
@@ -93,27 +113,32 @@ inline int wrap_to_valid(int v, int n, int nodal) {
     return v;
 }
 
-// multifab_fill_boundary for a periodic single-box domain: every ghost value
-// is copied from its periodic image in the valid region.
+// multifab_fill_boundary on a single box: every ghost value whose periodic
+// image lies in the valid region is copied from it.  Ghost cells outside a
+// wall-bounded side have no such image and keep their contents.
 inline void fill_boundary(Fab& f) {
     if (f.ng == 0) return;
+    auto image = [&](int d, int v, int& out) {
+        if (v >= f.vlo[d] && v <= f.vhi[d]) { out = v; return true; }
+        if (!f.per[d] || d >= f.dm) return false;
+        out = wrap_to_valid(v, f.n[d], f.nodal[d]);
+        return true;
+    };
 #pragma omp parallel for schedule(static)
     for (int k = f.lo[2]; k <= f.hi[2]; ++k) {
-        bool kg = k < f.vlo[2] || k > f.vhi[2];
-        int kk = (f.dm == 3) ? wrap_to_valid(k, f.n[2], f.nodal[2]) : k;
+        int kk;
+        if (!image(2, k, kk)) continue;
+        const bool kg = k < f.vlo[2] || k > f.vhi[2];
         for (int j = f.lo[1]; j <= f.hi[1]; ++j) {
-            bool jg = j < f.vlo[1] || j > f.vhi[1];
-            int jj = wrap_to_valid(j, f.n[1], f.nodal[1]);
-            if (kg || jg) {
-                for (int i = f.lo[0]; i <= f.hi[0]; ++i) {
-                    int ii = wrap_to_valid(i, f.n[0], f.nodal[0]);
-                    f(i, j, k) = f(ii, jj, kk);
-                }
-            } else {
-                for (int i = f.lo[0]; i < f.vlo[0]; ++i)
-                    f(i, j, k) = f(wrap_to_valid(i, f.n[0], f.nodal[0]), j, k);
-                for (int i = f.vhi[0] + 1; i <= f.hi[0]; ++i)
-                    f(i, j, k) = f(wrap_to_valid(i, f.n[0], f.nodal[0]), j, k);
+            int jj;
+            if (!image(1, j, jj)) continue;
+            const bool jg = j < f.vlo[1] || j > f.vhi[1];
+            for (int i = f.lo[0]; i <= f.hi[0]; ++i) {
+                const bool ig = i < f.vlo[0] || i > f.vhi[0];
+                if (!(ig || jg || kg)) continue;
+                int ii;
+                if (!image(0, i, ii)) continue;
+                f(i, j, k) = f(ii, jj, kk);
             }
         }
     }
@@ -123,7 +148,7 @@ inline void fill_boundary(Fab& f) {
 // duplicated nodal entries take the value of the lowest-indexed copy.
 inline void internal_sync(Fab& f) {
     for (int d = 0; d < f.dm; ++d) {
-        if (!f.nodal[d]) continue;
+        if (!f.nodal[d] || !f.per[d]) continue;
         for (int k = f.vlo[2]; k <= f.vhi[2]; ++k)
             for (int j = f.vlo[1]; j <= f.vhi[1]; ++j)
                 for (int i = f.vlo[0]; i <= f.vhi[0]; ++i) {
@@ -136,24 +161,45 @@ inline void internal_sync(Fab& f) {
     }
 }
 
-// compact (unique periodic, i fastest) <-> fab conversions
+// entries per direction of the compact layout: n (periodic; a wall-bounded
+// face direction, whose hi+1 wall face is implied zero), n+1 (an edge array
+// nodal in a wall-bounded direction)
+inline int compact_extent(const Fab& f, int d) {
+    if (d >= f.dm) return 1;
+    return f.n[d] + ((f.edge && f.nodal[d] && !f.per[d]) ? 1 : 0);
+}
+
+// compact (unique periodic, i fastest) <-> fab conversions.  Periodic
+// directions fill ghosts and the nodal seam from their images; in a
+// wall-bounded direction the stored entries are copied, the hi+1 wall face
+// of a face array is zero and ghost cells are zero (left to the physical
+// fills).
 inline void fab_from_compact(Fab& f, const double* c) {
-    int nx = f.n[0], ny = f.n[1];
+    int ext[3];
+    for (int d = 0; d < 3; ++d) ext[d] = compact_extent(f, d);
+    auto map = [&](int d, int v, int& out) {
+        if (d >= f.dm) { out = 0; return true; }
+        if (f.per[d]) { out = ((v % f.n[d]) + f.n[d]) % f.n[d]; return true; }
+        if (v < 0 || v >= ext[d]) return false;
+        out = v;
+        return true;
+    };
     for (int k = f.lo[2]; k <= f.hi[2]; ++k)
         for (int j = f.lo[1]; j <= f.hi[1]; ++j)
             for (int i = f.lo[0]; i <= f.hi[0]; ++i) {
-                int ii = ((i % nx) + nx) % nx;
-                int jj = ((j % ny) + ny) % ny;
-                int kk = (f.dm == 3) ? ((k % f.n[2]) + f.n[2]) % f.n[2] : 0;
-                f(i, j, k) = c[(size_t)ii + (size_t)nx * ((size_t)jj + (size_t)ny * kk)];
+                int ii, jj, kk;
+                if (map(0, i, ii) && map(1, j, jj) && map(2, k, kk))
+                    f(i, j, k) = c[(size_t)ii + (size_t)ext[0] * ((size_t)jj + (size_t)ext[1] * kk)];
+                else
+                    f(i, j, k) = 0.0;
             }
 }
 inline void compact_from_fab(double* c, const Fab& f) {
-    int nx = f.n[0], ny = f.n[1], nz = f.n[2];
-    for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < nx; ++i)
-                c[(size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)] = f(i, j, k);
+    const int ex = compact_extent(f, 0), ey = compact_extent(f, 1), ez = compact_extent(f, 2);
+    for (int k = 0; k < ez; ++k)
+        for (int j = 0; j < ey; ++j)
+            for (int i = 0; i < ex; ++i)
+                c[(size_t)i + (size_t)ex * ((size_t)j + (size_t)ey * k)] = f(i, j, k);
 }
 
 }  // namespace orc

@@ -48,8 +48,9 @@ Level make_level0(const Problem& P, double theta_alpha) {
 
 void apply_matrix(const Problem& P, double theta_alpha, Fab* b_u, Fab& b_p, Fab* x_u, Fab& x_p) {
     const int dm = P.geo.dm;
-    fill_boundary(x_p);
-    for (int i = 0; i < dm; ++i) fill_boundary(x_u[i]);
+    // ghost fills (apply_matrix.f90:60-87); the wall faces of x_u become zero
+    fill_pres(P.geo, x_p);
+    fill_vel(P.geo, x_u);
     Fab gx_p[3];
     for (int i = 0; i < dm; ++i) gx_p[i] = make_face(P.geo, i, 0);
     Level L = make_level0(P, theta_alpha);
@@ -162,6 +163,13 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         alphainv[i] = make_face(P.geo, i, 0);
         alphainv[i].setval(1.0);
         for_valid(alphainv[i], [&](double& d, int a, int b, int c) { d = d / P.alpha_fc[i](a, b, c); });
+        // on wall faces 1/alpha only ever multiplies the zero wall gradient;
+        // the compact layout stores no alpha on the hi+1 wall face
+        if (!P.geo.periodic(i))
+            for_valid(alphainv[i], [&](double& d, int a, int b, int c) {
+                const int idx[3] = {a, b, c};
+                if (idx[i] == 0 || idx[i] == P.geo.n[i]) d = 0.0;
+            });
         b_u_tmp[i] = make_face(P.geo, i, 0);
         one_fab[i] = make_face(P.geo, i, 0);
         one_fab[i].setval(1.0);
@@ -233,7 +241,7 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         if (pt == -2 || pt == -5) scale_valid(x_p, -1.0);
         if (std::abs(pt) == 5) {
             copy_valid(x_p_tmp, x_p);
-            fill_boundary(x_p_tmp);
+            fill_pres(P.geo, x_p_tmp);
             for (int i = 0; i < dm; ++i) copy_valid(b_u_tmp[i], b_u[i]);
             subtract_weighted_gradp(P, b_u_tmp, one_fab, x_p_tmp);
             stag_mg_solver(P, K, theta_alpha, x_u, b_u_tmp, vc);
@@ -249,7 +257,7 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
         else
             simple_schur();
         copy_valid(x_p_tmp, x_p);
-        fill_boundary(x_p_tmp);
+        fill_pres(P.geo, x_p_tmp);
         for (int i = 0; i < dm; ++i) copy_valid(b_u_tmp[i], b_u[i]);
         subtract_weighted_gradp(P, b_u_tmp, one_fab, x_p_tmp);
         stag_mg_solver(P, K, theta_alpha, x_u, b_u_tmp, vc);
@@ -294,12 +302,19 @@ void apply_precon(const Problem& P, const lmm_knobs& K, double theta_alpha, cons
     default:
         return;  // rejected before the solve starts
     }
-    // mean removal (apply_precon.f90:433-460): periodic domain, no no-slip walls
+    // mean removal (apply_precon.f90:433-460): the pressure always; with
+    // theta alpha = 0 and no no-slip wall, each periodic velocity component
     double mean_p, mean_u[3];
     sum_umac_press(P.geo, x_p, x_u, &mean_p, mean_u);
     for_valid(x_p, [&](double& d, int, int, int) { d = d - mean_p; });
-    if (theta_alpha == 0.0)
-        for (int i = 0; i < dm; ++i) for_valid(x_u[i], [&](double& d, int, int, int) { d = d - mean_u[i]; });
+    if (theta_alpha == 0.0) {
+        bool no_wall_is_no_slip = true;
+        for (int i = 0; i < dm; ++i)
+            if (bc_is_noslip(P.geo.bc_lo[i]) || bc_is_noslip(P.geo.bc_hi[i])) no_wall_is_no_slip = false;
+        if (no_wall_is_no_slip)
+            for (int i = 0; i < dm; ++i)
+                if (P.geo.periodic(i)) for_valid(x_u[i], [&](double& d, int, int, int) { d = d - mean_u[i]; });
+    }
 }
 
 // ---------------------------------------------------------------- GMRES pieces

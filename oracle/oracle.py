@@ -59,7 +59,7 @@ def fields_in(prob, b_u=None, b_p=None):
 
 
 def grid_of(prob) -> abi.Grid:
-    return abi.make_grid(prob.dm, prob.n, prob.dx)
+    return abi.make_grid(prob.dm, prob.n, prob.dx, getattr(prob, "bc", None))
 
 
 def solve(prob, knobs: abi.Knobs, x_u=None, x_p=None, theta_alpha=None):
@@ -107,7 +107,8 @@ def coarse_coeffs(prob, knobs, lev, theta_alpha=None):
     alpha = [np.zeros(shp) for _ in range(dm)]
     beta = np.zeros(shp)
     gamma = np.zeros(shp)
-    bed = [np.zeros(shp) for _ in range(1 if dm == 2 else 3)]
+    nl = [prob.n[d] >> lev for d in range(dm)]
+    bed = [np.zeros(abi.edge_shape(dm, nl, getattr(prob, "bc", None), e)) for e in range(1 if dm == 2 else 3)]
     th = prob.theta_alpha if theta_alpha is None else theta_alpha
     rc = lib().orc_coarse_coeffs(C.byref(grid_of(prob)), C.byref(knobs), C.byref(fields_in(prob)), C.c_double(th),
                                  C.c_int(lev), abi.ptr_array(alpha), abi.ptr(beta), abi.ptr_array(bed), abi.ptr(gamma))

@@ -32,6 +32,13 @@ struct Problem {
     Fab gamma;         // ng=1
 };
 
+// physbc.cpp (walls)
+void physbc_domainvel(const Geo& g, Fab& s, int comp);
+void physbc_macvel(const Geo& g, Fab& s, int comp);
+void physbc_pres(const Geo& g, Fab& p);
+void fill_vel(const Geo& g, Fab* u);
+void fill_pres(const Geo& g, Fab& p);
+
 // stag_ops.cpp
 void stag_applyop_level(const Level& L, const Fab* phi, Fab* Lphi, int color, int visc);
 void stag_mg_update(const Level& L, Fab* phi, const Fab* rhs, const Fab* Lphi, int color, int visc, double omega);

@@ -5,9 +5,9 @@
 //   src_gmres/stag_mg_solver.f90:37-868  (stag_mg_solver)
 //   src_gmres/stag_mg_solver.f90:873-1633 (cc/stag/nodal/edge restriction,
 //                                          stag_prolongation)
-// for one periodic box.  Physical-boundary calls (multifab_physbc_*) are
-// no-ops on a periodic domain and are left out; every multifab_fill_boundary
-// of the reference is kept.
+// for one box.  Every multifab_fill_boundary of the reference is kept, and
+// so are its physical-boundary fills (physbc.cpp), which act on
+// wall-bounded directions only.
 #include "oracle_internal.hpp"
 
 #include <cmath>
@@ -262,9 +262,8 @@ static double norm_inf_valid(const Fab& f) {
     return m;
 }
 
-static void fill_all(Fab* f, int dm) {
-    for (int j = 0; j < dm; ++j) fill_boundary(f[j]);
-}
+// physbc_domainvel + fill_boundary + physbc_macvel on every component
+static void fill_all(const Geo& g, Fab* f) { fill_vel(g, f); }
 
 // one pass of "nsmooths x colours" at level n (stag_mg_solver.f90:363-401)
 static void smooth_level(const Level& L, Fab* phi, const Fab* rhs, Fab* Lphi, int nsmooths, int cstart, int cend,
@@ -273,7 +272,7 @@ static void smooth_level(const Level& L, Fab* phi, const Fab* rhs, Fab* Lphi, in
         for (int color = cstart; color <= cend; ++color) {
             stag_applyop_level(L, phi, Lphi, color, visc);
             stag_mg_update(L, phi, rhs, Lphi, color, visc, omega);
-            fill_all(phi, L.geo.dm);
+            fill_all(L.geo, phi);
         }
 }
 
@@ -289,8 +288,8 @@ static void residual_level(const Level& L, const Fab* phi, const Fab* rhs, Fab* 
                     double v = Lp(i, jj, k) - r(i, jj, k);
                     Lp(i, jj, k) = v * -1.0;
                 }
-        fill_boundary(Lp);
     }
+    fill_all(L.geo, Lphi);
 }
 
 void stag_mg_solver(const Problem& P, const lmm_knobs& K, double theta_alpha, Fab* phi_fc, const Fab* rhs_fc,
@@ -321,8 +320,8 @@ void stag_mg_solver(const Problem& P, const lmm_knobs& K, double theta_alpha, Fa
                     p(ii, j, k) = phi_fc[i](ii, j, k);
                     rhs[0][i](ii, j, k) = rhs_fc[i](ii, j, k);
                 }
-        fill_boundary(p);
     }
+    fill_all(lev[0].geo, phi[0].data());
     // initial residual (:259-313)
     double resid0[3] = {0, 0, 0};
     stag_applyop_level(lev[0], phi[0].data(), Lphi[0].data(), 0, visc);
@@ -356,6 +355,8 @@ void stag_mg_solver(const Problem& P, const lmm_knobs& K, double theta_alpha, Fa
                          K.stag_mg_omega);
             residual_level(lev[n], phi[n].data(), rhs[n].data(), Lphi[n].data(), visc);
             stag_restriction(lev[n + 1].geo, Lphi[n].data(), rhs[n + 1].data(), false);
+            // residual zero on physical boundaries (:439-443)
+            for (int j = 0; j < dm; ++j) physbc_domainvel(lev[n + 1].geo, rhs[n + 1][j], j);
         }
         // bottom: smooths at the coarsest level (one box, so the "fancy" bottom
         // solver condition n_cells/max_grid_size >= 2 of :450 is false)
@@ -368,7 +369,7 @@ void stag_mg_solver(const Problem& P, const lmm_knobs& K, double theta_alpha, Fa
         // up
         for (int n = nlevs_mg - 2; n >= 0; --n) {
             stag_prolongation(lev[n].geo, phi[n].data(), phi[n + 1].data());
-            fill_all(phi[n].data(), dm);
+            fill_all(lev[n].geo, phi[n].data());
             smooth_level(lev[n], phi[n].data(), rhs[n].data(), Lphi[n].data(), K.stag_mg_nsmooths_up, cstart, cend, visc,
                          K.stag_mg_omega);
         }
@@ -392,8 +393,8 @@ void stag_mg_solver(const Problem& P, const lmm_knobs& K, double theta_alpha, Fa
         for (int k = p.vlo[2]; k <= p.vhi[2]; ++k)
             for (int jj = p.vlo[1]; jj <= p.vhi[1]; ++jj)
                 for (int i = p.vlo[0]; i <= p.vhi[0]; ++i) p(i, jj, k) = phi[0][j](i, jj, k);
-        fill_boundary(p);
     }
+    fill_all(P.geo, phi_fc);
     if (vcycle_counter) *vcycle_counter += dm * K.stag_mg_max_vcycles;
 }
 

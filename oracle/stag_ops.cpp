@@ -348,6 +348,8 @@ void stag_applyop_level(const Level& L, const Fab* phi, Fab* Lphi, int color, in
         applyop_2d(phi, Lphi, L.alpha, L.beta_cc, L.beta_ed[0], L.gamma_cc, L.dx, color, visc);
     else
         applyop_3d(phi, Lphi, L.alpha, L.beta_cc, L.beta_ed, L.gamma_cc, L.dx, color, visc);
+    // Lphi on physical domain boundaries is zero (stag_applyop.f90:197-201)
+    for (int c = 0; c < L.geo.dm; ++c) physbc_domainvel(L.geo, Lphi[c], c);
 }
 
 // ---------------------------------------------------------------- smoother update
