@@ -15,12 +15,18 @@
  * address and every size a plain integer.
  *
  * Conventions
- *  - Grid: one box, periodic in every direction, isotropic dx, dm = 2 or 3.
+ *  - Grid: one box, isotropic dx, dm = 2 or 3; each direction is periodic
+ *    or bounded by walls on both sides (no-slip or slip, lmm_grid.bc_lo /
+ *    bc_hi, the reference's bc_lo / bc_hi of src_common/bc.f90:23-44).
  *  - Face component d of a velocity-like field is nodal in direction d.
  *  - LMM_LAYOUT_COMPACT arrays hold the n[0]*n[1](*n[2]) unique periodic
  *    entries of a field, i fastest (Fortran column-major order), without
  *    ghost cells; the duplicated periodic seam face (index hi+1) is implied
- *    equal to face lo.
+ *    equal to face lo.  Along a wall-bounded direction d: face component d
+ *    stores faces lo..hi, face lo being the wall (taken as zero in b_u and
+ *    x_u: the wall-normal velocity is not an unknown) and the wall face hi+1
+ *    implied zero; a beta_ed array nodal in d stores its n[d]+1 nodes (both
+ *    walls), so it holds prod(n + wall-nodal) entries.
  *  - LMM_LAYOUT_BOXLIB arrays are the Fortran arrays exactly as BoxLib's
  *    dataptr() hands them over for a single box: column-major, ng ghost
  *    layers on every side, and n+1 valid entries in each nodal direction.
@@ -49,8 +55,10 @@ extern "C" {
 #define LMM_ERR_WATCHDOG      -5  /* a bounded device wait gave up */
 #define LMM_ERR_NO_DEVICE     -6  /* no CUDA device visible */
 
-/* ---- boundary-condition codes (src_common/bc.f90:44-50) ---- */
+/* ---- boundary-condition codes (src_common/bc.f90:23-44) ---- */
 #define LMM_BC_PERIODIC       -1
+#define LMM_BC_NO_SLIP_WALL  100  /* 100-103 (NO_SLIP_START..NO_SLIP_END): zero velocity */
+#define LMM_BC_SLIP_WALL     200  /* 200-203 (SLIP_START..SLIP_END): zero normal velocity and shear stress */
 
 /* ---- array layouts ---- */
 #define LMM_LAYOUT_COMPACT     0
@@ -71,7 +79,16 @@ typedef struct lmm_grid {
     int    dm;          /* 2 or 3 */
     int    n[3];        /* cells per direction (n[2] ignored when dm == 2) */
     double dx;          /* isotropic spacing; stag_applyop.f90:116-118 requires dx(1)==dx(2) */
-    int    bc_lo[3];    /* BC codes per face of the domain; only LMM_BC_PERIODIC */
+    int    bc_lo[3];    /* BC codes per side: LMM_BC_PERIODIC on both sides of a
+                           direction, or a wall code (100-103 no-slip, 200-203
+                           slip) on both.  Walls follow define_bc_tower.f90:219-234
+                           and multifab_physbc_stag.f90 for the homogeneous
+                           problem gmres(...) solves: normal velocity zero,
+                           transverse ghost -interior (no-slip) or +interior
+                           (slip), pressure extrapolated (zero wall gradient,
+                           div_and_grad.f90:139-182), pressure multigrid with
+                           homogeneous Neumann faces.  Not with
+                           visc_schur_approx = 1 or the learned stage. */
     int    bc_hi[3];
 } lmm_grid;
 

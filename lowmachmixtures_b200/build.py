@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
@@ -24,6 +25,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_fp32.cu", ["-fmad=true"]),
+    ("walls_fp64.cu", ["-fmad=false"]),
+    ("walls_fp32.cu", ["-fmad=true"]),
     ("krylov.cu", ["-fmad=false"]),
     ("solver.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
@@ -55,6 +58,7 @@ def build(verbose: bool = False, force: bool = False, extra: list | None = None)
     headers.append(os.path.join(os.path.dirname(PKG), "include", "lmm_stokes.h"))
     objs = []
     cc = nvcc()
+    jobs = []
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -63,7 +67,11 @@ def build(verbose: bool = False, force: bool = False, extra: list | None = None)
             cmd = [cc, "-c", s, "-o", o] + ARCH + COMMON + flags + (extra or [])
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
+    # translation units compile in parallel (the instantiation units dominate)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in jobs]:
+            f.result()
     if force or _stale(objs, LIB):
         cmd = [cc, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fPIC"]
         if verbose:

@@ -48,24 +48,25 @@ static inline G3 geom3(int nx, int ny, int nz) {
 }
 
 // --------------------------------------------------------------- applyop
-template <class T, int DM, int VISC>
+// W: a grid with walls; L phi is zero on the wall faces (stag_applyop.f90:197-201)
+template <class T, int DM, int VISC, bool W = false>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
                                                       const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                       T* __restrict__ o2, T dxsqinv, int color) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     const int i = q.i, j = q.j, k = q.k;
-    Nb nb = make_nb(D, i, j, k);
+    Nb nb = W ? make_nbw(D, i, j, k) : make_nb(D, i, j, k);
     const int t = nb.s;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
     // colour c >= 1 covers component (c-1)/2, faces with (i+j+k) even for odd c
     const int ccomp = (color - 1) / 2;
     const bool on = (color == 0) || ((((i + j + k) & 1) == ((color % 2 == 1) ? 0 : 1)));
-    if (color == 0 || (ccomp == 0 && on)) o0[t] = face_L<T, DM, VISC, 0>(phi, C, nb, dxsqinv, b, c);
-    if (color == 0 || (ccomp == 1 && on)) o1[t] = face_L<T, DM, VISC, 1>(phi, C, nb, dxsqinv, b, c);
+    if (color == 0 || (ccomp == 0 && on)) o0[t] = (W && wall_face(nb, 0)) ? T(0) : face_L<T, DM, VISC, 0, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+    if (color == 0 || (ccomp == 1 && on)) o1[t] = (W && wall_face(nb, 1)) ? T(0) : face_L<T, DM, VISC, 1, 0, T, W>(phi, C, nb, dxsqinv, b, c);
     if constexpr (DM == 3)
-        if (color == 0 || (ccomp == 2 && on)) o2[t] = face_L<T, DM, VISC, 2>(phi, C, nb, dxsqinv, b, c);
+        if (color == 0 || (ccomp == 2 && on)) o2[t] = (W && wall_face(nb, 2)) ? T(0) : face_L<T, DM, VISC, 2, 0, T, W>(phi, C, nb, dxsqinv, b, c);
 }
 
 // --------------------------------------------------------------- GS colour
@@ -73,18 +74,20 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Di
 // component COMP with (i+j+k) % 2 == parity are updated in place.  Faces of
 // one colour never read each other (even cell counts), so the in-place
 // update equals the reference's compute-all-then-update order.
-template <class T, int DM, int VISC, int COMP>
+// W: wall faces keep their zero (physbc_domainvel after every colour)
+template <class T, int DM, int VISC, int COMP, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const T* __restrict__ rhs, T* p0, T* p1, T* p2,
                                                         int parity, T omega, T dxsqinv) {
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
     const int j = q.j, k = q.k;
     const int i = 2 * q.i + ((j + k + parity) & 1);
-    Nb nb = make_nb(D, i, j, k);
+    Nb nb = W ? make_nbw(D, i, j, k) : make_nb(D, i, j, k);
+    if (W && wall_face(nb, COMP)) return;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
-    T Lp = face_L<T, DM, VISC, COMP>(phi, C, nb, dxsqinv, b, c);
-    T fac = face_diag<T, DM, VISC, COMP>(C, nb, dxsqinv, b, c);
+    T Lp = face_L<T, DM, VISC, COMP, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+    T fac = face_diag<T, DM, VISC, COMP, W>(C, nb, dxsqinv, b, c);
     T* p = (COMP == 0) ? p0 : (COMP == 1 ? p1 : p2);
     T cur = p[nb.s];
     p[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
@@ -100,14 +103,15 @@ __host__ __device__ __forceinline__ bool odd_level(const Dims& D) {
     return (D.nx & 1) || (D.ny & 1) || (D.dm == 3 && (D.nz & 1));
 }
 
-template <class T, int DM, int VISC, int COMP>
+template <class T, int DM, int VISC, int COMP, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_colour_update(Dims D, Coef<T> C, const T* __restrict__ rhs, const T* __restrict__ Lp,
                                                             T* p, int parity, T omega, T dxsqinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
-    Nb nb = make_nb(D, q.i, q.j, q.k);
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
+    if (W && wall_face(nb, COMP)) return;
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
-    T fac = face_diag<T, DM, VISC, COMP>(C, nb, dxsqinv, b, c);
+    T fac = face_diag<T, DM, VISC, COMP, W>(C, nb, dxsqinv, b, c);
     T cur = p[nb.s];
     p[nb.s] = cur + omega * (ld(rhs, nb.s) - ld(Lp, nb.s)) / fac;
 }
@@ -189,31 +193,39 @@ __global__ void __launch_bounds__(kThreads) k_gs_pair(Dims D, Coef<T> C, const T
 }
 
 // --------------------------------------------------------------- Jacobi
-template <class T, int DM, int VISC>
+template <class T, int DM, int VISC, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_jacobi(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
                                                      const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
                                                      const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                      T* __restrict__ o2, T omega, T dxsqinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
-    Nb nb = make_nb(D, q.i, q.j, q.k);
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
     const int t = nb.s;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
-    {
-        T Lp = face_L<T, DM, VISC, 0>(phi, C, nb, dxsqinv, b, c);
-        T fac = face_diag<T, DM, VISC, 0>(C, nb, dxsqinv, b, c);
+    if (W && wall_face(nb, 0)) {
+        o0[t] = T(0);
+    } else {
+        T Lp = face_L<T, DM, VISC, 0, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, 0, W>(C, nb, dxsqinv, b, c);
         o0[t] = ld(p0, t) + omega * (ld(r0, t) - Lp) / fac;
     }
-    {
-        T Lp = face_L<T, DM, VISC, 1>(phi, C, nb, dxsqinv, b, c);
-        T fac = face_diag<T, DM, VISC, 1>(C, nb, dxsqinv, b, c);
+    if (W && wall_face(nb, 1)) {
+        o1[t] = T(0);
+    } else {
+        T Lp = face_L<T, DM, VISC, 1, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, 1, W>(C, nb, dxsqinv, b, c);
         o1[t] = ld(p1, t) + omega * (ld(r1, t) - Lp) / fac;
     }
     if constexpr (DM == 3) {
-        T Lp = face_L<T, DM, VISC, 2>(phi, C, nb, dxsqinv, b, c);
-        T fac = face_diag<T, DM, VISC, 2>(C, nb, dxsqinv, b, c);
-        o2[t] = ld(p2, t) + omega * (ld(r2, t) - Lp) / fac;
+        if (W && wall_face(nb, 2)) {
+            o2[t] = T(0);
+        } else {
+            T Lp = face_L<T, DM, VISC, 2, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+            T fac = face_diag<T, DM, VISC, 2, W>(C, nb, dxsqinv, b, c);
+            o2[t] = ld(p2, t) + omega * (ld(r2, t) - Lp) / fac;
+        }
     }
 }
 
@@ -288,34 +300,46 @@ __device__ __forceinline__ void restrict_comp(int comp, const Dims& F, const Coe
 }
 
 // r = (L phi - rhs) * -1 on every face of one level (stag_mg_solver.f90:406-415)
-template <class T, int DM, int VISC>
+// W: the residual is zero on wall faces (physbc_domainvel, stag_mg_solver.f90:424-425)
+template <class T, int DM, int VISC, bool W = false>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_residual(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
                                                        const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
                                                        const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                        T* __restrict__ o2, T dxsqinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
-    Nb nb = make_nb(D, q.i, q.j, q.k);
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
     const int t = nb.s;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
-    {
-        T v = face_L<T, DM, VISC, 0>(phi, C, nb, dxsqinv, b, c) - ld(r0, t);
+    if (W && wall_face(nb, 0)) {
+        o0[t] = T(0);
+    } else {
+        T v = face_L<T, DM, VISC, 0, 0, T, W>(phi, C, nb, dxsqinv, b, c) - ld(r0, t);
         o0[t] = v * T(-1);
     }
-    {
-        T v = face_L<T, DM, VISC, 1>(phi, C, nb, dxsqinv, b, c) - ld(r1, t);
+    if (W && wall_face(nb, 1)) {
+        o1[t] = T(0);
+    } else {
+        T v = face_L<T, DM, VISC, 1, 0, T, W>(phi, C, nb, dxsqinv, b, c) - ld(r1, t);
         o1[t] = v * T(-1);
     }
     if constexpr (DM == 3) {
-        T v = face_L<T, DM, VISC, 2>(phi, C, nb, dxsqinv, b, c) - ld(r2, t);
-        o2[t] = v * T(-1);
+        if (W && wall_face(nb, 2)) {
+            o2[t] = T(0);
+        } else {
+            T v = face_L<T, DM, VISC, 2, 0, T, W>(phi, C, nb, dxsqinv, b, c) - ld(r2, t);
+            o2[t] = v * T(-1);
+        }
     }
 }
 
 // 6-point (2D) / 12-point (3D) restriction of precomputed fine residuals,
 // same summation order as restrict_face
-template <class T, int DM>
+// W: coarse wall faces are zero (physbc_domainvel on the restricted
+// residual, stag_mg_solver.f90:439-443); every other coarse face reads fine
+// faces inside the box
+template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restrict__ f0, const T* __restrict__ f1,
                                                        const T* __restrict__ f2, Dims Dc, T* __restrict__ c0, T* __restrict__ c1,
                                                        T* __restrict__ c2) {
@@ -323,6 +347,19 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
     if (!q.ok) return;
     const int t = q.i + Dc.nx * (q.j + Dc.ny * q.k);
     const int I = 2 * q.i, J = 2 * q.j, K = 2 * q.k;
+    if constexpr (W) {
+        // wall faces first; the others fall through to the periodic formula
+        const int x[3] = {q.i, q.j, q.k};
+        bool wf[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) wf[d] = d < DM && ((Dc.wall >> d) & 1) && x[d] == 0;
+        if (wf[0]) c0[t] = T(0);
+        if (wf[1]) c1[t] = T(0);
+        if (DM == 3 && wf[2]) c2[t] = T(0);
+        if (wf[0]) c0 = nullptr;
+        if (wf[1]) c1 = nullptr;
+        if (wf[2]) c2 = nullptr;
+    }
     auto R = [&](const T* f, int i, int j, int k) {
         i = wrapi(i, F.nx);
         j = wrapi(j, F.ny);
@@ -330,17 +367,22 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
         return ld(f, i + F.nx * (j + F.ny * k));
     };
     if constexpr (DM == 2) {
+        if (!W || c0)
         c0[t] = T(0.25) * (R(f0, I, J, 0) + R(f0, I, J + 1, 0)) +
                 T(0.125) * (R(f0, I + 1, J, 0) + R(f0, I + 1, J + 1, 0) + R(f0, I - 1, J, 0) + R(f0, I - 1, J + 1, 0));
+        if (!W || c1)
         c1[t] = T(0.25) * (R(f1, I, J, 0) + R(f1, I + 1, J, 0)) +
                 T(0.125) * (R(f1, I, J + 1, 0) + R(f1, I + 1, J + 1, 0) + R(f1, I, J - 1, 0) + R(f1, I + 1, J - 1, 0));
     } else {
+        if (!W || c0)
         c0[t] = T(0.125) * (R(f0, I, J, K) + R(f0, I, J + 1, K) + R(f0, I, J, K + 1) + R(f0, I, J + 1, K + 1)) +
                 T(0.0625) * (R(f0, I + 1, J, K) + R(f0, I + 1, J + 1, K) + R(f0, I + 1, J, K + 1) + R(f0, I + 1, J + 1, K + 1)) +
                 T(0.0625) * (R(f0, I - 1, J, K) + R(f0, I - 1, J + 1, K) + R(f0, I - 1, J, K + 1) + R(f0, I - 1, J + 1, K + 1));
+        if (!W || c1)
         c1[t] = T(0.125) * (R(f1, I, J, K) + R(f1, I + 1, J, K) + R(f1, I, J, K + 1) + R(f1, I + 1, J, K + 1)) +
                 T(0.0625) * (R(f1, I, J + 1, K) + R(f1, I + 1, J + 1, K) + R(f1, I, J + 1, K + 1) + R(f1, I + 1, J + 1, K + 1)) +
                 T(0.0625) * (R(f1, I, J - 1, K) + R(f1, I + 1, J - 1, K) + R(f1, I, J - 1, K + 1) + R(f1, I + 1, J - 1, K + 1));
+        if (!W || c2)
         c2[t] = T(0.125) * (R(f2, I, J, K) + R(f2, I + 1, J, K) + R(f2, I, J + 1, K) + R(f2, I + 1, J + 1, K)) +
                 T(0.0625) * (R(f2, I, J, K + 1) + R(f2, I + 1, J, K + 1) + R(f2, I, J + 1, K + 1) + R(f2, I + 1, J + 1, K + 1)) +
                 T(0.0625) * (R(f2, I, J, K - 1) + R(f2, I + 1, J, K - 1) + R(f2, I, J + 1, K - 1) + R(f2, I + 1, J + 1, K - 1));
@@ -372,83 +414,132 @@ __device__ __forceinline__ T cat(const T* a, const Dims& Dc, int i, int j, int k
     return ldp<LD>(a, i + Dc.nx * (j + Dc.ny * k));
 }
 
-// add the interpolated coarse correction to the DM fine faces at (i, j, k)
-template <class T, int DM, int LD = 0>
+// coarse value of component COMP at (i, j, k) on a grid with walls (the
+// coarse level's ghost fills): periodic directions wrap; across its own
+// walls the component is zero; across another direction's wall the ghost
+// mirrors the face, negated at a no-slip wall
+template <class T, int LD, int COMP>
+__device__ __forceinline__ T catw(const T* a, const Dims& Dc, int i, int j, int k) {
+    int x[3] = {i, j, (Dc.dm == 3) ? k : 0};
+    const int n[3] = {Dc.nx, Dc.ny, Dc.nz};
+    bool neg = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (d >= Dc.dm) continue;
+        if (!((Dc.wall >> d) & 1)) {
+            x[d] = wrapi(x[d], n[d]);
+            continue;
+        }
+        if (d == COMP) {
+            if (x[d] < 0 || x[d] >= n[d]) return T(0);
+            continue;
+        }
+        if (x[d] < 0) {
+            x[d] = 0;
+            if (!((Dc.slip_lo >> d) & 1)) neg = !neg;
+        } else if (x[d] >= n[d]) {
+            x[d] = n[d] - 1;
+            if (!((Dc.slip_hi >> d) & 1)) neg = !neg;
+        }
+    }
+    const T v = ldp<LD>(a, x[0] + Dc.nx * (x[1] + Dc.ny * x[2]));
+    return neg ? -v : v;
+}
+template <class T, int LD, bool W, int COMP>
+__device__ __forceinline__ T pcat(const T* a, const Dims& Dc, int i, int j, int k) {
+    if constexpr (W)
+        return catw<T, LD, COMP>(a, Dc, i, j, k);
+    else
+        return cat<T, LD>(a, Dc, i, j, k);
+}
+
+// add the interpolated coarse correction to the DM fine faces at (i, j, k);
+// W: fine wall faces keep their zero (physbc_domainvel after the
+// prolongation, stag_mg_solver.f90:681-690)
+template <class T, int DM, int LD = 0, bool W = false>
 __device__ __forceinline__ void prolong_cell(const Dims& Dc, const T* q0, const T* q1, const T* q2, T* f0, T* f1, T* f2, int t,
                                              int i, int j, int k) {
+    if constexpr (W) {
+        // the fine grid's wall bits are the coarse grid's
+        const int x[3] = {i, j, k};
+        if ((Dc.wall & 1) && x[0] == 0) f0 = nullptr;
+        if (((Dc.wall >> 1) & 1) && x[1] == 0) f1 = nullptr;
+        if (DM == 3 && ((Dc.wall >> 2) & 1) && x[2] == 0) f2 = nullptr;
+    }
+    (void)f2;
     const int i2 = i >> 1, j2 = j >> 1, k2 = k >> 1;
     if constexpr (DM == 2) {
-        {
+        if (!W || f0) {
             int joff = ((j & 1) == 0) ? -1 : 1;
             T v = (LD == 2) ? __ldcg(f0 + t) : f0[t];
             if ((i & 1) == 0)
-                v = v + T(0.75) * cat<T, LD>(q0, Dc, i2, j2, 0) + T(0.25) * cat<T, LD>(q0, Dc, i2, j2 + joff, 0);
+                v = v + T(0.75) * pcat<T, LD, W, 0>(q0, Dc, i2, j2, 0) + T(0.25) * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, 0);
             else
-                v = v + T(0.375) * cat<T, LD>(q0, Dc, i2, j2, 0) + T(0.125) * cat<T, LD>(q0, Dc, i2, j2 + joff, 0) + T(0.375) * cat<T, LD>(q0, Dc, i2 + 1, j2, 0) +
-                    T(0.125) * cat<T, LD>(q0, Dc, i2 + 1, j2 + joff, 0);
+                v = v + T(0.375) * pcat<T, LD, W, 0>(q0, Dc, i2, j2, 0) + T(0.125) * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, 0) + T(0.375) * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2, 0) +
+                    T(0.125) * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2 + joff, 0);
             f0[t] = v;
         }
-        {
+        if (!W || f1) {
             int ioff = ((i & 1) == 0) ? -1 : 1;
             T v = (LD == 2) ? __ldcg(f1 + t) : f1[t];
             if ((j & 1) == 0)
-                v = v + T(0.75) * cat<T, LD>(q1, Dc, i2, j2, 0) + T(0.25) * cat<T, LD>(q1, Dc, i2 + ioff, j2, 0);
+                v = v + T(0.75) * pcat<T, LD, W, 1>(q1, Dc, i2, j2, 0) + T(0.25) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, 0);
             else
-                v = v + T(0.375) * cat<T, LD>(q1, Dc, i2, j2, 0) + T(0.125) * cat<T, LD>(q1, Dc, i2 + ioff, j2, 0) + T(0.375) * cat<T, LD>(q1, Dc, i2, j2 + 1, 0) +
-                    T(0.125) * cat<T, LD>(q1, Dc, i2 + ioff, j2 + 1, 0);
+                v = v + T(0.375) * pcat<T, LD, W, 1>(q1, Dc, i2, j2, 0) + T(0.125) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, 0) + T(0.375) * pcat<T, LD, W, 1>(q1, Dc, i2, j2 + 1, 0) +
+                    T(0.125) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2 + 1, 0);
             f1[t] = v;
         }
     } else {
         const T n16 = T(9.0 / 16.0), t16 = T(3.0 / 16.0), o16 = T(1.0 / 16.0);
         const T n32 = T(9.0 / 32.0), t32 = T(3.0 / 32.0), o32 = T(1.0 / 32.0);
         const int ioff = ((i & 1) == 0) ? -1 : 1, joff = ((j & 1) == 0) ? -1 : 1, koff = ((k & 1) == 0) ? -1 : 1;
-        {
+        if (!W || f0) {
             T v = (LD == 2) ? __ldcg(f0 + t) : f0[t];
             if ((i & 1) == 0)
-                v = v + n16 * cat<T, LD>(q0, Dc, i2, j2, k2) + t16 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2) + t16 * cat<T, LD>(q0, Dc, i2, j2, k2 + koff) +
-                    o16 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2 + koff);
+                v = v + n16 * pcat<T, LD, W, 0>(q0, Dc, i2, j2, k2) + t16 * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, k2) + t16 * pcat<T, LD, W, 0>(q0, Dc, i2, j2, k2 + koff) +
+                    o16 * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, k2 + koff);
             else
-                v = v + n32 * cat<T, LD>(q0, Dc, i2, j2, k2) + t32 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2) + t32 * cat<T, LD>(q0, Dc, i2, j2, k2 + koff) +
-                    o32 * cat<T, LD>(q0, Dc, i2, j2 + joff, k2 + koff) + n32 * cat<T, LD>(q0, Dc, i2 + 1, j2, k2) +
-                    t32 * cat<T, LD>(q0, Dc, i2 + 1, j2 + joff, k2) + t32 * cat<T, LD>(q0, Dc, i2 + 1, j2, k2 + koff) +
-                    o32 * cat<T, LD>(q0, Dc, i2 + 1, j2 + joff, k2 + koff);
+                v = v + n32 * pcat<T, LD, W, 0>(q0, Dc, i2, j2, k2) + t32 * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, k2) + t32 * pcat<T, LD, W, 0>(q0, Dc, i2, j2, k2 + koff) +
+                    o32 * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, k2 + koff) + n32 * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2, k2) +
+                    t32 * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2 + joff, k2) + t32 * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2, k2 + koff) +
+                    o32 * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2 + joff, k2 + koff);
             f0[t] = v;
         }
-        {
+        if (!W || f1) {
             T v = (LD == 2) ? __ldcg(f1 + t) : f1[t];
             if ((j & 1) == 0)
-                v = v + n16 * cat<T, LD>(q1, Dc, i2, j2, k2) + t16 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2) + t16 * cat<T, LD>(q1, Dc, i2, j2, k2 + koff) +
-                    o16 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2 + koff);
+                v = v + n16 * pcat<T, LD, W, 1>(q1, Dc, i2, j2, k2) + t16 * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, k2) + t16 * pcat<T, LD, W, 1>(q1, Dc, i2, j2, k2 + koff) +
+                    o16 * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, k2 + koff);
             else
-                v = v + n32 * cat<T, LD>(q1, Dc, i2, j2, k2) + t32 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2) + t32 * cat<T, LD>(q1, Dc, i2, j2, k2 + koff) +
-                    o32 * cat<T, LD>(q1, Dc, i2 + ioff, j2, k2 + koff) + n32 * cat<T, LD>(q1, Dc, i2, j2 + 1, k2) +
-                    t32 * cat<T, LD>(q1, Dc, i2 + ioff, j2 + 1, k2) + t32 * cat<T, LD>(q1, Dc, i2, j2 + 1, k2 + koff) +
-                    o32 * cat<T, LD>(q1, Dc, i2 + ioff, j2 + 1, k2 + koff);
+                v = v + n32 * pcat<T, LD, W, 1>(q1, Dc, i2, j2, k2) + t32 * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, k2) + t32 * pcat<T, LD, W, 1>(q1, Dc, i2, j2, k2 + koff) +
+                    o32 * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, k2 + koff) + n32 * pcat<T, LD, W, 1>(q1, Dc, i2, j2 + 1, k2) +
+                    t32 * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2 + 1, k2) + t32 * pcat<T, LD, W, 1>(q1, Dc, i2, j2 + 1, k2 + koff) +
+                    o32 * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2 + 1, k2 + koff);
             f1[t] = v;
         }
-        {
+        if (!W || f2) {
             T v = (LD == 2) ? __ldcg(f2 + t) : f2[t];
             if ((k & 1) == 0)
-                v = v + n16 * cat<T, LD>(q2, Dc, i2, j2, k2) + t16 * cat<T, LD>(q2, Dc, i2 + ioff, j2, k2) + t16 * cat<T, LD>(q2, Dc, i2, j2 + joff, k2) +
-                    o16 * cat<T, LD>(q2, Dc, i2 + ioff, j2 + joff, k2);
+                v = v + n16 * pcat<T, LD, W, 2>(q2, Dc, i2, j2, k2) + t16 * pcat<T, LD, W, 2>(q2, Dc, i2 + ioff, j2, k2) + t16 * pcat<T, LD, W, 2>(q2, Dc, i2, j2 + joff, k2) +
+                    o16 * pcat<T, LD, W, 2>(q2, Dc, i2 + ioff, j2 + joff, k2);
             else
-                v = v + n32 * cat<T, LD>(q2, Dc, i2, j2, k2) + t32 * cat<T, LD>(q2, Dc, i2 + ioff, j2, k2) + t32 * cat<T, LD>(q2, Dc, i2, j2 + joff, k2) +
-                    o32 * cat<T, LD>(q2, Dc, i2 + ioff, j2 + joff, k2) + n32 * cat<T, LD>(q2, Dc, i2, j2, k2 + 1) +
-                    t32 * cat<T, LD>(q2, Dc, i2 + ioff, j2, k2 + 1) + t32 * cat<T, LD>(q2, Dc, i2, j2 + joff, k2 + 1) +
-                    o32 * cat<T, LD>(q2, Dc, i2 + ioff, j2 + joff, k2 + 1);
+                v = v + n32 * pcat<T, LD, W, 2>(q2, Dc, i2, j2, k2) + t32 * pcat<T, LD, W, 2>(q2, Dc, i2 + ioff, j2, k2) + t32 * pcat<T, LD, W, 2>(q2, Dc, i2, j2 + joff, k2) +
+                    o32 * pcat<T, LD, W, 2>(q2, Dc, i2 + ioff, j2 + joff, k2) + n32 * pcat<T, LD, W, 2>(q2, Dc, i2, j2, k2 + 1) +
+                    t32 * pcat<T, LD, W, 2>(q2, Dc, i2 + ioff, j2, k2 + 1) + t32 * pcat<T, LD, W, 2>(q2, Dc, i2, j2 + joff, k2 + 1) +
+                    o32 * pcat<T, LD, W, 2>(q2, Dc, i2 + ioff, j2 + joff, k2 + 1);
             f2[t] = v;
         }
     }
 }
 
-template <class T, int DM>
+template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_prolong_add(Dims F, Dims Dc, const T* __restrict__ q0, const T* __restrict__ q1,
                                                           const T* __restrict__ q2, T* __restrict__ f0, T* __restrict__ f1,
                                                           T* __restrict__ f2) {
     const Pos q = pos3(F.nx, F.ny);
     if (!q.ok) return;
     const int t = q.i + F.nx * (q.j + F.ny * q.k);
-    prolong_cell<T, DM, 0>(Dc, q0, q1, q2, f0, f1, f2, t, q.i, q.j, q.k);
+    prolong_cell<T, DM, 0, W>(Dc, q0, q1, q2, f0, f1, f2, t, q.i, q.j, q.k);
 }
 
 // --------------------------------------------------------------- coefficient coarsening
@@ -458,6 +549,8 @@ __device__ __forceinline__ T fat(const T* a, const Dims& F, int i, int j, int k)
     return ld(a, i + F.nx * (j + F.ny * (F.dm == 3 ? k : 0)));
 }
 
+// do_visc: 0 faces only, 1 faces + cells + edges, 2 faces + cells (the edges
+// of a grid with walls go through k_coarsen_edges_w)
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> Cf, T* a0, T* a1, T* a2, T* beta, T* gamma,
                                                       T* e0, T* e1, T* e2, int do_visc) {
@@ -474,7 +567,7 @@ __global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> C
             beta[t] = T(0.25) * (fat(b, F, I, J, 0) + fat(b, F, I + 1, J, 0) + fat(b, F, I, J + 1, 0) + fat(b, F, I + 1, J + 1, 0));
             const T* g = Cf.gamma;
             gamma[t] = T(0.25) * (fat(g, F, I, J, 0) + fat(g, F, I + 1, J, 0) + fat(g, F, I, J + 1, 0) + fat(g, F, I + 1, J + 1, 0));
-            e0[t] = fat(Cf.bed[0], F, I, J, 0);  // nodal injection
+            if (do_visc == 1) e0[t] = fat(Cf.bed[0], F, I, J, 0);  // nodal injection
         }
     } else {
         const T* A0 = Cf.alpha[0];
@@ -492,10 +585,38 @@ __global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> C
             gamma[t] = T(0.125) * (fat(g, F, I, J, K) + fat(g, F, I + 1, J, K) + fat(g, F, I, J + 1, K) + fat(g, F, I + 1, J + 1, K) +
                                    fat(g, F, I, J, K + 1) + fat(g, F, I + 1, J, K + 1) + fat(g, F, I, J + 1, K + 1) +
                                    fat(g, F, I + 1, J + 1, K + 1));
-            e0[t] = T(0.5) * (fat(Cf.bed[0], F, I, J, K) + fat(Cf.bed[0], F, I, J, K + 1));
-            e1[t] = T(0.5) * (fat(Cf.bed[1], F, I, J, K) + fat(Cf.bed[1], F, I, J + 1, K));
-            e2[t] = T(0.5) * (fat(Cf.bed[2], F, I, J, K) + fat(Cf.bed[2], F, I + 1, J, K));
+            if (do_visc == 1) {
+                e0[t] = T(0.5) * (fat(Cf.bed[0], F, I, J, K) + fat(Cf.bed[0], F, I, J, K + 1));
+                e1[t] = T(0.5) * (fat(Cf.bed[1], F, I, J, K) + fat(Cf.bed[1], F, I, J + 1, K));
+                e2[t] = T(0.5) * (fat(Cf.bed[2], F, I, J, K) + fat(Cf.bed[2], F, I + 1, J, K));
+            }
         }
+    }
+}
+
+// edge coefficients of a grid with walls (n+1 nodes along a nodal
+// wall-bounded direction): nodal injection in 2D (nodal_restriction,
+// stag_mg_solver.f90:1229-1244), two-point average along the edge in 3D
+// (edge_restriction, :1326-1367); the launch covers (nx+1, ny+1, nz+1)
+template <class T, int DM>
+__global__ void __launch_bounds__(kThreads) k_coarsen_edges_w(Dims F, Dims Dc, const T* f0, const T* f1, const T* f2, T* e0, T* e1,
+                                                              T* e2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    const int I = 2 * i, J = 2 * j, K = 2 * k;
+    const T* f[3] = {f0, f1, f2};
+    T* e[3] = {e0, e1, e2};
+#pragma unroll
+    for (int q = 0; q < (DM == 2 ? 1 : 3); ++q) {
+        const int cx = edge_ext(Dc, q, 0), cy = edge_ext(Dc, q, 1), cz = (DM == 3) ? edge_ext(Dc, q, 2) : 1;
+        if (i >= cx || j >= cy || k >= cz) continue;
+        const int fx = edge_ext(F, q, 0), fy = edge_ext(F, q, 1);
+        auto at = [&](int a, int b, int c) { return ld(f[q], a + fx * (b + fy * c)); };
+        T v;
+        if (DM == 2) v = at(I, J, 0);
+        else if (q == 0) v = T(0.5) * (at(I, J, K) + at(I, J, K + 1));
+        else if (q == 1) v = T(0.5) * (at(I, J, K) + at(I, J + 1, K));
+        else v = T(0.5) * (at(I, J, K) + at(I + 1, J, K));
+        e[q][i + cx * (j + cy * k)] = v;
     }
 }
 
@@ -599,31 +720,39 @@ __global__ void __launch_bounds__(kThreads) k_neg_cc_lap(Dims D, const T* a0, co
 }
 
 // --------------------------------------------------------------- div / grad pieces
-template <class T, int DM>
+// W: the hi+1 wall face of a wall-normal component is zero
+template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_div_plus(Dims D, const T* __restrict__ u0, const T* __restrict__ u1,
                                                        const T* __restrict__ u2, const T* __restrict__ bp, T* __restrict__ out,
                                                        T dxinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
-    Nb nb = make_nb(D, q.i, q.j, q.k);
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
     const int t = nb.s;
-    T v = (ld(u0, t + nb.op[0]) - ld(u0, t)) * dxinv + (ld(u1, t + nb.op[1]) - ld(u1, t)) * dxinv;
-    if constexpr (DM == 3) v = v + (ld(u2, t + nb.op[2]) - ld(u2, t)) * dxinv;
+    auto up = [&](const T* u, int d) {
+        const T v = ld(u, t + nb.op[d]);
+        return W ? wapply(wall_mul(nb, d, d, true), v) : v;
+    };
+    T v = (up(u0, 0) - ld(u0, t)) * dxinv + (up(u1, 1) - ld(u1, t)) * dxinv;
+    if constexpr (DM == 3) v = v + (up(u2, 2) - ld(u2, t)) * dxinv;
     out[t] = v + ld(bp, t);
 }
 
-template <class T, int DM>
+// W: wall faces are left alone (the wall gradient of a FOEXTRAP pressure
+// is zero, div_and_grad.f90:139-182)
+template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_sub_weighted_grad(Dims D, const T* c0, const T* c1, const T* c2,
                                                                 const T* __restrict__ phi, T* u0, T* u1, T* u2, T dxinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
-    Nb nb = make_nb(D, q.i, q.j, q.k);
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
     const int t = nb.s;
     const T p = ld(phi, t);
     T* u[3] = {u0, u1, u2};
     const T* c[3] = {c0, c1, c2};
 #pragma unroll
     for (int d = 0; d < DM; ++d) {
+        if (W && wall_face(nb, d)) continue;
         T g = (p - ld(phi, t + nb.om[d])) * dxinv;
         if (c[d]) g = g * ld(c[d], t);
         u[d][t] = u[d][t] + T(-1) * g;
@@ -874,6 +1003,7 @@ __global__ void __launch_bounds__(kThreads) k_div_mul(Dims D, const T* l0, const
 
 template <class T>
 void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color) {
+    if (L.D.wall) return wl_applyop<T>(L, visc, phi, out, s, color);
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2) {
@@ -886,6 +1016,7 @@ void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* co
 template <class T>
 void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega,
                       cudaStream_t s) {
+    if (L.D.wall) return wl_gs_colour<T>(L, visc, color, rhs, phi, omega, s);
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const int comp = (color - 1) / 2;
     const int parity = (color % 2 == 1) ? 0 : 1;
@@ -948,7 +1079,7 @@ static inline PairGeom pair_geom(const Dims& D, int tz_req) {
 
 template <class T>
 bool gs_pair_supported(const LevelDev<T>& L, int tz) {
-    return pair_geom(L.D, tz).ok;
+    return !L.D.wall && pair_geom(L.D, tz).ok;
 }
 
 template <class T>
@@ -974,6 +1105,7 @@ void launch_gs_pair(const LevelDev<T>& L, int visc, int comp, const T* const rhs
 template <class T>
 void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const pin[3], T* const pout[3],
                    double omega, cudaStream_t s) {
+    if (L.D.wall) return wl_jacobi<T>(L, visc, rhs, pin, pout, omega, s);
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     const T om = (T)omega;
@@ -987,6 +1119,7 @@ void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const 
 template <class T>
 void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
                               const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s) {
+    if (F.D.wall) return wl_residual_restrict<T>(F, Cc, visc, rhs_f, phi_f, rhs_c, s);
     // residual on every fine face into F.tmp, then the pure restriction
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
@@ -1006,6 +1139,7 @@ void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int v
 template <class T>
 void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3],
                         cudaStream_t s) {
+    if (F.D.wall) return wl_prolong_add<T>(F, Cc, phi_c, phi_f, s);
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
         k_prolong_add<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
@@ -1025,10 +1159,19 @@ void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pre
             k_coarsen<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.pa[0], Cc.pa[1], Cc.pa[2], nullptr, nullptr, nullptr, nullptr, nullptr, 0);
         return;
     }
+    const int dv = F.D.wall ? 2 : 1;
     if (F.D.dm == 2)
-        k_coarsen<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
+        k_coarsen<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], dv);
     else
-        k_coarsen<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], 1);
+        k_coarsen<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], dv);
+    if (F.D.wall) {
+        count_launch();
+        const G3 ge = geom3(Cc.D.nx + 1, Cc.D.ny + 1, Cc.D.dm == 3 ? Cc.D.nz + 1 : 1);
+        if (F.D.dm == 2)
+            k_coarsen_edges_w<T, 2><<<ge.grid, ge.block, 0, s>>>(F.D, Cc.D, F.bed[0], F.bed[1], F.bed[2], Cc.bed[0], Cc.bed[1], Cc.bed[2]);
+        else
+            k_coarsen_edges_w<T, 3><<<ge.grid, ge.block, 0, s>>>(F.D, Cc.D, F.bed[0], F.bed[1], F.bed[2], Cc.bed[0], Cc.bed[1], Cc.bed[2]);
+    }
 }
 
 template <class T>
@@ -1084,6 +1227,13 @@ template <class T>
 void launch_div_plus(const LevelDev<T>& L, const T* const u[3], const T* bp, T* out, cudaStream_t s) {
     const T dxinv = T(1.0 / L.dx);
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
+    if (L.D.wall) {
+        if (L.D.dm == 2)
+            k_div_plus<T, 2, true><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+        else
+            k_div_plus<T, 3, true><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+        return;
+    }
     if (L.D.dm == 2)
         k_div_plus<T, 2><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
     else
@@ -1097,6 +1247,13 @@ void launch_sub_weighted_grad(const LevelDev<T>& L, const T* const coef[3], cons
     const T* c0 = coef ? coef[0] : nullptr;
     const T* c1 = coef ? coef[1] : nullptr;
     const T* c2 = coef ? coef[2] : nullptr;
+    if (L.D.wall) {
+        if (L.D.dm == 2)
+            k_sub_weighted_grad<T, 2, true><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+        else
+            k_sub_weighted_grad<T, 3, true><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+        return;
+    }
     if (L.D.dm == 2)
         k_sub_weighted_grad<T, 2><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
     else

@@ -69,6 +69,21 @@ void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* co
 template <class T>
 void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s);
 
+// The same four operations on a grid with walls (walls.cuh; the launchers
+// above hand wall-bounded levels to these)
+template <class T>
+void wl_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color);
+template <class T>
+void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega, cudaStream_t s);
+template <class T>
+void wl_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const phi_in[3], T* const phi_out[3], double omega,
+               cudaStream_t s);
+template <class T>
+void wl_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3], const T* const phi_f[3],
+                          T* const rhs_c[3], cudaStream_t s);
+template <class T>
+void wl_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3], cudaStream_t s);
+
 // The coarse end of a V-cycle (levels L[0..nl-1], L[0] already holding its
 // rhs) in one single-block launch with every level in shared memory (tail.cuh).
 template <class T>

@@ -18,7 +18,10 @@ __device__ __forceinline__ void unflat3(const Dims& D, int t, int& i, int& j, in
 }  // namespace
 
 // b_u = stag_applyop(x_u) + grad(x_p);  b_p = -div(x_u)   (apply_matrix.f90:96-112)
-template <int DM, int VISC, class TX>
+// W: a grid with walls -- b_u is zero on the wall faces (the applyop is
+// zeroed there and the FOEXTRAP pressure has zero wall gradient), and the
+// divergence reads the hi+1 wall face as zero
+template <int DM, int VISC, class TX, bool W = false>
 __global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, const TX* __restrict__ u0,
                                                      const TX* __restrict__ u1, const TX* __restrict__ u2,
                                                      const TX* __restrict__ p, double* __restrict__ o0,
@@ -26,28 +29,40 @@ __global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, con
                                                      double dxsqinv, double dxinv) {
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
-    Nb nbr = make_nb(D, q.i, q.j, q.k);
+    Nb nbr = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
     const int t = nbr.s;
     const TX* phi[3] = {u0, u1, u2};
     const double b = ld(C.beta, 0), c = ld(C.gamma, 0);
     auto X = [](const TX* a, int i) { return (double)__ldg(a + i); };
+    auto XP = [&](const TX* a, int d) {
+        const double v = X(a, t + nbr.op[d]);
+        return W ? wapply(wall_mul(nbr, d, d, true), v) : v;
+    };
     const double pc = X(p, t);
-    {
-        double L = face_L<double, DM, VISC, 0, 0, TX>(phi, C, nbr, dxsqinv, b, c);
+    if (W && wall_face(nbr, 0)) {
+        o0[t] = 0.0;
+    } else {
+        double L = face_L<double, DM, VISC, 0, 0, TX, W>(phi, C, nbr, dxsqinv, b, c);
         double g = (pc - X(p, t + nbr.om[0])) * dxinv;
         o0[t] = L + g;
     }
-    {
-        double L = face_L<double, DM, VISC, 1, 0, TX>(phi, C, nbr, dxsqinv, b, c);
+    if (W && wall_face(nbr, 1)) {
+        o1[t] = 0.0;
+    } else {
+        double L = face_L<double, DM, VISC, 1, 0, TX, W>(phi, C, nbr, dxsqinv, b, c);
         double g = (pc - X(p, t + nbr.om[1])) * dxinv;
         o1[t] = L + g;
     }
-    double dv = (X(u0, t + nbr.op[0]) - X(u0, t)) * dxinv + (X(u1, t + nbr.op[1]) - X(u1, t)) * dxinv;
+    double dv = (XP(u0, 0) - X(u0, t)) * dxinv + (XP(u1, 1) - X(u1, t)) * dxinv;
     if constexpr (DM == 3) {
-        double L = face_L<double, DM, VISC, 2, 0, TX>(phi, C, nbr, dxsqinv, b, c);
-        double g = (pc - X(p, t + nbr.om[2])) * dxinv;
-        o2[t] = L + g;
-        dv = dv + (X(u2, t + nbr.op[2]) - X(u2, t)) * dxinv;
+        if (W && wall_face(nbr, 2)) {
+            o2[t] = 0.0;
+        } else {
+            double L = face_L<double, DM, VISC, 2, 0, TX, W>(phi, C, nbr, dxsqinv, b, c);
+            double g = (pc - X(p, t + nbr.om[2])) * dxinv;
+            o2[t] = L + g;
+        }
+        dv = dv + (XP(u2, 2) - X(u2, t)) * dxinv;
     }
     op[t] = dv * -1.0;
 }
@@ -66,7 +81,11 @@ static void apply_matrix_impl(const LevelDev<double>& L0, int visc, const TX* xb
     const TX* x2 = (dm == 3) ? xb + 2 * n : xb;
     const TX* xp = xb + (int64_t)dm * n;
     double* b2 = (b.dm == 3) ? b.c(2) : b.c(0);
-#define AM(DM_, V_) k_apply_matrix<DM_, V_, TX><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
+#define AM(DM_, V_)                                                                                                        \
+    if (L0.D.wall)                                                                                                         \
+        k_apply_matrix<DM_, V_, TX, true><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv); \
+    else                                                                                                                   \
+        k_apply_matrix<DM_, V_, TX><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
 #define AMV(DM_)                    \
     switch (visc) {                 \
     case -1: AM(DM_, -1); break;    \
@@ -221,6 +240,7 @@ template void launch_schur<float>(int, int, int, double, const float*, const flo
                                   const float*, float*, int64_t, cudaStream_t);
 
 // ---------------------------------------------------------------- mean removal
+// sub_u: bit d set = remove the mean of velocity component d
 template <class T, int DM>
 __global__ void k_sub_means(Dims D, T* u0, T* u1, T* u2, T* p, const double* __restrict__ sums, double total_volume, int sub_u) {
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -232,6 +252,7 @@ __global__ void k_sub_means(Dims D, T* u0, T* u1, T* u2, T* p, const double* __r
         T* u[3] = {u0, u1, u2};
 #pragma unroll
         for (int d = 0; d < DM; ++d) {
+            if (!((sub_u >> d) & 1)) continue;
             const double mu = sums[d] / total_volume;
             u[d][t] = (T)((double)u[d][t] - mu);
         }
@@ -286,6 +307,81 @@ void launch_gather_boxlib(const Dims& D, const int nodal[3], int ng, const doubl
     const int ex = D.nx + nodal[0] + 2 * ng, ey = D.ny + nodal[1] + 2 * ng;
     int64_t n = (int64_t)D.nx * D.ny * D.nz;
     k_gather_boxlib<<<nb(n), kT, 0, s>>>(D, ex, ey, ng, in, out);
+}
+
+// compact array with extents (cx, cy, cz) (an edge array of a grid with
+// walls keeps n+1 nodes along a nodal wall-bounded direction) from its
+// BoxLib array (n + nodal + 2 ng entries per direction)
+__global__ void k_gather_boxlib_ext(int cx, int cy, int cz, int dm, int ex, int ey, int ng, const double* __restrict__ in,
+                                    double* __restrict__ out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= cx * cy * cz) return;
+    const int i = t % cx, r = t / cx, j = r % cy, k = r / cy;
+    const int kg = (dm == 3) ? ng : 0;
+    out[t] = in[(int64_t)(i + ng) + (int64_t)ex * ((j + ng) + (int64_t)ey * (k + kg))];
+}
+
+void launch_gather_boxlib_ext(const Dims& D, const int cext[3], const int nodal[3], int ng, const double* in, double* out,
+                              cudaStream_t s) {
+    const int ex = D.nx + nodal[0] + 2 * ng, ey = D.ny + nodal[1] + 2 * ng;
+    const int cz = (D.dm == 3) ? cext[2] : 1;
+    k_gather_boxlib_ext<<<nb((int64_t)cext[0] * cext[1] * cz), kT, 0, s>>>(cext[0], cext[1], cz, D.dm, ex, ey, ng, in, out);
+}
+
+// BoxLib output of a grid with walls, per direction: periodic -> the image;
+// wall, for the face component normal to it -> zero outside lo+1..hi; wall,
+// otherwise -> the nearest valid entry, negated for a transverse velocity
+// at a no-slip wall.  kind = face component, or -1 for cells.
+__global__ void k_scatter_boxlib_w(Dims D, int kind, int ex, int ey, int ez, int ng, const double* __restrict__ in,
+                                   double* __restrict__ out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ex * ey * ez) return;
+    const int r = t / ex;
+    int x[3] = {t % ex - ng, r % ey - ng, (D.dm == 3) ? r / ey - ng : 0};
+    const int n[3] = {D.nx, D.ny, D.nz};
+    double sgn = 1.0;
+    for (int d = 0; d < D.dm; ++d) {
+        int& v = x[d];
+        if (!((D.wall >> d) & 1)) {
+            v = ((v % n[d]) + n[d]) % n[d];
+            continue;
+        }
+        if (kind == d) {
+            if (v <= 0 || v >= n[d]) sgn = 0.0;
+            v = v < 0 ? 0 : (v > n[d] - 1 ? n[d] - 1 : v);
+            continue;
+        }
+        if (v < 0) {
+            v = 0;
+            if (kind >= 0 && !((D.slip_lo >> d) & 1)) sgn = -sgn;
+        } else if (v > n[d] - 1) {
+            v = n[d] - 1;
+            if (kind >= 0 && !((D.slip_hi >> d) & 1)) sgn = -sgn;
+        }
+    }
+    const double v = (sgn == 0.0) ? 0.0 : in[(int64_t)x[0] + (int64_t)D.nx * (x[1] + (int64_t)D.ny * x[2])];
+    out[t] = (sgn < 0.0) ? -v : v;
+}
+
+void launch_scatter_boxlib_w(const Dims& D, int kind, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s) {
+    const int ex = D.nx + nodal[0] + 2 * ng, ey = D.ny + nodal[1] + 2 * ng;
+    const int ez = (D.dm == 3) ? D.nz + nodal[2] + 2 * ng : 1;
+    k_scatter_boxlib_w<<<nb((int64_t)ex * ey * ez), kT, 0, s>>>(D, kind, ex, ey, ez, ng, in, out);
+}
+
+// zero face 0 of each wall-normal component along its wall-bounded direction
+__global__ void k_zero_wall_faces(Dims D, double* u0, double* u1, double* u2) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= D.nx * D.ny * D.nz) return;
+    int i, j, k;
+    unflat3(D, t, i, j, k);
+    if ((D.wall & 1) && i == 0) u0[t] = 0.0;
+    if (((D.wall >> 1) & 1) && j == 0) u1[t] = 0.0;
+    if (D.dm == 3 && ((D.wall >> 2) & 1) && k == 0) u2[t] = 0.0;
+}
+
+void launch_zero_wall_faces(const Dims& D, double* const u[3], cudaStream_t s) {
+    k_zero_wall_faces<<<nb((int64_t)D.nx * D.ny * D.nz), kT, 0, s>>>(D, u[0], u[1], D.dm == 3 ? u[2] : u[0]);
 }
 
 void launch_scatter_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s) {

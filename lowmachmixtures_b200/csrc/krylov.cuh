@@ -59,7 +59,7 @@ void launch_add_scaled_f32(double* x, const float* Z, double y, int64_t n, cudaS
 template <class T>
 void launch_schur(int mode, int precon_type, int visc_abs, double theta_alpha, const T* mac_rhs, const T* src,
                   const T* beta, const T* gamma, T* phi, const T* bp, T* xp, int64_t n, cudaStream_t s);
-// x_p -= <p>; x_u[d] -= <u_d> when sub_u (means from reduction slots)
+// x_p -= <p>; x_u[d] -= <u_d> for each bit d of sub_u (means from reduction slots)
 template <class T>
 void launch_sub_means(const Dims& D, T* const u[3], T* p, const double* sums, double total_volume, int sub_u,
                       cudaStream_t s);
@@ -68,5 +68,13 @@ void launch_sub_means(const Dims& D, T* const u[3], T* p, const double* sums, do
 void launch_gather_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s);
 void launch_scatter_boxlib(const Dims& D, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s);
 int64_t boxlib_size(const Dims& D, const int nodal[3], int ng);
+// walls: gather into compact extents cext (edge arrays keep n+1 nodes along
+// a nodal wall-bounded direction); scatter a face component (kind = c) or
+// the cell field (kind = -1) with the wall ghost rules
+void launch_gather_boxlib_ext(const Dims& D, const int cext[3], const int nodal[3], int ng, const double* in, double* out,
+                              cudaStream_t s);
+void launch_scatter_boxlib_w(const Dims& D, int kind, const int nodal[3], int ng, const double* in, double* out, cudaStream_t s);
+// zero the wall faces (face 0 of each wall-normal component)
+void launch_zero_wall_faces(const Dims& D, double* const u[3], cudaStream_t s);
 
 }  // namespace lmm

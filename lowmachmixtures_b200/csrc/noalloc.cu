@@ -74,6 +74,7 @@ extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* cons
     D.ny = n[1];
     D.nz = dm == 3 ? n[2] : 1;
     D.dm = dm;
+    D.wall = D.slip_lo = D.slip_hi = 0;
     // each periodic seam face is stored once and weighed 1.5 per stored copy
     // in the reference's two copies (as lmm_op_inner_prod)
     const double w = 3.0;

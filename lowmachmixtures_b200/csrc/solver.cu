@@ -167,6 +167,30 @@ cudaError_t host_wait(lmm_handle* h) {
     return cudaEventSynchronize(h->wait_ev);
 }
 
+bool bc_wall(int c) { return (c >= 100 && c <= 103) || (c >= 200 && c <= 203); }  // bc.f90:23-35
+bool bc_noslip(int c) { return c >= 100 && c <= 103; }
+
+// the grid's wall bits (Dims::wall / slip_lo / slip_hi)
+void set_walls(Dims& D, const lmm_grid& g) {
+    D.wall = D.slip_lo = D.slip_hi = 0;
+    for (int d = 0; d < g.dm; ++d) {
+        if (g.bc_lo[d] == LMM_BC_PERIODIC) continue;
+        D.wall |= 1 << d;
+        if (!bc_noslip(g.bc_lo[d])) D.slip_lo |= 1 << d;
+        if (!bc_noslip(g.bc_hi[d])) D.slip_hi |= 1 << d;
+    }
+}
+
+// velocity components whose mean apply_precon removes
+// (apply_precon.f90:439-458): with theta alpha = 0 and no no-slip wall, the
+// periodic directions
+int mean_mask(const lmm_handle* h, double theta) {
+    if (theta != 0.0) return 0;
+    for (int d = 0; d < h->dm; ++d)
+        if (bc_noslip(h->grid.bc_lo[d]) || bc_noslip(h->grid.bc_hi[d])) return 0;
+    return ((1 << h->dm) - 1) & ~h->D0.wall;
+}
+
 int64_t level_cells(const int n[3], int dm, int lev) {
     int64_t c = 1;
     for (int d = 0; d < dm; ++d) c *= (n[d] >> lev);
@@ -180,10 +204,17 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
     auto add = [&](int64_t count, size_t sz) { tot += ((size_t)count * sz + 255) & ~(size_t)255; };
     for (int l = 0; l < std::max(nlev, nlev_p); ++l) {
         int64_t c = level_cells(g.n, dm, l);
+        Dims Dl;
+        Dl.dm = dm;
+        Dl.nx = g.n[0] >> l;
+        Dl.ny = g.n[1] >> l;
+        Dl.nz = (dm == 3) ? (g.n[2] >> l) : 1;
+        set_walls(Dl, g);
         for (int prec = 0; prec < 2; ++prec) {
             size_t sz = prec ? sizeof(float) : sizeof(double);
             if (l < nlev) {
-                for (int q = 0; q < 4 * dm + ne + 2; ++q) add(c, sz);  // alpha, phi, rhs, tmp, bed, beta, gamma
+                for (int q = 0; q < 4 * dm + 2; ++q) add(c, sz);     // alpha, phi, rhs, tmp, beta, gamma
+                for (int e = 0; e < ne; ++e) add(edge_count(Dl, e), sz);  // bed (n+1 nodes along walls)
             }
             if (l < nlev_p) {
                 for (int q = 0; q < dm + 3; ++q) add(c, sz);
@@ -241,13 +272,14 @@ void build_levels(lmm_handle* h) {
         v.D.nx = h->grid.n[0] >> l;
         v.D.ny = h->grid.n[1] >> l;
         v.D.nz = (dm == 3) ? (h->grid.n[2] >> l) : 1;
+        set_walls(v.D, h->grid);
         v.dx = h->grid.dx * (double)(1 << l);
         v.n = (int64_t)v.D.nx * v.D.ny * v.D.nz;
         if (l < h->nlev) {
             // the coefficients first and contiguous (one L2 persistence window
             // can cover them), then the fields
             for (int d = 0; d < dm; ++d) v.alpha[d] = h->alloc<T>(v.n);
-            for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) v.bed[e] = h->alloc<T>(v.n);
+            for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) v.bed[e] = h->alloc<T>(edge_count(v.D, e));
             v.beta = h->alloc<T>(v.n);
             v.gamma = h->alloc<T>(v.n);
             for (int d = 0; d < dm; ++d) {
@@ -366,7 +398,8 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
         LMM_CK(cudaMemsetAsync(L0.gamma, 0, n * sizeof(double), h->stream));
     }
     for (int e = 0; e < (dm == 2 ? 1 : 3); ++e)
-        if (bed[e] != L0.bed[e]) LMM_CK(cudaMemcpyAsync(L0.bed[e], bed[e], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        if (bed[e] != L0.bed[e])
+            LMM_CK(cudaMemcpyAsync(L0.bed[e], bed[e], edge_count(L0.D, e) * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     for (int l = 1; l < h->nlev; ++l) {
         launch_coarsen_coeffs<double>(h->L64[l - 1], h->L64[l], false, h->stream);
         check_launch();
@@ -375,6 +408,12 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
     if (h->nlev_p > 0) {
         for (int d = 0; d < dm; ++d)
             LMM_CK(cudaMemcpyAsync(h->L64[0].pa[d], h->alphainv[d], n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        if (h->D0.wall) {
+            // homogeneous Neumann pressure at walls: no flux crosses a wall
+            // face on any level (coarsening averages the zeros)
+            launch_zero_wall_faces(h->D0, h->L64[0].pa, h->stream);
+            check_launch();
+        }
         for (int l = 1; l < h->nlev_p; ++l) {
             launch_coarsen_coeffs<double>(h->L64[l - 1], h->L64[l], true, h->stream);
             check_launch();
@@ -400,7 +439,8 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
             LevelDev<float>& b = h->L32[l];
             if (l < h->nlev) {
                 for (int d = 0; d < dm; ++d) launch_convert<double, float>(a.alpha[d], b.alpha[d], a.n, h->stream);
-                for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) launch_convert<double, float>(a.bed[e], b.bed[e], a.n, h->stream);
+                for (int e = 0; e < (dm == 2 ? 1 : 3); ++e)
+                    launch_convert<double, float>(a.bed[e], b.bed[e], edge_count(a.D, e), h->stream);
                 launch_convert<double, float>(a.beta, b.beta, a.n, h->stream);
                 launch_convert<double, float>(a.gamma, b.gamma, a.n, h->stream);
             }
@@ -458,6 +498,7 @@ template <class T>
 int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool stag) {
     const int cells = h->knobs.tail_cells == 0 ? 4096 : h->knobs.tail_cells;
     if (cells < 0) return nl;
+    if (stag && h->D0.wall) return nl;  // the staggered tail kernel is periodic only
     const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
     const bool jacobi = stag && h->knobs.stag_mg_smoother == 0;
     int lc = nl;
@@ -831,11 +872,11 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
     default:
         throw LmmError(LMM_ERR_INVALID);
     }
-    // mean removal (apply_precon.f90:433-460); periodic: no no-slip walls
+    // mean removal (apply_precon.f90:433-460)
     reduce_means<T>(h, x_u, x_p, mean_slot);
     double tv = 1.0;
     for (int d = 0; d < dm; ++d) tv *= (double)h->grid.n[d];
-    launch_sub_means<T>(h->D0, x_u, x_p, h->slot(mean_slot), tv, theta == 0.0 ? 1 : 0, h->stream);
+    launch_sub_means<T>(h->D0, x_u, x_p, h->slot(mean_slot), tv, mean_mask(h, theta), h->stream);
     check_launch();
 }
 
@@ -1141,7 +1182,7 @@ void learned_stage(lmm_handle* h, const SVec& c, const SVec& v, int mode) {
         reduce_means<double>(h, cu, c.p(), S3);
         double tv = 1.0;
         for (int d = 0; d < h->dm; ++d) tv *= (double)h->grid.n[d];
-        launch_sub_means<double>(h->D0, cu, c.p(), h->slot(S3), tv, h->theta_loaded == 0.0 ? 1 : 0, h->stream);
+        launch_sub_means<double>(h->D0, cu, c.p(), h->slot(S3), tv, mean_mask(h, h->theta_loaded), h->stream);
         check_launch();
     }
     launch_apply_matrix(h->L64[0], h->knobs.visc_type, c, h->lAc, h->stream);
@@ -1261,12 +1302,15 @@ int validate(const lmm_grid* g, const lmm_knobs* k) {
     if (!g || !k) return LMM_ERR_INVALID;
     if (g->dm != 2 && g->dm != 3) return LMM_ERR_INVALID;
     if (!(g->dx > 0.0)) return LMM_ERR_INVALID;
+    bool walls = false;
     for (int d = 0; d < g->dm; ++d) {
         if (g->n[d] < 2) return LMM_ERR_INVALID;
-        if (g->bc_lo[d] != LMM_BC_PERIODIC || g->bc_hi[d] != LMM_BC_PERIODIC) {
-            g_last_error = "only periodic boundaries are supported";
+        const bool per = g->bc_lo[d] == LMM_BC_PERIODIC && g->bc_hi[d] == LMM_BC_PERIODIC;
+        if (!per && !(bc_wall(g->bc_lo[d]) && bc_wall(g->bc_hi[d]))) {
+            g_last_error = "a direction is periodic on both sides or bounded by walls (100-103 no-slip, 200-203 slip) on both";
             return LMM_ERR_INVALID;
         }
+        walls = walls || !per;
     }
     const int av = std::abs(k->visc_type);
     if (av < 1 || av > 3) return LMM_ERR_INVALID;
@@ -1297,6 +1341,22 @@ int validate(const lmm_grid* g, const lmm_knobs* k) {
     int nl = compute_nlevs(g->n, g->dm, k->stag_mg_minwidth);
     for (int d = 0; d < g->dm; ++d)
         if ((g->n[d] >> (nl - 1)) << (nl - 1) != g->n[d]) return LMM_ERR_INVALID;
+    if (walls) {
+        if (k->visc_schur_approx == 1) {
+            g_last_error = "the BFBt Schur approximation (visc_schur_approx = 1) needs a periodic box";
+            return LMM_ERR_INVALID;
+        }
+        if (k->learned_stage > 0) {
+            g_last_error = "the learned stage needs a periodic box";
+            return LMM_ERR_INVALID;
+        }
+        const int nlp = compute_nlevs(g->n, g->dm, k->mg_minwidth);
+        for (int d = 0; d < g->dm; ++d)
+            if ((g->n[d] >> (nl - 1)) < 2 || (g->n[d] >> (nlp - 1)) < 2) {
+                g_last_error = "with walls every multigrid level needs at least 2 cells per direction";
+                return LMM_ERR_INVALID;
+            }
+    }
     return LMM_OK;
 }
 
@@ -1383,6 +1443,7 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         h->D0.nx = g->n[0];
         h->D0.ny = g->n[1];
         h->D0.nz = (g->dm == 3) ? g->n[2] : 1;
+        set_walls(h->D0, *g);
         h->n = (int64_t)h->D0.nx * h->D0.ny * h->D0.nz;
         h->nlev = compute_nlevs(g->n, g->dm, k->stag_mg_minwidth);
         const int ap = std::abs(k->precon_type);
@@ -1399,7 +1460,7 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         build_levels<double>(h);
         if (k->precision == LMM_PRECISION_FP32) {
             build_levels<float>(h);
-            if (k->l2_persist > 0) set_l2_window(h);
+            if (k->l2_persist > 0 && !h->D0.wall) set_l2_window(h);
         }
         const int dm = h->dm;
         for (int d = 0; d < dm; ++d) {
@@ -1505,6 +1566,17 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
     else
         LMM_CK(cudaMemcpyAsync(h->x.p(), x0_p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     check_launch();
+    if (h->D0.wall) {
+        // wall-normal velocities on the walls are not unknowns: zero in x
+        // (apply_matrix's physbc_domainvel) and in b (the reference's
+        // preconditioner zeroes them in every correction)
+        double* bu[3] = {h->b.c(0), h->b.c(1), dm == 3 ? h->b.c(2) : h->b.c(0)};
+        double* xu[3] = {h->x.c(0), h->x.c(1), dm == 3 ? h->x.c(2) : h->x.c(0)};
+        launch_zero_wall_faces(h->D0, bu, h->stream);
+        check_launch();
+        launch_zero_wall_faces(h->D0, xu, h->stream);
+        check_launch();
+    }
     // coefficients (beta, beta_ed, gamma scaled by scale_factor)
     const double* beta = in->beta;
     const double* bed[3] = {in->beta_ed[0], in->beta_ed[1], in->beta_ed[2]};
@@ -1513,7 +1585,7 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
         launch_scale_copy<double>(in->beta, L0.beta, sf, n, h->stream);
         beta = L0.beta;
         for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) {
-            launch_scale_copy<double>(in->beta_ed[e], L0.bed[e], sf, n, h->stream);
+            launch_scale_copy<double>(in->beta_ed[e], L0.bed[e], sf, edge_count(L0.D, e), h->stream);
             bed[e] = L0.bed[e];
         }
         if (gamma) {
@@ -1581,9 +1653,12 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
         // host -> device: inputs land in the level-0 / Krylov buffers
         LevelDev<double>& L0 = h->L64[0];
         // staging targets: b -> r, x0 -> w, coefficients -> their level-0 homes
-        auto upload = [&](const double* src, double* dst, int layout, int ng, const int nodal[3]) {
+        // cext: compact extents (an edge array of a grid with walls keeps
+        // n+1 nodes along a nodal wall-bounded direction)
+        auto upload = [&](const double* src, double* dst, int layout, int ng, const int nodal[3], const int* cext = nullptr) {
+            const int64_t cn = cext ? (int64_t)cext[0] * cext[1] * (dm == 3 ? cext[2] : 1) : n;
             if (layout == LMM_LAYOUT_COMPACT) {
-                LMM_CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                LMM_CK(cudaMemcpyAsync(dst, src, cn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
             } else {
                 int64_t sz = boxlib_size(D, nodal, ng);
                 if (sz > h->stage_elems || ng > 4) {
@@ -1591,7 +1666,10 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
                     throw LmmError(LMM_ERR_INVALID);
                 }
                 LMM_CK(cudaMemcpyAsync(h->stage, src, sz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-                launch_gather_boxlib(D, nodal, ng, h->stage, dst, h->stream);
+                if (cext)
+                    launch_gather_boxlib_ext(D, cext, nodal, ng, h->stage, dst, h->stream);
+                else
+                    launch_gather_boxlib(D, nodal, ng, h->stage, dst, h->stream);
                 check_launch();
             }
         };
@@ -1608,7 +1686,10 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
         upload(in->b_p, h->r.p(), lay, in->ng_b_p, nod_cell);
         upload(out->x_p, h->w.p(), out->layout, out->ng_x_p, nod_cell);
         upload(in->beta, L0.beta, lay, in->ng_beta, nod_cell);
-        for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) upload(in->beta_ed[e], L0.bed[e], lay, in->ng_beta_ed, nod_edge[e]);
+        for (int e = 0; e < (dm == 2 ? 1 : 3); ++e) {
+            const int cext[3] = {edge_ext(D, e, 0), edge_ext(D, e, 1), edge_ext(D, e, 2)};
+            upload(in->beta_ed[e], L0.bed[e], lay, in->ng_beta_ed, nod_edge[e], D.wall ? cext : nullptr);
+        }
         if (in->gamma) upload(in->gamma, L0.gamma, lay, in->ng_gamma, nod_cell);
         LMM_CK(host_wait(h));
         auto t1 = std::chrono::steady_clock::now();
@@ -1628,20 +1709,23 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
         LMM_CK(cudaEventRecord(h->ev1, h->stream));
         // device -> host
         if (rc >= 0 || rc == LMM_ERR_BREAKDOWN || rc == LMM_ERR_NONFINITE) {
-            auto download = [&](const double* src, double* dst, int layout, int ng, const int nodal[3]) {
+            auto download = [&](const double* src, double* dst, int layout, int ng, const int nodal[3], int kind) {
                 if (layout == LMM_LAYOUT_COMPACT) {
                     LMM_CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
                 } else {
                     int64_t sz = boxlib_size(D, nodal, ng);
                     if (sz > h->stage_elems || ng > 4) throw LmmError(LMM_ERR_INVALID);
-                    launch_scatter_boxlib(D, nodal, ng, src, h->stage, h->stream);
+                    if (D.wall)
+                        launch_scatter_boxlib_w(D, kind, nodal, ng, src, h->stage, h->stream);
+                    else
+                        launch_scatter_boxlib(D, nodal, ng, src, h->stage, h->stream);
                     check_launch();
                     LMM_CK(cudaMemcpyAsync(dst, h->stage, sz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
                     LMM_CK(host_wait(h));
                 }
             };
-            for (int d = 0; d < dm; ++d) download(h->x.c(d), out->x_u[d], out->layout, out->ng_x_u, nod_face[d]);
-            download(h->x.p(), out->x_p, out->layout, out->ng_x_p, nod_cell);
+            for (int d = 0; d < dm; ++d) download(h->x.c(d), out->x_u[d], out->layout, out->ng_x_u, nod_face[d], d);
+            download(h->x.p(), out->x_p, out->layout, out->ng_x_p, nod_cell, -1);
         }
         LMM_CK(host_wait(h));
         auto t2 = std::chrono::steady_clock::now();
@@ -1910,6 +1994,10 @@ extern "C" int lmm_stokes_set_net(lmm_handle* h, lmm_net* net) {
         if (net) {
             int nx, ny, nz, B;
             nn::net_dims(net, &nx, &ny, &nz, &B);
+            if (h->D0.wall) {
+                g_last_error = "the learned stage needs a periodic box";
+                return LMM_ERR_INVALID;
+            }
             if (h->dm != 3 || nx != h->grid.n[0] || ny != h->grid.n[1] || nz != h->grid.n[2]) {
                 g_last_error = "the network's grid differs from the solver's (3D only)";
                 return LMM_ERR_INVALID;

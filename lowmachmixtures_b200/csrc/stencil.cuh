@@ -1,5 +1,5 @@
-// stencil.cuh - per-face staggered viscous operator on the compact periodic
-// layout (device side).
+// stencil.cuh - per-face staggered viscous operator on the compact layout
+// (device side), periodic or with walls.
 //
 // One face value of  L phi = theta*alpha phi - div(beta grad phi [+ grad^T]) ...
 // exactly as src_common/stag_applyop.f90:204-1067 writes it, and the diagonal
@@ -13,6 +13,15 @@
 // idx-e_d and idx.  The two transverse directions t1 < t2 and the edge arrays
 // follow the Fortran: x faces use (xy, xz), y faces (xy, yz), z faces
 // (xz, yz); 2D uses the single nodal beta_ed.
+//
+// Walls (template flag W): along a wall-bounded direction d the face array of
+// component d stores faces lo..hi, face lo being the wall (kept zero) and the
+// wall face hi+1 implied zero; every other array stores its n cells; an edge
+// array nodal in d stores n+1 nodes.  Neighbour values across a wall follow
+// the reference's ghost fills (multifab_physbc_stag.f90): the wall-normal
+// component is zero on and behind the wall (physbc_domainvel), a transverse
+// component's ghost is -interior at a no-slip wall and +interior at a slip
+// wall (physbc_macvel).
 #pragma once
 #include <cstdint>
 
@@ -20,15 +29,24 @@ namespace lmm {
 
 // neighbour offsets (with periodic wrap) of one index; 32-bit indices
 // (a field holds at most 2^31 - 1 entries)
+struct Dims {
+    int nx, ny, nz;  // nz == 1 in 2D
+    int dm;
+    // bit d of wall: direction d is bounded by walls (else periodic); bit d
+    // of slip_lo / slip_hi: that wall is a slip wall (else no-slip).  Plain
+    // members (Dims sits in shared-memory structs): every Dims built sets
+    // them, all zero for a periodic box.
+    int wall, slip_lo, slip_hi;
+};
+
 struct Nb {
     int s;       // linear index
     int op[3];   // offset to +1 in direction d
     int om[3];   // offset to -1 in direction d
-};
-
-struct Dims {
-    int nx, ny, nz;  // nz == 1 in 2D
-    int dm;
+    // walls (make_nbw only): the position, the grid, and bit masks of the
+    // wall-bounded directions in which it is the first (lo) / last (hi) index
+    int i, j, k, lo, hi;
+    Dims D;
 };
 
 __device__ __forceinline__ Nb make_nb(const Dims& D, int i, int j, int k) {
@@ -47,6 +65,76 @@ __device__ __forceinline__ Nb make_nb(const Dims& D, int i, int j, int k) {
         b.om[2] = 0;
     }
     return b;
+}
+
+// Neighbours on a grid with walls: as make_nb, except that an offset does
+// not wrap across a wall (it is 0 at the wall-adjacent index; the value
+// read there is then scaled by wall_mul).
+__device__ __forceinline__ Nb make_nbw(const Dims& D, int i, int j, int k) {
+    Nb b = make_nb(D, i, j, k);
+    b.i = i;
+    b.j = j;
+    b.k = k;
+    b.lo = 0;
+    b.hi = 0;
+    b.D = D;
+    const int x[3] = {i, j, k}, n[3] = {D.nx, D.ny, D.nz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (d >= D.dm || !((D.wall >> d) & 1)) continue;
+        if (x[d] == 0) {
+            b.lo |= 1 << d;
+            b.om[d] = 0;
+        }
+        if (x[d] == n[d] - 1) {
+            b.hi |= 1 << d;
+            b.op[d] = 0;
+        }
+    }
+    return b;
+}
+
+// multiplier of the value of component c read at the +1 (plus) / -1
+// neighbour in direction d: 1 inside, 0 for the wall-normal component
+// across its wall, -1 / +1 for a transverse component at a no-slip / slip
+// wall (the neighbour offset is then 0: the ghost mirrors the face itself)
+__device__ __forceinline__ int wall_mul(const Nb& n, int c, int d, bool plus) {
+    const int bit = 1 << d;
+    if (!((plus ? n.hi : n.lo) & bit)) return 1;
+    if (d == c) return 0;
+    return ((plus ? n.D.slip_hi : n.D.slip_lo) & bit) ? 1 : -1;
+}
+template <class T>
+__device__ __forceinline__ T wapply(int m, T v) {
+    return m > 0 ? v : (m < 0 ? -v : T(0));
+}
+// true when the face of component c at this position is a wall face
+__device__ __forceinline__ bool wall_face(const Nb& n, int c) { return (n.lo >> c) & 1; }
+
+// edge array e (2D: the nodal array; 3D: 0 xy, 1 xz, 2 yz) is nodal in d
+__host__ __device__ __forceinline__ bool edge_nodal(int dm, int e, int d) {
+    if (dm == 2) return d < 2;
+    return (e == 0) ? (d != 2) : (e == 1 ? (d != 1) : (d != 0));
+}
+// entries of edge array e along direction d (n+1 along a nodal wall-bounded d)
+__host__ __device__ __forceinline__ int edge_ext(const Dims& D, int e, int d) {
+    const int n = (d == 0) ? D.nx : (d == 1 ? D.ny : D.nz);
+    return n + ((d < D.dm && ((D.wall >> d) & 1) && edge_nodal(D.dm, e, d)) ? 1 : 0);
+}
+__host__ __device__ __forceinline__ int64_t edge_count(const Dims& D, int e) {
+    return (int64_t)edge_ext(D, e, 0) * edge_ext(D, e, 1) * (D.dm == 3 ? edge_ext(D, e, 2) : 1);
+}
+// index of edge e at the face position of n, moved +1 along direction t
+// (t < 0: no move); a periodic direction wraps
+__device__ __forceinline__ int edge_at(const Nb& n, int e, int t) {
+    int x[3] = {n.i, n.j, n.k};
+    const int nn[3] = {n.D.nx, n.D.ny, n.D.nz};
+    if (t >= 0) {
+        x[t] += 1;
+        if (x[t] == nn[t] && !((n.D.wall >> t) & 1)) x[t] = 0;
+    }
+    const int ex = edge_ext(n.D, e, 0), ey = edge_ext(n.D, e, 1);
+    return x[0] + ex * (x[1] + ey * (n.D.dm == 3 ? x[2] : 0));
 }
 
 template <class T>
@@ -106,7 +194,7 @@ template <> struct Perm3<2> { static constexpr int t1 = 0, t2 = 1, e1 = 1, e2 = 
 // nb = {+x, -x, +y, -y, +z, -z} supplied by the caller (global memory for the
 // plain kernels, shared memory for the fused red/black pair); the other two
 // components and the coefficients are read through phi / C.
-template <class T, int VISC, int D, int LD = 0, class TP = T>
+template <class T, int VISC, int D, int LD = 0, class TP = T, bool W = false>
 __device__ __forceinline__ T face_L3_own(const T p0, const T (&nb)[6], const TP* const phi[3], const Coef<T>& C, const Nb& n,
                                          T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
@@ -123,8 +211,16 @@ __device__ __forceinline__ T face_L3_own(const T p0, const T (&nb)[6], const TP*
     const T pp1 = nb[2 * t1], pm1 = nb[2 * t1 + 1];
     const T pp2 = nb[2 * t2], pm2 = nb[2 * t2 + 1];
     // cross terms q(i,+t) , q(i) , q(i-d,+t) , q(i-d)
-    const T c10 = (T)ldp<LD>(q1, s + n.op[t1]), c11 = (T)ldp<LD>(q1, s), c12 = (T)ldp<LD>(q1, s + n.om[D] + n.op[t1]), c13 = (T)ldp<LD>(q1, s + n.om[D]);
-    const T c20 = (T)ldp<LD>(q2, s + n.op[t2]), c21 = (T)ldp<LD>(q2, s), c22 = (T)ldp<LD>(q2, s + n.om[D] + n.op[t2]), c23 = (T)ldp<LD>(q2, s + n.om[D]);
+    T c10 = (T)ldp<LD>(q1, s + n.op[t1]), c11 = (T)ldp<LD>(q1, s), c12 = (T)ldp<LD>(q1, s + n.om[D] + n.op[t1]), c13 = (T)ldp<LD>(q1, s + n.om[D]);
+    T c20 = (T)ldp<LD>(q2, s + n.op[t2]), c21 = (T)ldp<LD>(q2, s), c22 = (T)ldp<LD>(q2, s + n.om[D] + n.op[t2]), c23 = (T)ldp<LD>(q2, s + n.om[D]);
+    if constexpr (W) {
+        // component t across its own wall at +t is zero (the face is not a wall face, so -d stays inside)
+        const int m1 = wall_mul(n, t1, t1, true), m2 = wall_mul(n, t2, t2, true);
+        c10 = wapply(m1, c10);
+        c12 = wapply(m1, c12);
+        c20 = wapply(m2, c20);
+        c22 = wapply(m2, c22);
+    }
     if (VISC == 2) {
         return p0 * (a + T(8) * b * dxsqinv) -
                (T(2) * ppd + T(2) * pmd + pp1 + pm1 + pp2 + pm2 + c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * b * dxsqinv;
@@ -139,8 +235,8 @@ __device__ __forceinline__ T face_L3_own(const T p0, const T (&nb)[6], const TP*
                 (c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * (onethird * b + c)) * dxsqinv;
     }
     const T be = ld(C.beta, s), bm = ld(C.beta, s + n.om[D]);
-    const T E1 = ld(C.bed[e1], s), E1p = ld(C.bed[e1], s + n.op[t1]);
-    const T E2 = ld(C.bed[e2], s), E2p = ld(C.bed[e2], s + n.op[t2]);
+    const T E1 = ld(C.bed[e1], W ? edge_at(n, e1, -1) : s), E1p = ld(C.bed[e1], W ? edge_at(n, e1, t1) : s + n.op[t1]);
+    const T E2 = ld(C.bed[e2], W ? edge_at(n, e2, -1) : s), E2p = ld(C.bed[e2], W ? edge_at(n, e2, t2) : s + n.op[t2]);
     if (VISC == -1) {
         return p0 * (a + (be + bm + E1 + E1p + E2 + E2p) * dxsqinv) -
                (ppd * be + pmd * bm + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2) * dxsqinv;
@@ -159,17 +255,24 @@ __device__ __forceinline__ T face_L3_own(const T p0, const T (&nb)[6], const TP*
             c22 * (E2p - twothirds * bm + gm) + c23 * (E2 - twothirds * bm + gm)) * dxsqinv;
 }
 
-template <class T, int VISC, int D, int LD = 0, class TP = T>
+template <class T, int VISC, int D, int LD = 0, class TP = T, bool W = false>
 __device__ __forceinline__ T face_L3(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     const TP* p = phi[D];
     const int s = n.s;
     const T p0 = (T)ldp<LD>(p, s);
-    const T nb[6] = {(T)ldp<LD>(p, s + n.op[0]), (T)ldp<LD>(p, s + n.om[0]), (T)ldp<LD>(p, s + n.op[1]),
-                     (T)ldp<LD>(p, s + n.om[1]), (T)ldp<LD>(p, s + n.op[2]), (T)ldp<LD>(p, s + n.om[2])};
-    return face_L3_own<T, VISC, D, LD, TP>(p0, nb, phi, C, n, dxsqinv, b, c);
+    T nb[6] = {(T)ldp<LD>(p, s + n.op[0]), (T)ldp<LD>(p, s + n.om[0]), (T)ldp<LD>(p, s + n.op[1]),
+               (T)ldp<LD>(p, s + n.om[1]), (T)ldp<LD>(p, s + n.op[2]), (T)ldp<LD>(p, s + n.om[2])};
+    if constexpr (W) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            nb[2 * d] = wapply(wall_mul(n, D, d, true), nb[2 * d]);
+            nb[2 * d + 1] = wapply(wall_mul(n, D, d, false), nb[2 * d + 1]);
+        }
+    }
+    return face_L3_own<T, VISC, D, LD, TP, W>(p0, nb, phi, C, n, dxsqinv, b, c);
 }
 
-template <class T, int VISC, int D>
+template <class T, int VISC, int D, bool W = false>
 __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
     const int s = n.s;
@@ -178,8 +281,8 @@ __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv
     if (VISC == 2) return a + T(8) * b * dxsqinv;
     if (VISC == 3) return a + (T(20) / T(3) * b + T(2) * c) * dxsqinv;
     const T be = ld(C.beta, s), bm = ld(C.beta, s + n.om[D]);
-    const T E1 = ld(C.bed[e1], s), E1p = ld(C.bed[e1], s + n.op[t1]);
-    const T E2 = ld(C.bed[e2], s), E2p = ld(C.bed[e2], s + n.op[t2]);
+    const T E1 = ld(C.bed[e1], W ? edge_at(n, e1, -1) : s), E1p = ld(C.bed[e1], W ? edge_at(n, e1, t1) : s + n.op[t1]);
+    const T E2 = ld(C.bed[e2], W ? edge_at(n, e2, -1) : s), E2p = ld(C.bed[e2], W ? edge_at(n, e2, t2) : s + n.op[t2]);
     if (VISC == -1) return a + (be + bm + E1 + E1p + E2 + E2p) * dxsqinv;
     if (VISC == -2) return a + (T(2) * be + T(2) * bm + E1 + E1p + E2 + E2p) * dxsqinv;
     const T fourthirds = T(4) / T(3);
@@ -188,7 +291,7 @@ __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv
 }
 
 // ------------------------------------------------------------------ 2D
-template <class T, int VISC, int D, int LD = 0, class TP = T>
+template <class T, int VISC, int D, int LD = 0, class TP = T, bool W = false>
 __device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t = 1 - D;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
@@ -197,13 +300,24 @@ __device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, c
     const int s = n.s;
     const T p0 = (T)ldp<LD>(p, s);
     const T a = ld(C.alpha[D], s);
-    const T ppd = (T)ldp<LD>(p, s + n.op[D]), pmd = (T)ldp<LD>(p, s + n.om[D]);
-    const T ppt = (T)ldp<LD>(p, s + n.op[t]), pmt = (T)ldp<LD>(p, s + n.om[t]);
+    T ppd = (T)ldp<LD>(p, s + n.op[D]), pmd = (T)ldp<LD>(p, s + n.om[D]);
+    T ppt = (T)ldp<LD>(p, s + n.op[t]), pmt = (T)ldp<LD>(p, s + n.om[t]);
+    if constexpr (W) {
+        ppd = wapply(wall_mul(n, D, D, true), ppd);
+        pmd = wapply(wall_mul(n, D, D, false), pmd);
+        ppt = wapply(wall_mul(n, D, t, true), ppt);
+        pmt = wapply(wall_mul(n, D, t, false), pmt);
+    }
     if (VISC == 1) {
         // x: i+1, i-1, j+1, j-1 ; y: j+1, j-1, i+1, i-1  (own direction first)
         return p0 * (a + T(4) * b * dxsqinv) - (ppd + pmd + ppt + pmt) * b * dxsqinv;
     }
-    const T c0 = (T)ldp<LD>(q, s + n.op[t]), c1 = (T)ldp<LD>(q, s), c2 = (T)ldp<LD>(q, s + n.om[D] + n.op[t]), c3 = (T)ldp<LD>(q, s + n.om[D]);
+    T c0 = (T)ldp<LD>(q, s + n.op[t]), c1 = (T)ldp<LD>(q, s), c2 = (T)ldp<LD>(q, s + n.om[D] + n.op[t]), c3 = (T)ldp<LD>(q, s + n.om[D]);
+    if constexpr (W) {
+        const int m = wall_mul(n, t, t, true);
+        c0 = wapply(m, c0);
+        c2 = wapply(m, c2);
+    }
     if (VISC == 2) {
         return p0 * (a + T(6) * b * dxsqinv) - (T(2) * ppd + T(2) * pmd + ppt + pmt + c0 - c1 - c2 + c3) * b * dxsqinv;
     }
@@ -212,7 +326,7 @@ __device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, c
                ((ppd + pmd) * (fourthirds * b + c) + (ppt + pmt) * b + (c0 - c1 - c2 + c3) * (onethird * b + c)) * dxsqinv;
     }
     const T be = ld(C.beta, s), bm = ld(C.beta, s + n.om[D]);
-    const T E = ld(C.bed[0], s), Ep = ld(C.bed[0], s + n.op[t]);
+    const T E = ld(C.bed[0], W ? edge_at(n, 0, -1) : s), Ep = ld(C.bed[0], W ? edge_at(n, 0, t) : s + n.op[t]);
     if (VISC == -1) {
         return p0 * (a + (be + bm + Ep + E) * dxsqinv) - (ppd * be + pmd * bm + ppt * Ep + pmt * E) * dxsqinv;
     }
@@ -226,7 +340,7 @@ __device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, c
             c1 * (E - twothirds * be + g) - c2 * (Ep - twothirds * bm + gm) + c3 * (E - twothirds * bm + gm)) * dxsqinv;
 }
 
-template <class T, int VISC, int D>
+template <class T, int VISC, int D, bool W = false>
 __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t = 1 - D;
     const int s = n.s;
@@ -235,7 +349,7 @@ __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv
     if (VISC == 2) return a + T(6) * b * dxsqinv;
     if (VISC == 3) return a + (T(14) / T(3) * b + T(2) * c) * dxsqinv;
     const T be = ld(C.beta, s), bm = ld(C.beta, s + n.om[D]);
-    const T E = ld(C.bed[0], s), Ep = ld(C.bed[0], s + n.op[t]);
+    const T E = ld(C.bed[0], W ? edge_at(n, 0, -1) : s), Ep = ld(C.bed[0], W ? edge_at(n, 0, t) : s + n.op[t]);
     if (VISC == -1) return a + (be + bm + E + Ep) * dxsqinv;
     if (VISC == -2) return a + (T(2) * be + T(2) * bm + E + Ep) * dxsqinv;
     const T fourthirds = T(4) / T(3);
@@ -243,19 +357,19 @@ __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv
     return a + (fourthirds * be + g + fourthirds * bm + gm + E + Ep) * dxsqinv;
 }
 
-template <class T, int DM, int VISC, int D, int LD = 0, class TP = T>
+template <class T, int DM, int VISC, int D, int LD = 0, class TP = T, bool W = false>
 __device__ __forceinline__ T face_L(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     if constexpr (DM == 2)
-        return face_L2<T, VISC, D, LD, TP>(phi, C, n, dxsqinv, b, c);
+        return face_L2<T, VISC, D, LD, TP, W>(phi, C, n, dxsqinv, b, c);
     else
-        return face_L3<T, VISC, D, LD, TP>(phi, C, n, dxsqinv, b, c);
+        return face_L3<T, VISC, D, LD, TP, W>(phi, C, n, dxsqinv, b, c);
 }
-template <class T, int DM, int VISC, int D>
+template <class T, int DM, int VISC, int D, bool W = false>
 __device__ __forceinline__ T face_diag(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     if constexpr (DM == 2)
-        return face_diag2<T, VISC, D>(C, n, dxsqinv, b, c);
+        return face_diag2<T, VISC, D, W>(C, n, dxsqinv, b, c);
     else
-        return face_diag3<T, VISC, D>(C, n, dxsqinv, b, c);
+        return face_diag3<T, VISC, D, W>(C, n, dxsqinv, b, c);
 }
 
 }  // namespace lmm

@@ -105,6 +105,7 @@ extern "C" int lmm_stochastic_rhs(int dm, const int n[3], double dx, double dt, 
     A.D.nx = n[0];
     A.D.ny = n[1];
     A.D.nz = dm == 3 ? n[2] : 1;
+    A.D.wall = A.D.slip_lo = A.D.slip_hi = 0;
     if (A.D.nx < 1 || A.D.ny < 1 || A.D.nz < 1) return LMM_ERR_INVALID;
     double dV = 1.0;
     for (int d = 0; d < dm; ++d) dV *= dx;

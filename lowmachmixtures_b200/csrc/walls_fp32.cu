@@ -1,0 +1,7 @@
+// walls_fp32.cu - FP32 instantiation of the wall-bounded multigrid kernels
+// (the mixed-precision preconditioner's V-cycle on grids with walls).
+#include "walls.cuh"
+
+namespace lmm {
+LMM_INSTANTIATE_WALLS(float)
+}  // namespace lmm

@@ -71,10 +71,15 @@ contains
     g%n = 1
     g%n(1:dm) = hi - lo + 1
     g%dx = dx(1,1)
+    ! physical BC codes per side (bc.f90: -1 periodic, 100-103 no-slip
+    ! walls, 200-203 slip walls), as define_bc_tower received them
     g%bc_lo = LMM_BC_PERIODIC
     g%bc_hi = LMM_BC_PERIODIC
     do d = 1, dm
-       if (.not. mla%pmask(d)) call bl_error("gmres: only periodic domains are supported")
+       if (.not. mla%pmask(d)) then
+          g%bc_lo(d) = the_bc_tower%domain_bc(d,1)
+          g%bc_hi(d) = the_bc_tower%domain_bc(d,2)
+       end if
     end do
 
     call lmm_default_knobs(k)

@@ -17,6 +17,7 @@ module lmm_stokes_iface
   integer(c_int), parameter :: LMM_PRECISION_FP64 = 0
   integer(c_int), parameter :: LMM_PRECISION_FP32 = 1
   integer(c_int), parameter :: LMM_BC_PERIODIC = -1
+  integer(c_int), parameter :: LMM_BC_NO_SLIP_WALL = 100, LMM_BC_SLIP_WALL = 200
   integer(c_int), parameter :: LMM_HISTORY_MAX = 512
 
   type, bind(c) :: lmm_grid

@@ -30,17 +30,21 @@ def _is_torch(a) -> bool:
 
 
 class StokesSolver:
-    """A persistent solver for one periodic grid and one knob set (the
-    handle of lmm_stokes_create).  Reuse it across calls: device memory is
-    allocated once."""
+    """A persistent solver for one grid and one knob set (the handle of
+    lmm_stokes_create).  Reuse it across calls: device memory is allocated
+    once.  bc: None (periodic box) or per direction a BC code or (lo, hi)
+    pair -- LMM_BC_PERIODIC, no-slip walls 100-103, slip walls 200-203
+    (src_common/bc.f90:23-44), as the reference's bc_lo / bc_hi."""
 
-    def __init__(self, dm: int, n, dx: float, knobs: abi.Knobs | None = None, device: int = 0, **knob_overrides):
+    def __init__(self, dm: int, n, dx: float, knobs: abi.Knobs | None = None, device: int = 0, bc=None,
+                 **knob_overrides):
         self.lib = load()
         self.dm = int(dm)
         self.n = tuple(int(v) for v in n)[: self.dm]
         self.dx = float(dx)
+        self.bc = None if bc is None else tuple(bc)
         self.knobs = knobs if knobs is not None else abi.make_knobs(**knob_overrides)
-        self.grid = abi.make_grid(self.dm, self.n, self.dx)
+        self.grid = abi.make_grid(self.dm, self.n, self.dx, self.bc)
         self._h = C.c_void_p()
         check(self.lib.lmm_stokes_create(C.byref(self.grid), C.byref(self.knobs), int(device), C.byref(self._h)),
               "lmm_stokes_create")
