@@ -97,7 +97,7 @@ typedef struct lmm_grid {
  * fills the reference defaults. */
 typedef struct lmm_knobs {
     int    precon_type;            /* +-1 projection, +-2 lower triangular, +-3 upper, +-4 diagonal, +-5 */
-    int    visc_schur_approx;      /* 0 only (BFBt is not built) */
+    int    visc_schur_approx;      /* 0 local viscosity, 1 BFBt (apply_precon.f90:538-685; periodic box) */
     double p_norm_weight;
     double scale_factor;
     /* pressure (cell-centred) multigrid */
@@ -204,6 +204,17 @@ int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fields_out* out
 /* Same solve on device-resident LMM_LAYOUT_COMPACT arrays (no host copies). */
 int lmm_stokes_solve_device(lmm_handle* h, const lmm_fields_in* in_dev, lmm_fields_out* out_dev,
                             double* theta_alpha, double* norm_pre_rhs, lmm_stats* st);
+
+/* Change the stopping rules of a handle between solves: gmres_rel_tol,
+ * gmres_abs_tol, gmres_max_outer, gmres_max_iter, gmres_min_iter,
+ * stag_mg_rel_tol, mg_rel_tol and the verbosity knobs take the values of *k;
+ * every other field of *k must equal the handle's (LMM_ERR_INVALID and no
+ * change otherwise).  The time steppers move gmres_abs_tol between the
+ * predictor and corrector solves of one step
+ * (advance_timestep_overdamped.f90:311-323,568;
+ * advance_timestep_inertial.f90:476-488,796-818); this keeps the handle, its
+ * device memory and its captured graphs. */
+int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k);
 
 int lmm_stokes_destroy(lmm_handle* h);
 const char* lmm_strerror(int code);

@@ -33,6 +33,8 @@ def load() -> C.CDLL:
     lib.lmm_stokes_create.argtypes = [P(abi.Grid), P(abi.Knobs), C.c_int, P(C.c_void_p)]
     lib.lmm_stokes_create.restype = C.c_int
     lib.lmm_stokes_destroy.argtypes = [C.c_void_p]
+    lib.lmm_stokes_update_knobs.argtypes = [C.c_void_p, P(abi.Knobs)]
+    lib.lmm_stokes_update_knobs.restype = C.c_int
     for name in ("lmm_stokes_solve", "lmm_stokes_solve_device"):
         f = getattr(lib, name)
         f.argtypes = [C.c_void_p, P(abi.FieldsIn), P(abi.FieldsOut), P(C.c_double), P(C.c_double), P(abi.Stats)]

@@ -1516,6 +1516,42 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
     return LMM_OK;
 }
 
+int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
+    if (!h || !k) return LMM_ERR_INVALID;
+    g_last_error.clear();
+    const lmm_knobs& a = h->knobs;
+#define SAME(f) (a.f == k->f)
+    const bool same = SAME(precon_type) && SAME(visc_schur_approx) && SAME(p_norm_weight) && SAME(scale_factor) &&
+                      SAME(mg_max_vcycles) && SAME(mg_minwidth) && SAME(mg_bottom_solver) && SAME(mg_nsmooths_down) &&
+                      SAME(mg_nsmooths_up) && SAME(mg_nsmooths_bottom) && SAME(mg_max_bottom_nlevels) &&
+                      SAME(stag_mg_max_vcycles) && SAME(stag_mg_minwidth) && SAME(stag_mg_bottom_solver) &&
+                      SAME(stag_mg_nsmooths_down) && SAME(stag_mg_nsmooths_up) && SAME(stag_mg_nsmooths_bottom) &&
+                      SAME(stag_mg_max_bottom_nlevels) && SAME(stag_mg_omega) && SAME(stag_mg_smoother) &&
+                      SAME(gmres_max_inner) && SAME(visc_type) && SAME(method) && SAME(precision) &&
+                      SAME(learned_stage) && SAME(tail_cells) && SAME(tail_smem_kb) && SAME(use_graphs) &&
+                      SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait);
+#undef SAME
+    if (!same) {
+        g_last_error = "lmm_stokes_update_knobs changes only the stopping rules; create a new handle for the rest";
+        return LMM_ERR_INVALID;
+    }
+    if (!(k->gmres_rel_tol >= 0.0) || !(k->gmres_abs_tol >= 0.0) || k->gmres_max_iter < 0 || k->gmres_max_outer < 0 ||
+        k->gmres_min_iter < 0 || !(k->stag_mg_rel_tol >= 0.0) || !(k->mg_rel_tol >= 0.0))
+        return LMM_ERR_INVALID;
+    h->knobs.gmres_rel_tol = k->gmres_rel_tol;
+    h->knobs.gmres_abs_tol = k->gmres_abs_tol;
+    h->knobs.gmres_max_outer = k->gmres_max_outer;
+    h->knobs.gmres_max_iter = k->gmres_max_iter;
+    h->knobs.gmres_min_iter = k->gmres_min_iter;
+    h->knobs.stag_mg_rel_tol = k->stag_mg_rel_tol;
+    h->knobs.mg_rel_tol = k->mg_rel_tol;
+    h->knobs.gmres_verbose = k->gmres_verbose;
+    h->knobs.mg_verbose = k->mg_verbose;
+    h->knobs.cg_verbose = k->cg_verbose;
+    h->knobs.stag_mg_verbosity = k->stag_mg_verbosity;
+    return LMM_OK;
+}
+
 int lmm_stokes_destroy(lmm_handle* h) {
     if (!h) return LMM_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);

@@ -121,6 +121,12 @@ contains
        if (.not. same_setup(g, k)) then
           rc = lmm_stokes_destroy(handle)
           handle = c_null_ptr
+       else if (.not. same_stopping(k)) then
+          ! the time steppers move gmres_abs_tol between predictor and
+          ! corrector: keep the handle, change its stopping rules
+          rc = lmm_stokes_update_knobs(handle, k)
+          if (rc < 0) call bl_error("gmres: " // trim(lmm_message(rc)))
+          handle_knobs = k
        end if
     end if
     if (.not. c_associated(handle)) then
@@ -200,11 +206,21 @@ contains
            .and. ka%stag_mg_max_vcycles == handle_knobs%stag_mg_max_vcycles &
            .and. ka%mg_nsmooths_down == handle_knobs%mg_nsmooths_down .and. ka%mg_nsmooths_up == handle_knobs%mg_nsmooths_up &
            .and. ka%mg_nsmooths_bottom == handle_knobs%mg_nsmooths_bottom .and. ka%mg_max_vcycles == handle_knobs%mg_max_vcycles &
-           .and. ka%gmres_rel_tol == handle_knobs%gmres_rel_tol .and. ka%gmres_abs_tol == handle_knobs%gmres_abs_tol &
-           .and. ka%gmres_max_outer == handle_knobs%gmres_max_outer .and. ka%gmres_max_iter == handle_knobs%gmres_max_iter &
-           .and. ka%gmres_min_iter == handle_knobs%gmres_min_iter .and. ka%p_norm_weight == handle_knobs%p_norm_weight &
-           .and. ka%scale_factor == handle_knobs%scale_factor
+           .and. ka%p_norm_weight == handle_knobs%p_norm_weight &
+           .and. ka%scale_factor == handle_knobs%scale_factor &
+           .and. all(ga%bc_lo == handle_grid%bc_lo) .and. all(ga%bc_hi == handle_grid%bc_hi)
     end function same_setup
+
+    ! the knobs lmm_stokes_update_knobs may change on a live handle
+    logical function same_stopping(ka)
+      type(lmm_knobs), intent(in) :: ka
+      same_stopping = ka%gmres_rel_tol == handle_knobs%gmres_rel_tol .and. ka%gmres_abs_tol == handle_knobs%gmres_abs_tol &
+           .and. ka%gmres_max_outer == handle_knobs%gmres_max_outer .and. ka%gmres_max_iter == handle_knobs%gmres_max_iter &
+           .and. ka%gmres_min_iter == handle_knobs%gmres_min_iter .and. ka%mg_rel_tol == handle_knobs%mg_rel_tol &
+           .and. ka%stag_mg_rel_tol == handle_knobs%stag_mg_rel_tol .and. ka%gmres_verbose == handle_knobs%gmres_verbose &
+           .and. ka%mg_verbose == handle_knobs%mg_verbose .and. ka%cg_verbose == handle_knobs%cg_verbose &
+           .and. ka%stag_mg_verbosity == handle_knobs%stag_mg_verbosity
+    end function same_stopping
 
   end subroutine gmres
 

@@ -105,6 +105,13 @@ module lmm_stokes_iface
        integer(c_int) :: rc
      end function lmm_stokes_solve
 
+     function lmm_stokes_update_knobs(h, k) bind(c, name="lmm_stokes_update_knobs") result(rc)
+       import :: c_int, c_ptr, lmm_knobs
+       type(c_ptr), value :: h
+       type(lmm_knobs), intent(in) :: k
+       integer(c_int) :: rc
+     end function lmm_stokes_update_knobs
+
      function lmm_stokes_destroy(h) bind(c, name="lmm_stokes_destroy") result(rc)
        import :: c_int, c_ptr
        type(c_ptr), value :: h

@@ -72,6 +72,17 @@ class StokesSolver:
     def handle(self):
         return self._h
 
+    def update_knobs(self, **stopping):
+        """Change the stopping rules (gmres_rel_tol, gmres_abs_tol,
+        gmres_max_outer / max_iter / min_iter, stag_mg_rel_tol, mg_rel_tol,
+        verbosity) of this handle between solves (lmm_stokes_update_knobs)."""
+        k = abi.Knobs()
+        C.memmove(C.byref(k), C.byref(self.knobs), C.sizeof(abi.Knobs))
+        for name, v in stopping.items():
+            setattr(k, name, v)
+        check(self.lib.lmm_stokes_update_knobs(self._h, C.byref(k)), "lmm_stokes_update_knobs")
+        self.knobs = k
+
     def num_levels(self) -> int:
         return self.lib.lmm_op_num_levels(self._h)
 

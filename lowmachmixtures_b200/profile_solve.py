@@ -25,6 +25,7 @@ def main():
     ap.add_argument("--warm", type=int, default=1)
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=INT",
                     help="extra lmm_knobs integer field (repeatable), e.g. --knob tail_cells=512")
+    ap.add_argument("--bc", default="", help="BC code per direction, both sides, e.g. -1,100,-1 (default periodic)")
     a = ap.parse_args()
 
     import numpy as np
@@ -33,7 +34,8 @@ def main():
     from lowmachmixtures_b200 import abi, synth
     from lowmachmixtures_b200.gmres import StokesSolver
 
-    prob = synth.config_3d_128(0, n=a.n)
+    bc = tuple(int(v) for v in a.bc.split(",")) if a.bc else None
+    prob = synth.config_3d_128(0, n=a.n) if bc is None else synth.make_problem(3, a.n, 100.0, 0, theta_alpha=0.1 * a.n * a.n, bc=bc)
     kn = dict(precon_type=2, visc_type=-2)
     if a.method == "mixed":
         kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
@@ -46,7 +48,7 @@ def main():
     bu, bp = [dev(x) for x in prob.b_u], dev(prob.b_p)
     al, be, bed, ga = [dev(x) for x in prob.alpha_fc], dev(prob.beta), [dev(x) for x in prob.beta_ed], dev(prob.gamma)
     xu, xp = [torch.zeros_like(bu[0]) for _ in range(3)], torch.zeros_like(bp)
-    with StokesSolver(3, (a.n,) * 3, prob.dx, knobs=abi.make_knobs(**kn)) as s:
+    with StokesSolver(3, (a.n,) * 3, prob.dx, knobs=abi.make_knobs(**kn), bc=bc) as s:
         out = []
         for i in range(a.warm + a.solves):
             for t in xu:

@@ -5,6 +5,7 @@ import os
 
 import numpy as np
 
+from lowmachmixtures_b200 import abi
 from lowmachmixtures_b200.synth import StokesProblem
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -31,3 +32,32 @@ def rel_err(a, b):
     b = np.asarray(b)
     den = max(np.abs(b).max(), 1e-300)
     return float(np.abs(a - b).max() / den)
+
+
+class OracleSolver:
+    """The StokesSolver calls predictor_corrector makes, answered by the oracle."""
+
+    def __init__(self, prob, oracle, **kn):
+        self.prob, self.oracle = prob, oracle
+        self.dm, self.shape = prob.dm, prob.shape
+        self.knobs = abi.make_knobs(**kn)
+        self.calls = []
+
+    def update_knobs(self, **kw):
+        for k, v in kw.items():
+            setattr(self.knobs, k, v)
+
+    def solve(self, b_u, b_p, x_u, x_p, alpha_fc, beta, beta_ed, gamma, theta_alpha):
+        self.calls.append(float(self.knobs.gmres_abs_tol))
+        p = self.prob
+        saved = (p.b_u, p.b_p)
+        p.b_u, p.b_p = b_u, b_p
+        try:
+            rc, xu, xp, th, npr, st = self.oracle.solve(p, self.knobs, x_u=x_u, x_p=x_p, theta_alpha=theta_alpha)
+        finally:
+            p.b_u, p.b_p = saved
+        assert rc >= 0
+        for a, b in zip(x_u, xu):
+            a[...] = b
+        x_p[...] = xp
+        return th, npr, st
