@@ -464,9 +464,9 @@ __device__ __forceinline__ void prolong_cell(const Dims& Dc, const T* q0, const 
         const int x[3] = {i, j, k};
         if ((Dc.wall & 1) && x[0] == 0) f0 = nullptr;
         if (((Dc.wall >> 1) & 1) && x[1] == 0) f1 = nullptr;
-        if (DM == 3 && ((Dc.wall >> 2) & 1) && x[2] == 0) f2 = nullptr;
+        if constexpr (DM == 3)
+            if (((Dc.wall >> 2) & 1) && x[2] == 0) f2 = nullptr;
     }
-    (void)f2;
     const int i2 = i >> 1, j2 = j >> 1, k2 = k >> 1;
     if constexpr (DM == 2) {
         if (!W || f0) {

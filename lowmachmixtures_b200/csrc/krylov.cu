@@ -129,6 +129,21 @@ void launch_div_by(const double* w, double* v, const double* den, int64_t n, cud
     k_div_by<<<nb(n), kT, 0, s>>>(w, v, den, n);
 }
 
+// v = w / *den, and v32 = (float)v: the next FGMRES basis vector together
+// with the FP32 input of the preconditioner that reads it next
+__global__ void k_div_by_f32(const double* __restrict__ w, double* __restrict__ v, float* __restrict__ v32,
+                             const double* __restrict__ den, int64_t n) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) {
+        const double q = w[t] / *den;
+        v[t] = q;
+        v32[t] = (float)q;
+    }
+}
+void launch_div_by_f32(const double* w, double* v, float* v32, const double* den, int64_t n, cudaStream_t s) {
+    k_div_by_f32<<<nb(n), kT, 0, s>>>(w, v, v32, den, n);
+}
+
 __global__ void k_sub_scaled(double* __restrict__ w, const double* __restrict__ V, const double* __restrict__ h, int64_t n) {
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) {
@@ -158,6 +173,35 @@ __global__ void k_add_scaled_f32(double* __restrict__ x, const float* __restrict
 }
 void launch_add_scaled_f32(double* x, const float* Z, double y, int64_t n, cudaStream_t s) {
     k_add_scaled_f32<<<nb(n), kT, 0, s>>>(x, Z, y, n);
+}
+
+// x += sum_k y_k Z_k in one pass over x: per entry the same sequence of
+// roundings as J launches of k_add_scaled_f32 (update_sol, gmres.f90:481-515)
+template <int J>
+__global__ void k_add_scaled_multi_f32(double* __restrict__ x, MZ32 Z, YS ys, int64_t n) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        double v = x[t];
+#pragma unroll
+        for (int k = 0; k < J; ++k) {
+            const double tmp = (double)Z.p[k][t] * ys.y[k];
+            v = v + tmp;
+        }
+        x[t] = v;
+    }
+}
+void launch_add_scaled_multi_f32(double* x, const MZ32& Z, const YS& ys, int J, int64_t n, cudaStream_t s) {
+    int64_t b = (n + kT - 1) / kT;
+    const int g = (int)(b > 8192 ? 8192 : b);
+    switch (J) {
+    case 1: k_add_scaled_multi_f32<1><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 2: k_add_scaled_multi_f32<2><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 3: k_add_scaled_multi_f32<3><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 4: k_add_scaled_multi_f32<4><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 5: k_add_scaled_multi_f32<5><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 6: k_add_scaled_multi_f32<6><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 7: k_add_scaled_multi_f32<7><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    default: k_add_scaled_multi_f32<8><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    }
 }
 
 // ---------------------------------------------------------------- Schur complement pieces
@@ -495,7 +539,93 @@ __global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restric
     }
 }
 
+// w -= sum_k h_k V_k (as k_maxpy) and, in the same pass, the Stokes norm of
+// the new w with the seam weight applied per entry: out[5] = sqrt(|u|^2 +
+// (pw |p|)^2), out[4] the squared form (as k_reduce's slots)
+template <int DM, int J>
+__global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __restrict__ w, MVecs V, const double* __restrict__ hs,
+                                                             double wseam, double pw, double* __restrict__ partials,
+                                                             unsigned* __restrict__ counter, double* __restrict__ out) {
+    constexpr int NC = DM + 1;
+    const int n = D.nx * D.ny * D.nz;
+    double h[J];
+#pragma unroll
+    for (int k = 0; k < J; ++k) h[k] = hs[k * 8 + 4];
+    double acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        const int i = t % D.nx, r = t / D.nx, j = r % D.ny, kk = r / D.ny;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int64_t e = (int64_t)c * n + t;
+            double x = w[e];
+#pragma unroll
+            for (int k = 0; k < J; ++k) x = x - V.p[k][e] * h[k];
+            w[e] = x;
+            const bool seam = (c == 0 && i == 0) || (c == 1 && j == 0) || (c == 2 && c < DM && kk == 0);
+            acc[c] += (seam ? wseam : 1.0) * (x * x);
+        }
+    }
+    __shared__ double sh[NC][kMdotThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[c][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NC) {
+        double v = 0.0;
+        for (int q = 0; q < kMdotThreads / 32; ++q) v += sh[threadIdx.x][q];
+        partials[blockIdx.x * NC + threadIdx.x] = v;
+    }
+    __threadfence();
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < NC) {
+        double v = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) v += ((volatile double*)partials)[b * NC + threadIdx.x];
+        sh[threadIdx.x][0] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double su = 0.0;
+        for (int c = 0; c < DM; ++c) su = su + sh[c][0];
+        out[4] = su + (pw * pw) * sh[DM][0];
+        const double nu = sqrt(su), np = pw * sqrt(sh[DM][0]);
+        out[5] = sqrt(nu * nu + np * np);
+        *counter = 0u;
+    }
+}
+
 }  // namespace
+
+void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
+                       unsigned* counter, double* out, cudaStream_t s) {
+    const int nb = mdot_blocks((int64_t)D.nx * D.ny * D.nz);
+#define MN(DM_, J_) k_maxpy_norm<DM_, J_><<<nb, kMdotThreads, 0, s>>>(D, w, V, hs, wseam, pw, partials, counter, out)
+#define MNJ(DM_)                               \
+    switch (J) {                               \
+    case 1: MN(DM_, 1); break;                 \
+    case 2: MN(DM_, 2); break;                 \
+    case 3: MN(DM_, 3); break;                 \
+    case 4: MN(DM_, 4); break;                 \
+    case 5: MN(DM_, 5); break;                 \
+    case 6: MN(DM_, 6); break;                 \
+    case 7: MN(DM_, 7); break;                 \
+    default: MN(DM_, 8); break;                \
+    }
+    if (D.dm == 2) { MNJ(2) } else { MNJ(3) }
+#undef MNJ
+#undef MN
+}
 
 int mdot_blocks(int64_t n) {
     int64_t b = (n + 2047) / 2048;

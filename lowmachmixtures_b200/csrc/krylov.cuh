@@ -39,6 +39,21 @@ int mdot_blocks(int64_t n);
 void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
                  double* out, cudaStream_t s);
 void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s);
+// the same update fused with the Stokes norm of the new w (seam weight per
+// entry): out[4] = |u|^2 + pw^2 |p|^2, out[5] = its square root form
+void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
+                       unsigned* counter, double* out, cudaStream_t s);
+// FP32 Krylov vectors (FGMRES Z basis) and their coefficients, up to 8
+struct MZ32 {
+    const float* p[8];
+};
+struct YS {
+    double y[8];
+};
+// x += sum_k y_k Z_k (k < J <= 8), one pass over x
+void launch_add_scaled_multi_f32(double* x, const MZ32& Z, const YS& ys, int J, int64_t n, cudaStream_t s);
+// v = w / *den and v32 = (float)v
+void launch_div_by_f32(const double* w, double* v, float* v32, const double* den, int64_t n, cudaStream_t s);
 
 void launch_apply_matrix(const LevelDev<double>& L0, int visc, const SVec& x, const SVec& b, cudaStream_t s);
 // the same operator applied to an FP32 Stokes vector (FGMRES Z storage), FP64 arithmetic

@@ -496,7 +496,10 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
 // phi/rhs fit the shared-memory budget
 template <class T>
 int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool stag) {
-    const int cells = h->knobs.tail_cells == 0 ? 4096 : h->knobs.tail_cells;
+    // default: the velocity tail from 8^3 cells down (a 16^3 level runs
+    // faster as per-level launches over many SMs than as ~50 barrier phases
+    // on one), the pressure tail from 16^3 down
+    const int cells = h->knobs.tail_cells == 0 ? (stag ? 512 : 4096) : h->knobs.tail_cells;
     if (cells < 0) return nl;
     if (stag && h->D0.wall) return nl;  // the staggered tail kernel is periodic only
     const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
@@ -935,13 +938,16 @@ void precon64(lmm_handle* h, const SVec& bin, const SVec& xout) {
     run_graphed(h, bin.base, xout.base, 0, [&]() { apply_precon<double>(h, bu, bin.p(), xu, xout.p()); });
 }
 
-// FP64 Stokes vector in, FP32 Stokes vector out (Z storage)
-void precon32(lmm_handle* h, const SVec& bin, float* zout) {
+// FP64 Stokes vector in, FP32 Stokes vector out (Z storage).  converted:
+// h->pin32 already holds bin in FP32 (written with bin by launch_div_by_f32)
+void precon32(lmm_handle* h, const SVec& bin, float* zout, bool converted = false) {
     const int dm = h->dm;
     const int64_t n = h->n;
-    run_graphed(h, bin.base, zout, 1, [&]() {
-        launch_convert<double, float>(bin.base, h->pin32, (int64_t)(dm + 1) * n, h->stream);
-        check_launch();
+    run_graphed(h, bin.base, zout, converted ? 2 : 1, [&]() {
+        if (!converted) {
+            launch_convert<double, float>(bin.base, h->pin32, (int64_t)(dm + 1) * n, h->stream);
+            check_launch();
+        }
         const float* bu[3] = {h->pin32, h->pin32 + n, dm == 3 ? h->pin32 + 2 * n : nullptr};
         float* xu[3] = {zout, zout + n, dm == 3 ? zout + 2 * n : nullptr};
         apply_precon<float>(h, bu, h->pin32 + (int64_t)dm * n, xu, zout + (int64_t)dm * n);
@@ -1031,10 +1037,15 @@ void arnoldi_column_cgs(lmm_handle* h, int i, std::vector<double>& col) {
         MVecs V{};
         const int J = std::min(8, i - k0);
         for (int j = 0; j < J; ++j) V.p[j] = h->V[k0 + j].base;
-        launch_maxpy(h->w.base, V, J, h->slot(k0 + 1), len, h->stream);
+        if (k0 + J < i) {
+            launch_maxpy(h->w.base, V, J, h->slot(k0 + 1), len, h->stream);
+        } else {
+            // the last projections and |w| in one pass over w
+            launch_maxpy_norm(h->D0, h->w.base, V, J, h->slot(k0 + 1), 3.0, h->knobs.p_norm_weight, h->partials, h->counter,
+                              h->slot(i + 1), h->stream);
+        }
         check_launch();
     }
-    stokes_norm(h, h->w, i + 1);
     LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
     LMM_CK(host_wait(h));
     col.assign(i + 2, 0.0);
@@ -1240,7 +1251,10 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             break;
         }
         iter = iter + 1;
-        launch_div_by(h->tmp.base, h->V[0].base, h->slot(0) + 5, len, h->stream);
+        if (fp32)
+            launch_div_by_f32(h->tmp.base, h->V[0].base, h->pin32, h->slot(0) + 5, len, h->stream);
+        else
+            launch_div_by(h->tmp.base, h->V[0].base, h->slot(0) + 5, len, h->stream);
         check_launch();
         std::fill(s.begin(), s.end(), 0.0);
         s[1] = norm_r;
@@ -1250,7 +1264,7 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             total_iter = total_iter + 1;
             i_copy = i;
             if (fp32) {
-                precon32(h, h->V[i - 1], h->Z32[i - 1]);
+                precon32(h, h->V[i - 1], h->Z32[i - 1], true);
                 launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[i - 1], h->n, h->dm, h->w, h->stream);
                 if (learned) learned_stage(h, h->Zc[i - 1], h->V[i - 1], K.learned_stage);
             } else {
@@ -1266,7 +1280,10 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             for (int k = 1; k <= i + 1; ++k)
                 if (!std::isfinite(col[k])) return LMM_ERR_NONFINITE;
             if (H(i + 1, i) != 0.0) {
-                launch_div_by(h->w.base, h->V[i].base, h->slot(i + 1) + 5, len, h->stream);
+                if (fp32)
+                    launch_div_by_f32(h->w.base, h->V[i].base, h->pin32, h->slot(i + 1) + 5, len, h->stream);
+                else
+                    launch_div_by(h->w.base, h->V[i].base, h->slot(i + 1) + 5, len, h->stream);
                 check_launch();
             } else {
                 happy = true;
@@ -1278,16 +1295,29 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             if (total_iter >= K.gmres_min_iter && (est <= K.gmres_rel_tol * norm_b || est <= K.gmres_abs_tol)) break;
         }
         solve_utri(i_copy - 1, H, s, y);
-        for (int it = 1; it <= i_copy; ++it) {
-            if (fp32) {
-                launch_add_scaled_f32(h->x.base, h->Z32[it - 1], y[it], len, h->stream);
-                if (learned) {
+        if (fp32 && !learned) {
+            // update_sol: x += sum y_k Z_k, up to 8 basis vectors per pass
+            for (int k0 = 1; k0 <= i_copy; k0 += 8) {
+                const int J = std::min(8, i_copy - k0 + 1);
+                MZ32 Z{};
+                YS ys{};
+                for (int j = 0; j < J; ++j) {
+                    Z.p[j] = h->Z32[k0 + j - 1];
+                    ys.y[j] = y[k0 + j];
+                }
+                launch_add_scaled_multi_f32(h->x.base, Z, ys, J, len, h->stream);
+                check_launch();
+            }
+        } else {
+            for (int it = 1; it <= i_copy; ++it) {
+                if (fp32) {
+                    launch_add_scaled_f32(h->x.base, h->Z32[it - 1], y[it], len, h->stream);
                     check_launch();
                     launch_add_scaled(h->x.base, h->Zc[it - 1].base, y[it], len, h->stream);
-                }
-            } else
-                launch_add_scaled(h->x.base, h->Z64[it - 1].base, y[it], len, h->stream);
-            check_launch();
+                } else
+                    launch_add_scaled(h->x.base, h->Z64[it - 1].base, y[it], len, h->stream);
+                check_launch();
+            }
         }
     }
     if (st) {
