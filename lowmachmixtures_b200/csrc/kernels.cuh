@@ -26,6 +26,31 @@ namespace lmm {
 
 constexpr int kThreads = 256;
 
+// Programmatic dependent launch for the multigrid level kernels: launched
+// with launch_pdl, a kernel may be scheduled while the kernel before it on
+// the stream drains; its first statement, pdl_enter(), waits for that
+// kernel's completion and memory (griddepcontrol.wait) before any access,
+// then lets the next kernel be scheduled (griddepcontrol.launch_dependents).
+// Launched without the attribute, both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <class... KArgs, class... Args>
+static inline void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 static inline int nblocks_for(int64_t n, int threads = kThreads) {
     int64_t b = (n + threads - 1) / threads;
     return (int)(b < 1 ? 1 : b);
@@ -53,6 +78,7 @@ template <class T, int DM, int VISC, bool W = false>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
                                                       const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                       T* __restrict__ o2, T dxsqinv, int color) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     const int i = q.i, j = q.j, k = q.k;
@@ -78,6 +104,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Di
 template <class T, int DM, int VISC, int COMP, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const T* __restrict__ rhs, T* p0, T* p1, T* p2,
                                                         int parity, T omega, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
     const int j = q.j, k = q.k;
@@ -106,6 +133,7 @@ __host__ __device__ __forceinline__ bool odd_level(const Dims& D) {
 template <class T, int DM, int VISC, int COMP, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_colour_update(Dims D, Coef<T> C, const T* __restrict__ rhs, const T* __restrict__ Lp,
                                                             T* p, int parity, T omega, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
     Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
@@ -198,6 +226,7 @@ __global__ void __launch_bounds__(kThreads) k_jacobi(Dims D, Coef<T> C, const T*
                                                      const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
                                                      const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                      T* __restrict__ o2, T omega, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
@@ -306,6 +335,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_residual(D
                                                        const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
                                                        const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
                                                        T* __restrict__ o2, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
@@ -343,6 +373,7 @@ template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restrict__ f0, const T* __restrict__ f1,
                                                        const T* __restrict__ f2, Dims Dc, T* __restrict__ c0, T* __restrict__ c1,
                                                        T* __restrict__ c2) {
+    pdl_enter();
     const Pos q = pos3(Dc.nx, Dc.ny);
     if (!q.ok) return;
     const int t = q.i + Dc.nx * (q.j + Dc.ny * q.k);
@@ -536,6 +567,7 @@ template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_prolong_add(Dims F, Dims Dc, const T* __restrict__ q0, const T* __restrict__ q1,
                                                           const T* __restrict__ q2, T* __restrict__ f0, T* __restrict__ f1,
                                                           T* __restrict__ f2) {
+    pdl_enter();
     const Pos q = pos3(F.nx, F.ny);
     if (!q.ok) return;
     const int t = q.i + F.nx * (q.j + F.ny * q.k);
@@ -642,6 +674,7 @@ __device__ __forceinline__ T cc_diag(const T* const a[3], const Nb& n, T dxsqinv
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ rhs,
                                                         T* phi, int parity, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
     const int j = q.j, k = q.k;
@@ -658,6 +691,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, con
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_smooth_odd(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ rhs,
                                                             const T* __restrict__ phi, T* __restrict__ out, int parity, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
     Nb nb = make_nb(D, q.i, q.j, q.k);
@@ -669,6 +703,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_smooth_odd(Dims D, const T* a0,
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_copy_parity(Dims D, const T* __restrict__ in, T* __restrict__ out, int parity) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
     const int s = q.i + D.nx * (q.j + D.ny * q.k);
@@ -686,6 +721,7 @@ template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const T* a0, const T* a1, const T* a2,
                                                                    const T* __restrict__ rhs, const T* __restrict__ phi, Dims Dc,
                                                                    T* __restrict__ rc, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(Dc.nx, Dc.ny);
     if (!q.ok) return;
     const int i = q.i, j = q.j, k = q.k;
@@ -703,6 +739,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_cc_prolong_add(Dims F, Dims Dc, const T* __restrict__ pc, T* __restrict__ pf) {
+    pdl_enter();
     const Pos q = pos3(F.nx, F.ny);
     if (!q.ok) return;
     const int t = q.i + F.nx * (q.j + F.ny * q.k);
@@ -1007,9 +1044,9 @@ void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* co
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_applyop<T, 2, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_applyop<T, 2, V>, g.grid, g.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_applyop<T, 3, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_applyop<T, 3, V>, g.grid, g.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
     }
 }
 
@@ -1027,7 +1064,7 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
         launch_applyop<T>(L, visc, pin, lp, s, color);
         count_launch();
         const G3 go = geom3(L.D.nx, L.D.ny, L.D.nz);
-#define CU(DM_, COMP_) k_colour_update<T, DM_, V, COMP_><<<go.grid, go.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], L.tmp[COMP_], phi[COMP_], parity, om, dxsqinv)
+#define CU(DM_, COMP_) launch_pdl(k_colour_update<T, DM_, V, COMP_>, go.grid, go.block, 0, s, L.D, L.coef(), rhs[COMP_], L.tmp[COMP_], phi[COMP_], parity, om, dxsqinv)
         if (L.D.dm == 2) {
             if (comp == 0) { LMM_VISC_DISPATCH(visc, CU(2, 0)) }
             else { LMM_VISC_DISPATCH(visc, CU(2, 1)) }
@@ -1040,7 +1077,7 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
         return;
     }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
-#define GS(DM_, COMP_) k_gs_colour<T, DM_, V, COMP_><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
+#define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
         else { LMM_VISC_DISPATCH(visc, GS(2, 1)) }
@@ -1110,9 +1147,9 @@ void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const 
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     const T om = (T)omega;
     if (L.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 2, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_jacobi<T, 2, V>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 3, V><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_jacobi<T, 3, V>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
     }
 }
 
@@ -1124,16 +1161,16 @@ void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int v
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_residual<T, 2, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 2, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_residual<T, 3, V><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 3, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     }
     count_launch();
     const G3 gc = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
     if (F.D.dm == 2)
-        k_restrict<T, 2><<<gc.grid, gc.block, 0, s>>>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
+        launch_pdl(k_restrict<T, 2>, gc.grid, gc.block, 0, s, F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
     else
-        k_restrict<T, 3><<<gc.grid, gc.block, 0, s>>>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
+        launch_pdl(k_restrict<T, 3>, gc.grid, gc.block, 0, s, F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
 }
 
 template <class T>
@@ -1142,9 +1179,9 @@ void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* co
     if (F.D.wall) return wl_prolong_add<T>(F, Cc, phi_c, phi_f, s);
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
-        k_prolong_add<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+        launch_pdl(k_prolong_add<T, 2>, g.grid, g.block, 0, s, F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
     else
-        k_prolong_add<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+        launch_pdl(k_prolong_add<T, 3>, g.grid, g.block, 0, s, F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
 }
 
 template <class T>
@@ -1180,18 +1217,18 @@ void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s) {
     if (odd_level(L.D)) {
         const G3 go = geom3(L.D.nx, L.D.ny, L.D.nz);
         if (L.D.dm == 2)
-            k_cc_smooth_odd<T, 2><<<go.grid, go.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, L.ptmp, parity, dxsqinv);
+            launch_pdl(k_cc_smooth_odd<T, 2>, go.grid, go.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, L.ptmp, parity, dxsqinv);
         else
-            k_cc_smooth_odd<T, 3><<<go.grid, go.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, L.ptmp, parity, dxsqinv);
+            launch_pdl(k_cc_smooth_odd<T, 3>, go.grid, go.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, L.ptmp, parity, dxsqinv);
         count_launch();
-        k_copy_parity<T><<<go.grid, go.block, 0, s>>>(L.D, L.ptmp, L.pphi, parity);
+        launch_pdl(k_copy_parity<T>, go.grid, go.block, 0, s, L.D, L.ptmp, L.pphi, parity);
         return;
     }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
     if (L.D.dm == 2)
-        k_cc_smooth<T, 2><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+        launch_pdl(k_cc_smooth<T, 2>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
     else
-        k_cc_smooth<T, 3><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+        launch_pdl(k_cc_smooth<T, 3>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
 }
 
 template <class T>
@@ -1199,18 +1236,18 @@ void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cu
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
     const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
     if (F.D.dm == 2)
-        k_cc_residual_restrict<T, 2><<<g.grid, g.block, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+        launch_pdl(k_cc_residual_restrict<T, 2>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
     else
-        k_cc_residual_restrict<T, 3><<<g.grid, g.block, 0, s>>>(F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+        launch_pdl(k_cc_residual_restrict<T, 3>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
 }
 
 template <class T>
 void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s) {
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
-        k_cc_prolong_add<T, 2><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
+        launch_pdl(k_cc_prolong_add<T, 2>, g.grid, g.block, 0, s, F.D, Cc.D, Cc.pphi, F.pphi);
     else
-        k_cc_prolong_add<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, Cc.pphi, F.pphi);
+        launch_pdl(k_cc_prolong_add<T, 3>, g.grid, g.block, 0, s, F.D, Cc.D, Cc.pphi, F.pphi);
 }
 
 template <class T>

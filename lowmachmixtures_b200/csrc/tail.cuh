@@ -202,6 +202,7 @@ __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool sta
 // memory.
 template <class T, int DM, int VISC>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_constant__ TailArgs<T> A) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char tail_smem[];
     T* sm = reinterpret_cast<T*>(tail_smem);
     __shared__ TailView<T> V[kMaxTail];
@@ -301,6 +302,7 @@ __device__ void tail_cc_smooth(const TailView<T>& L, int nsweeps) {
 
 template <class T, int DM>
 __global__ void __launch_bounds__(kTailThreads, 1) k_ccmg_tail(const __grid_constant__ TailArgs<T> A) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char tail_smem[];
     T* sm = reinterpret_cast<T*>(tail_smem);
     __shared__ TailView<T> V[kMaxTail];
@@ -398,7 +400,7 @@ template <class K, class A>
 static cudaError_t launch_tail(K kernel, const A& args, size_t smem, cudaStream_t s) {
     cudaError_t e = raise_smem_limit((const void*)kernel, smem);
     if (e != cudaSuccess) return e;
-    kernel<<<1, kTailThreads, smem, s>>>(args);
+    launch_pdl(kernel, dim3(1), dim3(kTailThreads), smem, s, args);
     return cudaGetLastError();
 }
 

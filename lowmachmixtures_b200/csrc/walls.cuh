@@ -15,9 +15,9 @@ void wl_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const 
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_applyop<T, 2, V, true><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_applyop<T, 2, V, true>, g.grid, g.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_applyop<T, 3, V, true><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_applyop<T, 3, V, true>, g.grid, g.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
     }
 }
 
@@ -33,7 +33,7 @@ void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[
         wl_applyop<T>(L, visc, pin, lp, s, color);
         count_launch();
         const G3 go = geom3(L.D.nx, L.D.ny, L.D.nz);
-#define CU(DM_, COMP_) k_colour_update<T, DM_, V, COMP_, true><<<go.grid, go.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], L.tmp[COMP_], phi[COMP_], parity, om, dxsqinv)
+#define CU(DM_, COMP_) launch_pdl(k_colour_update<T, DM_, V, COMP_, true>, go.grid, go.block, 0, s, L.D, L.coef(), rhs[COMP_], L.tmp[COMP_], phi[COMP_], parity, om, dxsqinv)
         if (L.D.dm == 2) {
             if (comp == 0) { LMM_VISC_DISPATCH(visc, CU(2, 0)) }
             else { LMM_VISC_DISPATCH(visc, CU(2, 1)) }
@@ -46,7 +46,7 @@ void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[
         return;
     }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
-#define GS(DM_, COMP_) k_gs_colour<T, DM_, V, COMP_, true><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
+#define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_, true>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
         else { LMM_VISC_DISPATCH(visc, GS(2, 1)) }
@@ -65,9 +65,9 @@ void wl_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* c
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     const T om = (T)omega;
     if (L.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 2, V, true><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_jacobi<T, 2, V, true>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_jacobi<T, 3, V, true><<<g.grid, g.block, 0, s>>>(L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_jacobi<T, 3, V, true>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[0], rhs[1], rhs[2], pin[0], pin[1], pin[2], pout[0], pout[1], pout[2], om, dxsqinv)))
     }
 }
 
@@ -77,25 +77,25 @@ void wl_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc,
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (k_residual<T, 2, V, true><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 2, V, true>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (k_residual<T, 3, V, true><<<g.grid, g.block, 0, s>>>(F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 3, V, true>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     }
     count_launch();
     const G3 gc = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
     if (F.D.dm == 2)
-        k_restrict<T, 2, true><<<gc.grid, gc.block, 0, s>>>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
+        launch_pdl(k_restrict<T, 2, true>, gc.grid, gc.block, 0, s, F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
     else
-        k_restrict<T, 3, true><<<gc.grid, gc.block, 0, s>>>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
+        launch_pdl(k_restrict<T, 3, true>, gc.grid, gc.block, 0, s, F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2]);
 }
 
 template <class T>
 void wl_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3], cudaStream_t s) {
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
-        k_prolong_add<T, 2, true><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+        launch_pdl(k_prolong_add<T, 2, true>, g.grid, g.block, 0, s, F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
     else
-        k_prolong_add<T, 3, true><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
+        launch_pdl(k_prolong_add<T, 3, true>, g.grid, g.block, 0, s, F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
 }
 
 #define LMM_INSTANTIATE_WALLS(T)                                                                                           \
