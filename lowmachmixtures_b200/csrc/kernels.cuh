@@ -20,36 +20,13 @@
 #include <cstdint>
 
 #include "kernels.h"
+#include "pdl.cuh"
 #include "stencil.cuh"
 
 namespace lmm {
 
 constexpr int kThreads = 256;
 
-// Programmatic dependent launch for the multigrid level kernels: launched
-// with launch_pdl, a kernel may be scheduled while the kernel before it on
-// the stream drains; its first statement, pdl_enter(), waits for that
-// kernel's completion and memory (griddepcontrol.wait) before any access,
-// then lets the next kernel be scheduled (griddepcontrol.launch_dependents).
-// Launched without the attribute, both instructions are no-ops.
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-template <class... KArgs, class... Args>
-static inline void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k, args...);
-}
 
 static inline int nblocks_for(int64_t n, int threads = kThreads) {
     int64_t b = (n + threads - 1) / threads;
@@ -749,6 +726,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_prolong_add(Dims F, Dims Dc, co
 template <class T, int DM>
 __global__ void __launch_bounds__(kThreads) k_neg_cc_lap(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ phi,
                                                          T* __restrict__ out, T dxsqinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nb = make_nb(D, q.i, q.j, q.k);
@@ -762,6 +740,7 @@ template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_div_plus(Dims D, const T* __restrict__ u0, const T* __restrict__ u1,
                                                        const T* __restrict__ u2, const T* __restrict__ bp, T* __restrict__ out,
                                                        T dxinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
@@ -780,6 +759,7 @@ __global__ void __launch_bounds__(kThreads) k_div_plus(Dims D, const T* __restri
 template <class T, int DM, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_sub_weighted_grad(Dims D, const T* c0, const T* c1, const T* c2,
                                                                 const T* __restrict__ phi, T* u0, T* u1, T* u2, T dxinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
@@ -799,26 +779,31 @@ __global__ void __launch_bounds__(kThreads) k_sub_weighted_grad(Dims D, const T*
 // --------------------------------------------------------------- small vector ops
 template <class Tin, class Tout>
 __global__ void k_convert(const Tin* __restrict__ in, Tout* __restrict__ out, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) out[t] = (Tout)in[t];
 }
 template <class T>
 __global__ void k_scale_copy(const T* __restrict__ in, T* __restrict__ out, T s, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) out[t] = in[t] * s;
 }
 template <class T>
 __global__ void k_add_to(T* __restrict__ x, const T* __restrict__ y, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) x[t] = x[t] + y[t];
 }
 template <class T>
 __global__ void k_recip(const T* __restrict__ in, T* __restrict__ out, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) out[t] = T(1) / in[t];
 }
 template <class T>
 __global__ void k_fill(T* __restrict__ out, T v, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) out[t] = v;
 }
@@ -840,6 +825,7 @@ template <class T, int DM, int MODE>
 __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const T* a1, const T* a2, const T* a3, const T* b0,
                                                      const T* b1, const T* b2, const T* b3, double w0, double w1, double w2,
                                                      double pw, double* partials, unsigned* counter, double* out) {
+    pdl_enter();
     constexpr int NC = DM + 1;
     const T* A[4] = {a0, a1, a2, a3};
     const T* B[4] = {b0, b1, b2, b3};
@@ -1255,9 +1241,9 @@ void launch_neg_cc_lap(const LevelDev<T>& L, const T* phi, T* out, cudaStream_t 
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2)
-        k_neg_cc_lap<T, 2><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
+        launch_pdl(k_neg_cc_lap<T, 2>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
     else
-        k_neg_cc_lap<T, 3><<<g.grid, g.block, 0, s>>>(L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
+        launch_pdl(k_neg_cc_lap<T, 3>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], phi, out, dxsqinv);
 }
 
 template <class T>
@@ -1266,15 +1252,15 @@ void launch_div_plus(const LevelDev<T>& L, const T* const u[3], const T* bp, T* 
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.wall) {
         if (L.D.dm == 2)
-            k_div_plus<T, 2, true><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+            launch_pdl(k_div_plus<T, 2, true>, g.grid, g.block, 0, s, L.D, u[0], u[1], u[2], bp, out, dxinv);
         else
-            k_div_plus<T, 3, true><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+            launch_pdl(k_div_plus<T, 3, true>, g.grid, g.block, 0, s, L.D, u[0], u[1], u[2], bp, out, dxinv);
         return;
     }
     if (L.D.dm == 2)
-        k_div_plus<T, 2><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+        launch_pdl(k_div_plus<T, 2>, g.grid, g.block, 0, s, L.D, u[0], u[1], u[2], bp, out, dxinv);
     else
-        k_div_plus<T, 3><<<g.grid, g.block, 0, s>>>(L.D, u[0], u[1], u[2], bp, out, dxinv);
+        launch_pdl(k_div_plus<T, 3>, g.grid, g.block, 0, s, L.D, u[0], u[1], u[2], bp, out, dxinv);
 }
 
 template <class T>
@@ -1286,43 +1272,43 @@ void launch_sub_weighted_grad(const LevelDev<T>& L, const T* const coef[3], cons
     const T* c2 = coef ? coef[2] : nullptr;
     if (L.D.wall) {
         if (L.D.dm == 2)
-            k_sub_weighted_grad<T, 2, true><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+            launch_pdl(k_sub_weighted_grad<T, 2, true>, g.grid, g.block, 0, s, L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
         else
-            k_sub_weighted_grad<T, 3, true><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+            launch_pdl(k_sub_weighted_grad<T, 3, true>, g.grid, g.block, 0, s, L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
         return;
     }
     if (L.D.dm == 2)
-        k_sub_weighted_grad<T, 2><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+        launch_pdl(k_sub_weighted_grad<T, 2>, g.grid, g.block, 0, s, L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
     else
-        k_sub_weighted_grad<T, 3><<<g.grid, g.block, 0, s>>>(L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
+        launch_pdl(k_sub_weighted_grad<T, 3>, g.grid, g.block, 0, s, L.D, c0, c1, c2, phi, u[0], u[1], u[2], dxinv);
 }
 
 template <class Tin, class Tout>
 void launch_convert(const Tin* in, Tout* out, int64_t n, cudaStream_t s) {
-    k_convert<Tin, Tout><<<nblocks_for(n), kThreads, 0, s>>>(in, out, n);
+    launch_pdl(k_convert<Tin, Tout>, nblocks_for(n), kThreads, 0, s, in, out, n);
 }
 template <class T>
 void launch_add_to(T* x, const T* y, int64_t n, cudaStream_t s) {
-    k_add_to<T><<<nblocks_for(n), kThreads, 0, s>>>(x, y, n);
+    launch_pdl(k_add_to<T>, nblocks_for(n), kThreads, 0, s, x, y, n);
 }
 
 template <class T>
 void launch_scale_copy(const T* in, T* out, double scale, int64_t n, cudaStream_t s) {
-    k_scale_copy<T><<<nblocks_for(n), kThreads, 0, s>>>(in, out, (T)scale, n);
+    launch_pdl(k_scale_copy<T>, nblocks_for(n), kThreads, 0, s, in, out, (T)scale, n);
 }
 template <class T>
 void launch_recip(const T* in, T* out, int64_t n, cudaStream_t s) {
-    k_recip<T><<<nblocks_for(n), kThreads, 0, s>>>(in, out, n);
+    launch_pdl(k_recip<T>, nblocks_for(n), kThreads, 0, s, in, out, n);
 }
 template <class T>
 void launch_fill(T* out, double v, int64_t n, cudaStream_t s) {
-    k_fill<T><<<nblocks_for(n), kThreads, 0, s>>>(out, (T)v, n);
+    launch_pdl(k_fill<T>, nblocks_for(n), kThreads, 0, s, out, (T)v, n);
 }
 
 template <class T>
 void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const b[4], const double wseam[3], double pw,
                    double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s) {
-#define RED(DM_, M_) k_reduce<T, DM_, M_><<<nblocks, kThreads, 0, s>>>(D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out)
+#define RED(DM_, M_) launch_pdl(k_reduce<T, DM_, M_>, nblocks, kThreads, 0, s, D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out)
     if (D.dm == 2) {
         if (mode == 0) RED(2, 0); else if (mode == 1) RED(2, 1); else RED(2, 2);
     } else {

@@ -1,6 +1,7 @@
 // krylov.cu - FP64 Krylov-side kernels (see krylov.cuh).  Built with
 // -fmad=false so every operation rounds like the reference Fortran.
 #include "krylov.cuh"
+#include "pdl.cuh"
 #include "stencil.cuh"
 
 namespace lmm {
@@ -27,6 +28,7 @@ __global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, con
                                                      const TX* __restrict__ p, double* __restrict__ o0,
                                                      double* __restrict__ o1, double* __restrict__ o2, double* __restrict__ op,
                                                      double dxsqinv, double dxinv) {
+    pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
     if (!q.ok) return;
     Nb nbr = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
@@ -83,9 +85,9 @@ static void apply_matrix_impl(const LevelDev<double>& L0, int visc, const TX* xb
     double* b2 = (b.dm == 3) ? b.c(2) : b.c(0);
 #define AM(DM_, V_)                                                                                                        \
     if (L0.D.wall)                                                                                                         \
-        k_apply_matrix<DM_, V_, TX, true><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv); \
+        launch_pdl(k_apply_matrix<DM_, V_, TX, true>, grd, blk, 0, s, L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv); \
     else                                                                                                                   \
-        k_apply_matrix<DM_, V_, TX><<<grd, blk, 0, s>>>(L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
+        launch_pdl(k_apply_matrix<DM_, V_, TX>, grd, blk, 0, s, L0.D, L0.coef(), x0, x1, x2, xp, b.c(0), b.c(1), b2, b.p(), dxsqinv, dxinv)
 #define AMV(DM_)                    \
     switch (visc) {                 \
     case -1: AM(DM_, -1); break;    \
@@ -113,26 +115,29 @@ void launch_apply_matrix_f32(const LevelDev<double>& L0, int visc, const float* 
 }
 
 __global__ void k_neg_resid(double* __restrict__ out, const double* __restrict__ b, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) {
         double v = out[t] - b[t];
         out[t] = v * -1.0;
     }
 }
-void launch_neg_resid(double* out, const double* b, int64_t n, cudaStream_t s) { k_neg_resid<<<nb(n), kT, 0, s>>>(out, b, n); }
+void launch_neg_resid(double* out, const double* b, int64_t n, cudaStream_t s) { launch_pdl(k_neg_resid, nb(n), kT, 0, s, out, b, n); }
 
 __global__ void k_div_by(const double* __restrict__ w, double* __restrict__ v, const double* __restrict__ den, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) v[t] = w[t] / *den;
 }
 void launch_div_by(const double* w, double* v, const double* den, int64_t n, cudaStream_t s) {
-    k_div_by<<<nb(n), kT, 0, s>>>(w, v, den, n);
+    launch_pdl(k_div_by, nb(n), kT, 0, s, w, v, den, n);
 }
 
 // v = w / *den, and v32 = (float)v: the next FGMRES basis vector together
 // with the FP32 input of the preconditioner that reads it next
 __global__ void k_div_by_f32(const double* __restrict__ w, double* __restrict__ v, float* __restrict__ v32,
                              const double* __restrict__ den, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) {
         const double q = w[t] / *den;
@@ -141,10 +146,11 @@ __global__ void k_div_by_f32(const double* __restrict__ w, double* __restrict__ 
     }
 }
 void launch_div_by_f32(const double* w, double* v, float* v32, const double* den, int64_t n, cudaStream_t s) {
-    k_div_by_f32<<<nb(n), kT, 0, s>>>(w, v, v32, den, n);
+    launch_pdl(k_div_by_f32, nb(n), kT, 0, s, w, v, v32, den, n);
 }
 
 __global__ void k_sub_scaled(double* __restrict__ w, const double* __restrict__ V, const double* __restrict__ h, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) {
         double tmp = V[t] * *h;
@@ -152,19 +158,21 @@ __global__ void k_sub_scaled(double* __restrict__ w, const double* __restrict__ 
     }
 }
 void launch_sub_scaled(double* w, const double* V, const double* h, int64_t n, cudaStream_t s) {
-    k_sub_scaled<<<nb(n), kT, 0, s>>>(w, V, h, n);
+    launch_pdl(k_sub_scaled, nb(n), kT, 0, s, w, V, h, n);
 }
 
 __global__ void k_add_scaled(double* __restrict__ x, const double* __restrict__ V, double y, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) {
         double tmp = V[t] * y;
         x[t] = x[t] + tmp;
     }
 }
-void launch_add_scaled(double* x, const double* V, double y, int64_t n, cudaStream_t s) { k_add_scaled<<<nb(n), kT, 0, s>>>(x, V, y, n); }
+void launch_add_scaled(double* x, const double* V, double y, int64_t n, cudaStream_t s) { launch_pdl(k_add_scaled, nb(n), kT, 0, s, x, V, y, n); }
 
 __global__ void k_add_scaled_f32(double* __restrict__ x, const float* __restrict__ Z, double y, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t < n) {
         double tmp = (double)Z[t] * y;
@@ -172,13 +180,14 @@ __global__ void k_add_scaled_f32(double* __restrict__ x, const float* __restrict
     }
 }
 void launch_add_scaled_f32(double* x, const float* Z, double y, int64_t n, cudaStream_t s) {
-    k_add_scaled_f32<<<nb(n), kT, 0, s>>>(x, Z, y, n);
+    launch_pdl(k_add_scaled_f32, nb(n), kT, 0, s, x, Z, y, n);
 }
 
 // x += sum_k y_k Z_k in one pass over x: per entry the same sequence of
 // roundings as J launches of k_add_scaled_f32 (update_sol, gmres.f90:481-515)
 template <int J>
 __global__ void k_add_scaled_multi_f32(double* __restrict__ x, MZ32 Z, YS ys, int64_t n) {
+    pdl_enter();
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         double v = x[t];
 #pragma unroll
@@ -193,14 +202,14 @@ void launch_add_scaled_multi_f32(double* x, const MZ32& Z, const YS& ys, int J, 
     int64_t b = (n + kT - 1) / kT;
     const int g = (int)(b > 8192 ? 8192 : b);
     switch (J) {
-    case 1: k_add_scaled_multi_f32<1><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    case 2: k_add_scaled_multi_f32<2><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    case 3: k_add_scaled_multi_f32<3><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    case 4: k_add_scaled_multi_f32<4><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    case 5: k_add_scaled_multi_f32<5><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    case 6: k_add_scaled_multi_f32<6><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    case 7: k_add_scaled_multi_f32<7><<<g, kT, 0, s>>>(x, Z, ys, n); break;
-    default: k_add_scaled_multi_f32<8><<<g, kT, 0, s>>>(x, Z, ys, n); break;
+    case 1: launch_pdl(k_add_scaled_multi_f32<1>, g, kT, 0, s, x, Z, ys, n); break;
+    case 2: launch_pdl(k_add_scaled_multi_f32<2>, g, kT, 0, s, x, Z, ys, n); break;
+    case 3: launch_pdl(k_add_scaled_multi_f32<3>, g, kT, 0, s, x, Z, ys, n); break;
+    case 4: launch_pdl(k_add_scaled_multi_f32<4>, g, kT, 0, s, x, Z, ys, n); break;
+    case 5: launch_pdl(k_add_scaled_multi_f32<5>, g, kT, 0, s, x, Z, ys, n); break;
+    case 6: launch_pdl(k_add_scaled_multi_f32<6>, g, kT, 0, s, x, Z, ys, n); break;
+    case 7: launch_pdl(k_add_scaled_multi_f32<7>, g, kT, 0, s, x, Z, ys, n); break;
+    default: launch_pdl(k_add_scaled_multi_f32<8>, g, kT, 0, s, x, Z, ys, n); break;
     }
 }
 
@@ -209,6 +218,7 @@ template <class T>
 __global__ void k_schur(int mode, int pt, int av, double theta, const T* __restrict__ mac, const T* __restrict__ src,
                         const T* __restrict__ beta, const T* __restrict__ gamma, T* __restrict__ phi, const T* __restrict__ bp,
                         T* __restrict__ xp, int64_t n) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= n) return;
     const T th = (T)theta;
@@ -276,7 +286,7 @@ __global__ void k_schur(int mode, int pt, int av, double theta, const T* __restr
 template <class T>
 void launch_schur(int mode, int precon_type, int visc_abs, double theta_alpha, const T* mac_rhs, const T* src,
                   const T* beta, const T* gamma, T* phi, const T* bp, T* xp, int64_t n, cudaStream_t s) {
-    k_schur<T><<<nb(n), kT, 0, s>>>(mode, precon_type, visc_abs, theta_alpha, mac_rhs, src, beta, gamma, phi, bp, xp, n);
+    launch_pdl(k_schur<T>, nb(n), kT, 0, s, mode, precon_type, visc_abs, theta_alpha, mac_rhs, src, beta, gamma, phi, bp, xp, n);
 }
 template void launch_schur<double>(int, int, int, double, const double*, const double*, const double*, const double*, double*,
                                    const double*, double*, int64_t, cudaStream_t);
@@ -287,6 +297,7 @@ template void launch_schur<float>(int, int, int, double, const float*, const flo
 // sub_u: bit d set = remove the mean of velocity component d
 template <class T, int DM>
 __global__ void k_sub_means(Dims D, T* u0, T* u1, T* u2, T* p, const double* __restrict__ sums, double total_volume, int sub_u) {
+    pdl_enter();
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t n = (int64_t)D.nx * D.ny * D.nz;
     if (t >= n) return;
@@ -307,9 +318,9 @@ template <class T>
 void launch_sub_means(const Dims& D, T* const u[3], T* p, const double* sums, double total_volume, int sub_u, cudaStream_t s) {
     int64_t n = (int64_t)D.nx * D.ny * D.nz;
     if (D.dm == 2)
-        k_sub_means<T, 2><<<nb(n), kT, 0, s>>>(D, u[0], u[1], u[2], p, sums, total_volume, sub_u);
+        launch_pdl(k_sub_means<T, 2>, nb(n), kT, 0, s, D, u[0], u[1], u[2], p, sums, total_volume, sub_u);
     else
-        k_sub_means<T, 3><<<nb(n), kT, 0, s>>>(D, u[0], u[1], u[2], p, sums, total_volume, sub_u);
+        launch_pdl(k_sub_means<T, 3>, nb(n), kT, 0, s, D, u[0], u[1], u[2], p, sums, total_volume, sub_u);
 }
 template void launch_sub_means<double>(const Dims&, double* const[3], double*, const double*, double, int, cudaStream_t);
 template void launch_sub_means<float>(const Dims&, float* const[3], float*, const double*, double, int, cudaStream_t);
@@ -450,6 +461,7 @@ template <int DM, int J>
 __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __restrict__ w, MVecs V, double wseam, double pw,
                                                        double* __restrict__ partials, unsigned* __restrict__ counter,
                                                        double* __restrict__ out) {
+    pdl_enter();
     constexpr int NC = DM + 1;
     const int n = D.nx * D.ny * D.nz;
     double acc[J][NC];
@@ -528,6 +540,7 @@ __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __r
 // w -= sum_k h_k V_k, h_k = hs[k * 8 + 4]
 template <int J>
 __global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restrict__ hs, int64_t len) {
+    pdl_enter();
     double h[J];
 #pragma unroll
     for (int k = 0; k < J; ++k) h[k] = hs[k * 8 + 4];
@@ -546,6 +559,7 @@ template <int DM, int J>
 __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __restrict__ w, MVecs V, const double* __restrict__ hs,
                                                              double wseam, double pw, double* __restrict__ partials,
                                                              unsigned* __restrict__ counter, double* __restrict__ out) {
+    pdl_enter();
     constexpr int NC = DM + 1;
     const int n = D.nx * D.ny * D.nz;
     double h[J];
@@ -610,7 +624,7 @@ __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __r
 void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
                        unsigned* counter, double* out, cudaStream_t s) {
     const int nb = mdot_blocks((int64_t)D.nx * D.ny * D.nz);
-#define MN(DM_, J_) k_maxpy_norm<DM_, J_><<<nb, kMdotThreads, 0, s>>>(D, w, V, hs, wseam, pw, partials, counter, out)
+#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, nb, kMdotThreads, 0, s, D, w, V, hs, wseam, pw, partials, counter, out)
 #define MNJ(DM_)                               \
     switch (J) {                               \
     case 1: MN(DM_, 1); break;                 \
@@ -636,7 +650,7 @@ int mdot_blocks(int64_t n) {
 void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
                  double* out, cudaStream_t s) {
     const int nb = mdot_blocks((int64_t)D.nx * D.ny * D.nz);
-#define MD(DM_, J_) k_mdot<DM_, J_><<<nb, kMdotThreads, 0, s>>>(D, w, V, wseam, pw, partials, counter, out)
+#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, nb, kMdotThreads, 0, s, D, w, V, wseam, pw, partials, counter, out)
 #define MDJ(DM_)                               \
     switch (J) {                               \
     case 1: MD(DM_, 1); break;                 \
@@ -657,14 +671,14 @@ void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t le
     int64_t b = (len + kT - 1) / kT;
     const int nb = (int)(b > 8192 ? 8192 : b);
     switch (J) {
-    case 1: k_maxpy<1><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    case 2: k_maxpy<2><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    case 3: k_maxpy<3><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    case 4: k_maxpy<4><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    case 5: k_maxpy<5><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    case 6: k_maxpy<6><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    case 7: k_maxpy<7><<<nb, kT, 0, s>>>(w, V, hs, len); break;
-    default: k_maxpy<8><<<nb, kT, 0, s>>>(w, V, hs, len); break;
+    case 1: launch_pdl(k_maxpy<1>, nb, kT, 0, s, w, V, hs, len); break;
+    case 2: launch_pdl(k_maxpy<2>, nb, kT, 0, s, w, V, hs, len); break;
+    case 3: launch_pdl(k_maxpy<3>, nb, kT, 0, s, w, V, hs, len); break;
+    case 4: launch_pdl(k_maxpy<4>, nb, kT, 0, s, w, V, hs, len); break;
+    case 5: launch_pdl(k_maxpy<5>, nb, kT, 0, s, w, V, hs, len); break;
+    case 6: launch_pdl(k_maxpy<6>, nb, kT, 0, s, w, V, hs, len); break;
+    case 7: launch_pdl(k_maxpy<7>, nb, kT, 0, s, w, V, hs, len); break;
+    default: launch_pdl(k_maxpy<8>, nb, kT, 0, s, w, V, hs, len); break;
     }
 }
 
