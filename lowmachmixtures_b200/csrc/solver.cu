@@ -125,6 +125,7 @@ struct lmm_handle {
     int vcycles = 0, pvcycles = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t wait_ev = nullptr;  // knobs.host_wait = 1: host waits block instead of spinning
+    cudaEvent_t col_ev = nullptr;   // FGMRES: the Hessenberg column has reached the host
     bool coeffs_loaded = false;
     double theta_loaded = 0.0;
     // captured preconditioner applications: (input, output, theta, precision)
@@ -1005,7 +1006,10 @@ void push_hist(lmm_stats* st, double v) {
 
 // MGS of w against V_0..V_{i-1} with H(k,i) kept on the device, then
 // H(i+1,i) = |w|; returns the Hessenberg column on the host.
-void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
+// Arnoldi column i in two halves: enqueue the projections of w and its norm
+// (slots 1..i+1) and the copy of those slots to the host, then -- after the
+// caller has enqueued whatever may run meanwhile -- wait for the copy only.
+void arnoldi_column_enqueue(lmm_handle* h, int i) {
     const int64_t len = h->w.size();
     for (int k = 1; k <= i; ++k) {
         stokes_dot(h, h->w, h->V[k - 1], k);
@@ -1014,7 +1018,10 @@ void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
     }
     stokes_norm(h, h->w, i + 1);
     LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
-    LMM_CK(host_wait(h));
+    LMM_CK(cudaEventRecord(h->col_ev, h->stream));
+}
+void arnoldi_column_collect(lmm_handle* h, int i, std::vector<double>& col) {
+    LMM_CK(cudaEventSynchronize(h->col_ev));
     col.assign(i + 2, 0.0);
     for (int k = 1; k <= i; ++k) col[k] = h->hscal[8 * k + 4];
     col[i + 1] = h->hscal[8 * (i + 1) + 5];
@@ -1024,7 +1031,12 @@ void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
 // <w, V_k> from the unmodified w in one pass, then one pass subtracting
 // all projections, then the norm.  Same H entries up to rounding; three
 // launches and about 2i+5 vector passes instead of 2i+1 launches and 5i+3.
-void arnoldi_column_cgs(lmm_handle* h, int i, std::vector<double>& col) {
+void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
+    arnoldi_column_enqueue(h, i);
+    arnoldi_column_collect(h, i, col);
+}
+
+void arnoldi_column_cgs_enqueue(lmm_handle* h, int i) {
     const int64_t len = h->w.size();
     for (int k0 = 0; k0 < i; k0 += 8) {
         MVecs V{};
@@ -1047,10 +1059,7 @@ void arnoldi_column_cgs(lmm_handle* h, int i, std::vector<double>& col) {
         check_launch();
     }
     LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
-    LMM_CK(host_wait(h));
-    col.assign(i + 2, 0.0);
-    for (int k = 1; k <= i; ++k) col[k] = h->hscal[8 * k + 4];
-    col[i + 1] = h->hscal[8 * (i + 1) + 5];
+    LMM_CK(cudaEventRecord(h->col_ev, h->stream));
 }
 
 // ------------------------------------------------------------ the reference GMRES
@@ -1260,39 +1269,68 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
         s[1] = norm_r;
         int i, i_copy = 0;
         bool happy = false;
+        // While the host reads column i of H and applies its Givens rotation,
+        // the device may already run the next column's preconditioner and
+        // operator application (V_i = w / H(i+1,i) is formed on the device):
+        // done when the last residual estimate is far (50x) above the
+        // stopping threshold, so a column computed ahead is almost never
+        // thrown away.
+        const bool can_ahead = !learned && K.stag_mg_max_vcycles <= 1;
+        const double thr = std::max(K.gmres_rel_tol * norm_b, K.gmres_abs_tol);
+        double est_prev = norm_r;
+        bool ahead = false;
+        int ahead_v = 0, ahead_p = 0;
+        auto column_work = [&](int c) {  // Z_c = M^-1 V_c, w = A Z_c (c 0-based)
+            if (fp32) {
+                precon32(h, h->V[c], h->Z32[c], true);
+                launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[c], h->n, h->dm, h->w, h->stream);
+                if (learned) learned_stage(h, h->Zc[c], h->V[c], K.learned_stage);
+            } else {
+                precon64(h, h->V[c], h->Z64[c]);
+                launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[c], h->w, h->stream);
+            }
+            check_launch();
+        };
         for (i = 1; i <= m; ++i) {
             total_iter = total_iter + 1;
             i_copy = i;
-            if (fp32) {
-                precon32(h, h->V[i - 1], h->Z32[i - 1], true);
-                launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[i - 1], h->n, h->dm, h->w, h->stream);
-                if (learned) learned_stage(h, h->Zc[i - 1], h->V[i - 1], K.learned_stage);
-            } else {
-                precon64(h, h->V[i - 1], h->Z64[i - 1]);
-                launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[i - 1], h->w, h->stream);
-            }
-            check_launch();
+            if (!ahead) column_work(i - 1);
+            ahead = false;
             if (K.orthogonalization == 1)
-                arnoldi_column_cgs(h, i, col);
+                arnoldi_column_cgs_enqueue(h, i);
             else
-                arnoldi_column(h, i, col);
+                arnoldi_column_enqueue(h, i);
+            // V_i = w / H(i+1,i) (a zero H(i+1,i) ends the cycle below, V_i unused)
+            if (fp32)
+                launch_div_by_f32(h->w.base, h->V[i].base, h->pin32, h->slot(i + 1) + 5, len, h->stream);
+            else
+                launch_div_by(h->w.base, h->V[i].base, h->slot(i + 1) + 5, len, h->stream);
+            check_launch();
+            if (can_ahead && i < m && total_iter < K.gmres_max_iter &&
+                (total_iter < K.gmres_min_iter || est_prev > 50.0 * thr)) {
+                ahead_v = h->vcycles;
+                ahead_p = h->pvcycles;
+                column_work(i);
+                ahead_v = h->vcycles - ahead_v;
+                ahead_p = h->pvcycles - ahead_p;
+                ahead = true;
+            }
+            arnoldi_column_collect(h, i, col);
             for (int k = 1; k <= i + 1; ++k) H(k, i) = col[k];
             for (int k = 1; k <= i + 1; ++k)
                 if (!std::isfinite(col[k])) return LMM_ERR_NONFINITE;
-            if (H(i + 1, i) != 0.0) {
-                if (fp32)
-                    launch_div_by_f32(h->w.base, h->V[i].base, h->pin32, h->slot(i + 1) + 5, len, h->stream);
-                else
-                    launch_div_by(h->w.base, h->V[i].base, h->slot(i + 1) + 5, len, h->stream);
-                check_launch();
-            } else {
-                happy = true;
-            }
+            if (H(i + 1, i) == 0.0) happy = true;
             least_squares(i, H, cs, sn, s);
             const double est = std::fabs(s[i + 1]);
             push_hist(st, est);
+            est_prev = est;
             if (happy || total_iter >= K.gmres_max_iter) break;
             if (total_iter >= K.gmres_min_iter && (est <= K.gmres_rel_tol * norm_b || est <= K.gmres_abs_tol)) break;
+        }
+        if (ahead) {
+            // a column computed ahead of a converged cycle: not part of the solve
+            h->vcycles -= ahead_v;
+            h->pvcycles -= ahead_p;
         }
         solve_utri(i_copy - 1, H, s, y);
         if (fp32 && !learned) {
@@ -1484,6 +1522,7 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         LMM_CK(cudaEventCreate(&h->ev0));
         LMM_CK(cudaEventCreate(&h->ev1));
         if (k->host_wait == 1) LMM_CK(cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+        LMM_CK(cudaEventCreateWithFlags(&h->col_ev, cudaEventDisableTiming | (k->host_wait == 1 ? cudaEventBlockingSync : 0)));
         h->arena_bytes = plan_bytes(*g, *k, h->nlev, h->nlev_p);
         LMM_CK(cudaMalloc(&h->arena, h->arena_bytes));
         LMM_CK(cudaMemset(h->arena, 0, h->arena_bytes));
@@ -1593,6 +1632,7 @@ int lmm_stokes_destroy(lmm_handle* h) {
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->wait_ev) cudaEventDestroy(h->wait_ev);
+    if (h->col_ev) cudaEventDestroy(h->col_ev);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LMM_OK;
