@@ -72,6 +72,81 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Di
         if (color == 0 || (ccomp == 2 && on)) o2[t] = (W && wall_face(nb, 2)) ? T(0) : face_L<T, DM, VISC, 2, 0, T, W>(phi, C, nb, dxsqinv, b, c);
 }
 
+// --------------------------------------------------------------- one component per thread
+// The same face values as k_applyop (colour 0) and k_residual with one face
+// component per thread: grid.z covers nz * DM, component = blockIdx.z % DM
+// (uniform per block), so a thread keeps one stencil live instead of DM.
+struct PosC {
+    int i, j, k, comp;
+    bool ok;
+};
+template <int DM>
+__device__ __forceinline__ PosC posc(int nx, int ny) {
+    PosC p;
+    p.i = blockIdx.x * blockDim.x + threadIdx.x;
+    p.j = blockIdx.y * blockDim.y + threadIdx.y;
+    p.k = blockIdx.z / DM;
+    p.comp = blockIdx.z - p.k * DM;
+    p.ok = (p.i < nx) && (p.j < ny);
+    return p;
+}
+
+template <class T, int DM, int VISC, bool W = false>
+__global__ void __launch_bounds__(kThreads) k_applyop_c(Dims D, Coef<T> C, const T* __restrict__ p0, const T* __restrict__ p1,
+                                                        const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
+                                                        T* __restrict__ o2, T dxsqinv) {
+    pdl_enter();
+    const PosC q = posc<DM>(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    if (q.comp == 0) {
+        o0[t] = (W && wall_face(nb, 0)) ? T(0) : face_L<T, DM, VISC, 0, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+    } else if (q.comp == 1) {
+        o1[t] = (W && wall_face(nb, 1)) ? T(0) : face_L<T, DM, VISC, 1, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+    } else if constexpr (DM == 3) {
+        o2[t] = (W && wall_face(nb, 2)) ? T(0) : face_L<T, DM, VISC, 2, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+    }
+}
+
+template <class T, int DM, int VISC, bool W = false>
+__global__ void __launch_bounds__(kThreads) k_residual_c(Dims D, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
+                                                         const T* __restrict__ r2, const T* __restrict__ p0, const T* __restrict__ p1,
+                                                         const T* __restrict__ p2, T* __restrict__ o0, T* __restrict__ o1,
+                                                         T* __restrict__ o2, T dxsqinv) {
+    pdl_enter();
+    const PosC q = posc<DM>(D.nx, D.ny);
+    if (!q.ok) return;
+    Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
+    const int t = nb.s;
+    const T* phi[3] = {p0, p1, p2};
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    if (q.comp == 0) {
+        if (W && wall_face(nb, 0)) {
+            o0[t] = T(0);
+        } else {
+            T v = face_L<T, DM, VISC, 0, 0, T, W>(phi, C, nb, dxsqinv, b, c) - ld(r0, t);
+            o0[t] = v * T(-1);
+        }
+    } else if (q.comp == 1) {
+        if (W && wall_face(nb, 1)) {
+            o1[t] = T(0);
+        } else {
+            T v = face_L<T, DM, VISC, 1, 0, T, W>(phi, C, nb, dxsqinv, b, c) - ld(r1, t);
+            o1[t] = v * T(-1);
+        }
+    } else if constexpr (DM == 3) {
+        if (W && wall_face(nb, 2)) {
+            o2[t] = T(0);
+        } else {
+            T v = face_L<T, DM, VISC, 2, 0, T, W>(phi, C, nb, dxsqinv, b, c) - ld(r2, t);
+            o2[t] = v * T(-1);
+        }
+    }
+}
+
 // --------------------------------------------------------------- GS colour
 // One colour of stag_applyop_level(color) + stag_mg_update(color): faces of
 // component COMP with (i+j+k) % 2 == parity are updated in place.  Faces of
@@ -1028,6 +1103,15 @@ template <class T>
 void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color) {
     if (L.D.wall) return wl_applyop<T>(L, visc, phi, out, s, color);
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    if (color == 0) {
+        const G3 gc = geom3(L.D.nx, L.D.ny, L.D.nz * L.D.dm);
+        if (L.D.dm == 2) {
+            LMM_VISC_DISPATCH(visc, launch_pdl(k_applyop_c<T, 2, V>, gc.grid, gc.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv))
+        } else {
+            LMM_VISC_DISPATCH(visc, launch_pdl(k_applyop_c<T, 3, V>, gc.grid, gc.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv))
+        }
+        return;
+    }
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2) {
         LMM_VISC_DISPATCH(visc, (launch_pdl(k_applyop<T, 2, V>, g.grid, g.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
@@ -1145,11 +1229,11 @@ void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int v
     if (F.D.wall) return wl_residual_restrict<T>(F, Cc, visc, rhs_f, phi_f, rhs_c, s);
     // residual on every fine face into F.tmp, then the pure restriction
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
-    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
+    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz * F.D.dm);
     if (F.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 2, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, launch_pdl(k_residual_c<T, 2, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv))
     } else {
-        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 3, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, launch_pdl(k_residual_c<T, 3, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv))
     }
     count_launch();
     const G3 gc = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);

@@ -13,6 +13,15 @@ namespace lmm {
 template <class T>
 void wl_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
+    if (color == 0) {
+        const G3 gc = geom3(L.D.nx, L.D.ny, L.D.nz * L.D.dm);
+        if (L.D.dm == 2) {
+            LMM_VISC_DISPATCH(visc, launch_pdl(k_applyop_c<T, 2, V, true>, gc.grid, gc.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv))
+        } else {
+            LMM_VISC_DISPATCH(visc, launch_pdl(k_applyop_c<T, 3, V, true>, gc.grid, gc.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv))
+        }
+        return;
+    }
     const G3 g = geom3(L.D.nx, L.D.ny, L.D.nz);
     if (L.D.dm == 2) {
         LMM_VISC_DISPATCH(visc, (launch_pdl(k_applyop<T, 2, V, true>, g.grid, g.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv, color)))
@@ -75,11 +84,11 @@ template <class T>
 void wl_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3], const T* const phi_f[3],
                           T* const rhs_c[3], cudaStream_t s) {
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
-    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
+    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz * F.D.dm);
     if (F.D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 2, V, true>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual_c<T, 2, V, true>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     } else {
-        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual<T, 3, V, true>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
+        LMM_VISC_DISPATCH(visc, (launch_pdl(k_residual_c<T, 3, V, true>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv)))
     }
     count_launch();
     const G3 gc = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
