@@ -26,6 +26,9 @@ def main():
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=INT",
                     help="extra lmm_knobs integer field (repeatable), e.g. --knob tail_cells=512")
     ap.add_argument("--bc", default="", help="BC code per direction, both sides, e.g. -1,100,-1 (default periodic)")
+    ap.add_argument("--op", default="", choices=["", "smooth", "applyop", "apply_matrix", "vcycle", "macproject"],
+                    help="instead of solves: time one operation (lmm_time_op) --solves times after one warm-up; "
+                         "'smooth' and 'vcycle' run in the method's precision")
     a = ap.parse_args()
 
     import numpy as np
@@ -49,6 +52,13 @@ def main():
     al, be, bed, ga = [dev(x) for x in prob.alpha_fc], dev(prob.beta), [dev(x) for x in prob.beta_ed], dev(prob.gamma)
     xu, xp = [torch.zeros_like(bu[0]) for _ in range(3)], torch.zeros_like(bp)
     with StokesSolver(3, (a.n,) * 3, prob.dx, knobs=abi.make_knobs(**kn), bc=bc) as s:
+        if a.op:
+            s.load_coeffs(al, be, bed, ga, prob.theta_alpha)
+            fp32 = a.method == "mixed"
+            which = {"smooth": 1 if fp32 else 0, "applyop": 2, "apply_matrix": 3, "vcycle": 5 if fp32 else 4,
+                     "macproject": 6}[a.op]
+            print(json.dumps({"op": a.op, "us": s.time_op(which, reps=a.solves) * 1000.0}))
+            return
         out = []
         for i in range(a.warm + a.solves):
             for t in xu:
