@@ -139,7 +139,9 @@ typedef struct lmm_knobs {
                                       classical Gram-Schmidt, all projections in one pass */
     int    host_wait;              /* 0 = the host spins on the stream when it reads a scalar (lowest
                                       latency), 1 = it blocks (many host threads driving solvers) */
-    int    reserved[1];
+    int    ensemble_batch;         /* lmm_ensemble_*: 0 = 2D problems whose knobs allow it are solved
+                                      in batches (lmm_stokes_create_batch), -1 = always the worker
+                                      pool of one-problem handles; a solver handle ignores it */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

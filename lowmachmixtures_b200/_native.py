@@ -73,6 +73,8 @@ def load() -> C.CDLL:
     lib.lmm_ensemble_create.argtypes = [ci, P(abi.Knobs), ci, P(abi.EnsembleItem), ci, ci, P(vp)]
     lib.lmm_ensemble_run.argtypes = [vp, P(abi.EnsembleItem), ci]
     lib.lmm_ensemble_destroy.argtypes = [vp]
+    lib.lmm_stokes_create_batch.argtypes = [P(abi.Grid), P(abi.Knobs), ci, ci, P(vp)]
+    lib.lmm_stokes_solve_batch.argtypes = [vp, P(abi.EnsembleItem), ci]
     lib.lmm_stochastic_rhs.argtypes = [ci, P(ci), C.c_double, C.c_double, C.c_double, _dp, _dpp, C.c_ulonglong, _dpp, vp]
     lib.lmm_inner_prod_noalloc.argtypes = [C.c_int, P(C.c_int), _dpp, _dp, _dpp, _dp, C.c_double, C.c_void_p, _dp]
     lib.lmm_op_num_levels.argtypes = [C.c_void_p]

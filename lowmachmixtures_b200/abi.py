@@ -88,7 +88,7 @@ _KNOB_FIELDS = [
     ("l2_persist", C.c_int),
     ("orthogonalization", C.c_int),
     ("host_wait", C.c_int),
-    ("reserved", C.c_int * 1),
+    ("ensemble_batch", C.c_int),
 ]
 
 
@@ -112,6 +112,7 @@ KNOB_DEFAULTS = dict(
     gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1,
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
     tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0, orthogonalization=0, host_wait=0,
+    ensemble_batch=0,
 )
 
 

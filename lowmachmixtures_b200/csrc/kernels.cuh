@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_applyop(Di
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
     // colour c >= 1 covers component (c-1)/2, faces with (i+j+k) even for odd c
     const int ccomp = (color - 1) / 2;
-    const bool on = (color == 0) || ((((i + j + k) & 1) == ((color % 2 == 1) ? 0 : 1)));
+    const bool on = (color == 0) || ((((i + j + ck<DM>(k)) & 1) == ((color % 2 == 1) ? 0 : 1)));
     if (color == 0 || (ccomp == 0 && on)) o0[t] = (W && wall_face(nb, 0)) ? T(0) : face_L<T, DM, VISC, 0, 0, T, W>(phi, C, nb, dxsqinv, b, c);
     if (color == 0 || (ccomp == 1 && on)) o1[t] = (W && wall_face(nb, 1)) ? T(0) : face_L<T, DM, VISC, 1, 0, T, W>(phi, C, nb, dxsqinv, b, c);
     if constexpr (DM == 3)
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
     const int j = q.j, k = q.k;
-    const int i = 2 * q.i + ((j + k + parity) & 1);
+    const int i = 2 * q.i + ((j + ck<DM>(k) + parity) & 1);
     Nb nb = W ? make_nbw(D, i, j, k) : make_nb(D, i, j, k);
     if (W && wall_face(nb, COMP)) return;
     const T* phi[3] = {p0, p1, p2};
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_colour_update(Dims D, Coef<T> C, c
                                                             T* p, int parity, T omega, T dxsqinv) {
     pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
-    if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
+    if (!q.ok || ((q.i + q.j + ck<DM>(q.k)) & 1) != parity) return;
     Nb nb = W ? make_nbw(D, q.i, q.j, q.k) : make_nb(D, q.i, q.j, q.k);
     if (W && wall_face(nb, COMP)) return;
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
@@ -317,7 +317,7 @@ __device__ __forceinline__ T fine_resid(const Dims& F, const Coef<T>& C, const T
                                         T dxsqinv, T b, T c) {
     i = wrapi(i, F.nx);
     j = wrapi(j, F.ny);
-    k = (DM == 3) ? wrapi(k, F.nz) : 0;
+    k = (DM == 3) ? wrapi(k, F.nz) : k;
     Nb nb = make_nb(F, i, j, k);
     T v = face_L<T, DM, VISC, D_, LD>(phi, C, nb, dxsqinv, b, c) - ldp<LD>(rhs, nb.s);
     return v * T(-1);
@@ -351,7 +351,7 @@ __device__ __forceinline__ T restrict_face(const Dims& F, const Coef<T>& C, cons
             for (int q = 0; q < 4; ++q) { qi[q] = a_[q]; qj[q] = b_[q]; qk[q] = c_[q]; } }
     }
     T r[3 * NQ];
-    const int I = 2 * i, J = 2 * j, K = 2 * k;
+    const int I = 2 * i, J = 2 * j, K = (DM == 3) ? 2 * k : k;
 #pragma unroll 1
     for (int m = 0; m < 3 * NQ; ++m) {
         const int nrm = (m < NQ) ? 0 : (m < 2 * NQ ? 1 : -1);
@@ -446,16 +446,16 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
     auto R = [&](const T* f, int i, int j, int k) {
         i = wrapi(i, F.nx);
         j = wrapi(j, F.ny);
-        k = (DM == 3) ? wrapi(k, F.nz) : 0;
+        k = (DM == 3) ? wrapi(k, F.nz) : k;
         return ld(f, i + F.nx * (j + F.ny * k));
     };
     if constexpr (DM == 2) {
         if (!W || c0)
-        c0[t] = T(0.25) * (R(f0, I, J, 0) + R(f0, I, J + 1, 0)) +
-                T(0.125) * (R(f0, I + 1, J, 0) + R(f0, I + 1, J + 1, 0) + R(f0, I - 1, J, 0) + R(f0, I - 1, J + 1, 0));
+        c0[t] = T(0.25) * (R(f0, I, J, q.k) + R(f0, I, J + 1, q.k)) +
+                T(0.125) * (R(f0, I + 1, J, q.k) + R(f0, I + 1, J + 1, q.k) + R(f0, I - 1, J, q.k) + R(f0, I - 1, J + 1, q.k));
         if (!W || c1)
-        c1[t] = T(0.25) * (R(f1, I, J, 0) + R(f1, I + 1, J, 0)) +
-                T(0.125) * (R(f1, I, J + 1, 0) + R(f1, I + 1, J + 1, 0) + R(f1, I, J - 1, 0) + R(f1, I + 1, J - 1, 0));
+        c1[t] = T(0.25) * (R(f1, I, J, q.k) + R(f1, I + 1, J, q.k)) +
+                T(0.125) * (R(f1, I, J + 1, q.k) + R(f1, I + 1, J + 1, q.k) + R(f1, I, J - 1, q.k) + R(f1, I + 1, J - 1, q.k));
     } else {
         if (!W || c0)
         c0[t] = T(0.125) * (R(f0, I, J, K) + R(f0, I, J + 1, K) + R(f0, I, J, K + 1) + R(f0, I, J + 1, K + 1)) +
@@ -493,7 +493,7 @@ template <class T, int LD = 0>
 __device__ __forceinline__ T cat(const T* a, const Dims& Dc, int i, int j, int k) {
     i = wrapi(i, Dc.nx);
     j = wrapi(j, Dc.ny);
-    k = (Dc.dm == 3) ? wrapi(k, Dc.nz) : 0;
+    k = (Dc.dm == 3) ? wrapi(k, Dc.nz) : k;
     return ldp<LD>(a, i + Dc.nx * (j + Dc.ny * k));
 }
 
@@ -503,7 +503,7 @@ __device__ __forceinline__ T cat(const T* a, const Dims& Dc, int i, int j, int k
 // mirrors the face, negated at a no-slip wall
 template <class T, int LD, int COMP>
 __device__ __forceinline__ T catw(const T* a, const Dims& Dc, int i, int j, int k) {
-    int x[3] = {i, j, (Dc.dm == 3) ? k : 0};
+    int x[3] = {i, j, k};
     const int n[3] = {Dc.nx, Dc.ny, Dc.nz};
     bool neg = false;
 #pragma unroll
@@ -556,20 +556,20 @@ __device__ __forceinline__ void prolong_cell(const Dims& Dc, const T* q0, const 
             int joff = ((j & 1) == 0) ? -1 : 1;
             T v = (LD == 2) ? __ldcg(f0 + t) : f0[t];
             if ((i & 1) == 0)
-                v = v + T(0.75) * pcat<T, LD, W, 0>(q0, Dc, i2, j2, 0) + T(0.25) * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, 0);
+                v = v + T(0.75) * pcat<T, LD, W, 0>(q0, Dc, i2, j2, k) + T(0.25) * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, k);
             else
-                v = v + T(0.375) * pcat<T, LD, W, 0>(q0, Dc, i2, j2, 0) + T(0.125) * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, 0) + T(0.375) * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2, 0) +
-                    T(0.125) * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2 + joff, 0);
+                v = v + T(0.375) * pcat<T, LD, W, 0>(q0, Dc, i2, j2, k) + T(0.125) * pcat<T, LD, W, 0>(q0, Dc, i2, j2 + joff, k) + T(0.375) * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2, k) +
+                    T(0.125) * pcat<T, LD, W, 0>(q0, Dc, i2 + 1, j2 + joff, k);
             f0[t] = v;
         }
         if (!W || f1) {
             int ioff = ((i & 1) == 0) ? -1 : 1;
             T v = (LD == 2) ? __ldcg(f1 + t) : f1[t];
             if ((j & 1) == 0)
-                v = v + T(0.75) * pcat<T, LD, W, 1>(q1, Dc, i2, j2, 0) + T(0.25) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, 0);
+                v = v + T(0.75) * pcat<T, LD, W, 1>(q1, Dc, i2, j2, k) + T(0.25) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, k);
             else
-                v = v + T(0.375) * pcat<T, LD, W, 1>(q1, Dc, i2, j2, 0) + T(0.125) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, 0) + T(0.375) * pcat<T, LD, W, 1>(q1, Dc, i2, j2 + 1, 0) +
-                    T(0.125) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2 + 1, 0);
+                v = v + T(0.375) * pcat<T, LD, W, 1>(q1, Dc, i2, j2, k) + T(0.125) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2, k) + T(0.375) * pcat<T, LD, W, 1>(q1, Dc, i2, j2 + 1, k) +
+                    T(0.125) * pcat<T, LD, W, 1>(q1, Dc, i2 + ioff, j2 + 1, k);
             f1[t] = v;
         }
     } else {
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(kThreads) k_prolong_add(Dims F, Dims Dc, const
 // fine-grid value at (i, j, k), all indices inside the fine box
 template <class T>
 __device__ __forceinline__ T fat(const T* a, const Dims& F, int i, int j, int k) {
-    return ld(a, i + F.nx * (j + F.ny * (F.dm == 3 ? k : 0)));
+    return ld(a, i + F.nx * (j + F.ny * k));
 }
 
 // do_visc: 0 faces only, 1 faces + cells + edges, 2 faces + cells (the edges
@@ -644,14 +644,14 @@ __global__ void __launch_bounds__(kThreads) k_coarsen(Dims F, Dims Dc, Coef<T> C
     const int t = i + Dc.nx * (j + Dc.ny * k);
     const int I = 2 * i, J = 2 * j, K = 2 * k;
     if constexpr (DM == 2) {
-        a0[t] = T(0.5) * (fat(Cf.alpha[0], F, I, J, 0) + fat(Cf.alpha[0], F, I, J + 1, 0));
-        a1[t] = T(0.5) * (fat(Cf.alpha[1], F, I, J, 0) + fat(Cf.alpha[1], F, I + 1, J, 0));
+        a0[t] = T(0.5) * (fat(Cf.alpha[0], F, I, J, k) + fat(Cf.alpha[0], F, I, J + 1, k));
+        a1[t] = T(0.5) * (fat(Cf.alpha[1], F, I, J, k) + fat(Cf.alpha[1], F, I + 1, J, k));
         if (do_visc) {
             const T* b = Cf.beta;
-            beta[t] = T(0.25) * (fat(b, F, I, J, 0) + fat(b, F, I + 1, J, 0) + fat(b, F, I, J + 1, 0) + fat(b, F, I + 1, J + 1, 0));
+            beta[t] = T(0.25) * (fat(b, F, I, J, k) + fat(b, F, I + 1, J, k) + fat(b, F, I, J + 1, k) + fat(b, F, I + 1, J + 1, k));
             const T* g = Cf.gamma;
-            gamma[t] = T(0.25) * (fat(g, F, I, J, 0) + fat(g, F, I + 1, J, 0) + fat(g, F, I, J + 1, 0) + fat(g, F, I + 1, J + 1, 0));
-            if (do_visc == 1) e0[t] = fat(Cf.bed[0], F, I, J, 0);  // nodal injection
+            gamma[t] = T(0.25) * (fat(g, F, I, J, k) + fat(g, F, I + 1, J, k) + fat(g, F, I, J + 1, k) + fat(g, F, I + 1, J + 1, k));
+            if (do_visc == 1) e0[t] = fat(Cf.bed[0], F, I, J, k);  // nodal injection
         }
     } else {
         const T* A0 = Cf.alpha[0];
@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, con
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
     const int j = q.j, k = q.k;
-    const int i = 2 * q.i + ((j + k + parity) & 1);
+    const int i = 2 * q.i + ((j + ck<DM>(k) + parity) & 1);
     Nb nb = make_nb(D, i, j, k);
     const T* a[3] = {a0, a1, a2};
     T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_smooth_odd(Dims D, const T* a0,
                                                             const T* __restrict__ phi, T* __restrict__ out, int parity, T dxsqinv) {
     pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
-    if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
+    if (!q.ok || ((q.i + q.j + ck<DM>(q.k)) & 1) != parity) return;
     Nb nb = make_nb(D, q.i, q.j, q.k);
     const T* a[3] = {a0, a1, a2};
     T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
@@ -757,7 +757,7 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) k_copy_parity(Dims D, const T* __restrict__ in, T* __restrict__ out, int parity) {
     pdl_enter();
     const Pos q = pos3(D.nx, D.ny);
-    if (!q.ok || ((q.i + q.j + q.k) & 1) != parity) return;
+    if (!q.ok || ((q.i + q.j + (D.dm == 3 ? q.k : 0)) & 1) != parity) return;
     const int s = q.i + D.nx * (q.j + D.ny * q.k);
     out[s] = in[s];
 }
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(kThreads) k_copy_parity(Dims D, const T* __res
 template <class T, int DM, int LD = 0>
 __device__ __forceinline__ T cc_res_at(const Dims& F, const T* const a[3], const T* phi, const T* rhs, int i, int j, int k,
                                        T dxsqinv) {
-    Nb nb = make_nb(F, i, j, (DM == 3) ? k : 0);
+    Nb nb = make_nb(F, i, j, k);
     return ldp<LD>(rhs, nb.s) - cc_lap<T, DM, LD>(a, phi, nb, dxsqinv);
 }
 
@@ -782,7 +782,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const
     const int I = 2 * i, J = 2 * j, K = 2 * k;
 #define R(ii, jj, kk) cc_res_at<T, DM>(F, a, phi, rhs, ii, jj, kk, dxsqinv)
     if constexpr (DM == 2)
-        rc[t] = T(0.25) * (R(I, J, 0) + R(I + 1, J, 0) + R(I, J + 1, 0) + R(I + 1, J + 1, 0));
+        rc[t] = T(0.25) * (R(I, J, k) + R(I + 1, J, k) + R(I, J + 1, k) + R(I + 1, J + 1, k));
     else
         rc[t] = T(0.125) * (R(I, J, K) + R(I + 1, J, K) + R(I, J + 1, K) + R(I + 1, J + 1, K) + R(I, J, K + 1) + R(I + 1, J, K + 1) +
                             R(I, J + 1, K + 1) + R(I + 1, J + 1, K + 1));
@@ -795,7 +795,7 @@ __global__ void __launch_bounds__(kThreads) k_cc_prolong_add(Dims F, Dims Dc, co
     const Pos q = pos3(F.nx, F.ny);
     if (!q.ok) return;
     const int t = q.i + F.nx * (q.j + F.ny * q.k);
-    pf[t] = pf[t] + ld(pc, (q.i >> 1) + Dc.nx * ((q.j >> 1) + Dc.ny * (q.k >> 1)));
+    pf[t] = pf[t] + ld(pc, (q.i >> 1) + Dc.nx * ((q.j >> 1) + Dc.ny * ((DM == 3) ? (q.k >> 1) : q.k)));
 }
 
 template <class T, int DM>
@@ -896,19 +896,39 @@ __global__ void k_fill(T* __restrict__ out, T v, int64_t n) {
 // out[0..dm] per component; out[4] = sum_d out[d] + pw^2 out[dm] (the
 // Hessenberg entry of gmres.f90:344), out[5] = sqrt(|u|^2 + (pw |p|)^2)
 // (the Stokes norm of gmres.f90:127-130).
+//
+// 2D batches (D.nz instances of nx*ny cells): blockIdx.y is the instance,
+// with its own partials, counter and 8-double output slot out + 8 * b; the
+// grid's x extent and every summation order are those of one instance
+// reduced alone, so each instance's result has the same bits.
 template <class T, int DM, int MODE>
 __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const T* a1, const T* a2, const T* a3, const T* b0,
                                                      const T* b1, const T* b2, const T* b3, double w0, double w1, double w2,
                                                      double pw, double* partials, unsigned* counter, double* out) {
     pdl_enter();
     constexpr int NC = DM + 1;
+    const int nzi = (DM == 3) ? D.nz : 1;  // third extent of one instance
+    const int n = D.nx * D.ny * nzi;
+    {
+        const int64_t off = (int64_t)blockIdx.y * n;
+        a0 = a0 ? a0 + off : a0;
+        a1 = a1 ? a1 + off : a1;
+        a2 = a2 ? a2 + off : a2;
+        a3 = a3 ? a3 + off : a3;
+        b0 = b0 ? b0 + off : b0;
+        b1 = b1 ? b1 + off : b1;
+        b2 = b2 ? b2 + off : b2;
+        b3 = b3 ? b3 + off : b3;
+        partials += (int64_t)blockIdx.y * gridDim.x * NC;
+        counter += blockIdx.y;
+        out += (int64_t)blockIdx.y * 8;
+    }
     const T* A[4] = {a0, a1, a2, a3};
     const T* B[4] = {b0, b1, b2, b3};
     const double W[3] = {w0, w1, w2};
     double acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-    const int n = D.nx * D.ny * D.nz;
     const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const T* AA[NC];
@@ -939,7 +959,7 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
             const T* a = A[c];
             const T* b = B[c];
             if (!a || W[c] == 1.0) continue;
-            const int m = (c == 0) ? D.ny * D.nz : (c == 1 ? D.nx * D.nz : D.nx * D.ny);
+            const int m = (c == 0) ? D.ny * nzi : (c == 1 ? D.nx * nzi : D.nx * D.ny);
             double v = 0.0;
             for (int q = tid; q < m; q += stride) {
                 int t;
@@ -1391,8 +1411,9 @@ void launch_fill(T* out, double v, int64_t n, cudaStream_t s) {
 
 template <class T>
 void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const b[4], const double wseam[3], double pw,
-                   double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s) {
-#define RED(DM_, M_) launch_pdl(k_reduce<T, DM_, M_>, nblocks, kThreads, 0, s, D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out)
+                   double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s, int ninst) {
+    const dim3 grid(nblocks, ninst);
+#define RED(DM_, M_) launch_pdl(k_reduce<T, DM_, M_>, grid, dim3(kThreads), 0, s, D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out)
     if (D.dm == 2) {
         if (mode == 0) RED(2, 0); else if (mode == 1) RED(2, 1); else RED(2, 2);
     } else {
@@ -1459,6 +1480,6 @@ void launch_div_mul(const LevelDev<T>& L, const T* const l[3], const T* const m[
     template void launch_recip<T>(const T*, T*, int64_t, cudaStream_t);                                                        \
     template void launch_fill<T>(T*, double, int64_t, cudaStream_t);                                                           \
     template void launch_reduce<T>(const Dims&, int, const T* const[4], const T* const[4], const double[3], double,            \
-                                   double*, unsigned*, double*, int, cudaStream_t);
+                                   double*, unsigned*, double*, int, cudaStream_t, int);
 
 }  // namespace lmm

@@ -143,9 +143,12 @@ void launch_fill(T* out, double v, int64_t n, cudaStream_t s);
 // components c = 0..dm-1 are faces, c = dm the cell field (weight 1).
 // a entries may be nullptr to skip a component.  out[4] and out[5] receive
 // the combined Hessenberg entry and Stokes norm (see k_reduce).
+// ninst > 1: a 2D batch (D.nz = ninst instances), one reduction per
+// instance into out + 8 * b, nblocks blocks each (partials: ninst * nblocks
+// * (dm + 1) doubles; counter: ninst entries, zero on entry and on exit).
 template <class T>
 void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const b[4], const double wseam[3], double pw,
-                   double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s);
+                   double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s, int ninst = 1);
 
 int reduce_blocks(int64_t n);
 // raise a kernel's dynamic shared-memory limit to at least `bytes` on the

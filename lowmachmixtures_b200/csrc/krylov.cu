@@ -301,6 +301,8 @@ __global__ void k_sub_means(Dims D, T* u0, T* u1, T* u2, T* p, const double* __r
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t n = (int64_t)D.nx * D.ny * D.nz;
     if (t >= n) return;
+    // 2D batch: the sums of this entry's instance (slot stride 8)
+    if (DM == 2) sums += (int64_t)((int)t / (D.nx * D.ny)) * 8;
     const double mp = sums[DM] / total_volume;
     p[t] = (T)((double)p[t] - mp);
     if (sub_u) {
@@ -680,6 +682,100 @@ void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t le
     case 7: launch_pdl(k_maxpy<7>, nb, kT, 0, s, w, V, hs, len); break;
     default: launch_pdl(k_maxpy<8>, nb, kT, 0, s, w, V, hs, len); break;
     }
+}
+
+// ---------------------------------------------------------------- 2D batches
+// A batch stacks B independent 2D problems of ni = nx*ny cells along the
+// third index: entry e of a Stokes vector (component c at c*n, n = ni*B)
+// belongs to instance (e % n) / ni.  Per-instance scalars live in slot
+// arrays of B x 8 doubles (instance b at [8b], the k_reduce layout).  Each
+// kernel computes, per entry, the expression of its one-problem counterpart
+// above with that instance's scalar.
+namespace {
+
+__device__ __forceinline__ int inst_of(int64_t e, int64_t n, int ni) { return (int)((e % n) / ni); }
+
+// v = w / den_b (den_b = slots[8b + 5]); v32 (may be null) = (float)v.  A
+// zero norm (an instance that has stopped: its column is not used) divides
+// by 1 instead.
+__global__ void k_div_by_batch(const double* __restrict__ w, double* __restrict__ v, float* __restrict__ v32,
+                               const double* __restrict__ slots, int64_t n, int ni, int64_t len) {
+    pdl_enter();
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= len) return;
+    const double d = slots[(int64_t)inst_of(e, n, ni) * 8 + 5];
+    const double q = w[e] / (d != 0.0 ? d : 1.0);
+    v[e] = q;
+    if (v32) v32[e] = (float)q;
+}
+
+// w -= V * h_b (h_b = slots[8b + 4])
+__global__ void k_sub_scaled_batch(double* __restrict__ w, const double* __restrict__ V, const double* __restrict__ slots, int64_t n,
+                                   int ni, int64_t len) {
+    pdl_enter();
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= len) return;
+    const double tmp = V[e] * slots[(int64_t)inst_of(e, n, ni) * 8 + 4];
+    w[e] = w[e] - tmp;
+}
+
+// x += sum_{k<J} ys[k*B + b] Z_k, in k order; a zero coefficient (an
+// instance whose cycle had fewer columns) is skipped
+template <class TZ>
+__global__ void k_add_scaled_multi_batch(double* __restrict__ x, const TZ* const* __restrict__ Z, const double* __restrict__ ys, int J,
+                                         int nbatch, int64_t n, int ni, int64_t len) {
+    pdl_enter();
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
+        const int b = inst_of(e, n, ni);
+        double v = x[e];
+        for (int k = 0; k < J; ++k) {
+            const double y = ys[(int64_t)k * nbatch + b];
+            if (y == 0.0) continue;
+            const double tmp = (double)Z[k][e] * y;
+            v = v + tmp;
+        }
+        x[e] = v;
+    }
+}
+
+// dst[b * ni + t] = src[b][t] and back (per-instance arrays <-> batch array)
+__global__ void k_gather_ptrs(const double* const* __restrict__ src, double* __restrict__ dst, int ni, int count) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= (int64_t)ni * count) return;
+    const int b = (int)(e / ni), t = (int)(e - (int64_t)b * ni);
+    dst[e] = src[b][t];
+}
+__global__ void k_scatter_ptrs(const double* __restrict__ src, double* const* __restrict__ dst, int ni, int count) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= (int64_t)ni * count) return;
+    const int b = (int)(e / ni), t = (int)(e - (int64_t)b * ni);
+    dst[b][t] = src[e];
+}
+
+}  // namespace
+
+void launch_div_by_batch(const double* w, double* v, float* v32, const double* slots, int64_t n, int ni, int64_t len, cudaStream_t s) {
+    launch_pdl(k_div_by_batch, nb(len), kT, 0, s, w, v, v32, slots, n, ni, len);
+}
+void launch_sub_scaled_batch(double* w, const double* V, const double* slots, int64_t n, int ni, int64_t len, cudaStream_t s) {
+    launch_pdl(k_sub_scaled_batch, nb(len), kT, 0, s, w, V, slots, n, ni, len);
+}
+template <class TZ>
+void launch_add_scaled_multi_batch(double* x, const TZ* const* Z_dev, const double* ys_dev, int J, int nbatch, int64_t n, int ni,
+                                   int64_t len, cudaStream_t s) {
+    const int64_t b = (len + kT - 1) / kT;
+    const int g = (int)(b > 8192 ? 8192 : b);
+    launch_pdl(k_add_scaled_multi_batch<TZ>, g, kT, 0, s, x, Z_dev, ys_dev, J, nbatch, n, ni, len);
+}
+template void launch_add_scaled_multi_batch<float>(double*, const float* const*, const double*, int, int, int64_t, int, int64_t,
+                                                   cudaStream_t);
+template void launch_add_scaled_multi_batch<double>(double*, const double* const*, const double*, int, int, int64_t, int, int64_t,
+                                                    cudaStream_t);
+void launch_gather_ptrs(const double* const* src_dev, double* dst, int ni, int count, cudaStream_t s) {
+    k_gather_ptrs<<<nb((int64_t)ni * count), kT, 0, s>>>(src_dev, dst, ni, count);
+}
+void launch_scatter_ptrs(const double* src, double* const* dst_dev, int ni, int count, cudaStream_t s) {
+    k_scatter_ptrs<<<nb((int64_t)ni * count), kT, 0, s>>>(src, dst_dev, ni, count);
 }
 
 }  // namespace lmm

@@ -92,4 +92,19 @@ void launch_scatter_boxlib_w(const Dims& D, int kind, const int nodal[3], int ng
 // zero the wall faces (face 0 of each wall-normal component)
 void launch_zero_wall_faces(const Dims& D, double* const u[3], cudaStream_t s);
 
+// 2D batches: B instances of ni cells stacked along the third index (n =
+// ni*B per component, len = (dm+1)*n); per-instance scalars in slot arrays
+// of B x 8 doubles.
+// v = w / slots[8b+5] (v32, if not null, = (float)v)
+void launch_div_by_batch(const double* w, double* v, float* v32, const double* slots, int64_t n, int ni, int64_t len, cudaStream_t s);
+// w -= V * slots[8b+4]
+void launch_sub_scaled_batch(double* w, const double* V, const double* slots, int64_t n, int ni, int64_t len, cudaStream_t s);
+// x += sum_{k<J} ys[k*B+b] Z_k (Z_dev: device table of J vectors)
+template <class TZ>
+void launch_add_scaled_multi_batch(double* x, const TZ* const* Z_dev, const double* ys_dev, int J, int nbatch, int64_t n, int ni,
+                                   int64_t len, cudaStream_t s);
+// dst[b*ni + t] = src[b][t] / dst[b][t] = src[b*ni + t] (device pointer tables)
+void launch_gather_ptrs(const double* const* src_dev, double* dst, int ni, int count, cudaStream_t s);
+void launch_scatter_ptrs(const double* src, double* const* dst_dev, int ni, int count, cudaStream_t s);
+
 }  // namespace lmm

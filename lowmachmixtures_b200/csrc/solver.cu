@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -27,6 +28,7 @@
 #include <tuple>
 #include <vector>
 
+#include "../../include/lmm_ensemble.h"
 #include "../../include/lmm_noalloc.h"
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
@@ -39,11 +41,27 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// LMM_DEBUG set in the environment: every launch is followed by a
+// synchronisation of the solving thread's stream (outside graph capture),
+// so a failing kernel is reported at its own launch; errors go to stderr
+const bool g_debug = std::getenv("LMM_DEBUG") != nullptr;
+thread_local cudaStream_t g_debug_stream = nullptr;
+thread_local int g_debug_dims[3] = {0, 0, 0};  // the solving handle's nx, ny, nz
+
+// a failed CUDA call or launch: its text and source line in the calling
+// thread's last error
+void note_error(const std::string& what, const char* fn, int line) {
+    g_last_error = what + " (" + fn + ":" + std::to_string(line) + ")";
+    if (g_debug)
+        std::fprintf(stderr, "lmm: %s [handle %d x %d x %d]\n", g_last_error.c_str(), g_debug_dims[0], g_debug_dims[1],
+                     g_debug_dims[2]);
+}
+
 #define LMM_CK(call)                                                                     \
     do {                                                                                 \
         cudaError_t e_ = (call);                                                         \
         if (e_ != cudaSuccess) {                                                         \
-            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);           \
+            note_error(std::string(#call) + ": " + cudaGetErrorString(e_), __func__, __LINE__); \
             throw LmmError(LMM_ERR_CUDA);                                                \
         }                                                                                \
     } while (0)
@@ -53,11 +71,16 @@ struct LmmError {
     explicit LmmError(int c) : code(c) {}
 };
 
-inline void check_launch() {
+inline void check_launch(const char* fn = __builtin_FUNCTION(), int line = __builtin_LINE()) {
     lmm::count_launch();
     cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && g_debug && g_debug_stream) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(g_debug_stream, &cs);
+        if (cs == cudaStreamCaptureStatusNone) e = cudaStreamSynchronize(g_debug_stream);
+    }
     if (e != cudaSuccess) {
-        g_last_error = std::string("kernel launch: ") + cudaGetErrorString(e);
+        note_error(std::string("kernel launch: ") + cudaGetErrorString(e), fn, line);
         throw LmmError(LMM_ERR_CUDA);
     }
 }
@@ -145,6 +168,21 @@ struct lmm_handle {
     float* lz32 = nullptr;
     int* luses = nullptr;  // [accepted, tried] of the current solve
     static constexpr int kLrnSlot = 250;
+    // a batch of 2D problems (lmm_stokes_create_batch): `batch` instances of
+    // one grid stacked along the third index of every array (D0.nz = batch);
+    // per-instance scalars in slot arrays of batch x 8 doubles
+    int batch = 1;
+    bool batched = false;
+    static constexpr int kBSlots = 48;
+    static constexpr int kGatherFields = 11;  // b_u(2), b_p, alpha_fc(2), beta, beta_ed, gamma, x_u(2), x_p
+    double* bslots = nullptr;                 // kBSlots slot arrays (device)
+    double* bhost = nullptr;                  // pinned mirror
+    double* ys = nullptr;                     // (m + 1) x batch update coefficients (device)
+    double* ys_host = nullptr;                // pinned
+    void** ztab = nullptr;                    // device table of the m Z vectors
+    const double** gtab = nullptr;            // device table: kGatherFields x batch array pointers
+    const double** gtab_host = nullptr;       // pinned
+    double* bslot(int k) { return bslots + (int64_t)k * batch * 8; }
 
     template <class T>
     T* alloc(int64_t count) {
@@ -192,24 +230,35 @@ int mean_mask(const lmm_handle* h, double theta) {
     return ((1 << h->dm) - 1) & ~h->D0.wall;
 }
 
+// reduction partials: k_mdot's 592 blocks x 8 vectors x 4 components, or
+// per instance of a batch k_reduce's blocks x 3 components
+int64_t partials_count(const lmm_grid& g, int batch) {
+    const int64_t one = 4096 * 8;
+    if (g.dm != 2 || batch <= 1) return one;
+    return std::max<int64_t>(one, (int64_t)batch * reduce_blocks((int64_t)g.n[0] * g.n[1]) * 3);
+}
+
 int64_t level_cells(const int n[3], int dm, int lev) {
     int64_t c = 1;
     for (int d = 0; d < dm; ++d) c *= (n[d] >> lev);
     return c;
 }
 
-size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
+// batch: 2D instances stacked along the third index (1 for one problem);
+// batched: a batch handle (its slot arrays, tables and pinned mirrors)
+size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p, int batch = 1, bool batched = false) {
     const int dm = g.dm;
+    const int64_t nb = (dm == 2) ? batch : 1;
     const int ne = (dm == 2) ? 1 : 3;
     size_t tot = 0;
     auto add = [&](int64_t count, size_t sz) { tot += ((size_t)count * sz + 255) & ~(size_t)255; };
     for (int l = 0; l < std::max(nlev, nlev_p); ++l) {
-        int64_t c = level_cells(g.n, dm, l);
+        int64_t c = level_cells(g.n, dm, l) * nb;
         Dims Dl;
         Dl.dm = dm;
         Dl.nx = g.n[0] >> l;
         Dl.ny = g.n[1] >> l;
-        Dl.nz = (dm == 3) ? (g.n[2] >> l) : 1;
+        Dl.nz = (dm == 3) ? (g.n[2] >> l) : batch;
         set_walls(Dl, g);
         for (int prec = 0; prec < 2; ++prec) {
             size_t sz = prec ? sizeof(float) : sizeof(double);
@@ -224,7 +273,7 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
             }
         }
     }
-    int64_t n = level_cells(g.n, dm, 0);
+    int64_t n = level_cells(g.n, dm, 0) * nb;
     int64_t vec = (int64_t)(dm + 1) * n;
     add(n, sizeof(double) * 2 * dm);                    // alpha_fc, alphainv
     add(n, sizeof(float) * dm);                         // alphainv32
@@ -240,8 +289,8 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
     for (int q = 0; q < 3 + dm; ++q) add(n, sizeof(float));
     add(vec, sizeof(float));
     add(vec, sizeof(float));
-    add(4096 * 8, sizeof(double));  // reduction partials (k_mdot: 592 blocks x 8 vectors x 4 components)
-    add(64, sizeof(unsigned));
+    add(partials_count(g, batch), sizeof(double));  // reduction partials
+    add(std::max(64, batch), sizeof(unsigned));
     add(8 * lmm_handle::kSlots, sizeof(double));
     // BoxLib staging: the largest field with up to 4 ghost layers
     int64_t st = 1;
@@ -250,6 +299,12 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p) {
     if (k.visc_schur_approx == 1)
         for (int prec = 0; prec < 2; ++prec)
             for (int q = 0; q < 8; ++q) add(n, prec ? sizeof(float) : sizeof(double));  // BFBt scratch
+    if (batched) {
+        add((int64_t)lmm_handle::kBSlots * batch * 8, sizeof(double));  // slot arrays
+        add((int64_t)(k.gmres_max_inner + 1) * batch, sizeof(double));  // ys
+        add(k.gmres_max_inner + 1, sizeof(void*));                     // ztab
+        add((int64_t)lmm_handle::kGatherFields * batch, sizeof(void*));  // gtab
+    }
     return tot + (1 << 20);
 }
 
@@ -272,7 +327,7 @@ void build_levels(lmm_handle* h) {
         v.D.dm = dm;
         v.D.nx = h->grid.n[0] >> l;
         v.D.ny = h->grid.n[1] >> l;
-        v.D.nz = (dm == 3) ? (h->grid.n[2] >> l) : 1;
+        v.D.nz = (dm == 3) ? (h->grid.n[2] >> l) : h->batch;
         set_walls(v.D, h->grid);
         v.dx = h->grid.dx * (double)(1 << l);
         v.n = (int64_t)v.D.nx * v.D.ny * v.D.nz;
@@ -337,6 +392,11 @@ SVec make_svec(lmm_handle* h) {
 }
 
 // ------------------------------------------------------------ reductions
+// a reduction's output slot and instance count: one slot for one problem;
+// on a batch handle a slot array (instance b at + 8b), one result each
+double* rslot(lmm_handle* h, int k) { return h->batched ? h->bslot(k) : h->slot(k); }
+int ninst(const lmm_handle* h) { return h->batched ? h->batch : 1; }
+
 void stokes_reduce(lmm_handle* h, int mode, const double* const a[4], const double* const b[4], int slot) {
     double w[3];
     if (mode == 0) {
@@ -350,8 +410,8 @@ void stokes_reduce(lmm_handle* h, int mode, const double* const a[4], const doub
             w[d] = (nd / tile[d] < 2) ? 3.0 : 2.0;
         }
     }
-    launch_reduce<double>(h->D0, mode, a, b, w, h->knobs.p_norm_weight, h->partials, h->counter, h->slot(slot),
-                          h->red_blocks, h->stream);
+    launch_reduce<double>(h->D0, mode, a, b, w, h->knobs.p_norm_weight, h->partials, h->counter, rslot(h, slot),
+                          h->red_blocks, h->stream, ninst(h));
     check_launch();
 }
 
@@ -503,6 +563,7 @@ int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool st
     const int cells = h->knobs.tail_cells == 0 ? (stag ? 512 : 4096) : h->knobs.tail_cells;
     if (cells < 0) return nl;
     if (stag && h->D0.wall) return nl;  // the staggered tail kernel is periodic only
+    if (h->batched) return nl;           // the tails solve one instance per launch
     const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
     const bool jacobi = stag && h->knobs.stag_mg_smoother == 0;
     int lc = nl;
@@ -688,7 +749,7 @@ void reduce_means<float>(lmm_handle* h, float* const u[3], const float* p, int s
         int nd = (d < h->dm) ? h->grid.n[d] : 1;
         w[d] = (nd / tile[d] < 2) ? 3.0 : 2.0;
     }
-    launch_reduce<float>(h->D0, 1, a, b, w, 0.0, h->partials, h->counter, h->slot(slot), h->red_blocks, h->stream);
+    launch_reduce<float>(h->D0, 1, a, b, w, 0.0, h->partials, h->counter, rslot(h, slot), h->red_blocks, h->stream, ninst(h));
     check_launch();
 }
 
@@ -762,7 +823,7 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
     auto& L = levels<T>(h);
     LevelDev<T>& L0 = L[0];
     PrecScratch<T> S = prec_scratch<T>(h);
-    const int mean_slot = h->kSlots - 3;
+    const int mean_slot = h->batched ? lmm_handle::kBSlots - 1 : h->kSlots - 3;
 
     // the staggered solve reads its rhs from L0.rhs and iterates on L0.phi
     auto vel_solve = [&](const T* const rhs[3], bool zero_guess) {
@@ -880,7 +941,7 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
     reduce_means<T>(h, x_u, x_p, mean_slot);
     double tv = 1.0;
     for (int d = 0; d < dm; ++d) tv *= (double)h->grid.n[d];
-    launch_sub_means<T>(h->D0, x_u, x_p, h->slot(mean_slot), tv, mean_mask(h, theta), h->stream);
+    launch_sub_means<T>(h->D0, x_u, x_p, rslot(h, mean_slot), tv, mean_mask(h, theta), h->stream);
     check_launch();
 }
 
@@ -899,6 +960,7 @@ void run_graphed(lmm_handle* h, const void* in, const void* out, int prec, F bod
     lmm_handle::Graph& g = h->graphs[key];
     if (g.exec) {
         LMM_CK(cudaGraphLaunch(g.exec, h->stream));
+        if (g_debug) LMM_CK(cudaStreamSynchronize(h->stream));
         for (int64_t q = 0; q < g.launches; ++q) count_launch();
         h->vcycles += g.vcycles;
         h->pvcycles += g.pvcycles;
@@ -930,6 +992,7 @@ void run_graphed(lmm_handle* h, const void* in, const void* out, int prec, F bod
     g.vcycles = h->vcycles - v0;
     g.pvcycles = h->pvcycles - p0;
     LMM_CK(cudaGraphLaunch(g.exec, h->stream));
+    if (g_debug) LMM_CK(cudaStreamSynchronize(h->stream));
 }
 
 // FP64 Stokes vector in, FP64 Stokes vector out
@@ -1366,6 +1429,200 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
     return status;
 }
 
+// ------------------------------------------------------------ batches of 2D problems
+// FGMRES (modified Gram-Schmidt) on the instances of a batch handle at once:
+// every vector operation, preconditioner application and reduction covers
+// the whole batch in one launch, while the host keeps per instance the
+// Hessenberg matrix, Givens sequence, stopping decisions and statistics of
+// run_fgmres.  Per instance the arithmetic is run_fgmres's with
+// orthogonalization 0 (the reductions partition and sum each instance as
+// they would one problem).  An instance that has stopped rides along: its
+// columns are computed and not used, its update coefficients are zero.
+int run_fgmres_batch(lmm_handle* h, int count, lmm_stats* stats, int* status) {
+    const lmm_knobs& K = h->knobs;
+    const int m = K.gmres_max_inner, B = h->batch, ni = h->D0.nx * h->D0.ny;
+    const int64_t n = h->n, len = h->b.size();
+    const bool fp32 = (K.precision == LMM_PRECISION_FP32);
+    // slots s0 .. s0+ns-1 to the host: bhost[(k - s0) * B * 8 + b * 8 + c]
+    auto fetch = [&](int s0, int ns) {
+        LMM_CK(cudaMemcpyAsync(h->bhost, h->bslot(s0), sizeof(double) * ns * B * 8, cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(host_wait(h));
+    };
+    auto at = [&](int k, int s0, int b, int c) { return h->bhost[(int64_t)(k - s0) * B * 8 + b * 8 + c]; };
+    struct Inst {
+        Hess H;
+        std::vector<double> cs, sn, s, y;
+        double norm_b = 0.0, norm_init = 0.0, norm_r = 0.0;
+        bool done = false, stop = false;
+        int ib = 0, total = 0, outer = 0, status = LMM_OK;
+    };
+    std::vector<Inst> P(B);
+    int64_t apps = 0;  // preconditioner applications (each covers the batch)
+    for (auto& p : P) {
+        p.H = Hess{m + 1, std::vector<double>((size_t)(m + 1) * m, 0.0)};
+        p.cs.assign(m + 2, 0.0);
+        p.sn.assign(m + 2, 0.0);
+        p.s.assign(m + 3, 0.0);
+        p.y.assign(m + 2, 0.0);
+    }
+    h->vcycles = 0;
+    stokes_norm(h, h->b, 0);
+    fetch(0, 1);
+    for (int b = 0; b < B; ++b) {
+        Inst& p = P[b];
+        p.norm_b = at(0, 0, b, 5);
+        if (b < count) stats[b].norm_b = p.norm_b;
+        if (!std::isfinite(p.norm_b)) {
+            p.status = LMM_ERR_NONFINITE;
+            p.done = true;
+        } else if (p.norm_b <= 0.0) {
+            p.done = true;  // x = 0 (gmres.f90:142-150)
+            for (int c = 0; c <= h->dm; ++c)
+                LMM_CK(cudaMemsetAsync(h->x.c(c) + (int64_t)b * ni, 0, sizeof(double) * ni, h->stream));
+        }
+    }
+    auto column_work = [&](int c) {  // Z_c = M^-1 V_c, w = A Z_c
+        if (fp32) {
+            precon32(h, h->V[c], h->Z32[c], true);
+            launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[c], h->n, h->dm, h->w, h->stream);
+        } else {
+            precon64(h, h->V[c], h->Z64[c]);
+            launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[c], h->w, h->stream);
+        }
+        check_launch();
+        ++apps;
+    };
+    int iter = 0;
+    bool first = true;
+    for (;;) {
+        launch_apply_matrix(h->L64[0], K.visc_type, h->x, h->tmp, h->stream);
+        check_launch();
+        launch_neg_resid(h->tmp.base, h->b.base, len, h->stream);
+        check_launch();
+        stokes_norm(h, h->tmp, 0);
+        fetch(0, 1);
+        bool any = false;
+        for (int b = 0; b < B; ++b) {
+            Inst& p = P[b];
+            if (p.done) continue;
+            p.norm_r = at(0, 0, b, 5);
+            if (!std::isfinite(p.norm_r)) {
+                p.status = LMM_ERR_NONFINITE;
+                p.done = true;
+                continue;
+            }
+            if (first) p.norm_init = p.norm_r;
+            if (p.total >= K.gmres_min_iter && (p.norm_r <= K.gmres_rel_tol * p.norm_b || p.norm_r <= K.gmres_abs_tol)) {
+                p.done = true;
+            } else if (p.total >= K.gmres_max_iter) {
+                p.status = LMM_WARN_MAX_ITER;
+                p.done = true;
+            } else if (iter >= K.gmres_max_outer) {
+                p.status = LMM_WARN_MAX_OUTER;
+                p.done = true;
+            } else {
+                any = true;
+            }
+        }
+        first = false;
+        if (!any) break;
+        iter = iter + 1;
+        launch_div_by_batch(h->tmp.base, h->V[0].base, fp32 ? h->pin32 : nullptr, h->bslot(0), n, ni, len, h->stream);
+        check_launch();
+        for (auto& p : P) {
+            if (!p.done) p.outer = iter;
+            p.stop = p.done;
+            p.ib = 0;
+            std::fill(p.s.begin(), p.s.end(), 0.0);
+            p.s[1] = p.norm_r;
+        }
+        for (int i = 1; i <= m; ++i) {
+            column_work(i - 1);
+            for (int k = 1; k <= i; ++k) {
+                stokes_dot(h, h->w, h->V[k - 1], k);
+                launch_sub_scaled_batch(h->w.base, h->V[k - 1].base, h->bslot(k), n, ni, len, h->stream);
+                check_launch();
+            }
+            stokes_norm(h, h->w, i + 1);
+            launch_div_by_batch(h->w.base, h->V[i].base, fp32 ? h->pin32 : nullptr, h->bslot(i + 1), n, ni, len, h->stream);
+            check_launch();
+            fetch(1, i + 1);
+            bool cont = false;
+            for (int b = 0; b < B; ++b) {
+                Inst& p = P[b];
+                if (p.stop) continue;
+                p.total = p.total + 1;
+                bool bad = false;
+                for (int k = 1; k <= i; ++k) p.H(k, i) = at(k, 1, b, 4);
+                p.H(i + 1, i) = at(i + 1, 1, b, 5);
+                for (int k = 1; k <= i + 1; ++k) bad = bad || !std::isfinite(p.H(k, i));
+                if (bad) {
+                    p.status = LMM_ERR_NONFINITE;
+                    p.done = p.stop = true;
+                    p.ib = 0;
+                    continue;
+                }
+                // a zero H(i+1,i) (happy breakdown) is read before the
+                // Givens rotation of least_squares overwrites it
+                const bool happy = (p.H(i + 1, i) == 0.0);
+                least_squares(i, p.H, p.cs, p.sn, p.s);
+                p.ib = i;
+                const double est = std::fabs(p.s[i + 1]);
+                if (b < count) push_hist(&stats[b], est);
+                if (happy || p.total >= K.gmres_max_iter)
+                    p.stop = true;
+                else if (p.total >= K.gmres_min_iter && (est <= K.gmres_rel_tol * p.norm_b || est <= K.gmres_abs_tol))
+                    p.stop = true;
+                else
+                    cont = true;
+            }
+            if (!cont) break;
+        }
+        // x += sum_k y_k Z_k per instance (update_sol)
+        int J = 0;
+        for (auto& p : P) {
+            if (p.done || p.ib == 0) continue;
+            solve_utri(p.ib - 1, p.H, p.s, p.y);
+            J = std::max(J, p.ib);
+        }
+        if (J > 0) {
+            for (int k = 0; k < J; ++k)
+                for (int b = 0; b < B; ++b) {
+                    const Inst& p = P[b];
+                    h->ys_host[(int64_t)k * B + b] = (!p.done && k < p.ib) ? p.y[k + 1] : 0.0;
+                }
+            LMM_CK(cudaMemcpyAsync(h->ys, h->ys_host, sizeof(double) * J * B, cudaMemcpyHostToDevice, h->stream));
+            if (fp32)
+                launch_add_scaled_multi_batch<float>(h->x.base, reinterpret_cast<const float* const*>(h->ztab), h->ys, J, B, n, ni,
+                                                     len, h->stream);
+            else
+                launch_add_scaled_multi_batch<double>(h->x.base, reinterpret_cast<const double* const*>(h->ztab), h->ys, J, B, n,
+                                                      ni, len, h->stream);
+            check_launch();
+        }
+    }
+    // per instance as one solve reports them: V-cycles of its own columns
+    const int64_t v_per = apps > 0 ? h->vcycles / apps : 0, p_per = apps > 0 ? h->pvcycles / apps : 0;
+    int worst = LMM_OK;
+    for (int b = 0; b < count; ++b) {
+        const Inst& p = P[b];
+        lmm_stats& st = stats[b];
+        st.total_iter = p.total;
+        st.outer_iter = p.outer;
+        st.vcycles = (int)(v_per * p.total);
+        st.pressure_vcycles = (int)(p_per * p.total);
+        st.norm_resid_true = p.norm_r;
+        st.norm_init_true = p.norm_init;
+        st.norm_resid = p.norm_r;
+        status[b] = p.status;
+        if (p.status < 0)
+            worst = std::min(worst, p.status);
+        else if (worst >= 0)
+            worst = std::max(worst, p.status);
+    }
+    return worst;
+}
+
 int validate(const lmm_grid* g, const lmm_knobs* k) {
     if (!g || !k) return LMM_ERR_INVALID;
     if (g->dm != 2 && g->dm != 3) return LMM_ERR_INVALID;
@@ -1489,7 +1746,8 @@ void lmm_default_knobs(lmm_knobs* k) {
     k->learned_stage = 0;
 }
 
-int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_handle** out) {
+// one problem (batch 1, batched false) or a batch handle of `batch` 2D instances
+static int create_impl(const lmm_grid* g, const lmm_knobs* k, int device, int batch, bool batched, lmm_handle** out) {
     if (!out) return LMM_ERR_INVALID;
     *out = nullptr;
     g_last_error.clear();
@@ -1510,7 +1768,9 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         h->D0.dm = g->dm;
         h->D0.nx = g->n[0];
         h->D0.ny = g->n[1];
-        h->D0.nz = (g->dm == 3) ? g->n[2] : 1;
+        h->batch = batch;
+        h->batched = batched;
+        h->D0.nz = (g->dm == 3) ? g->n[2] : batch;
         set_walls(h->D0, *g);
         h->n = (int64_t)h->D0.nx * h->D0.ny * h->D0.nz;
         h->nlev = compute_nlevs(g->n, g->dm, k->stag_mg_minwidth);
@@ -1523,9 +1783,12 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         LMM_CK(cudaEventCreate(&h->ev1));
         if (k->host_wait == 1) LMM_CK(cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming));
         LMM_CK(cudaEventCreateWithFlags(&h->col_ev, cudaEventDisableTiming | (k->host_wait == 1 ? cudaEventBlockingSync : 0)));
-        h->arena_bytes = plan_bytes(*g, *k, h->nlev, h->nlev_p);
+        h->arena_bytes = plan_bytes(*g, *k, h->nlev, h->nlev_p, batch, batched);
         LMM_CK(cudaMalloc(&h->arena, h->arena_bytes));
-        LMM_CK(cudaMemset(h->arena, 0, h->arena_bytes));
+        // zeroed on the handle's own (non-blocking) stream: a cudaMemset on
+        // the legacy stream may still run when later copies on h->stream
+        // (the batch pointer tables) have landed, and would wipe them
+        LMM_CK(cudaMemsetAsync(h->arena, 0, h->arena_bytes, h->stream));
         build_levels<double>(h);
         if (k->precision == LMM_PRECISION_FP32) {
             build_levels<float>(h);
@@ -1567,15 +1830,30 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
         for (int d = 0; d < dm; ++d) h->butmp32[d] = h->alloc<float>(h->n);
         h->pin32 = h->alloc<float>((int64_t)(dm + 1) * h->n);
         h->pout32 = h->alloc<float>((int64_t)(dm + 1) * h->n);
-        h->red_blocks = reduce_blocks(h->n);
-        h->partials = h->alloc<double>(4096 * 8);
-        h->counter = h->alloc<unsigned>(64);
+        // a batch reduces each instance with one problem's block count
+        h->red_blocks = reduce_blocks(batched ? (int64_t)g->n[0] * g->n[1] : h->n);
+        h->partials = h->alloc<double>(partials_count(*g, batch));
+        h->counter = h->alloc<unsigned>(std::max(64, batch));
         h->scal = h->alloc<double>(8 * lmm_handle::kSlots);
         int64_t st = 1;
         for (int d = 0; d < dm; ++d) st *= (g->n[d] + 1 + 8);
         h->stage_elems = st;
         h->stage = h->alloc<double>(st);
         LMM_CK(cudaMallocHost(&h->hscal, 8 * sizeof(double) * lmm_handle::kSlots));
+        if (batched) {
+            h->bslots = h->alloc<double>((int64_t)lmm_handle::kBSlots * batch * 8);
+            h->ys = h->alloc<double>((int64_t)(h->m + 1) * batch);
+            h->ztab = h->alloc<void*>(h->m + 1);
+            h->gtab = h->alloc<const double*>((int64_t)lmm_handle::kGatherFields * batch);
+            LMM_CK(cudaMallocHost(&h->bhost, sizeof(double) * lmm_handle::kBSlots * batch * 8));
+            LMM_CK(cudaMallocHost(&h->ys_host, sizeof(double) * (h->m + 1) * batch));
+            LMM_CK(cudaMallocHost(&h->gtab_host, sizeof(const double*) * lmm_handle::kGatherFields * batch));
+            // the Z basis table never changes
+            std::vector<void*> zt(h->m + 1, nullptr);
+            for (int q = 0; q < h->m; ++q)
+                zt[q] = (k->precision == LMM_PRECISION_FP32) ? (void*)h->Z32[q] : (void*)h->Z64[q].base;
+            LMM_CK(cudaMemcpyAsync(h->ztab, zt.data(), sizeof(void*) * (h->m + 1), cudaMemcpyHostToDevice, h->stream));
+        }
         LMM_CK(host_wait(h));
     } catch (const LmmError& e) {
         lmm_stokes_destroy(h);
@@ -1583,6 +1861,35 @@ int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_han
     }
     *out = h;
     return LMM_OK;
+}
+
+int lmm_stokes_create(const lmm_grid* g, const lmm_knobs* k, int device, lmm_handle** out) {
+    return create_impl(g, k, device, 1, false, out);
+}
+
+int lmm_stokes_create_batch(const lmm_grid* g, const lmm_knobs* k, int batch, int device, lmm_handle** out) {
+    if (!out) return LMM_ERR_INVALID;
+    *out = nullptr;
+    g_last_error.clear();
+    if (!g || !k || batch < 1 || batch > 4096) return LMM_ERR_INVALID;
+    if (g->dm != 2 || k->method != LMM_METHOD_FGMRES || k->visc_type >= 0 || k->learned_stage != 0 || k->visc_schur_approx != 0 ||
+        k->stag_mg_max_vcycles > 1 || k->scale_factor != 1.0 || k->gmres_max_inner > lmm_handle::kBSlots - 3 ||
+        k->orthogonalization != 0) {
+        g_last_error =
+            "batches: 2D, FGMRES with modified Gram-Schmidt, visc_type < 0, one V-cycle per application, scale_factor 1, "
+            "gmres_max_inner <= 45, no BFBt or learned stage";
+        return LMM_ERR_INVALID;
+    }
+    for (int d = 0; d < 2; ++d)
+        if (g->bc_lo[d] != LMM_BC_PERIODIC || g->bc_hi[d] != LMM_BC_PERIODIC) {
+            g_last_error = "batches: periodic grids";
+            return LMM_ERR_INVALID;
+        }
+    if ((int64_t)g->n[0] * g->n[1] * batch > (int64_t)INT32_MAX / 4) {
+        g_last_error = "batches: at most 2^29 cells per batch";
+        return LMM_ERR_INVALID;
+    }
+    return create_impl(g, k, device, batch, true, out);
 }
 
 int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
@@ -1629,6 +1936,9 @@ int lmm_stokes_destroy(lmm_handle* h) {
     if (h->arena) cudaFree(h->arena);
     if (h->lrn_block) cudaFree(h->lrn_block);
     if (h->hscal) cudaFreeHost(h->hscal);
+    if (h->bhost) cudaFreeHost(h->bhost);
+    if (h->ys_host) cudaFreeHost(h->ys_host);
+    if (h->gtab_host) cudaFreeHost(h->gtab_host);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->wait_ev) cudaEventDestroy(h->wait_ev);
@@ -1718,7 +2028,7 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
 
 extern "C" int lmm_stokes_solve_device(lmm_handle* h, const lmm_fields_in* in, lmm_fields_out* out, double* theta_alpha,
                                        double* norm_pre_rhs, lmm_stats* st) {
-    if (!h || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
+    if (!h || h->batched || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
     if (in->layout != LMM_LAYOUT_COMPACT || out->layout != LMM_LAYOUT_COMPACT) return LMM_ERR_INVALID;
     g_last_error.clear();
     try {
@@ -1747,7 +2057,7 @@ extern "C" int lmm_stokes_solve_device(lmm_handle* h, const lmm_fields_in* in, l
 
 extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fields_out* out, double* theta_alpha,
                                 double* norm_pre_rhs, lmm_stats* st) {
-    if (!h || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
+    if (!h || h->batched || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
     g_last_error.clear();
     const int dm = h->dm;
     const int64_t n = h->n;
@@ -1848,6 +2158,106 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
     }
 }
 
+// ------------------------------------------------------------ batches of 2D problems
+extern "C" int lmm_stokes_solve_batch(lmm_handle* h, lmm_ensemble_item* items, int count) {
+    if (!h || !h->batched || !items || count < 1 || count > h->batch) return LMM_ERR_INVALID;
+    g_last_error.clear();
+    const int B = h->batch, ni = h->D0.nx * h->D0.ny;
+    const double theta = items[0].theta_alpha;
+    const bool has_gamma = items[0].gamma != nullptr;
+    for (int q = 0; q < count; ++q) {
+        const lmm_ensemble_item& it = items[q];
+        if (it.n[0] != h->grid.n[0] || it.n[1] != h->grid.n[1] || it.dx != h->grid.dx || it.theta_alpha != theta) {
+            g_last_error = "a batch holds problems of one grid, spacing and theta_alpha";
+            return LMM_ERR_INVALID;
+        }
+        if (!it.b_u[0] || !it.b_u[1] || !it.b_p || !it.alpha_fc[0] || !it.alpha_fc[1] || !it.beta || !it.beta_ed[0] ||
+            !it.x_u[0] || !it.x_u[1] || !it.x_p || (it.gamma != nullptr) != has_gamma) {
+            g_last_error = "a batch item lacks an array (gamma: all or none)";
+            return LMM_ERR_INVALID;
+        }
+    }
+    try {
+        LMM_CK(cudaSetDevice(h->device));
+        g_debug_stream = h->stream;
+        g_debug_dims[0] = h->D0.nx;
+        g_debug_dims[1] = h->D0.ny;
+        g_debug_dims[2] = h->D0.nz;
+        LevelDev<double>& L0 = h->L64[0];
+        std::vector<lmm_stats> st(count);
+        std::vector<int> status(count, LMM_OK);
+        for (auto& x : st) std::memset(&x, 0, sizeof(x));
+        LMM_CK(cudaEventRecord(h->ev0, h->stream));
+        // gather: table entry f*B + b is field f of instance b; instances
+        // past count are zero problems (rhs and initial guess zeroed below)
+        // on the first instance's coefficients
+        double* dst[lmm_handle::kGatherFields] = {h->b.c(0), h->b.c(1), h->b.p(),   h->alpha_fc[0], h->alpha_fc[1], L0.beta,
+                                                  L0.bed[0], L0.gamma,  h->x.c(0), h->x.c(1),      h->x.p()};
+        auto field = [&](const lmm_ensemble_item& it, int f) -> const double* {
+            switch (f) {
+            case 0: return it.b_u[0];
+            case 1: return it.b_u[1];
+            case 2: return it.b_p;
+            case 3: return it.alpha_fc[0];
+            case 4: return it.alpha_fc[1];
+            case 5: return it.beta;
+            case 6: return it.beta_ed[0];
+            case 7: return it.gamma;
+            case 8: return it.x_u[0];
+            case 9: return it.x_u[1];
+            default: return it.x_p;
+            }
+        };
+        // the pinned table may still be read by the previous call's copy
+        LMM_CK(host_wait(h));
+        for (int f = 0; f < lmm_handle::kGatherFields; ++f)
+            for (int b = 0; b < B; ++b) h->gtab_host[(int64_t)f * B + b] = field(items[b < count ? b : 0], f);
+        LMM_CK(cudaMemcpyAsync(h->gtab, h->gtab_host, sizeof(const double*) * lmm_handle::kGatherFields * B, cudaMemcpyHostToDevice,
+                               h->stream));
+        for (int f = 0; f < lmm_handle::kGatherFields; ++f) {
+            if (f == 7 && !has_gamma) {
+                LMM_CK(cudaMemsetAsync(L0.gamma, 0, sizeof(double) * h->n, h->stream));
+                continue;
+            }
+            launch_gather_ptrs(h->gtab + (int64_t)f * B, dst[f], ni, B, h->stream);
+            check_launch();
+        }
+        if (count < B) {
+            const size_t rest = sizeof(double) * (size_t)(B - count) * ni;
+            for (int c = 0; c < 3; ++c) {
+                LMM_CK(cudaMemsetAsync(h->b.c(c) + (int64_t)count * ni, 0, rest, h->stream));
+                LMM_CK(cudaMemsetAsync(h->x.c(c) + (int64_t)count * ni, 0, rest, h->stream));
+            }
+        }
+        const double* al[3] = {h->alpha_fc[0], h->alpha_fc[1], nullptr};
+        const double* bed[3] = {L0.bed[0], nullptr, nullptr};
+        load_coeffs(h, al, L0.beta, bed, L0.gamma, theta);
+        h->pvcycles = 0;
+        const int rc = run_fgmres_batch(h, count, st.data(), status.data());
+        // scatter x_u, x_p to the instances' arrays (table entries (f-8)*B + b)
+        LMM_CK(host_wait(h));
+        for (int f = 8; f < lmm_handle::kGatherFields; ++f)
+            for (int b = 0; b < count; ++b) h->gtab_host[(int64_t)(f - 8) * B + b] = field(items[b], f);
+        LMM_CK(cudaMemcpyAsync(h->gtab, h->gtab_host, sizeof(const double*) * 3 * B, cudaMemcpyHostToDevice, h->stream));
+        for (int f = 8; f < lmm_handle::kGatherFields; ++f) {
+            launch_scatter_ptrs(dst[f], const_cast<double* const*>(h->gtab + (int64_t)(f - 8) * B), ni, count, h->stream);
+            check_launch();
+        }
+        LMM_CK(cudaEventRecord(h->ev1, h->stream));
+        LMM_CK(host_wait(h));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        for (int q = 0; q < count; ++q) {
+            st[q].solve_ms = ms;
+            items[q].stats = st[q];
+            items[q].status = status[q];
+        }
+        return rc;
+    } catch (const LmmError& e) {
+        return e.code;
+    }
+}
+
 // ------------------------------------------------------------ operator-level entry points
 extern "C" int64_t lmm_kernel_launches(void) { return lmm::launches_total(); }
 
@@ -1891,7 +2301,7 @@ extern "C" int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_re
 }
 
 extern "C" int lmm_op_load_coeffs(lmm_handle* h, const lmm_fields_in* c, double theta_alpha) {
-    if (!h || !c) return LMM_ERR_INVALID;
+    if (!h || h->batched || !c) return LMM_ERR_INVALID;
     try {
         const double* al[3] = {c->alpha_fc[0], c->alpha_fc[1], c->alpha_fc[2]};
         const double* bed[3] = {c->beta_ed[0], c->beta_ed[1], c->beta_ed[2]};
@@ -1904,7 +2314,7 @@ extern "C" int lmm_op_load_coeffs(lmm_handle* h, const lmm_fields_in* c, double 
 }
 
 extern "C" int lmm_op_stag_applyop(lmm_handle* h, const double* const phi[3], double* const Lphi[3], int color) {
-    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded) return LMM_ERR_INVALID;
     try {
         if (color < 0 || color > 2 * h->dm) return LMM_ERR_INVALID;
         launch_applyop<double>(h->L64[0], h->knobs.visc_type, phi, Lphi, h->stream, color);
@@ -1918,7 +2328,7 @@ extern "C" int lmm_op_stag_applyop(lmm_handle* h, const double* const phi[3], do
 
 extern "C" int lmm_op_apply_matrix(lmm_handle* h, const double* const x_u[3], const double* x_p, double* const b_u[3],
                                    double* b_p) {
-    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded) return LMM_ERR_INVALID;
     try {
         const int dm = h->dm;
         const int64_t n = h->n;
@@ -1939,7 +2349,7 @@ extern "C" int lmm_op_apply_matrix(lmm_handle* h, const double* const x_u[3], co
 
 extern "C" int lmm_op_apply_precon(lmm_handle* h, const double* const b_u[3], const double* b_p, double* const x_u[3],
                                    double* x_p) {
-    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded) return LMM_ERR_INVALID;
     try {
         const int dm = h->dm;
         const int64_t n = h->n;
@@ -1964,7 +2374,7 @@ extern "C" int lmm_op_apply_precon(lmm_handle* h, const double* const b_u[3], co
 }
 
 extern "C" int lmm_op_stag_mg_solver(lmm_handle* h, const double* const rhs[3], double* const phi[3]) {
-    if (!h || !h->coeffs_loaded) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded) return LMM_ERR_INVALID;
     try {
         LevelDev<double>& L0 = h->L64[0];
         for (int d = 0; d < h->dm; ++d) {
@@ -1982,7 +2392,7 @@ extern "C" int lmm_op_stag_mg_solver(lmm_handle* h, const double* const rhs[3], 
 }
 
 extern "C" int lmm_op_smooth(lmm_handle* h, int lev, const double* const rhs[3], double* const phi[3], int color) {
-    if (!h || !h->coeffs_loaded || lev < 0 || lev >= h->nlev) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded || lev < 0 || lev >= h->nlev) return LMM_ERR_INVALID;
     try {
         LevelDev<double>& L = h->L64[lev];
         for (int d = 0; d < h->dm; ++d) {
@@ -2009,7 +2419,7 @@ extern "C" int lmm_op_smooth(lmm_handle* h, int lev, const double* const rhs[3],
 
 extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* const rhs[3], const double* const phi[3],
                                         double* const rhs_coarse[3]) {
-    if (!h || !h->coeffs_loaded || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
     try {
         launch_residual_restrict<double>(h->L64[lev], h->L64[lev + 1], h->knobs.visc_type, rhs, phi, rhs_coarse, h->stream);
         check_launch();
@@ -2021,7 +2431,7 @@ extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* co
 }
 
 extern "C" int lmm_op_prolong_add(lmm_handle* h, int lev, const double* const phi_coarse[3], double* const phi_fine[3]) {
-    if (!h || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
+    if (!h || h->batched || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
     try {
         launch_prolong_add<double>(h->L64[lev], h->L64[lev + 1], phi_coarse, phi_fine, h->stream);
         check_launch();
@@ -2034,7 +2444,7 @@ extern "C" int lmm_op_prolong_add(lmm_handle* h, int lev, const double* const ph
 
 extern "C" int lmm_op_inner_prod(lmm_handle* h, const double* const a_u[3], const double* a_p, const double* const b_u[3],
                                  const double* b_p, double* out_host) {
-    if (!h) return LMM_ERR_INVALID;
+    if (!h || h->batched) return LMM_ERR_INVALID;
     try {
         const double* a[4] = {a_u[0], a_u[1], h->dm == 3 ? a_u[2] : nullptr, a_p};
         const double* b[4] = {b_u[0], b_u[1], h->dm == 3 ? b_u[2] : nullptr, b_p};
@@ -2049,7 +2459,7 @@ extern "C" int lmm_op_inner_prod(lmm_handle* h, const double* const a_u[3], cons
 }
 
 extern "C" int lmm_op_sum_umac_press(lmm_handle* h, const double* const u[3], const double* p, double* out_host) {
-    if (!h) return LMM_ERR_INVALID;
+    if (!h || h->batched) return LMM_ERR_INVALID;
     try {
         const double* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
         const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -2095,7 +2505,7 @@ int reduce_blocks(int64_t n) {
 
 // ------------------------------------------------------------ learned stage entry points
 extern "C" int lmm_stokes_set_net(lmm_handle* h, lmm_net* net) {
-    if (!h) return LMM_ERR_INVALID;
+    if (!h || h->batched) return LMM_ERR_INVALID;
     try {
         if (net) {
             int nx, ny, nz, B;
@@ -2139,7 +2549,7 @@ extern "C" int lmm_stokes_set_net(lmm_handle* h, lmm_net* net) {
 // preconditioner), e1 = e0 - z1, r1 = A e1; pair q gets the network input
 // rows of r1 and the target rows of e1.
 extern "C" int lmm_learned_make_pairs(lmm_handle* h, unsigned long long seed, int count, void* x_out, float* t_out) {
-    if (!h || !h->coeffs_loaded || !h->lrn_block || count < 1 || !x_out || !t_out) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->coeffs_loaded || !h->lrn_block || count < 1 || !x_out || !t_out) return LMM_ERR_INVALID;
     try {
         const int64_t len = (int64_t)(h->dm + 1) * h->n;
         const int S1 = lmm_handle::kLrnSlot, S3 = S1 + 2;
@@ -2180,7 +2590,7 @@ extern "C" int lmm_learned_make_pairs(lmm_handle* h, unsigned long long seed, in
 // (what the preconditioner alone leaves), ratios[1] = |r1 - A c| / |r1|
 // (what the network's correction leaves of that).
 extern "C" int lmm_learned_eval(lmm_handle* h, unsigned long long seed, double* ratios) {
-    if (!h || !h->net || !h->coeffs_loaded || !ratios) return LMM_ERR_INVALID;
+    if (!h || h->batched || !h->net || !h->coeffs_loaded || !ratios) return LMM_ERR_INVALID;
     try {
         const int64_t len = (int64_t)(h->dm + 1) * h->n;
         const int S1 = lmm_handle::kLrnSlot, S2 = S1 + 1, S3 = S1 + 2;

@@ -30,7 +30,11 @@ namespace lmm {
 // neighbour offsets (with periodic wrap) of one index; 32-bit indices
 // (a field holds at most 2^31 - 1 entries)
 struct Dims {
-    int nx, ny, nz;  // nz == 1 in 2D
+    // 2D: nz is the number of independent instances stacked along the third
+    // index (1 for one grid; a batch of B problems of one grid has nz = B).
+    // The third index of a 2D array is then the instance: never wrapped,
+    // coarsened or part of a colour.
+    int nx, ny, nz;
     int dm;
     // bit d of wall: direction d is bounded by walls (else periodic); bit d
     // of slip_lo / slip_hi: that wall is a slip wall (else no-slip).  Plain
@@ -122,7 +126,7 @@ __host__ __device__ __forceinline__ int edge_ext(const Dims& D, int e, int d) {
     return n + ((d < D.dm && ((D.wall >> d) & 1) && edge_nodal(D.dm, e, d)) ? 1 : 0);
 }
 __host__ __device__ __forceinline__ int64_t edge_count(const Dims& D, int e) {
-    return (int64_t)edge_ext(D, e, 0) * edge_ext(D, e, 1) * (D.dm == 3 ? edge_ext(D, e, 2) : 1);
+    return (int64_t)edge_ext(D, e, 0) * edge_ext(D, e, 1) * (D.dm == 3 ? edge_ext(D, e, 2) : D.nz);
 }
 // index of edge e at the face position of n, moved +1 along direction t
 // (t < 0: no move); a periodic direction wraps
@@ -134,7 +138,14 @@ __device__ __forceinline__ int edge_at(const Nb& n, int e, int t) {
         if (x[t] == nn[t] && !((n.D.wall >> t) & 1)) x[t] = 0;
     }
     const int ex = edge_ext(n.D, e, 0), ey = edge_ext(n.D, e, 1);
-    return x[0] + ex * (x[1] + ey * (n.D.dm == 3 ? x[2] : 0));
+    return x[0] + ex * (x[1] + ey * x[2]);
+}
+
+// the third index's share of a colour: (i + j + k) % 2 in 3D, (i + j) % 2
+// in 2D (k is the instance)
+template <int DM>
+__host__ __device__ __forceinline__ int ck(int k) {
+    return DM == 3 ? k : 0;
 }
 
 template <class T>

@@ -141,6 +141,10 @@ def main():
     ap.add_argument("--rel-tol", type=float, default=1e-8)
     ap.add_argument("--repeats", type=int, default=3)
     ap.add_argument("--host-wait", type=int, default=0, help="0: worker threads spin on their streams (1: block)")
+    ap.add_argument("--mode", choices=("batch", "pool"), default="batch",
+                    help="batch: one batch handle per grid size; pool: worker threads with one-problem handles")
+    ap.add_argument("--orthogonalization", type=int, default=0, help="pool mode: 0 modified, 1 classical Gram-Schmidt")
+    ap.add_argument("--knob", action="append", default=[], metavar="NAME=VALUE", help="any other lmm_knobs field")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -159,8 +163,13 @@ def main():
     mine = shard([n * n for n in sizes], world)[rank]
     allp = make_instances(a.count)
     probs = [allp[i] for i in mine]
+    pool = a.mode == "pool"
     kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
-                        orthogonalization=1, gmres_rel_tol=a.rel_tol, host_wait=a.host_wait)
+                        orthogonalization=a.orthogonalization if pool else 0, gmres_rel_tol=a.rel_tol, host_wait=a.host_wait,
+                        ensemble_batch=-1 if pool else 0)
+    for kv in a.knob:
+        name, val = kv.split("=", 1)
+        setattr(kn, name, type(getattr(kn, name))(float(val)))
     from . import _native
     lib = _native.load()
     import time
@@ -172,6 +181,9 @@ def main():
         if dist is not None:
             dist.barrier()
         st, stats, _, secs = ens.run(probs)
+        bad = sorted({p.n[0] for c, p in zip(st, probs) if c < 0})
+        if bad:
+            raise RuntimeError(f"instances of sizes {bad} failed: " + lib.lmm_strerror(min(st)).decode())
         best = secs if best is None else min(best, secs)
     ens.close()
     ok = [s for s, c in zip(stats, st) if c >= 0]
@@ -179,7 +191,8 @@ def main():
     for c, p in zip(st, probs):
         if c < 0:
             errors.setdefault(lib.lmm_strerror(c).decode(), []).append(p.n[0])
-    out = dict(rank=rank, workers=a.workers, instances=len(probs), seconds=best, instances_per_s=len(probs) / best,
+    out = dict(rank=rank, mode=a.mode, workers=a.workers if pool else None, instances=len(probs), seconds=best,
+               instances_per_s=len(probs) / best,
                pool_creation_seconds=create_s,
                failed=int(sum(1 for c in st if c < 0)), unconverged=int(sum(1 for c in st if c > 0)), errors=errors,
                iterations_mean=float(np.mean([s["total_iter"] for s in ok])) if ok else None,

@@ -48,7 +48,7 @@ module lmm_stokes_iface
      integer(c_int) :: method, precision, learned_stage
      integer(c_int) :: tail_cells, tail_smem_kb, use_graphs, smoother_fusion, l2_persist
      integer(c_int) :: orthogonalization, host_wait
-     integer(c_int) :: reserved(1)
+     integer(c_int) :: ensemble_batch
   end type lmm_knobs
 
   type, bind(c) :: lmm_fields_in

@@ -1,30 +1,140 @@
-"""lmm_ensemble_solve: independent problems of uneven sizes solved
-concurrently give the same bits as one solve per instance, and every
-instance meets its tolerance."""
+"""lmm_ensemble_solve and batches of 2D problems (lmm_stokes_solve_batch):
+independent problems of uneven sizes give the same bits, iteration counts
+and residual histories as one lmm_stokes_solve_device call per instance,
+and every instance meets its tolerance -- whether the ensemble runs them in
+batches (one launch per operation for all problems of a grid) or through
+the worker pool of one-problem handles."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def test_ensemble_equals_individual_solves():
+def _dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def _single(p, kn):
+    """one problem on a one-problem handle: (x_u, x_p, stats)"""
     import torch
 
-    from lowmachmixtures_b200 import abi, ensemble
     from lowmachmixtures_b200.gmres import StokesSolver
-    probs = ensemble.make_instances(10, seed=5, sizes=(32, 48, 64, 96))
-    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
-                        gmres_rel_tol=1e-8)
-    st, stats, sols, _ = ensemble.solve(probs, kn, workers=4)
-    assert all(s == 0 for s in st)
-    for p, s in zip(probs, stats):
-        assert s["norm_resid_true"] <= 1e-8 * s["norm_b"]
-    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
-    for p, (xu, xp) in zip(probs, sols):
-        with StokesSolver(2, p.n[:2], p.dx, knobs=kn) as s:
-            yu, yp = [torch.zeros_like(xp) for _ in range(2)], torch.zeros_like(xp)
-            s.solve_device([dev(a) for a in p.b_u], dev(p.b_p), yu, yp, [dev(a) for a in p.alpha_fc], dev(p.beta),
-                           [dev(a) for a in p.beta_ed], dev(p.gamma), p.theta_alpha)
+    with StokesSolver(2, p.n[:2], p.dx, knobs=kn) as s:
+        yp = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+        yu = [torch.zeros_like(yp) for _ in range(2)]
+        _, _, st = s.solve_device([_dev(a) for a in p.b_u], _dev(p.b_p), yu, yp, [_dev(a) for a in p.alpha_fc], _dev(p.beta),
+                                  [_dev(a) for a in p.beta_ed], _dev(p.gamma), p.theta_alpha)
+    return yu, yp, st
+
+
+def _assert_same_as_single(probs, sols, stats, kn):
+    import torch
+    for p, (xu, xp), s in zip(probs, sols, stats):
+        yu, yp, st1 = _single(p, kn)
         for c in range(2):
             assert torch.equal(xu[c], yu[c])
         assert torch.equal(xp, yp)
+        assert s["total_iter"] == st1["total_iter"]
+        assert s["history"] == st1["history"]
+
+
+@pytest.mark.parametrize("precision,theta", [(abi_p, th) for abi_p in (1, 0) for th in (0.0, 25.0)])
+def test_batched_ensemble_equals_individual_solves(precision, theta):
+    from lowmachmixtures_b200 import abi, ensemble
+    probs = ensemble.make_instances(12, seed=5, sizes=(32, 48, 64, 96), theta_alpha=theta)
+    kn = abi.make_knobs(precon_type=2 if theta == 0.0 else 1, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=precision,
+                        gmres_rel_tol=1e-8)
+    st, stats, sols, _ = ensemble.solve(probs, kn, workers=4)
+    assert all(s == 0 for s in st)
+    for s in stats:
+        assert s["norm_resid_true"] <= 1e-8 * s["norm_b"]
+    _assert_same_as_single(probs, sols, stats, kn)
+
+
+def test_worker_pool_equals_individual_solves():
+    from lowmachmixtures_b200 import abi, ensemble
+    probs = ensemble.make_instances(8, seed=7, sizes=(32, 48, 64))
+    for kn in (abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_GMRES, gmres_rel_tol=1e-8),
+               abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                              gmres_rel_tol=1e-8, ensemble_batch=-1)):
+        st, stats, sols, _ = ensemble.solve(probs, kn, workers=3)
+        assert all(s == 0 for s in st)
+        _assert_same_as_single(probs, sols, stats, kn)
+
+
+def test_batch_handle_padding_repeats_and_zero_rhs():
+    """fewer problems than the handle holds, twice on one handle, one problem
+    with a zero right-hand side (x = 0 at once)"""
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    lib = _native.load()
+    probs = [synth.make_problem(2, 64, 10.0 ** (1 + i / 3), 300 + i) for i in range(5)]
+    probs[2].b_u = [np.zeros_like(a) for a in probs[2].b_u]
+    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                        gmres_rel_tol=1e-9)
+    h = C.c_void_p()
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (64, 64), 1 / 64)), C.byref(kn), 8, 0, C.byref(h)) == 0
+    try:
+        for _ in range(2):
+            items, keep, sols = ensemble._items(probs, 0)
+            assert lib.lmm_stokes_solve_batch(h, items, len(probs)) == 0
+            assert all(it.status == 0 for it in items)
+            assert all(float(x.abs().max()) == 0.0 for x in sols[2][0])
+            assert items[2].stats.total_iter == 0
+            live = [i for i in range(len(probs)) if i != 2]
+            _assert_same_as_single([probs[i] for i in live], [sols[i] for i in live],
+                                   [items[i].stats.as_dict() for i in live], kn)
+    finally:
+        lib.lmm_stokes_destroy(h)
+
+
+def test_batch_handle_rejects_what_it_does_not_cover():
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    lib = _native.load()
+    ok = dict(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES)
+    g2 = abi.make_grid(2, (32, 32), 1 / 32)
+    h = C.c_void_p()
+    for g, kn in ((abi.make_grid(3, (16, 16, 16), 1 / 16), abi.make_knobs(**ok)),
+                  (g2, abi.make_knobs(**dict(ok, visc_type=2))),
+                  (g2, abi.make_knobs(**dict(ok, method=abi.LMM_METHOD_GMRES))),
+                  (g2, abi.make_knobs(**dict(ok, stag_mg_max_vcycles=2))),
+                  (abi.make_grid(2, (32, 32), 1 / 32, bc=(abi.LMM_BC_PERIODIC, abi.LMM_BC_NO_SLIP_WALL)), abi.make_knobs(**ok))):
+        assert lib.lmm_stokes_create_batch(C.byref(g), C.byref(kn), 4, 0, C.byref(h)) == abi.LMM_ERR_INVALID
+    assert lib.lmm_stokes_create_batch(C.byref(g2), C.byref(abi.make_knobs(**ok)), 2, 0, C.byref(h)) == 0
+    try:
+        p = synth.make_problem(2, 32, 10.0, 1)
+        q = synth.make_problem(2, 64, 10.0, 2)
+        items, keep, sols = ensemble._items([p, p, p], 0)
+        assert lib.lmm_stokes_solve_batch(h, items, 3) == abi.LMM_ERR_INVALID   # more than the handle holds
+        items, keep, sols = ensemble._items([p, q], 0)
+        assert lib.lmm_stokes_solve_batch(h, items, 2) == abi.LMM_ERR_INVALID   # another grid
+        # a one-problem entry point refuses the batch handle
+        fin, fout = abi.FieldsIn(), abi.FieldsOut()
+        th, npr, st = C.c_double(0.0), C.c_double(0.0), abi.Stats()
+        assert lib.lmm_stokes_solve_device(h, C.byref(fin), C.byref(fout), C.byref(th), C.byref(npr),
+                                           C.byref(st)) == abi.LMM_ERR_INVALID
+    finally:
+        lib.lmm_stokes_destroy(h)
+
+
+def test_large_batch_handle():
+    """64 instances of 128^2 (an arena of about a gigabyte): the handle's
+    buffers are zeroed in stream order before its pointer tables are written"""
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    lib = _native.load()
+    probs = [synth.make_problem(2, 128, 10.0 ** (1 + (i % 7) / 3), 900 + i) for i in range(64)]
+    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                        gmres_rel_tol=1e-8)
+    h = C.c_void_p()
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (128, 128), 1 / 128)), C.byref(kn), 64, 0, C.byref(h)) == 0
+    try:
+        items, keep, sols = ensemble._items(probs, 0)
+        assert lib.lmm_stokes_solve_batch(h, items, 64) == 0
+        assert all(it.status == 0 for it in items)
+        assert all(it.stats.norm_resid_true <= 1e-8 * it.stats.norm_b for it in items)
+        pick = [0, 31, 63]
+        _assert_same_as_single([probs[i] for i in pick], [sols[i] for i in pick], [items[i].stats.as_dict() for i in pick], kn)
+    finally:
+        lib.lmm_stokes_destroy(h)
