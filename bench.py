@@ -63,24 +63,42 @@ def parse():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """nvidia-smi samples every 50 ms.  Entering starts the sampler and waits
+    for its first row (nvidia-smi takes longer to start than a short timed
+    region lasts), so the rows taken between enter and exit are the timed
+    region's; when the region is shorter than one period, the first row
+    after it stands in (window "adjacent")."""
+
+    PERIOD_MS = 50
+
     def __init__(self, device_index: int):
         self.dev = device_index
         self.rows = []
-        self._stop = threading.Event()
         self._proc = None
+        self._lo = self._hi = 0
+        self.window = "during"
 
-    def __enter__(self):
+    def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self._proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
+                 str(self.PERIOD_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except (OSError, FileNotFoundError):
             self._proc = None
+            return
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 5.0 and self._proc.poll() is None:
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self._proc is None:
+            self.start()
+        self._lo = len(self.rows)
         return self
 
     def _read(self):
@@ -88,26 +106,35 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def __exit__(self, *exc):
-        if self._proc is not None:
-            self._proc.terminate()
-            try:
-                self._proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self._proc.kill()
+        self._hi = len(self.rows)
+        if self._proc is None:
+            return
+        if self._hi == self._lo:
+            self.window = "adjacent"
+            t0 = time.time()
+            while len(self.rows) == self._lo and time.time() - t0 < 1.0 and self._proc.poll() is None:
+                time.sleep(0.005)
+            self._hi = len(self.rows)
+        self._proc.terminate()
+        try:
+            self._proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self._proc.kill()
 
     def summary(self):
-        if not self.rows:
+        rows = self.rows[self._lo:self._hi]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
-        mx = max((float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()), default=None)
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in rows:
             for i, nm in enumerate(names):
                 if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(self.rows)}
+                "samples": len(rows), "window": self.window, "period_ms": self.PERIOD_MS}
 
 
 # ------------------------------------------------------------------ distributed plumbing
