@@ -1,5 +1,7 @@
 // krylov.cu - FP64 Krylov-side kernels (see krylov.cuh).  Built with
 // -fmad=false so every operation rounds like the reference Fortran.
+#include <algorithm>
+
 #include "krylov.cuh"
 #include "pdl.cuh"
 #include "stencil.cuh"
@@ -623,10 +625,14 @@ __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __r
 
 }  // namespace
 
+namespace {
+template <int DM, int J, bool NORM>
+int cgs_blocks(int64_t n);
+}
 void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
                        unsigned* counter, double* out, cudaStream_t s) {
-    const int nb = mdot_blocks((int64_t)D.nx * D.ny * D.nz);
-#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, nb, kMdotThreads, 0, s, D, w, V, hs, wseam, pw, partials, counter, out)
+    const int64_t n = (int64_t)D.nx * D.ny * D.nz;
+#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, cgs_blocks<DM_, J_, true>(n), kMdotThreads, 0, s, D, w, V, hs, wseam, pw, partials, counter, out)
 #define MNJ(DM_)                               \
     switch (J) {                               \
     case 1: MN(DM_, 1); break;                 \
@@ -649,10 +655,31 @@ int mdot_blocks(int64_t n) {
     return (int)(b < 1 ? 1 : b);
 }
 
+namespace {
+// blocks of one Gram-Schmidt pass: mdot_blocks(n), but no more than fit in
+// one wave of this kernel (its resident blocks per SM x SMs): a second,
+// partial wave would leave most SMs idle while it runs
+template <int DM, int J, bool NORM>
+int cgs_blocks(int64_t n) {
+    static const int wave = [] {
+        int dev = 0, sms = 148, per_sm = 4;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const void* k = NORM ? (const void*)k_maxpy_norm<DM, J> : (const void*)k_mdot<DM, J>;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kMdotThreads, 0) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        return per_sm * sms;
+    }();
+    return std::min(mdot_blocks(n), wave);
+}
+}  // namespace
+
 void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
                  double* out, cudaStream_t s) {
-    const int nb = mdot_blocks((int64_t)D.nx * D.ny * D.nz);
-#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, nb, kMdotThreads, 0, s, D, w, V, wseam, pw, partials, counter, out)
+    const int64_t n = (int64_t)D.nx * D.ny * D.nz;
+#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, cgs_blocks<DM_, J_, false>(n), kMdotThreads, 0, s, D, w, V, wseam, pw, partials, counter, out)
 #define MDJ(DM_)                               \
     switch (J) {                               \
     case 1: MD(DM_, 1); break;                 \
