@@ -145,6 +145,8 @@ def main():
                     help="batch: one batch handle per grid size; pool: worker threads with one-problem handles")
     ap.add_argument("--orthogonalization", type=int, default=0, help="pool mode: 0 modified, 1 classical Gram-Schmidt")
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=VALUE", help="any other lmm_knobs field")
+    ap.add_argument("--sizes", default=",".join(str(n) for n in SIZES_2D),
+                    help="comma-separated grid sizes the instances are drawn from")
     a = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -159,9 +161,10 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
-    sizes = instance_sizes(a.count)
+    pool_sizes = tuple(int(v) for v in a.sizes.split(","))
+    sizes = instance_sizes(a.count, sizes=pool_sizes)
     mine = shard([n * n for n in sizes], world)[rank]
-    allp = make_instances(a.count)
+    allp = make_instances(a.count, sizes=pool_sizes)
     probs = [allp[i] for i in mine]
     pool = a.mode == "pool"
     kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
