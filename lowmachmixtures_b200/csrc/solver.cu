@@ -563,11 +563,11 @@ int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool st
     const int cells = h->knobs.tail_cells == 0 ? (stag ? 512 : 4096) : h->knobs.tail_cells;
     if (cells < 0) return nl;
     if (stag && h->D0.wall) return nl;  // the staggered tail kernel is periodic only
-    if (h->batched) return nl;           // the tails solve one instance per launch
     const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
     const bool jacobi = stag && h->knobs.stag_mg_smoother == 0;
+    const int64_t inst = (h->dm == 2) ? h->batch : 1;  // a 2D batch: one tail block per instance
     int lc = nl;
-    while (lc > 0 && nl - (lc - 1) <= 12 && L[lc - 1].n <= cells &&
+    while (lc > 0 && nl - (lc - 1) <= 12 && L[lc - 1].n / inst <= cells &&
            tail_smem_bytes<T>(&L[lc - 1], nl - (lc - 1), stag, jacobi) <= budget)
         --lc;
     return lc;

@@ -10,6 +10,10 @@
 // collapse into one.  Only the first tail level's phi goes back to global
 // memory.  The arithmetic is the same device code as the per-level kernels,
 // so results are bit-identical.
+//
+// 2D batches (Dims::nz instances stacked along the third index): one block
+// per instance, blockIdx.x = the instance; its views see one instance
+// (nz = 1, every array offset by instance x nx*ny of that level).
 #pragma once
 #include <cstring>
 
@@ -168,6 +172,17 @@ __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega
     }
 }
 
+// this block's offset into a level's arrays: 2D, instance blockIdx.x of
+// the batch; 3D, none
+template <int DM>
+__device__ __forceinline__ int64_t inst_offset(const Dims& D) {
+    return DM == 2 ? (int64_t)blockIdx.x * D.nx * D.ny : 0;
+}
+template <class T>
+__device__ __forceinline__ const T* shift(const T* p, int64_t o) {
+    return p ? p + o : p;
+}
+
 // carve the dynamic shared memory into per-level phi / rhs / (tmp) arrays
 template <class T, int DM>
 __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool stag, bool jacobi) {
@@ -177,9 +192,17 @@ __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool sta
         v.D = A.L[l].D;
         v.dxsqinv = A.L[l].dxsqinv;
         v.C = A.L[l].C;
+        const int64_t io = inst_offset<DM>(v.D);
+        if (DM == 2) v.D.nz = 1;
+        for (int d = 0; d < 3; ++d) {
+            v.C.alpha[d] = shift(v.C.alpha[d], io);
+            v.C.bed[d] = shift(v.C.bed[d], io);
+        }
+        v.C.beta = shift(v.C.beta, io);
+        v.C.gamma = shift(v.C.gamma, io);
         const int n = ncells(v.D);
         for (int d = 0; d < 3; ++d) {
-            v.pa[d] = A.L[l].pa[d];
+            v.pa[d] = shift(A.L[l].pa[d], io);
             v.phi[d] = v.rhs[d] = v.tmp[d] = nullptr;
         }
         v.pphi = v.prhs = v.ptmp = nullptr;
@@ -208,12 +231,13 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_co
     __shared__ TailView<T> V[kMaxTail];
     if (threadIdx.x == 0) tail_views<T, DM>(A, sm, V, true, A.smoother == 0);
     __syncthreads();
+    const int64_t g0 = inst_offset<DM>(A.L[0].D);
     {
         const int n0 = ncells(V[0].D);
         for (int w = threadIdx.x; w < n0; w += blockDim.x)
             for (int d = 0; d < DM; ++d) {
-                V[0].phi[d][w] = A.g_phi[d][w];
-                V[0].rhs[d][w] = A.g_rhs[d][w];
+                V[0].phi[d][w] = A.g_phi[d][g0 + w];
+                V[0].rhs[d][w] = A.g_rhs[d][g0 + w];
             }
         for (int l = 1; l < A.nl; ++l) {
             const int n = ncells(V[l].D);
@@ -252,7 +276,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_co
     }
     const int n0 = ncells(V[0].D);
     for (int w = threadIdx.x; w < n0; w += blockDim.x)
-        for (int d = 0; d < DM; ++d) A.g_phi[d][w] = V[0].phi[d][w];
+        for (int d = 0; d < DM; ++d) A.g_phi[d][g0 + w] = V[0].phi[d][w];
 }
 
 // ------------------------------------------------------------------ pressure
@@ -308,11 +332,12 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_ccmg_tail(const __grid_cons
     __shared__ TailView<T> V[kMaxTail];
     if (threadIdx.x == 0) tail_views<T, DM>(A, sm, V, false, false);
     __syncthreads();
+    const int64_t g0 = inst_offset<DM>(A.L[0].D);
     {
         const int n0 = ncells(V[0].D);
         for (int w = threadIdx.x; w < n0; w += blockDim.x) {
-            V[0].pphi[w] = A.g_pphi[w];
-            V[0].prhs[w] = A.g_prhs[w];
+            V[0].pphi[w] = A.g_pphi[g0 + w];
+            V[0].prhs[w] = A.g_prhs[g0 + w];
         }
         for (int l = 1; l < A.nl; ++l) {
             const int n = ncells(V[l].D);
@@ -353,7 +378,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_ccmg_tail(const __grid_cons
         tail_cc_smooth<T, DM>(F, A.nu2);
     }
     const int n0 = ncells(V[0].D);
-    for (int w = threadIdx.x; w < n0; w += blockDim.x) A.g_pphi[w] = V[0].pphi[w];
+    for (int w = threadIdx.x; w < n0; w += blockDim.x) A.g_pphi[g0 + w] = V[0].pphi[w];
 }
 
 // ------------------------------------------------------------------ launchers
@@ -389,7 +414,8 @@ size_t tail_smem_bytes(const LevelDev<T>* L, int nl, bool stag, bool jacobi) {
     size_t e = 0;
     for (int l = 0; l < nl; ++l) {
         const bool odd = odd_level(L[l].D);
-        e += (size_t)L[l].n * (stag ? (size_t)L[l].D.dm * ((jacobi || odd) ? 3 : 2) : (odd ? 3 : 2));
+        const size_t n = (size_t)L[l].n / (L[l].D.dm == 2 ? L[l].D.nz : 1);  // one instance
+        e += n * (stag ? (size_t)L[l].D.dm * ((jacobi || odd) ? 3 : 2) : (odd ? 3 : 2));
     }
     return e * sizeof(T);
 }
@@ -400,7 +426,9 @@ template <class K, class A>
 static cudaError_t launch_tail(K kernel, const A& args, size_t smem, cudaStream_t s) {
     cudaError_t e = raise_smem_limit((const void*)kernel, smem);
     if (e != cudaSuccess) return e;
-    launch_pdl(kernel, dim3(1), dim3(kTailThreads), smem, s, args);
+    // one block per instance of a 2D batch (nz instances), else one block
+    const int blocks = args.L[0].D.dm == 2 ? args.L[0].D.nz : 1;
+    launch_pdl(kernel, dim3(blocks), dim3(kTailThreads), smem, s, args);
     return cudaGetLastError();
 }
 
