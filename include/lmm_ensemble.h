@@ -65,7 +65,7 @@ int lmm_ensemble_destroy(lmm_ensemble* ens);
  * knobs.  The items' arrays are device arrays in the compact layout; all
  * items share theta_alpha and the gamma / no-gamma choice; solve_ms is the
  * batch's time.  Knobs: LMM_METHOD_FGMRES (FP32 or FP64 preconditioner),
- * orthogonalization 0, visc_type < 0, stag_mg_max_vcycles <= 1,
+ * visc_type < 0, stag_mg_max_vcycles <= 1,
  * scale_factor 1, gmres_max_inner <= 45, no BFBt or learned stage; grids
  * periodic, at most 2^29 cells per batch.  A batch handle is accepted by these two calls,
  * lmm_time_op and lmm_stokes_destroy only.  Returns the most negative

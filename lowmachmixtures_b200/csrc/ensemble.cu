@@ -44,7 +44,7 @@ BatchKey batch_key(const lmm_ensemble_item& it) { return std::make_tuple(it.n[0]
 // the knobs lmm_stokes_create_batch accepts
 bool batchable(int dm, const lmm_knobs& k) {
     return k.ensemble_batch == 0 && dm == 2 && k.method == LMM_METHOD_FGMRES && k.visc_type < 0 && k.learned_stage == 0 &&
-           k.visc_schur_approx == 0 && k.stag_mg_max_vcycles <= 1 && k.scale_factor == 1.0 && k.gmres_max_inner <= 45 && k.orthogonalization == 0;
+           k.visc_schur_approx == 0 && k.stag_mg_max_vcycles <= 1 && k.scale_factor == 1.0 && k.gmres_max_inner <= 45;
 }
 
 }  // namespace

@@ -460,14 +460,29 @@ constexpr int kMdotThreads = 256;
 
 // Stokes inner products <w, V_k>, k < J, in one pass over w: per component
 // the plain sum plus (seam weight - 1) x the seam-plane sum, as k_reduce
-// weighs them; out[k*8 + 4] = sum_d <w_d, V_k,d> + pw^2 <w_p, V_k,p>.
+// weighs them; out[k*ss + 4] = sum_d <w_d, V_k,d> + pw^2 <w_p, V_k,p> (ss:
+// the stride between consecutive slots).
+//
+// 2D batches (D.nz instances): blockIdx.y is the instance, with its own
+// partials, counter and slot entry (+8 per instance); each instance is
+// partitioned and summed as one problem alone.
 template <int DM, int J>
 __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __restrict__ w, MVecs V, double wseam, double pw,
                                                        double* __restrict__ partials, unsigned* __restrict__ counter,
-                                                       double* __restrict__ out) {
+                                                       double* __restrict__ out, int64_t ss) {
     pdl_enter();
     constexpr int NC = DM + 1;
-    const int n = D.nx * D.ny * D.nz;
+    const int n = D.nx * D.ny * (DM == 3 ? D.nz : 1);  // one instance
+    const int64_t N = (int64_t)n * gridDim.y;           // entries per component
+    {
+        const int64_t io = (int64_t)blockIdx.y * n;
+        w += io;
+#pragma unroll
+        for (int k = 0; k < J; ++k) V.p[k] += io;
+        partials += (int64_t)blockIdx.y * gridDim.x * J * NC;
+        counter += blockIdx.y;
+        out += (int64_t)blockIdx.y * 8;
+    }
     double acc[J][NC];
 #pragma unroll
     for (int k = 0; k < J; ++k)
@@ -478,15 +493,16 @@ __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __r
     for (int t = tid; t < n; t += stride) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            const double x = __ldg(w + (int64_t)c * n + t);
+            const double x = __ldg(w + (int64_t)c * N + t);
 #pragma unroll
-            for (int k = 0; k < J; ++k) acc[k][c] += x * __ldg(V.p[k] + (int64_t)c * n + t);
+            for (int k = 0; k < J; ++k) acc[k][c] += x * __ldg(V.p[k] + (int64_t)c * N + t);
         }
     }
     // seam planes of the face components (x: i == 0, y: j == 0, z: k == 0)
 #pragma unroll
     for (int c = 0; c < DM; ++c) {
-        const int m = (c == 0) ? D.ny * D.nz : (c == 1 ? D.nx * D.nz : D.nx * D.ny);
+        const int nzi = (DM == 3) ? D.nz : 1;
+        const int m = (c == 0) ? D.ny * nzi : (c == 1 ? D.nx * nzi : D.nx * D.ny);
         double v[J];
 #pragma unroll
         for (int k = 0; k < J; ++k) v[k] = 0.0;
@@ -495,9 +511,9 @@ __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __r
             if (c == 0) t = D.nx * q;
             else if (c == 1) t = (q % D.nx) + D.nx * D.ny * (q / D.nx);
             else t = q;
-            const double x = __ldg(w + (int64_t)c * n + t);
+            const double x = __ldg(w + (int64_t)c * N + t);
 #pragma unroll
-            for (int k = 0; k < J; ++k) v[k] += x * __ldg(V.p[k] + (int64_t)c * n + t);
+            for (int k = 0; k < J; ++k) v[k] += x * __ldg(V.p[k] + (int64_t)c * N + t);
         }
 #pragma unroll
         for (int k = 0; k < J; ++k) acc[k][c] += (wseam - 1.0) * v[k];
@@ -536,22 +552,21 @@ __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __r
         const int k = threadIdx.x;
         double su = 0.0;
         for (int c = 0; c < DM; ++c) su = su + sh[k * NC + c][0];
-        out[k * 8 + 4] = su + (pw * pw) * sh[k * NC + DM][0];
+        out[k * ss + 4] = su + (pw * pw) * sh[k * NC + DM][0];
     }
     if (threadIdx.x == 0) *counter = 0u;
 }
 
-// w -= sum_k h_k V_k, h_k = hs[k * 8 + 4]
+// w -= sum_k h_k V_k, h_k = hs[k * ss + 4] (a 2D batch: the entry's
+// instance b = (t % N) / ni reads hs[k * ss + 8b + 4]; one problem: N = ni)
 template <int J>
-__global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restrict__ hs, int64_t len) {
+__global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restrict__ hs, int64_t len, int64_t N, int64_t ni, int64_t ss) {
     pdl_enter();
-    double h[J];
-#pragma unroll
-    for (int k = 0; k < J; ++k) h[k] = hs[k * 8 + 4];
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x) {
+        const double* hb = (N >= len) ? hs : hs + ((t % N) / ni) * 8;
         double x = w[t];
 #pragma unroll
-        for (int k = 0; k < J; ++k) x = x - V.p[k][t] * h[k];
+        for (int k = 0; k < J; ++k) x = x - V.p[k][t] * hb[k * ss + 4];
         w[t] = x;
     }
 }
@@ -562,13 +577,24 @@ __global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restric
 template <int DM, int J>
 __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __restrict__ w, MVecs V, const double* __restrict__ hs,
                                                              double wseam, double pw, double* __restrict__ partials,
-                                                             unsigned* __restrict__ counter, double* __restrict__ out) {
+                                                             unsigned* __restrict__ counter, double* __restrict__ out, int64_t ss) {
     pdl_enter();
     constexpr int NC = DM + 1;
-    const int n = D.nx * D.ny * D.nz;
+    const int n = D.nx * D.ny * (DM == 3 ? D.nz : 1);  // one instance (blockIdx.y, as k_mdot)
+    const int64_t N = (int64_t)n * gridDim.y;
+    {
+        const int64_t io = (int64_t)blockIdx.y * n;
+        w += io;
+#pragma unroll
+        for (int k = 0; k < J; ++k) V.p[k] += io;
+        hs += (int64_t)blockIdx.y * 8;
+        partials += (int64_t)blockIdx.y * gridDim.x * NC;
+        counter += blockIdx.y;
+        out += (int64_t)blockIdx.y * 8;
+    }
     double h[J];
 #pragma unroll
-    for (int k = 0; k < J; ++k) h[k] = hs[k * 8 + 4];
+    for (int k = 0; k < J; ++k) h[k] = hs[k * ss + 4];
     double acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] = 0.0;
@@ -577,7 +603,7 @@ __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __r
         const int i = t % D.nx, r = t / D.nx, j = r % D.ny, kk = r / D.ny;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            const int64_t e = (int64_t)c * n + t;
+            const int64_t e = (int64_t)c * N + t;
             double x = w[e];
 #pragma unroll
             for (int k = 0; k < J; ++k) x = x - V.p[k][e] * h[k];
@@ -630,9 +656,9 @@ template <int DM, int J, bool NORM>
 int cgs_blocks(int64_t n);
 }
 void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
-                       unsigned* counter, double* out, cudaStream_t s) {
-    const int64_t n = (int64_t)D.nx * D.ny * D.nz;
-#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, cgs_blocks<DM_, J_, true>(n), kMdotThreads, 0, s, D, w, V, hs, wseam, pw, partials, counter, out)
+                       unsigned* counter, double* out, cudaStream_t s, int ninst, int64_t ss) {
+    const int64_t n = (int64_t)D.nx * D.ny * (D.dm == 3 ? D.nz : 1);
+#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, dim3(cgs_blocks<DM_, J_, true>(n), ninst), dim3(kMdotThreads), 0, s, D, w, V, hs, wseam, pw, partials, counter, out, ss)
 #define MNJ(DM_)                               \
     switch (J) {                               \
     case 1: MN(DM_, 1); break;                 \
@@ -677,9 +703,9 @@ int cgs_blocks(int64_t n) {
 }  // namespace
 
 void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
-                 double* out, cudaStream_t s) {
-    const int64_t n = (int64_t)D.nx * D.ny * D.nz;
-#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, cgs_blocks<DM_, J_, false>(n), kMdotThreads, 0, s, D, w, V, wseam, pw, partials, counter, out)
+                 double* out, cudaStream_t s, int ninst, int64_t ss) {
+    const int64_t n = (int64_t)D.nx * D.ny * (D.dm == 3 ? D.nz : 1);
+#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, dim3(cgs_blocks<DM_, J_, false>(n), ninst), dim3(kMdotThreads), 0, s, D, w, V, wseam, pw, partials, counter, out, ss)
 #define MDJ(DM_)                               \
     switch (J) {                               \
     case 1: MD(DM_, 1); break;                 \
@@ -696,18 +722,19 @@ void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double w
 #undef MD
 }
 
-void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s) {
+void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s, int64_t N, int64_t ni, int64_t ss) {
     int64_t b = (len + kT - 1) / kT;
     const int nb = (int)(b > 8192 ? 8192 : b);
+    if (N <= 0) N = ni = len;  // one problem: every entry reads hs[k * ss + 4]
     switch (J) {
-    case 1: launch_pdl(k_maxpy<1>, nb, kT, 0, s, w, V, hs, len); break;
-    case 2: launch_pdl(k_maxpy<2>, nb, kT, 0, s, w, V, hs, len); break;
-    case 3: launch_pdl(k_maxpy<3>, nb, kT, 0, s, w, V, hs, len); break;
-    case 4: launch_pdl(k_maxpy<4>, nb, kT, 0, s, w, V, hs, len); break;
-    case 5: launch_pdl(k_maxpy<5>, nb, kT, 0, s, w, V, hs, len); break;
-    case 6: launch_pdl(k_maxpy<6>, nb, kT, 0, s, w, V, hs, len); break;
-    case 7: launch_pdl(k_maxpy<7>, nb, kT, 0, s, w, V, hs, len); break;
-    default: launch_pdl(k_maxpy<8>, nb, kT, 0, s, w, V, hs, len); break;
+    case 1: launch_pdl(k_maxpy<1>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    case 2: launch_pdl(k_maxpy<2>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    case 3: launch_pdl(k_maxpy<3>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    case 4: launch_pdl(k_maxpy<4>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    case 5: launch_pdl(k_maxpy<5>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    case 6: launch_pdl(k_maxpy<6>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    case 7: launch_pdl(k_maxpy<7>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
+    default: launch_pdl(k_maxpy<8>, nb, kT, 0, s, w, V, hs, len, N, ni, ss); break;
     }
 }
 

@@ -33,16 +33,21 @@ struct SVec {
 struct MVecs {
     const double* p[8];
 };
-// classical Gram-Schmidt pieces: out[k*8+4] = <w, V_k> (Stokes inner product
-// with the seam weight), then w -= sum_k out[k*8+4] V_k; J <= 8
+// classical Gram-Schmidt pieces: out[k*ss+4] = <w, V_k> (Stokes inner
+// product with the seam weight), then w -= sum_k out[k*ss+4] V_k; J <= 8.
+// ss: stride between consecutive slots (8 for one problem).  A 2D batch
+// (D.nz = ninst instances, slot arrays of ninst x 8): one result per
+// instance at + 8b, ss = 8 * ninst; N = entries per component and ni per
+// instance (k_maxpy; N = 0: one problem)
 int mdot_blocks(int64_t n);
 void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
-                 double* out, cudaStream_t s);
-void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s);
+                 double* out, cudaStream_t s, int ninst = 1, int64_t ss = 8);
+void launch_maxpy(double* w, const MVecs& V, int J, const double* hs, int64_t len, cudaStream_t s, int64_t N = 0, int64_t ni = 0,
+                  int64_t ss = 8);
 // the same update fused with the Stokes norm of the new w (seam weight per
 // entry): out[4] = |u|^2 + pw^2 |p|^2, out[5] = its square root form
 void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
-                       unsigned* counter, double* out, cudaStream_t s);
+                       unsigned* counter, double* out, cudaStream_t s, int ninst = 1, int64_t ss = 8);
 // FP32 Krylov vectors (FGMRES Z basis) and their coefficients, up to 8
 struct MZ32 {
     const float* p[8];

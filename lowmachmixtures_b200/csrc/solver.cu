@@ -235,7 +235,9 @@ int mean_mask(const lmm_handle* h, double theta) {
 int64_t partials_count(const lmm_grid& g, int batch) {
     const int64_t one = 4096 * 8;
     if (g.dm != 2 || batch <= 1) return one;
-    return std::max<int64_t>(one, (int64_t)batch * reduce_blocks((int64_t)g.n[0] * g.n[1]) * 3);
+    const int64_t ni = (int64_t)g.n[0] * g.n[1];
+    // per instance: k_reduce's blocks x 3 components, k_mdot's x 8 vectors x 3
+    return std::max<int64_t>(one, (int64_t)batch * std::max<int64_t>(reduce_blocks(ni) * 3, (int64_t)mdot_blocks(ni) * 8 * 3));
 }
 
 int64_t level_cells(const int n[3], int dm, int lev) {
@@ -1099,13 +1101,19 @@ void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
     arnoldi_column_collect(h, i, col);
 }
 
-void arnoldi_column_cgs_enqueue(lmm_handle* h, int i) {
+// The classical Gram-Schmidt column, launches only: H(k,i) into slots 1..i
+// (entry 4), |w| into slot i+1 (entry 5); on a batch handle one of each per
+// problem (slot arrays, stride batch * 8 between slots).
+void cgs_column(lmm_handle* h, int i) {
     const int64_t len = h->w.size();
+    const int64_t ss = h->batched ? (int64_t)h->batch * 8 : 8;
+    const int64_t N = h->batched ? h->n : 0, ni = h->batched ? (int64_t)h->D0.nx * h->D0.ny : 0;
     for (int k0 = 0; k0 < i; k0 += 8) {
         MVecs V{};
         const int J = std::min(8, i - k0);
         for (int j = 0; j < J; ++j) V.p[j] = h->V[k0 + j].base;
-        launch_mdot(h->D0, h->w.base, V, J, 3.0, h->knobs.p_norm_weight, h->partials, h->counter, h->slot(k0 + 1), h->stream);
+        launch_mdot(h->D0, h->w.base, V, J, 3.0, h->knobs.p_norm_weight, h->partials, h->counter, rslot(h, k0 + 1), h->stream,
+                    ninst(h), ss);
         check_launch();
     }
     for (int k0 = 0; k0 < i; k0 += 8) {
@@ -1113,14 +1121,18 @@ void arnoldi_column_cgs_enqueue(lmm_handle* h, int i) {
         const int J = std::min(8, i - k0);
         for (int j = 0; j < J; ++j) V.p[j] = h->V[k0 + j].base;
         if (k0 + J < i) {
-            launch_maxpy(h->w.base, V, J, h->slot(k0 + 1), len, h->stream);
+            launch_maxpy(h->w.base, V, J, rslot(h, k0 + 1), len, h->stream, N, ni, ss);
         } else {
             // the last projections and |w| in one pass over w
-            launch_maxpy_norm(h->D0, h->w.base, V, J, h->slot(k0 + 1), 3.0, h->knobs.p_norm_weight, h->partials, h->counter,
-                              h->slot(i + 1), h->stream);
+            launch_maxpy_norm(h->D0, h->w.base, V, J, rslot(h, k0 + 1), 3.0, h->knobs.p_norm_weight, h->partials, h->counter,
+                              rslot(h, i + 1), h->stream, ninst(h), ss);
         }
         check_launch();
     }
+}
+
+void arnoldi_column_cgs_enqueue(lmm_handle* h, int i) {
+    cgs_column(h, i);
     LMM_CK(cudaMemcpyAsync(h->hscal, h->scal, 8 * sizeof(double) * (i + 2), cudaMemcpyDeviceToHost, h->stream));
     LMM_CK(cudaEventRecord(h->col_ev, h->stream));
 }
@@ -1430,13 +1442,13 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
 }
 
 // ------------------------------------------------------------ batches of 2D problems
-// FGMRES (modified Gram-Schmidt) on the instances of a batch handle at once:
+// FGMRES (modified or classical Gram-Schmidt, knobs.orthogonalization) on
+// the instances of a batch handle at once:
 // every vector operation, preconditioner application and reduction covers
 // the whole batch in one launch, while the host keeps per instance the
 // Hessenberg matrix, Givens sequence, stopping decisions and statistics of
-// run_fgmres.  Per instance the arithmetic is run_fgmres's with
-// orthogonalization 0 (the reductions partition and sum each instance as
-// they would one problem).  An instance that has stopped rides along: its
+// run_fgmres.  Per instance the arithmetic is run_fgmres's (the reductions
+// partition and sum each instance as they would one problem).  An instance that has stopped rides along: its
 // columns are computed and not used, its update coefficients are zero.
 int run_fgmres_batch(lmm_handle* h, int count, lmm_stats* stats, int* status) {
     const lmm_knobs& K = h->knobs;
@@ -1538,12 +1550,16 @@ int run_fgmres_batch(lmm_handle* h, int count, lmm_stats* stats, int* status) {
         }
         for (int i = 1; i <= m; ++i) {
             column_work(i - 1);
-            for (int k = 1; k <= i; ++k) {
-                stokes_dot(h, h->w, h->V[k - 1], k);
-                launch_sub_scaled_batch(h->w.base, h->V[k - 1].base, h->bslot(k), n, ni, len, h->stream);
-                check_launch();
+            if (K.orthogonalization == 1) {
+                cgs_column(h, i);
+            } else {
+                for (int k = 1; k <= i; ++k) {
+                    stokes_dot(h, h->w, h->V[k - 1], k);
+                    launch_sub_scaled_batch(h->w.base, h->V[k - 1].base, h->bslot(k), n, ni, len, h->stream);
+                    check_launch();
+                }
+                stokes_norm(h, h->w, i + 1);
             }
-            stokes_norm(h, h->w, i + 1);
             launch_div_by_batch(h->w.base, h->V[i].base, fp32 ? h->pin32 : nullptr, h->bslot(i + 1), n, ni, len, h->stream);
             check_launch();
             fetch(1, i + 1);
@@ -1873,11 +1889,10 @@ int lmm_stokes_create_batch(const lmm_grid* g, const lmm_knobs* k, int batch, in
     g_last_error.clear();
     if (!g || !k || batch < 1 || batch > 4096) return LMM_ERR_INVALID;
     if (g->dm != 2 || k->method != LMM_METHOD_FGMRES || k->visc_type >= 0 || k->learned_stage != 0 || k->visc_schur_approx != 0 ||
-        k->stag_mg_max_vcycles > 1 || k->scale_factor != 1.0 || k->gmres_max_inner > lmm_handle::kBSlots - 3 ||
-        k->orthogonalization != 0) {
+        k->stag_mg_max_vcycles > 1 || k->scale_factor != 1.0 || k->gmres_max_inner > lmm_handle::kBSlots - 3) {
         g_last_error =
-            "batches: 2D, FGMRES with modified Gram-Schmidt, visc_type < 0, one V-cycle per application, scale_factor 1, "
-            "gmres_max_inner <= 45, no BFBt or learned stage";
+            "batches: 2D, FGMRES, visc_type < 0, one V-cycle per application, scale_factor 1, gmres_max_inner <= 45, no BFBt or "
+            "learned stage";
         return LMM_ERR_INVALID;
     }
     for (int d = 0; d < 2; ++d)

@@ -143,7 +143,8 @@ def main():
     ap.add_argument("--host-wait", type=int, default=0, help="0: worker threads spin on their streams (1: block)")
     ap.add_argument("--mode", choices=("batch", "pool"), default="batch",
                     help="batch: one batch handle per grid size; pool: worker threads with one-problem handles")
-    ap.add_argument("--orthogonalization", type=int, default=0, help="pool mode: 0 modified, 1 classical Gram-Schmidt")
+    ap.add_argument("--orthogonalization", type=int, default=None,
+                    help="0 modified, 1 classical Gram-Schmidt (default: 1 in batches, 0 in the pool, the faster of each)")
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=VALUE", help="any other lmm_knobs field")
     ap.add_argument("--sizes", default=",".join(str(n) for n in SIZES_2D),
                     help="comma-separated grid sizes the instances are drawn from")
@@ -168,7 +169,8 @@ def main():
     probs = [allp[i] for i in mine]
     pool = a.mode == "pool"
     kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
-                        orthogonalization=a.orthogonalization if pool else 0, gmres_rel_tol=a.rel_tol, host_wait=a.host_wait,
+                        orthogonalization=(0 if pool else 1) if a.orthogonalization is None else a.orthogonalization,
+                        gmres_rel_tol=a.rel_tol, host_wait=a.host_wait,
                         ensemble_batch=-1 if pool else 0)
     for kv in a.knob:
         name, val = kv.split("=", 1)

@@ -41,12 +41,14 @@ def _assert_same_as_single(probs, sols, stats, kn):
         assert s["history"] == st1["history"]
 
 
-@pytest.mark.parametrize("precision,theta", [(abi_p, th) for abi_p in (1, 0) for th in (0.0, 25.0)])
-def test_batched_ensemble_equals_individual_solves(precision, theta):
+@pytest.mark.parametrize("precision,theta,ortho", [(1, 0.0, 0), (1, 25.0, 0), (0, 0.0, 0), (0, 25.0, 0), (1, 0.0, 1), (0, 25.0, 1)])
+def test_batched_ensemble_equals_individual_solves(precision, theta, ortho):
+    """ortho: 0 modified, 1 classical Gram-Schmidt (one pass for all
+    projections, one for the update and the norm)"""
     from lowmachmixtures_b200 import abi, ensemble
     probs = ensemble.make_instances(12, seed=5, sizes=(32, 48, 64, 96), theta_alpha=theta)
     kn = abi.make_knobs(precon_type=2 if theta == 0.0 else 1, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=precision,
-                        gmres_rel_tol=1e-8)
+                        gmres_rel_tol=1e-8, orthogonalization=ortho)
     st, stats, sols, _ = ensemble.solve(probs, kn, workers=4)
     assert all(s == 0 for s in st)
     for s in stats:
@@ -119,22 +121,25 @@ def test_batch_handle_rejects_what_it_does_not_cover():
         lib.lmm_stokes_destroy(h)
 
 
-def test_large_batch_handle():
-    """64 instances of 128^2 (an arena of about a gigabyte): the handle's
-    buffers are zeroed in stream order before its pointer tables are written"""
+@pytest.mark.parametrize("n,count,ortho", [(128, 64, 0), (256, 48, 1)])
+def test_large_batch_handle(n, count, ortho):
+    """Arenas of one to two gigabytes: the handle's buffers are zeroed in
+    stream order before its pointer tables are written; 48 problems of 256^2
+    with classical Gram-Schmidt need more reduction partials than one
+    problem does"""
     from lowmachmixtures_b200 import _native, abi, ensemble, synth
     lib = _native.load()
-    probs = [synth.make_problem(2, 128, 10.0 ** (1 + (i % 7) / 3), 900 + i) for i in range(64)]
+    probs = [synth.make_problem(2, n, 10.0 ** (1 + (i % 7) / 3), 900 + i) for i in range(count)]
     kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
-                        gmres_rel_tol=1e-8)
+                        gmres_rel_tol=1e-8, orthogonalization=ortho)
     h = C.c_void_p()
-    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (128, 128), 1 / 128)), C.byref(kn), 64, 0, C.byref(h)) == 0
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (n, n), 1 / n)), C.byref(kn), count, 0, C.byref(h)) == 0
     try:
         items, keep, sols = ensemble._items(probs, 0)
-        assert lib.lmm_stokes_solve_batch(h, items, 64) == 0
+        assert lib.lmm_stokes_solve_batch(h, items, count) == 0
         assert all(it.status == 0 for it in items)
         assert all(it.stats.norm_resid_true <= 1e-8 * it.stats.norm_b for it in items)
-        pick = [0, 31, 63]
+        pick = [0, count // 2, count - 1]
         _assert_same_as_single([probs[i] for i in pick], [sols[i] for i in pick], [items[i].stats.as_dict() for i in pick], kn)
     finally:
         lib.lmm_stokes_destroy(h)
