@@ -2121,7 +2121,10 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
             const int cext[3] = {edge_ext(D, e, 0), edge_ext(D, e, 1), edge_ext(D, e, 2)};
             upload(in->beta_ed[e], L0.bed[e], lay, in->ng_beta_ed, nod_edge[e], D.wall ? cext : nullptr);
         }
-        if (in->gamma) upload(in->gamma, L0.gamma, lay, in->ng_gamma, nod_cell);
+        // gamma enters only the visc_type +-3 operator (stag_applyop.f90): not
+        // copied otherwise (solve_core then zeroes the device copy)
+        const bool use_gamma = in->gamma && std::abs(h->knobs.visc_type) == 3;
+        if (use_gamma) upload(in->gamma, L0.gamma, lay, in->ng_gamma, nod_cell);
         LMM_CK(host_wait(h));
         auto t1 = std::chrono::steady_clock::now();
         lmm_fields_in din{};
@@ -2132,7 +2135,7 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
         }
         din.b_p = h->r.p();
         din.beta = L0.beta;
-        din.gamma = in->gamma ? L0.gamma : nullptr;
+        din.gamma = use_gamma ? L0.gamma : nullptr;
         din.layout = LMM_LAYOUT_COMPACT;
         const double* x0u[3] = {h->w.c(0), h->w.c(1), dm == 3 ? h->w.c(2) : nullptr};
         LMM_CK(cudaEventRecord(h->ev0, h->stream));
