@@ -92,3 +92,25 @@ def test_create_rejects_bad_arguments_without_gpu(lib):
     k = abi.make_knobs(visc_schur_approx=1, visc_type=3)  # inverse_diag_lap has no |visc_type| = 3
     assert lib.lmm_stokes_create(C.byref(g), C.byref(k), 0, C.byref(h)) == abi.LMM_ERR_INVALID
     assert lib.lmm_strerror(abi.LMM_ERR_BREAKDOWN) == b"gmres: error in orthogonalization"
+
+
+def test_batch_entry_points_reject_bad_arguments_without_gpu(lib):
+    """lmm_stokes_create_batch checks its grid and knobs before touching a
+    device; lmm_stokes_solve_batch refuses a null or non-batch handle"""
+    g2 = abi.make_grid(2, (32, 32), 1.0 / 32)
+    ok = dict(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES)
+    h = C.c_void_p()
+    bad = [
+        (abi.make_grid(3, (16, 16, 16), 1.0 / 16), abi.make_knobs(**ok), 4),           # 3D
+        (g2, abi.make_knobs(**dict(ok, visc_type=2)), 4),                             # constant coefficients
+        (g2, abi.make_knobs(**dict(ok, method=abi.LMM_METHOD_GMRES)), 4),             # left-preconditioned GMRES
+        (g2, abi.make_knobs(**dict(ok, scale_factor=2.0)), 4),
+        (g2, abi.make_knobs(**dict(ok, gmres_max_inner=46)), 4),
+        (abi.make_grid(2, (32, 32), 1.0 / 32, bc=(abi.LMM_BC_PERIODIC, abi.LMM_BC_SLIP_WALL)), abi.make_knobs(**ok), 4),
+        (g2, abi.make_knobs(**ok), 0),                                                 # empty batch
+    ]
+    for g, k, b in bad:
+        assert lib.lmm_stokes_create_batch(C.byref(g), C.byref(k), b, 0, C.byref(h)) == abi.LMM_ERR_INVALID
+        assert not h.value
+    items = (abi.EnsembleItem * 1)()
+    assert lib.lmm_stokes_solve_batch(None, items, 1) == abi.LMM_ERR_INVALID
