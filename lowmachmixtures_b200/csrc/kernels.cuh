@@ -417,22 +417,17 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 5 : 0) k_residual(D
 }
 
 // 6-point (2D) / 12-point (3D) restriction of precomputed fine residuals,
-// same summation order as restrict_face
-// W: coarse wall faces are zero (physbc_domainvel on the restricted
-// residual, stag_mg_solver.f90:439-443); every other coarse face reads fine
-// faces inside the box
-template <class T, int DM, bool W = false>
-__global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restrict__ f0, const T* __restrict__ f1,
-                                                       const T* __restrict__ f2, Dims Dc, T* __restrict__ c0, T* __restrict__ c1,
-                                                       T* __restrict__ c2) {
-    pdl_enter();
-    const Pos q = pos3(Dc.nx, Dc.ny);
-    if (!q.ok) return;
-    const int t = q.i + Dc.nx * (q.j + Dc.ny * q.k);
-    const int I = 2 * q.i, J = 2 * q.j, K = 2 * q.k;
+// same summation order as restrict_face, for the coarse cell (i, j, k) at
+// coarse index t.  W: coarse wall faces are zero (physbc_domainvel on the
+// restricted residual, stag_mg_solver.f90:439-443); every other coarse face
+// reads fine faces inside the box.  LD: load mode of the fine arrays (ldp).
+template <class T, int DM, bool W = false, int LD = 0>
+__device__ __forceinline__ void restrict_cell(const Dims& F, const T* f0, const T* f1, const T* f2, const Dims& Dc, T* c0, T* c1,
+                                              T* c2, int i, int j, int k, int t) {
+    const int I = 2 * i, J = 2 * j, K = 2 * k;
     if constexpr (W) {
         // wall faces first; the others fall through to the periodic formula
-        const int x[3] = {q.i, q.j, q.k};
+        const int x[3] = {i, j, k};
         bool wf[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) wf[d] = d < DM && ((Dc.wall >> d) & 1) && x[d] == 0;
@@ -443,19 +438,19 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
         if (wf[1]) c1 = nullptr;
         if (wf[2]) c2 = nullptr;
     }
-    auto R = [&](const T* f, int i, int j, int k) {
-        i = wrapi(i, F.nx);
-        j = wrapi(j, F.ny);
-        k = (DM == 3) ? wrapi(k, F.nz) : k;
-        return ld(f, i + F.nx * (j + F.ny * k));
+    auto R = [&](const T* f, int ii, int jj, int kk) {
+        ii = wrapi(ii, F.nx);
+        jj = wrapi(jj, F.ny);
+        kk = (DM == 3) ? wrapi(kk, F.nz) : kk;
+        return ldp<LD>(f, ii + F.nx * (jj + F.ny * kk));
     };
     if constexpr (DM == 2) {
         if (!W || c0)
-        c0[t] = T(0.25) * (R(f0, I, J, q.k) + R(f0, I, J + 1, q.k)) +
-                T(0.125) * (R(f0, I + 1, J, q.k) + R(f0, I + 1, J + 1, q.k) + R(f0, I - 1, J, q.k) + R(f0, I - 1, J + 1, q.k));
+        c0[t] = T(0.25) * (R(f0, I, J, k) + R(f0, I, J + 1, k)) +
+                T(0.125) * (R(f0, I + 1, J, k) + R(f0, I + 1, J + 1, k) + R(f0, I - 1, J, k) + R(f0, I - 1, J + 1, k));
         if (!W || c1)
-        c1[t] = T(0.25) * (R(f1, I, J, q.k) + R(f1, I + 1, J, q.k)) +
-                T(0.125) * (R(f1, I, J + 1, q.k) + R(f1, I + 1, J + 1, q.k) + R(f1, I, J - 1, q.k) + R(f1, I + 1, J - 1, q.k));
+        c1[t] = T(0.25) * (R(f1, I, J, k) + R(f1, I + 1, J, k)) +
+                T(0.125) * (R(f1, I, J + 1, k) + R(f1, I + 1, J + 1, k) + R(f1, I, J - 1, k) + R(f1, I + 1, J - 1, k));
     } else {
         if (!W || c0)
         c0[t] = T(0.125) * (R(f0, I, J, K) + R(f0, I, J + 1, K) + R(f0, I, J, K + 1) + R(f0, I, J + 1, K + 1)) +
@@ -470,6 +465,17 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
                 T(0.0625) * (R(f2, I, J, K + 1) + R(f2, I + 1, J, K + 1) + R(f2, I, J + 1, K + 1) + R(f2, I + 1, J + 1, K + 1)) +
                 T(0.0625) * (R(f2, I, J, K - 1) + R(f2, I + 1, J, K - 1) + R(f2, I, J + 1, K - 1) + R(f2, I + 1, J + 1, K - 1));
     }
+}
+
+template <class T, int DM, bool W = false>
+__global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restrict__ f0, const T* __restrict__ f1,
+                                                       const T* __restrict__ f2, Dims Dc, T* __restrict__ c0, T* __restrict__ c1,
+                                                       T* __restrict__ c2) {
+    pdl_enter();
+    const Pos q = pos3(Dc.nx, Dc.ny);
+    if (!q.ok) return;
+    const int t = q.i + Dc.nx * (q.j + Dc.ny * q.k);
+    restrict_cell<T, DM, W, 0>(F, f0, f1, f2, Dc, c0, c1, c2, q.i, q.j, q.k, t);
 }
 
 template <class T, int DM, int VISC>

@@ -564,7 +564,6 @@ int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool st
     // on one), the pressure tail from 16^3 down
     const int cells = h->knobs.tail_cells == 0 ? (stag ? 512 : 4096) : h->knobs.tail_cells;
     if (cells < 0) return nl;
-    if (stag && h->D0.wall) return nl;  // the staggered tail kernel is periodic only
     const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
     const bool jacobi = stag && h->knobs.stag_mg_smoother == 0;
     const int64_t inst = (h->dm == 2) ? h->batch : 1;  // a 2D batch: one tail block per instance

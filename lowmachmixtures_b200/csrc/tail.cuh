@@ -68,7 +68,9 @@ __device__ __forceinline__ void unflat3d(const Dims& D, int w, int& i, int& j, i
     k = r / D.ny;
 }
 
-template <class T, int DM, int VISC, int COMP>
+// W: a grid with walls (wall faces keep their zero; the stencils and ghost
+// rules of the per-level wall kernels)
+template <class T, int DM, int VISC, int COMP, bool W>
 __device__ __forceinline__ void tail_colour(const TailView<T>& L, int parity, T omega) {
     const T b = ld(L.C.beta, 0), c = ld(L.C.gamma, 0);
     const int half = L.D.nx >> 1;
@@ -81,9 +83,10 @@ __device__ __forceinline__ void tail_colour(const TailView<T>& L, int parity, T 
         const int q = w / half;
         const int j = q % L.D.ny, k = q / L.D.ny;
         const int i = 2 * ih + ((j + k + parity) & 1);
-        Nb nb = make_nb(L.D, i, j, k);
-        T Lp = face_L<T, DM, VISC, COMP, 1>(phi, L.C, nb, L.dxsqinv, b, c);
-        T fac = face_diag<T, DM, VISC, COMP>(L.C, nb, L.dxsqinv, b, c);
+        Nb nb = W ? make_nbw(L.D, i, j, k) : make_nb(L.D, i, j, k);
+        if (W && wall_face(nb, COMP)) continue;
+        T Lp = face_L<T, DM, VISC, COMP, 1, T, W>(phi, L.C, nb, L.dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, COMP, W>(L.C, nb, L.dxsqinv, b, c);
         T cur = p[nb.s];
         p[nb.s] = cur + omega * (r[nb.s] - Lp) / fac;
     }
@@ -91,7 +94,7 @@ __device__ __forceinline__ void tail_colour(const TailView<T>& L, int parity, T 
 
 // a colour on an odd level (as k_colour_update): every new value from the
 // values before the colour's pass, staged in L.tmp[COMP]
-template <class T, int DM, int VISC, int COMP>
+template <class T, int DM, int VISC, int COMP, bool W>
 __device__ __forceinline__ void tail_colour_odd(const TailView<T>& L, int parity, T omega) {
     const T b = ld(L.C.beta, 0), c = ld(L.C.gamma, 0);
     const int n = ncells(L.D);
@@ -102,9 +105,13 @@ __device__ __forceinline__ void tail_colour_odd(const TailView<T>& L, int parity
         int i, j, k;
         unflat3d(L.D, w, i, j, k);
         if (((i + j + k) & 1) != parity) continue;
-        Nb nb = make_nb(L.D, i, j, k);
-        T Lp = face_L<T, DM, VISC, COMP, 1>(phi, L.C, nb, L.dxsqinv, b, c);
-        T fac = face_diag<T, DM, VISC, COMP>(L.C, nb, L.dxsqinv, b, c);
+        Nb nb = W ? make_nbw(L.D, i, j, k) : make_nb(L.D, i, j, k);
+        if (W && wall_face(nb, COMP)) {
+            L.tmp[COMP][w] = p[nb.s];  // stays zero
+            continue;
+        }
+        T Lp = face_L<T, DM, VISC, COMP, 1, T, W>(phi, L.C, nb, L.dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, COMP, W>(L.C, nb, L.dxsqinv, b, c);
         T cur = p[nb.s];
         L.tmp[COMP][w] = cur + omega * (r[nb.s] - Lp) / fac;
     }
@@ -116,7 +123,7 @@ __device__ __forceinline__ void tail_colour_odd(const TailView<T>& L, int parity
     }
 }
 
-template <class T, int DM, int VISC>
+template <class T, int DM, int VISC, bool W>
 __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega) {
     const T b = ld(L.C.beta, 0), c = ld(L.C.gamma, 0);
     const int n = ncells(L.D);
@@ -126,21 +133,29 @@ __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega
             for (int w = threadIdx.x; w < n; w += blockDim.x) {
                 int i, j, k;
                 unflat3d(L.D, w, i, j, k);
-                Nb nb = make_nb(L.D, i, j, k);
-                {
-                    T Lp = face_L<T, DM, VISC, 0, 1>(phi, L.C, nb, L.dxsqinv, b, c);
-                    T fac = face_diag<T, DM, VISC, 0>(L.C, nb, L.dxsqinv, b, c);
+                Nb nb = W ? make_nbw(L.D, i, j, k) : make_nb(L.D, i, j, k);
+                if (W && wall_face(nb, 0)) {
+                    L.tmp[0][w] = T(0);
+                } else {
+                    T Lp = face_L<T, DM, VISC, 0, 1, T, W>(phi, L.C, nb, L.dxsqinv, b, c);
+                    T fac = face_diag<T, DM, VISC, 0, W>(L.C, nb, L.dxsqinv, b, c);
                     L.tmp[0][w] = L.phi[0][w] + omega * (L.rhs[0][w] - Lp) / fac;
                 }
-                {
-                    T Lp = face_L<T, DM, VISC, 1, 1>(phi, L.C, nb, L.dxsqinv, b, c);
-                    T fac = face_diag<T, DM, VISC, 1>(L.C, nb, L.dxsqinv, b, c);
+                if (W && wall_face(nb, 1)) {
+                    L.tmp[1][w] = T(0);
+                } else {
+                    T Lp = face_L<T, DM, VISC, 1, 1, T, W>(phi, L.C, nb, L.dxsqinv, b, c);
+                    T fac = face_diag<T, DM, VISC, 1, W>(L.C, nb, L.dxsqinv, b, c);
                     L.tmp[1][w] = L.phi[1][w] + omega * (L.rhs[1][w] - Lp) / fac;
                 }
                 if constexpr (DM == 3) {
-                    T Lp = face_L<T, DM, VISC, 2, 1>(phi, L.C, nb, L.dxsqinv, b, c);
-                    T fac = face_diag<T, DM, VISC, 2>(L.C, nb, L.dxsqinv, b, c);
-                    L.tmp[2][w] = L.phi[2][w] + omega * (L.rhs[2][w] - Lp) / fac;
+                    if (W && wall_face(nb, 2)) {
+                        L.tmp[2][w] = T(0);
+                    } else {
+                        T Lp = face_L<T, DM, VISC, 2, 1, T, W>(phi, L.C, nb, L.dxsqinv, b, c);
+                        T fac = face_diag<T, DM, VISC, 2, W>(L.C, nb, L.dxsqinv, b, c);
+                        L.tmp[2][w] = L.phi[2][w] + omega * (L.rhs[2][w] - Lp) / fac;
+                    }
                 }
             }
             __syncthreads();
@@ -153,18 +168,18 @@ __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega
                 const int parity = (color % 2 == 1) ? 0 : 1;
                 if (odd_level(L.D)) {
                     if (comp == 0)
-                        tail_colour_odd<T, DM, VISC, 0>(L, parity, omega);
+                        tail_colour_odd<T, DM, VISC, 0, W>(L, parity, omega);
                     else if (comp == 1)
-                        tail_colour_odd<T, DM, VISC, 1>(L, parity, omega);
+                        tail_colour_odd<T, DM, VISC, 1, W>(L, parity, omega);
                     else if constexpr (DM == 3)
-                        tail_colour_odd<T, DM, VISC, 2>(L, parity, omega);
+                        tail_colour_odd<T, DM, VISC, 2, W>(L, parity, omega);
                 } else {
                     if (comp == 0)
-                        tail_colour<T, DM, VISC, 0>(L, parity, omega);
+                        tail_colour<T, DM, VISC, 0, W>(L, parity, omega);
                     else if (comp == 1)
-                        tail_colour<T, DM, VISC, 1>(L, parity, omega);
+                        tail_colour<T, DM, VISC, 1, W>(L, parity, omega);
                     else if constexpr (DM == 3)
-                        tail_colour<T, DM, VISC, 2>(L, parity, omega);
+                        tail_colour<T, DM, VISC, 2, W>(L, parity, omega);
                 }
                 __syncthreads();
             }
@@ -186,6 +201,7 @@ __device__ __forceinline__ const T* shift(const T* p, int64_t o) {
 // carve the dynamic shared memory into per-level phi / rhs / (tmp) arrays
 template <class T, int DM>
 __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool stag, bool jacobi) {
+    const bool wall = A.L[0].D.wall != 0;  // wall levels hold the residual in tmp
     size_t off = 0;
     for (int l = 0; l < A.nl; ++l) {
         TailView<T>& v = V[l];
@@ -210,7 +226,7 @@ __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool sta
         if (stag) {
             for (int d = 0; d < DM; ++d) { v.phi[d] = sm + off; off += n; }
             for (int d = 0; d < DM; ++d) { v.rhs[d] = sm + off; off += n; }
-            if (jacobi || odd)
+            if (jacobi || odd || wall)
                 for (int d = 0; d < DM; ++d) { v.tmp[d] = sm + off; off += n; }
         } else {
             v.pphi = sm + off; off += n;
@@ -223,7 +239,7 @@ __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool sta
 // The coarse end of a staggered V-cycle.  In: the first tail level's rhs and
 // phi (global); out: its phi (global).  Levels below are zeroed in shared
 // memory.
-template <class T, int DM, int VISC>
+template <class T, int DM, int VISC, bool W = false>
 __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_constant__ TailArgs<T> A) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char tail_smem[];
@@ -247,21 +263,49 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_co
     }
     __syncthreads();
     for (int l = 0; l < A.nl - 1; ++l) {
-        tail_smooth<T, DM, VISC>(V[l], A.nu1, A.smoother, A.omega);
+        tail_smooth<T, DM, VISC, W>(V[l], A.nu1, A.smoother, A.omega);
         const TailView<T>& F = V[l];
         const TailView<T>& Cc = V[l + 1];
         const int nc = ncells(Cc.D);
         const T* rf[3] = {F.rhs[0], F.rhs[1], F.rhs[2]};
         const T* pf[3] = {F.phi[0], F.phi[1], F.phi[2]};
-        for (int w2 = threadIdx.x; w2 < nc * DM; w2 += blockDim.x) {
-            const int comp = w2 / nc, w = w2 - comp * nc;
-            int i, j, k;
-            unflat3d(Cc.D, w, i, j, k);
-            restrict_comp<T, DM, VISC, 1>(comp, F.D, F.C, rf, pf, Cc.rhs, w, i, j, k, F.dxsqinv);
+        if constexpr (W) {
+            // the wall levels' residual_restrict: residual on every fine face
+            // (zero on wall faces) into F.tmp, then the restriction
+            const int nf = ncells(F.D);
+            for (int w2 = threadIdx.x; w2 < nf * DM; w2 += blockDim.x) {
+                const int comp = w2 / nf, w = w2 - comp * nf;
+                int i, j, k;
+                unflat3d(F.D, w, i, j, k);
+                const Nb nb = make_nbw(F.D, i, j, k);
+                const T b = ld(F.C.beta, 0), c = ld(F.C.gamma, 0);
+                T v = T(0);
+                if (comp == 0) {
+                    if (!wall_face(nb, 0)) v = (face_L<T, DM, VISC, 0, 1, T, true>(pf, F.C, nb, F.dxsqinv, b, c) - rf[0][w]) * T(-1);
+                } else if (comp == 1) {
+                    if (!wall_face(nb, 1)) v = (face_L<T, DM, VISC, 1, 1, T, true>(pf, F.C, nb, F.dxsqinv, b, c) - rf[1][w]) * T(-1);
+                } else if constexpr (DM == 3) {
+                    if (!wall_face(nb, 2)) v = (face_L<T, DM, VISC, 2, 1, T, true>(pf, F.C, nb, F.dxsqinv, b, c) - rf[2][w]) * T(-1);
+                }
+                F.tmp[comp][w] = v;
+            }
+            __syncthreads();
+            for (int w = threadIdx.x; w < nc; w += blockDim.x) {
+                int i, j, k;
+                unflat3d(Cc.D, w, i, j, k);
+                restrict_cell<T, DM, true, 1>(F.D, F.tmp[0], F.tmp[1], F.tmp[2], Cc.D, Cc.rhs[0], Cc.rhs[1], Cc.rhs[2], i, j, k, w);
+            }
+        } else {
+            for (int w2 = threadIdx.x; w2 < nc * DM; w2 += blockDim.x) {
+                const int comp = w2 / nc, w = w2 - comp * nc;
+                int i, j, k;
+                unflat3d(Cc.D, w, i, j, k);
+                restrict_comp<T, DM, VISC, 1>(comp, F.D, F.C, rf, pf, Cc.rhs, w, i, j, k, F.dxsqinv);
+            }
         }
         __syncthreads();
     }
-    tail_smooth<T, DM, VISC>(V[A.nl - 1], A.nub, A.smoother, A.omega);
+    tail_smooth<T, DM, VISC, W>(V[A.nl - 1], A.nub, A.smoother, A.omega);
     for (int l = A.nl - 2; l >= 0; --l) {
         const TailView<T>& F = V[l];
         const TailView<T>& Cc = V[l + 1];
@@ -269,10 +313,10 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_vcycle_tail(const __grid_co
         for (int w = threadIdx.x; w < nf; w += blockDim.x) {
             int i, j, k;
             unflat3d(F.D, w, i, j, k);
-            prolong_cell<T, DM, 1>(Cc.D, Cc.phi[0], Cc.phi[1], Cc.phi[2], F.phi[0], F.phi[1], F.phi[2], w, i, j, k);
+            prolong_cell<T, DM, 1, W>(Cc.D, Cc.phi[0], Cc.phi[1], Cc.phi[2], F.phi[0], F.phi[1], F.phi[2], w, i, j, k);
         }
         __syncthreads();
-        tail_smooth<T, DM, VISC>(F, A.nu2, A.smoother, A.omega);
+        tail_smooth<T, DM, VISC, W>(F, A.nu2, A.smoother, A.omega);
     }
     const int n0 = ncells(V[0].D);
     for (int w = threadIdx.x; w < n0; w += blockDim.x)
@@ -412,6 +456,7 @@ static TailArgs<T> tail_args(const LevelDev<T>* L, int nl, int nu1, int nu2, int
 template <class T>
 size_t tail_smem_bytes(const LevelDev<T>* L, int nl, bool stag, bool jacobi) {
     size_t e = 0;
+    jacobi = jacobi || L[0].D.wall != 0;  // wall levels hold the residual in tmp as well
     for (int l = 0; l < nl; ++l) {
         const bool odd = odd_level(L[l].D);
         const size_t n = (size_t)L[l].n / (L[l].D.dm == 2 ? L[l].D.nz : 1);  // one instance
@@ -439,10 +484,19 @@ cudaError_t launch_vcycle_tail(const LevelDev<T>* L, int nl, int visc, int nu1, 
     TailArgs<T> a = tail_args<T>(L, nl, nu1, nu2, nub, smoother, omega);
     const size_t smem = tail_smem_bytes<T>(L, nl, true, smoother == 0);
     cudaError_t e = cudaErrorInvalidValue;
+    const bool wall = L[0].D.wall != 0;
     if (L[0].D.dm == 2) {
-        LMM_VISC_DISPATCH(visc, (e = launch_tail(k_vcycle_tail<T, 2, V>, a, smem, s)))
+        if (wall) {
+            LMM_VISC_DISPATCH(visc, (e = launch_tail(k_vcycle_tail<T, 2, V, true>, a, smem, s)))
+        } else {
+            LMM_VISC_DISPATCH(visc, (e = launch_tail(k_vcycle_tail<T, 2, V>, a, smem, s)))
+        }
     } else {
-        LMM_VISC_DISPATCH(visc, (e = launch_tail(k_vcycle_tail<T, 3, V>, a, smem, s)))
+        if (wall) {
+            LMM_VISC_DISPATCH(visc, (e = launch_tail(k_vcycle_tail<T, 3, V, true>, a, smem, s)))
+        } else {
+            LMM_VISC_DISPATCH(visc, (e = launch_tail(k_vcycle_tail<T, 3, V>, a, smem, s)))
+        }
     }
     return e;
 }

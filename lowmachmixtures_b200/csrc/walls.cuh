@@ -3,8 +3,8 @@
 // once per precision by walls_fp64.cu and walls_fp32.cu; the launchers of
 // kernels.cuh hand every wall-bounded level here.
 //
-// The coarse tail kernel is not used on such grids: every level runs these
-// per-level kernels down to the coarsest.
+// The levels below the tail threshold run in the coarse tail kernel
+// (tail.cuh, with its wall variant), as on a periodic grid.
 #pragma once
 #include "kernels.cuh"
 

@@ -134,11 +134,14 @@ def test_walls_residual_restrict_and_prolong_bit_exact(oracle, dm, n, bc, visc):
 @pytest.mark.parametrize("dm,n,bc", [(2, 32, bc) for bc in BCS_2D] + [(3, 16, bc) for bc in BCS_3D] + [(2, 48, (NS, SL))])
 @pytest.mark.parametrize("visc", [-1, -2, -3])
 @pytest.mark.parametrize("smoother", [1, 0])
-def test_walls_vcycle_bit_exact(oracle, dm, n, bc, visc, smoother):
+@pytest.mark.parametrize("tail_cells", [0, -1])
+def test_walls_vcycle_bit_exact(oracle, dm, n, bc, visc, smoother, tail_cells):
+    """tail_cells 0: the coarse levels in the single-block tail (its wall
+    variant); -1: every level by per-level kernels"""
     p, rng = random_problem(dm, n, 24, visc, bc, theta=3.0)
     kn = dict(visc_type=visc, stag_mg_smoother=smoother, stag_mg_omega=1.0 if smoother else 0.7)
     k = oracle.default_knobs(**kn)
-    s = make_solver(p, **kn)
+    s = make_solver(p, **kn, tail_cells=tail_cells)
     rhs = [rng.standard_normal(p.shape) for _ in range(dm)]
     ref = oracle.stag_mg_solver(p, k, rhs)
     phi = [dev(np.zeros(p.shape)) for _ in range(dm)]
