@@ -40,7 +40,7 @@ def shard(costs, world: int):
 
 
 def make_instances(count: int, seed: int = 0, dm: int = 2, sizes=SIZES_2D, theta_alpha: float = 0.0):
-    """The config-3 ensemble: instance i has grid size instance_sizes()[i],
+    """The 512-problem 2D ensemble (by default): instance i has grid size instance_sizes()[i],
     its own seeded log-viscosity field with contrast instance_contrast(i)
     and an N(0,1) mean-removed face rhs."""
     from . import synth
@@ -135,7 +135,7 @@ def main():
     import os
 
     from . import abi
-    ap = argparse.ArgumentParser(description="config-3 ensemble: independent 2D periodic Stokes problems of uneven sizes")
+    ap = argparse.ArgumentParser(description="ensemble of independent 2D periodic Stokes problems of uneven sizes")
     ap.add_argument("--count", type=int, default=512)
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--rel-tol", type=float, default=1e-8)

@@ -164,7 +164,7 @@ def solve_with(prob, net: Net | None, knobs: abi.Knobs | None = None, repeats: i
 
 
 def evaluate(net: Net, seeds, n: int = 64, log=None):
-    """Held-out comparison on `seeds` (config 4 problems: n^3, theta = 0,
+    """Held-out comparison on `seeds` (the learned-stage problems: n^3, theta = 0,
     contrast log-uniform in [10, 1000]): FGMRES + FP32 V-cycles with and
     without the learned stage, and the residual ratios of one application."""
     out = []

@@ -5,7 +5,7 @@ divergence of a stochastic stress generated on the GPU
 FGMRES with a 20-vector FP64 Krylov basis; the FP32-V-cycle method against
 the plain FP64 one, both to |b - Ax| / |b| <= 1e-9.
 
-    python -m lowmachmixtures_b200.config5 --n 256
+    python -m lowmachmixtures_b200.mixture_solve --n 256
 """
 from __future__ import annotations
 

@@ -53,7 +53,7 @@ def test_gpu_forcing_matches_oracle(dm, n):
 
 @pytest.mark.gpu
 def test_stochastic_mixture_solve_parity_small(oracle):
-    """The config-5 recipe at 32^3: GPU forcing, then the FP64 solve equals
+    """The 256^3 mixture recipe at 32^3: GPU forcing, then the FP64 solve equals
     the oracle's (same forcing from the oracle generator) within 1e-10, and
     the mixed method meets the tolerance."""
     import torch
