@@ -143,3 +143,51 @@ def test_large_batch_handle(n, count, ortho):
         _assert_same_as_single([probs[i] for i in pick], [sols[i] for i in pick], [items[i].stats.as_dict() for i in pick], kn)
     finally:
         lib.lmm_stokes_destroy(h)
+
+
+def test_batch_statuses_per_problem():
+    """A problem with a non-finite right-hand side fails alone
+    (LMM_ERR_NONFINITE); under a tight iteration limit each problem stops
+    with its own status (converged or LMM_WARN_MAX_ITER), and every
+    problem's bits and status are those of its one-problem solve."""
+    import torch
+
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    from lowmachmixtures_b200.gmres import StokesSolver
+    lib = _native.load()
+    probs = [synth.make_problem(2, 64, 10.0 ** (1 + i / 2), 500 + i) for i in range(5)]
+    probs[1].b_u[0] = probs[1].b_u[0].copy()
+    probs[1].b_u[0][3, 5] = np.nan
+    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                        gmres_rel_tol=1e-10, gmres_max_iter=9)
+    h = C.c_void_p()
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (64, 64), 1 / 64)), C.byref(kn), 5, 0, C.byref(h)) == 0
+    try:
+        items, keep, sols = ensemble._items(probs, 0)
+        rc = lib.lmm_stokes_solve_batch(h, items, 5)
+        assert rc == abi.LMM_ERR_NONFINITE
+        assert items[1].status == abi.LMM_ERR_NONFINITE
+        statuses = set()
+        for q in (0, 2, 3, 4):
+            p = probs[q]
+            with StokesSolver(2, p.n[:2], p.dx, knobs=kn) as s:
+                yp = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
+                yu = [torch.zeros_like(yp) for _ in range(2)]
+                fin = s._fields([_dev(a) for a in p.b_u], _dev(p.b_p), [_dev(a) for a in p.alpha_fc], _dev(p.beta),
+                                [_dev(a) for a in p.beta_ed], _dev(p.gamma), abi.LMM_LAYOUT_COMPACT, None)
+                fout = abi.FieldsOut()
+                fout.x_u = abi.ptr_array(yu)
+                fout.x_p = abi.ptr(yp)
+                fout.layout = abi.LMM_LAYOUT_COMPACT
+                th, npr, st = C.c_double(p.theta_alpha), C.c_double(0.0), abi.Stats()
+                rc1 = lib.lmm_stokes_solve_device(s._h, C.byref(fin), C.byref(fout), C.byref(th), C.byref(npr), C.byref(st))
+            assert items[q].status == rc1
+            statuses.add(rc1)
+            assert items[q].stats.total_iter == st.total_iter
+            xu, xp = sols[q]
+            for c in range(2):
+                assert torch.equal(xu[c], yu[c])
+            assert torch.equal(xp, yp)
+        assert abi.LMM_WARN_MAX_ITER in statuses
+    finally:
+        lib.lmm_stokes_destroy(h)
