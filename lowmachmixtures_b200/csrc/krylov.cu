@@ -21,11 +21,13 @@ __device__ __forceinline__ void unflat3(const Dims& D, int t, int& i, int& j, in
 }  // namespace
 
 // b_u = stag_applyop(x_u) + grad(x_p);  b_p = -div(x_u)   (apply_matrix.f90:96-112)
+// Register budget: 4 blocks of 256 per SM (64 registers; the |visc| = 3
+// stencil, which would spill there, 3 blocks).
 // W: a grid with walls -- b_u is zero on the wall faces (the applyop is
 // zeroed there and the FOEXTRAP pressure has zero wall gradient), and the
 // divergence reads the hi+1 wall face as zero
 template <int DM, int VISC, class TX, bool W = false>
-__global__ void __launch_bounds__(kT) k_apply_matrix(Dims D, Coef<double> C, const TX* __restrict__ u0,
+__global__ void __launch_bounds__(kT, (VISC == 3 || VISC == -3) ? 3 : 4) k_apply_matrix(Dims D, Coef<double> C, const TX* __restrict__ u0,
                                                      const TX* __restrict__ u1, const TX* __restrict__ u2,
                                                      const TX* __restrict__ p, double* __restrict__ o0,
                                                      double* __restrict__ o1, double* __restrict__ o2, double* __restrict__ op,
