@@ -1979,6 +1979,10 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
     const int64_t n = h->n;
     double theta = *theta_alpha;
     const double sf = K.scale_factor;
+    g_debug_stream = h->stream;  // LMM_DEBUG: launch checks on this solve's stream
+    g_debug_dims[0] = h->D0.nx;
+    g_debug_dims[1] = h->D0.ny;
+    g_debug_dims[2] = h->D0.nz;
     // scale_factor (gmres.f90:106-122): applied to device copies only
     if (sf != 1.0) theta = theta * sf;
     LevelDev<double>& L0 = h->L64[0];
