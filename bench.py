@@ -420,14 +420,9 @@ def run_product(args, world, rank, local):
         line["learned_stage"] = learned_leg(args, prob, n, local, solve_dev, d_in, d_xu, d_xp, world)
     traffic = profiled_traffic("gs_colour_fp32_128")
     if traffic is not None and n == 128:
-        rl = line["roofline"]
-        rl["traffic"] = traffic * 6  # six colour launches per smooth
-        # the same launches against the DRAM bytes they move (each colour
-        # reads its component's operand arrays in full sectors): how close
-        # the kernel runs to HBM for its access pattern, beside `frac`,
-        # which is against the fused minimum of one read per array per smooth
-        rl["traffic_gbs"] = gbs(rl["traffic"], rl["ms_per_smooth"])
-        rl["traffic_frac"] = rl["traffic_gbs"] / peak
+        # six colour launches per smooth, each captured alone with cold caches
+        # (live, consecutive colours of a component share part of it in L2)
+        line["roofline"]["traffic"] = traffic * 6
     for s in (mixed, plain, refg):
         s.close()
     if rank == 0:

@@ -48,6 +48,12 @@ const bool g_debug = std::getenv("LMM_DEBUG") != nullptr;
 thread_local cudaStream_t g_debug_stream = nullptr;
 thread_local int g_debug_dims[3] = {0, 0, 0};  // the solving handle's nx, ny, nz
 
+// the handle whose stream LMM_DEBUG checks while a solve runs on this thread
+struct DebugScope {
+    explicit DebugScope(const lmm_handle* h);
+    ~DebugScope() { g_debug_stream = nullptr; }
+};
+
 // a failed CUDA call or launch: its text and source line in the calling
 // thread's last error
 void note_error(const std::string& what, const char* fn, int line) {
@@ -194,6 +200,13 @@ struct lmm_handle {
     }
     double* slot(int k) { return scal + 8 * k; }
 };
+
+DebugScope::DebugScope(const lmm_handle* h) {
+    g_debug_stream = h->stream;
+    g_debug_dims[0] = h->D0.nx;
+    g_debug_dims[1] = h->D0.ny;
+    g_debug_dims[2] = h->D0.nz;
+}
 
 namespace {
 
@@ -1979,10 +1992,7 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
     const int64_t n = h->n;
     double theta = *theta_alpha;
     const double sf = K.scale_factor;
-    g_debug_stream = h->stream;  // LMM_DEBUG: launch checks on this solve's stream
-    g_debug_dims[0] = h->D0.nx;
-    g_debug_dims[1] = h->D0.ny;
-    g_debug_dims[2] = h->D0.nz;
+    DebugScope dbg(h);  // LMM_DEBUG: launch checks on this solve's stream
     // scale_factor (gmres.f90:106-122): applied to device copies only
     if (sf != 1.0) theta = theta * sf;
     LevelDev<double>& L0 = h->L64[0];
@@ -2200,10 +2210,7 @@ extern "C" int lmm_stokes_solve_batch(lmm_handle* h, lmm_ensemble_item* items, i
     }
     try {
         LMM_CK(cudaSetDevice(h->device));
-        g_debug_stream = h->stream;
-        g_debug_dims[0] = h->D0.nx;
-        g_debug_dims[1] = h->D0.ny;
-        g_debug_dims[2] = h->D0.nz;
+        DebugScope dbg(h);
         LevelDev<double>& L0 = h->L64[0];
         std::vector<lmm_stats> st(count);
         std::vector<int> status(count, LMM_OK);
