@@ -68,7 +68,8 @@ int lmm_ensemble_destroy(lmm_ensemble* ens);
  * visc_type < 0, stag_mg_max_vcycles <= 1,
  * scale_factor 1, gmres_max_inner <= 45, no BFBt or learned stage; grids
  * periodic, at most 2^29 cells per batch.  A batch handle is accepted by these two calls,
- * lmm_time_op and lmm_stokes_destroy only.  Returns the most negative
+ * lmm_stokes_update_knobs (stopping rules between solves), lmm_time_op and
+ * lmm_stokes_destroy only.  Returns the most negative
  * problem status, else the largest warning, else LMM_OK; per item status
  * and stats.  lmm_ensemble_* uses batches for 2D problems whose knobs
  * allow it (knobs->ensemble_batch = 0). */

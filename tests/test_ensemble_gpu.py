@@ -191,3 +191,28 @@ def test_batch_statuses_per_problem():
         assert abi.LMM_WARN_MAX_ITER in statuses
     finally:
         lib.lmm_stokes_destroy(h)
+
+
+def test_batch_handle_update_knobs():
+    """lmm_stokes_update_knobs on a live batch handle: a tighter tolerance
+    gives each problem the solve of a fresh one-problem handle with it"""
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    lib = _native.load()
+    probs = [synth.make_problem(2, 48, 10.0 ** (1 + i / 2), 700 + i) for i in range(3)]
+    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                        gmres_rel_tol=1e-6)
+    h = C.c_void_p()
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (48, 48), 1 / 48)), C.byref(kn), 3, 0, C.byref(h)) == 0
+    try:
+        items, keep, sols = ensemble._items(probs, 0)
+        assert lib.lmm_stokes_solve_batch(h, items, 3) == 0
+        loose = [it.stats.total_iter for it in items]
+        tight = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                               gmres_rel_tol=1e-10)
+        assert lib.lmm_stokes_update_knobs(h, C.byref(tight)) == 0
+        items, keep, sols = ensemble._items(probs, 0)
+        assert lib.lmm_stokes_solve_batch(h, items, 3) == 0
+        assert all(it.stats.total_iter > q for it, q in zip(items, loose))
+        _assert_same_as_single(probs, sols, [it.stats.as_dict() for it in items], tight)
+    finally:
+        lib.lmm_stokes_destroy(h)
