@@ -67,7 +67,9 @@ int lmm_ensemble_destroy(lmm_ensemble* ens);
  * batch's time.  Knobs: LMM_METHOD_FGMRES (FP32 or FP64 preconditioner),
  * visc_type < 0, stag_mg_max_vcycles <= 1,
  * scale_factor 1, gmres_max_inner <= 45, no BFBt or learned stage; grids
- * periodic, at most 2^29 cells per batch.  A batch handle is accepted by these two calls,
+ * periodic or with walls (as lmm_stokes_create; the edge arrays then keep
+ * n+1 nodes along a nodal wall-bounded direction), at most 2^29 cells per
+ * batch.  lmm_ensemble_* batches periodic grids.  A batch handle is accepted by these two calls,
  * lmm_stokes_update_knobs (stopping rules between solves), lmm_time_op and
  * lmm_stokes_destroy only.  Returns the most negative
  * problem status, else the largest warning, else LMM_OK; per item status

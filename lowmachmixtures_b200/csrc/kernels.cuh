@@ -697,12 +697,13 @@ __global__ void __launch_bounds__(kThreads) k_coarsen_edges_w(Dims F, Dims Dc, c
     T* e[3] = {e0, e1, e2};
 #pragma unroll
     for (int q = 0; q < (DM == 2 ? 1 : 3); ++q) {
-        const int cx = edge_ext(Dc, q, 0), cy = edge_ext(Dc, q, 1), cz = (DM == 3) ? edge_ext(Dc, q, 2) : 1;
+        // 2D: the third index is the instance (a batch stacks nz of them)
+        const int cx = edge_ext(Dc, q, 0), cy = edge_ext(Dc, q, 1), cz = (DM == 3) ? edge_ext(Dc, q, 2) : Dc.nz;
         if (i >= cx || j >= cy || k >= cz) continue;
         const int fx = edge_ext(F, q, 0), fy = edge_ext(F, q, 1);
         auto at = [&](int a, int b, int c) { return ld(f[q], a + fx * (b + fy * c)); };
         T v;
-        if (DM == 2) v = at(I, J, 0);
+        if (DM == 2) v = at(I, J, k);
         else if (q == 0) v = T(0.5) * (at(I, J, K) + at(I, J, K + 1));
         else if (q == 1) v = T(0.5) * (at(I, J, K) + at(I, J + 1, K));
         else v = T(0.5) * (at(I, J, K) + at(I + 1, J, K));
@@ -1299,7 +1300,7 @@ void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pre
         k_coarsen<T, 3><<<g.grid, g.block, 0, s>>>(F.D, Cc.D, cf, Cc.alpha[0], Cc.alpha[1], Cc.alpha[2], Cc.beta, Cc.gamma, Cc.bed[0], Cc.bed[1], Cc.bed[2], dv);
     if (F.D.wall) {
         count_launch();
-        const G3 ge = geom3(Cc.D.nx + 1, Cc.D.ny + 1, Cc.D.dm == 3 ? Cc.D.nz + 1 : 1);
+        const G3 ge = geom3(Cc.D.nx + 1, Cc.D.ny + 1, Cc.D.dm == 3 ? Cc.D.nz + 1 : Cc.D.nz);
         if (F.D.dm == 2)
             k_coarsen_edges_w<T, 2><<<ge.grid, ge.block, 0, s>>>(F.D, Cc.D, F.bed[0], F.bed[1], F.bed[2], Cc.bed[0], Cc.bed[1], Cc.bed[2]);
         else

@@ -1907,11 +1907,6 @@ int lmm_stokes_create_batch(const lmm_grid* g, const lmm_knobs* k, int batch, in
             "learned stage";
         return LMM_ERR_INVALID;
     }
-    for (int d = 0; d < 2; ++d)
-        if (g->bc_lo[d] != LMM_BC_PERIODIC || g->bc_hi[d] != LMM_BC_PERIODIC) {
-            g_last_error = "batches: periodic grids";
-            return LMM_ERR_INVALID;
-        }
     if ((int64_t)g->n[0] * g->n[1] * batch > (int64_t)INT32_MAX / 4) {
         g_last_error = "batches: at most 2^29 cells per batch";
         return LMM_ERR_INVALID;
@@ -2247,7 +2242,9 @@ extern "C" int lmm_stokes_solve_batch(lmm_handle* h, lmm_ensemble_item* items, i
                 LMM_CK(cudaMemsetAsync(L0.gamma, 0, sizeof(double) * h->n, h->stream));
                 continue;
             }
-            launch_gather_ptrs(h->gtab + (int64_t)f * B, dst[f], ni, B, h->stream);
+            // an edge array (field 6) keeps n+1 nodes along a nodal wall-bounded direction
+            const int nf = (f == 6) ? edge_ext(h->D0, 0, 0) * edge_ext(h->D0, 0, 1) : ni;
+            launch_gather_ptrs(h->gtab + (int64_t)f * B, dst[f], nf, B, h->stream);
             check_launch();
         }
         if (count < B) {
@@ -2256,6 +2253,15 @@ extern "C" int lmm_stokes_solve_batch(lmm_handle* h, lmm_ensemble_item* items, i
                 LMM_CK(cudaMemsetAsync(h->b.c(c) + (int64_t)count * ni, 0, rest, h->stream));
                 LMM_CK(cudaMemsetAsync(h->x.c(c) + (int64_t)count * ni, 0, rest, h->stream));
             }
+        }
+        if (h->D0.wall) {
+            // wall-normal velocities on the walls are not unknowns (as solve_core)
+            double* bu[3] = {h->b.c(0), h->b.c(1), h->b.c(0)};
+            double* xu[3] = {h->x.c(0), h->x.c(1), h->x.c(0)};
+            launch_zero_wall_faces(h->D0, bu, h->stream);
+            check_launch();
+            launch_zero_wall_faces(h->D0, xu, h->stream);
+            check_launch();
         }
         const double* al[3] = {h->alpha_fc[0], h->alpha_fc[1], nullptr};
         const double* bed[3] = {L0.bed[0], nullptr, nullptr};

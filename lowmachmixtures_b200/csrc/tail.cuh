@@ -209,10 +209,12 @@ __device__ void tail_views(const TailArgs<T>& A, T* sm, TailView<T>* V, bool sta
         v.dxsqinv = A.L[l].dxsqinv;
         v.C = A.L[l].C;
         const int64_t io = inst_offset<DM>(v.D);
+        // an instance's edge array: n+1 nodes along a nodal wall-bounded direction
+        const int64_t ie = DM == 2 ? (int64_t)blockIdx.x * edge_ext(v.D, 0, 0) * edge_ext(v.D, 0, 1) : 0;
         if (DM == 2) v.D.nz = 1;
         for (int d = 0; d < 3; ++d) {
             v.C.alpha[d] = shift(v.C.alpha[d], io);
-            v.C.bed[d] = shift(v.C.bed[d], io);
+            v.C.bed[d] = shift(v.C.bed[d], ie);
         }
         v.C.beta = shift(v.C.beta, io);
         v.C.gamma = shift(v.C.gamma, io);

@@ -106,7 +106,6 @@ def test_batch_entry_points_reject_bad_arguments_without_gpu(lib):
         (g2, abi.make_knobs(**dict(ok, method=abi.LMM_METHOD_GMRES)), 4),             # left-preconditioned GMRES
         (g2, abi.make_knobs(**dict(ok, scale_factor=2.0)), 4),
         (g2, abi.make_knobs(**dict(ok, gmres_max_inner=46)), 4),
-        (abi.make_grid(2, (32, 32), 1.0 / 32, bc=(abi.LMM_BC_PERIODIC, abi.LMM_BC_SLIP_WALL)), abi.make_knobs(**ok), 4),
         (g2, abi.make_knobs(**ok), 0),                                                 # empty batch
     ]
     for g, k, b in bad:

@@ -22,7 +22,7 @@ def _single(p, kn):
     import torch
 
     from lowmachmixtures_b200.gmres import StokesSolver
-    with StokesSolver(2, p.n[:2], p.dx, knobs=kn) as s:
+    with StokesSolver(2, p.n[:2], p.dx, knobs=kn, bc=getattr(p, "bc", None)) as s:
         yp = torch.zeros(p.shape, dtype=torch.float64, device="cuda")
         yu = [torch.zeros_like(yp) for _ in range(2)]
         _, _, st = s.solve_device([_dev(a) for a in p.b_u], _dev(p.b_p), yu, yp, [_dev(a) for a in p.alpha_fc], _dev(p.beta),
@@ -101,8 +101,7 @@ def test_batch_handle_rejects_what_it_does_not_cover():
     for g, kn in ((abi.make_grid(3, (16, 16, 16), 1 / 16), abi.make_knobs(**ok)),
                   (g2, abi.make_knobs(**dict(ok, visc_type=2))),
                   (g2, abi.make_knobs(**dict(ok, method=abi.LMM_METHOD_GMRES))),
-                  (g2, abi.make_knobs(**dict(ok, stag_mg_max_vcycles=2))),
-                  (abi.make_grid(2, (32, 32), 1 / 32, bc=(abi.LMM_BC_PERIODIC, abi.LMM_BC_NO_SLIP_WALL)), abi.make_knobs(**ok))):
+                  (g2, abi.make_knobs(**dict(ok, stag_mg_max_vcycles=2)))):
         assert lib.lmm_stokes_create_batch(C.byref(g), C.byref(kn), 4, 0, C.byref(h)) == abi.LMM_ERR_INVALID
     assert lib.lmm_stokes_create_batch(C.byref(g2), C.byref(abi.make_knobs(**ok)), 2, 0, C.byref(h)) == 0
     try:
@@ -214,5 +213,26 @@ def test_batch_handle_update_knobs():
         assert lib.lmm_stokes_solve_batch(h, items, 3) == 0
         assert all(it.stats.total_iter > q for it, q in zip(items, loose))
         _assert_same_as_single(probs, sols, [it.stats.as_dict() for it in items], tight)
+    finally:
+        lib.lmm_stokes_destroy(h)
+
+
+@pytest.mark.parametrize("bc", [(-1, 100), (100, 200), (100, 100)])
+@pytest.mark.parametrize("precision", [1, 0])
+def test_batch_with_walls(bc, precision):
+    """2D batches on grids with walls (no-slip 100, slip 200, periodic -1 per
+    direction): the bits of one-problem solves"""
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    lib = _native.load()
+    n = 32
+    probs = [synth.make_problem(2, n, 10.0 ** (1 + i / 2), 800 + i, bc=bc) for i in range(4)]
+    kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=precision, gmres_rel_tol=1e-9)
+    h = C.c_void_p()
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (n, n), 1 / n, bc=bc)), C.byref(kn), 4, 0, C.byref(h)) == 0
+    try:
+        items, keep, sols = ensemble._items(probs, 0)
+        assert lib.lmm_stokes_solve_batch(h, items, 4) == 0
+        assert all(it.status == 0 for it in items)
+        _assert_same_as_single(probs, sols, [it.stats.as_dict() for it in items], kn)
     finally:
         lib.lmm_stokes_destroy(h)
