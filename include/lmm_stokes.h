@@ -123,7 +123,8 @@ typedef struct lmm_knobs {
                                       (3D FGMRES; needs lmm_stokes_set_net) */
     int    tail_cells;             /* coarse multigrid levels with at most this many cells run in
                                       one single-block launch; 0 = default (512 for the velocity
-                                      V-cycle, 4096 for the pressure V-cycle), -1 = never */
+                                      V-cycle, 1024 for one 2D problem, 4096 for the pressure
+                                      V-cycle), -1 = never */
     int    tail_smem_kb;           /* shared-memory budget of that launch in KiB; 0 = 200 */
     int    use_graphs;             /* replay each preconditioner application from a captured
                                       CUDA graph: 0 = default (on), -1 = off */

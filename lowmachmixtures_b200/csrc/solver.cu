@@ -574,8 +574,11 @@ template <class T>
 int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool stag) {
     // default: the velocity tail from 8^3 cells down (a 16^3 level runs
     // faster as per-level launches over many SMs than as ~50 barrier phases
-    // on one), the pressure tail from 16^3 down
-    const int cells = h->knobs.tail_cells == 0 ? (stag ? 512 : 4096) : h->knobs.tail_cells;
+    // on one) -- one 2D problem from 32^2 down (64^2 solve 2.71 -> 2.58 ms;
+    // a batch's per-problem tails were slower from 32^2) -- and the
+    // pressure tail from 16^3 down
+    const int vel_cells = (h->dm == 2 && !h->batched) ? 1024 : 512;
+    const int cells = h->knobs.tail_cells == 0 ? (stag ? vel_cells : 4096) : h->knobs.tail_cells;
     if (cells < 0) return nl;
     const size_t budget = (size_t)(h->knobs.tail_smem_kb > 0 ? h->knobs.tail_smem_kb : 200) * 1024;
     const bool jacobi = stag && h->knobs.stag_mg_smoother == 0;

@@ -20,6 +20,8 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--dm", type=int, default=3, choices=[2, 3],
+                    help="2: the 2D steady workload (n^2, contrast 10, theta = 0); 3: 3D n^3, contrast 100, theta*alpha = 0.1/dx^2")
     ap.add_argument("--method", default="mixed", choices=["mixed", "plain", "reference"])
     ap.add_argument("--solves", type=int, default=1)
     ap.add_argument("--warm", type=int, default=1)
@@ -38,7 +40,10 @@ def main():
     from lowmachmixtures_b200.gmres import StokesSolver
 
     bc = tuple(int(v) for v in a.bc.split(",")) if a.bc else None
-    prob = synth.config_3d_128(0, n=a.n) if bc is None else synth.make_problem(3, a.n, 100.0, 0, theta_alpha=0.1 * a.n * a.n, bc=bc)
+    if a.dm == 2:
+        prob = synth.make_problem(2, a.n, 10.0, 0, theta_alpha=0.0, bc=bc)
+    else:
+        prob = synth.config_3d_128(0, n=a.n) if bc is None else synth.make_problem(3, a.n, 100.0, 0, theta_alpha=0.1 * a.n * a.n, bc=bc)
     kn = dict(precon_type=2, visc_type=-2)
     if a.method == "mixed":
         kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
@@ -50,8 +55,8 @@ def main():
     dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()  # noqa: E731
     bu, bp = [dev(x) for x in prob.b_u], dev(prob.b_p)
     al, be, bed, ga = [dev(x) for x in prob.alpha_fc], dev(prob.beta), [dev(x) for x in prob.beta_ed], dev(prob.gamma)
-    xu, xp = [torch.zeros_like(bu[0]) for _ in range(3)], torch.zeros_like(bp)
-    with StokesSolver(3, (a.n,) * 3, prob.dx, knobs=abi.make_knobs(**kn), bc=bc) as s:
+    xu, xp = [torch.zeros_like(bu[0]) for _ in range(a.dm)], torch.zeros_like(bp)
+    with StokesSolver(a.dm, (a.n,) * a.dm, prob.dx, knobs=abi.make_knobs(**kn), bc=bc) as s:
         if a.op:
             s.load_coeffs(al, be, bed, ga, prob.theta_alpha)
             fp32 = a.method == "mixed"
