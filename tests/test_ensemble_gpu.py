@@ -236,3 +236,25 @@ def test_batch_with_walls(bc, precision):
         _assert_same_as_single(probs, sols, [it.stats.as_dict() for it in items], kn)
     finally:
         lib.lmm_stokes_destroy(h)
+
+
+@pytest.mark.parametrize("visc", [-1, -3])
+@pytest.mark.parametrize("precon", [1, 4])
+def test_batch_other_viscous_operators(visc, precon):
+    """visc_type -1 and -3 (gamma enters the operator and the Schur step),
+    preconditioners 1 and 4, theta_alpha > 0: the bits of one-problem solves"""
+    from lowmachmixtures_b200 import _native, abi, ensemble, synth
+    lib = _native.load()
+    n = 32
+    probs = [synth.make_problem(2, n, 10.0 ** (1 + i / 2), 900 + i, theta_alpha=20.0) for i in range(3)]
+    kn = abi.make_knobs(precon_type=precon, visc_type=visc, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                        gmres_rel_tol=1e-9)
+    h = C.c_void_p()
+    assert lib.lmm_stokes_create_batch(C.byref(abi.make_grid(2, (n, n), 1 / n)), C.byref(kn), 3, 0, C.byref(h)) == 0
+    try:
+        items, keep, sols = ensemble._items(probs, 0)
+        rc = lib.lmm_stokes_solve_batch(h, items, 3)
+        assert rc >= 0
+        _assert_same_as_single(probs, sols, [it.stats.as_dict() for it in items], kn)
+    finally:
+        lib.lmm_stokes_destroy(h)
