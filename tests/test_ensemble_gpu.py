@@ -239,10 +239,11 @@ def test_batch_with_walls(bc, precision):
 
 
 @pytest.mark.parametrize("visc", [-1, -3])
-@pytest.mark.parametrize("precon", [1, 4])
+@pytest.mark.parametrize("precon", [1, 4, 3, 5, -2])
 def test_batch_other_viscous_operators(visc, precon):
     """visc_type -1 and -3 (gamma enters the operator and the Schur step),
-    preconditioners 1 and 4, theta_alpha > 0: the bits of one-problem solves"""
+    the other preconditioner types, theta_alpha > 0: the bits of one-problem
+    solves"""
     from lowmachmixtures_b200 import _native, abi, ensemble, synth
     lib = _native.load()
     n = 32
