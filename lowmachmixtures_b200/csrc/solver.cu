@@ -748,17 +748,21 @@ PrecScratch<float> prec_scratch<float>(lmm_handle* h) {
             {h->bf32[0], h->bf32[1], h->bf32[2], h->bf32[3], h->bf32[4], h->bf32[5], h->bf32[6], h->bf32[7]}};
 }
 
+// sums of p and of the velocity components d in umask (bit d); the others
+// are not read
 template <class T>
-void reduce_means(lmm_handle* h, T* const u[3], const T* p, int slot);
+void reduce_means(lmm_handle* h, T* const u[3], const T* p, int slot, int umask = 7);
 template <>
-void reduce_means<double>(lmm_handle* h, double* const u[3], const double* p, int slot) {
-    const double* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
+void reduce_means<double>(lmm_handle* h, double* const u[3], const double* p, int slot, int umask) {
+    const double* a[4] = {(umask & 1) ? u[0] : nullptr, (umask & 2) ? u[1] : nullptr,
+                          (h->dm == 3 && (umask & 4)) ? u[2] : nullptr, p};
     const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
     stokes_reduce(h, 1, a, b, slot);
 }
 template <>
-void reduce_means<float>(lmm_handle* h, float* const u[3], const float* p, int slot) {
-    const float* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
+void reduce_means<float>(lmm_handle* h, float* const u[3], const float* p, int slot, int umask) {
+    const float* a[4] = {(umask & 1) ? u[0] : nullptr, (umask & 2) ? u[1] : nullptr,
+                         (h->dm == 3 && (umask & 4)) ? u[2] : nullptr, p};
     const float* b[4] = {nullptr, nullptr, nullptr, nullptr};
     const int tile[3] = {1024000, 8, 8};
     double w[3];
@@ -955,7 +959,8 @@ void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x
         throw LmmError(LMM_ERR_INVALID);
     }
     // mean removal (apply_precon.f90:433-460)
-    reduce_means<T>(h, x_u, x_p, mean_slot);
+    // only the sums the subtraction uses: p, and the velocity components of the mask
+    reduce_means<T>(h, x_u, x_p, mean_slot, mean_mask(h, theta));
     double tv = 1.0;
     for (int d = 0; d < dm; ++d) tv *= (double)h->grid.n[d];
     launch_sub_means<T>(h->D0, x_u, x_p, rslot(h, mean_slot), tv, mean_mask(h, theta), h->stream);
