@@ -17,8 +17,9 @@ A step is one full solve.  Reported:
           GMRES, FP64) timed on the GPU;
   roofline of the dominant kernel (one Gauss-Seidel smooth of the finest
           level), measured live with CUDA events on the solver's stream;
-  cpu_baseline  the CPU oracle (C++ restatement of the reference algorithm)
-          on a bounded sample of the same solve, rank 0 only;
+  cpu_baseline  the CPU oracle (C++ restatement of the reference algorithm):
+          one full solve of the same problem on every host thread, plus one
+          full 64^3 solve of the same family on one core, rank 0 only;
   learned_stage  the same mixed method with the learned correction stage
           (network trained on the GPU before the timed region, on 64^3
           problems of this workload's family) -- measured beside `value`,
@@ -28,7 +29,7 @@ A step is one full solve.  Reported:
 N > 1 GPUs: replicas only (one independent solve per GPU, a different seed
 per rank, no collective on the data path); value = total solves / max time.
 `--impl reference` times the CPU oracle (the reference Fortran cannot be
-built on this machine) on the same workload.
+built on this machine) on the same workload: every step one full solve.
 """
 from __future__ import annotations
 
@@ -182,19 +183,24 @@ def sum_over_ranks(world, v):
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-def cpu_sample(prob, sample_iters: int, full_precon_applications: int, knobs_kw: dict):
-    """Time the oracle's reference GMRES on `sample_iters` inner iterations of
-    the same solve and scale to a full solve by preconditioner applications
-    (the V-cycles dominate both codes)."""
+def cpu_solve(prob, knobs_kw: dict, threads: int | None = None):
+    """Time one full solve of `prob` by the CPU oracle (the C++ restatement of
+    the reference's left-preconditioned GMRES, FP64) with `threads` OpenMP
+    threads (None: all).  Returns (seconds, stats)."""
     from oracle import oracle as O
-    k = O.default_knobs(**knobs_kw, gmres_max_iter=sample_iters)
-    t0 = time.perf_counter()
-    rc, _, _, _, _, st = O.solve(prob, k)
-    dt = time.perf_counter() - t0
-    # applications in the sample: |M^-1 b|, one per restart residual, one per inner iteration
-    sample_apps = 1 + (st["outer_iter"] + 1) + st["total_iter"]
-    solve_s = dt * full_precon_applications / sample_apps
-    return dt, sample_apps, solve_s
+    O.build()
+    if threads is not None:
+        O.set_threads(threads)
+    try:
+        t0 = time.perf_counter()
+        rc, _, _, _, _, st = O.solve(prob, O.default_knobs(**knobs_kw))
+        dt = time.perf_counter() - t0
+    finally:
+        if threads is not None:
+            O.set_threads(omp_threads())
+    if rc < 0:
+        raise RuntimeError(f"oracle solve failed with status {rc}")
+    return dt, st
 
 
 def omp_threads():
@@ -204,33 +210,36 @@ def omp_threads():
         return os.cpu_count()
 
 
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args, world, rank):
+    """Every step is one full oracle solve of the benchmark problem on all
+    host threads (nothing extrapolated)."""
     if rank != 0:
         return
     from lowmachmixtures_b200 import synth
-    from oracle import oracle as O
-    O.build()
     prob = synth.config_3d_128(0, n=args.n)
     kn = dict(precon_type=2, visc_type=-2)
-    # calibration: the oracle's preconditioner applications for the full solve
-    # come from one full solve on a 2x smaller grid of the same family (the
-    # iteration count of this multigrid-preconditioned GMRES varies little
-    # between 64^3 and 128^3)
-    calib = synth.config_3d_128(0, n=max(16, args.n // 2))
-    _, _, _, _, _, stc = O.solve(calib, O.default_knobs(**kn))
-    full_apps = 1 + (stc["outer_iter"] + 1) + stc["total_iter"]
-    sample_iters = 2
-    times = []
+    times, iters = [], []
     for s in range(args.warmup + args.steps):
-        dt, apps, solve_s = cpu_sample(prob, sample_iters, full_apps, kn)
+        dt, st = cpu_solve(prob, kn)
         if s >= args.warmup:
-            times.append(solve_s)
+            times.append(dt)
+            iters.append(st["total_iter"])
     solve_s = sum(times) / len(times)
     v = 1.0 / solve_s
     cores = omp_threads()
-    sample = (f"{sample_iters} GMRES iterations ({apps} preconditioner applications) of the {args.n}^3 solve per step, "
-              f"scaled to a full solve's {full_apps} applications (counted on the {calib.n[0]}^3 solve)")
+    sample = (f"one full solve of the {args.n}^3 problem per step (reference GMRES(5) to the reference stop rule, "
+              f"{iters[-1]} iterations), {cores} threads of {cpu_model()}")
     line = {
         "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -238,6 +247,7 @@ def run_reference(args, world, rank):
         "config": {"workload": f"stokes_3d_{args.n}^3_inertial_contrast100", "precon_type": 2,
                    "method": "reference GMRES(5), FP64 (CPU oracle restating the Fortran; the Fortran itself "
                              "cannot be built: no Fortran compiler, BoxLib not vendored)"},
+        "iterations": iters, "seconds_per_solve": times,
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -400,12 +410,22 @@ def run_product(args, world, rank, local):
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        full_apps = 1 + st_ref[-1]["outer_iter"] + 1 + st_ref[-1]["total_iter"]
-        dt, apps, solve_s = cpu_sample(prob, 2, full_apps, base)
+        # one full oracle solve of the same problem on every host thread, and
+        # one full solve of the 64^3 problem of the same family on one core
+        # (a 128^3 solve on one core takes minutes)
+        dt, st = cpu_solve(prob, base)
+        prob64 = synth.config_3d_128(rank, n=64)
+        dt1, st1 = cpu_solve(prob64, base, threads=1)
+        dt64, st64 = cpu_solve(prob64, base)
         line["cpu_baseline"] = {
-            "value": 1.0 / solve_s, "unit": "solves/s", "cores": omp_threads(), "kind": "port",
-            "sample": (f"oracle reference GMRES: 2 inner iterations ({apps} preconditioner applications, "
-                       f"{dt:.1f} s) of the same {n}^3 solve, scaled to the full solve's {full_apps} applications")}
+            "value": 1.0 / dt, "unit": "solves/s", "cores": omp_threads(), "kind": "port",
+            "sample": (f"one full oracle solve (reference GMRES(5), FP64) of the same {n}^3 problem: {dt:.1f} s, "
+                       f"{st['total_iter']} iterations, {omp_threads()} threads of {cpu_model()}"),
+            "single_core": {"value": 1.0 / dt1, "unit": "solves/s", "cores": 1, "seconds": dt1,
+                            "iterations": st1["total_iter"],
+                            "sample": "one full oracle solve of the 64^3 problem of the same family on one core"},
+            "all_cores_64": {"value": 1.0 / dt64, "unit": "solves/s", "cores": omp_threads(), "seconds": dt64,
+                             "sample": "the same 64^3 solve on every host thread"}}
     # error of the mixed-precision solution against the FP64 one (same inputs;
     # the FP64 path is bit-for-bit the oracle's arithmetic)
     solve_dev(mixed)

@@ -19,8 +19,13 @@
  *  - dm is 2 or 3, every n[d] >= 1 for d < dm, and the cell count
  *    n[0]*n[1](*n[2]) is at most LMM_NOALLOC_MAX_CELLS; larger grids are
  *    rejected with LMM_ERR_TOO_LARGE before anything is launched.  The
+ *    limit is 2^31 - 1 less one grid-stride (LMM_NOALLOC_MAX_BLOCKS x 256
+ *    threads), so the reduction's 32-bit element index cannot wrap.  The
  *    static scratch holds LMM_NOALLOC_MAX_BLOCKS partial sums of 4
  *    components (about 19 KB), which every accepted size fits.
+ *  - The scratch address of a device is looked up once and kept for the
+ *    life of the process; do not call this entry point on a device after
+ *    resetting it (cudaDeviceReset), which unloads the module.
  *  - The first call on a device does that device's set-up (the library's
  *    device module is loaded if it is not yet, and the scratch address is
  *    looked up); make that first call before any stream capture.
@@ -35,7 +40,8 @@
  *    p_norm_weight^2 * cell sum; out_host[5] = sqrt of that for a == b.
  *    out_host must hold 6 doubles.
  * Returns LMM_OK, LMM_ERR_INVALID (bad dm, n or pointer), LMM_ERR_TOO_LARGE,
- * LMM_ERR_NO_DEVICE or LMM_ERR_CUDA. */
+ * LMM_ERR_NO_DEVICE or LMM_ERR_CUDA; on an error lmm_strerror names the
+ * failing check or CUDA call. */
 #ifndef LMM_NOALLOC_H
 #define LMM_NOALLOC_H
 
@@ -46,8 +52,8 @@ extern "C" {
 #endif
 
 #define LMM_ERR_TOO_LARGE      -7  /* grid larger than a fixed-size entry point accepts */
-#define LMM_NOALLOC_MAX_CELLS  2147483647LL
 #define LMM_NOALLOC_MAX_BLOCKS 592
+#define LMM_NOALLOC_MAX_CELLS  (2147483647LL - LMM_NOALLOC_MAX_BLOCKS * 256LL)  /* 2147332095 */
 
 int lmm_inner_prod_noalloc(int dm, const int n[3], const double* const a_u[3], const double* a_p,
                            const double* const b_u[3], const double* b_p, double p_norm_weight,

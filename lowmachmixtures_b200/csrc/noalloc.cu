@@ -12,9 +12,14 @@
 
 #include <cstdint>
 #include <mutex>
+#include <string>
 
 #include "kernels.cuh"
 #include "../../include/lmm_noalloc.h"
+
+namespace lmm {
+void set_last_error(const std::string& what);  // solver.cu
+}
 
 namespace {
 
@@ -30,16 +35,37 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 NoallocScratch* g_addr[kMaxDevices] = {};
 
+// a failed CUDA call: its text becomes the calling thread's lmm_strerror message
+int cuda_failed(const char* call, cudaError_t e) {
+    lmm::set_last_error(std::string("lmm_inner_prod_noalloc: ") + call + ": " + cudaGetErrorString(e));
+    return LMM_ERR_CUDA;
+}
+
 // Set-up, once per device with that device current: the address of the
-// static scratch in this device's copy of the module.
+// static scratch in this device's copy of the module.  The address is kept
+// for the life of the process; a device reset (cudaDeviceReset) unloads the
+// module and invalidates it, so a process that resets a device must not call
+// this entry point on that device again.
 int scratch_address(NoallocScratch** out) {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess) return LMM_ERR_NO_DEVICE;
-    if (dev < 0 || dev >= kMaxDevices) return LMM_ERR_INVALID;
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        lmm::set_last_error(std::string("lmm_inner_prod_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+        return LMM_ERR_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        lmm::set_last_error("lmm_inner_prod_noalloc: device ordinal above 63");
+        return LMM_ERR_INVALID;
+    }
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_addr[dev]) {
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return LMM_ERR_CUDA;
+        const cudaError_t es = cudaGetSymbolAddress(&p, g_scratch);
+        if (es != cudaSuccess) return cuda_failed("cudaGetSymbolAddress", es);
+        if (!p) {
+            lmm::set_last_error("lmm_inner_prod_noalloc: cudaGetSymbolAddress returned no address");
+            return LMM_ERR_CUDA;
+        }
         g_addr[dev] = static_cast<NoallocScratch*>(p);
     }
     *out = g_addr[dev];
@@ -52,15 +78,26 @@ extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* cons
                                       const double* const b_u[3], const double* b_p, double p_norm_weight, void* stream,
                                       double* out_host) {
     using namespace lmm;
-    if ((dm != 2 && dm != 3) || !n || !a_u || !b_u || !a_p || !b_p || !out_host) return LMM_ERR_INVALID;
+    if ((dm != 2 && dm != 3) || !n || !a_u || !b_u || !a_p || !b_p || !out_host) {
+        lmm::set_last_error("lmm_inner_prod_noalloc: dm must be 2 or 3 and every pointer non-null");
+        return LMM_ERR_INVALID;
+    }
     int64_t cells = 1;
     for (int d = 0; d < dm; ++d) {
-        if (n[d] < 1) return LMM_ERR_INVALID;
+        if (n[d] < 1) {
+            lmm::set_last_error("lmm_inner_prod_noalloc: every n[d] must be at least 1");
+            return LMM_ERR_INVALID;
+        }
         cells *= n[d];
         if (cells > LMM_NOALLOC_MAX_CELLS) return LMM_ERR_TOO_LARGE;
     }
     for (int d = 0; d < dm; ++d)
-        if (!a_u[d] || !b_u[d]) return LMM_ERR_INVALID;
+        if (!a_u[d] || !b_u[d]) {
+            lmm::set_last_error("lmm_inner_prod_noalloc: a face-array pointer is null");
+            return LMM_ERR_INVALID;
+        }
+    // reduce_blocks never returns more than LMM_NOALLOC_MAX_BLOCKS today; the
+    // check keeps the fixed scratch safe should that clamp ever change
     const int nblocks = reduce_blocks(cells);
     if (nblocks > LMM_NOALLOC_MAX_BLOCKS) return LMM_ERR_TOO_LARGE;
 
@@ -78,16 +115,18 @@ extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* cons
     // each periodic seam face is stored once and weighed 1.5 per stored copy
     // in the reference's two copies (as lmm_op_inner_prod)
     const double w = 3.0;
-    if (cudaMemsetAsync(&scr->counter, 0, sizeof(unsigned), s) != cudaSuccess) return LMM_ERR_CUDA;
+    cudaError_t e = cudaMemsetAsync(&scr->counter, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return cuda_failed("cudaMemsetAsync", e);
     if (dm == 2)
         k_reduce<double, 2, 0><<<nblocks, kThreads, 0, s>>>(D, a_u[0], a_u[1], nullptr, a_p, b_u[0], b_u[1], nullptr, b_p, w, w, w,
                                                              p_norm_weight, scr->partials, &scr->counter, scr->out);
     else
         k_reduce<double, 3, 0><<<nblocks, kThreads, 0, s>>>(D, a_u[0], a_u[1], a_u[2], a_p, b_u[0], b_u[1], b_u[2], b_p, w, w, w,
                                                              p_norm_weight, scr->partials, &scr->counter, scr->out);
-    if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_failed("k_reduce launch", e);
     count_launch();
-    if (cudaMemcpyAsync(out_host, scr->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return LMM_ERR_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return LMM_ERR_CUDA;
+    if ((e = cudaMemcpyAsync(out_host, scr->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_failed("cudaMemcpyAsync", e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_failed("cudaStreamSynchronize", e);
     return LMM_OK;
 }

@@ -14,6 +14,7 @@
 // reads one Hessenberg column per inner iteration to run the Givens
 // rotations and the stopping tests exactly as the reference does.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -40,6 +41,17 @@ using namespace lmm;
 namespace {
 
 thread_local std::string g_last_error;
+
+// NVTX range over one phase of a solve (solve, Krylov cycle, Arnoldi column,
+// preconditioner, V-cycle, pressure solve, learned stage); a profiler shows
+// them on the host timeline, and they cost one call each when none is
+// attached
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // LMM_DEBUG set in the environment: every launch is followed by a
 // synchronisation of the solving thread's stream (outside graph capture),
@@ -105,6 +117,12 @@ int compute_nlevs(const int n[3], int dm, int minwidth) {
 }
 
 }  // namespace
+
+namespace lmm {
+// the calling thread's message for lmm_strerror, for entry points defined
+// outside this file
+void set_last_error(const std::string& what) { g_last_error = what; }
+}  // namespace lmm
 
 // ============================================================ handle
 struct lmm_handle {
@@ -592,6 +610,7 @@ int tail_start(lmm_handle* h, const std::vector<LevelDev<T>>& L, int nl, bool st
 
 template <class T>
 void vcycle(lmm_handle* h, std::vector<LevelDev<T>>& L) {
+    NvtxRange nvtx_("stag_mg V-cycle");
     const lmm_knobs& K = h->knobs;
     const int nl = h->nlev;
     const int lc = tail_start<T>(h, L, nl, true);
@@ -695,6 +714,7 @@ void cc_smooth(lmm_handle* h, LevelDev<T>& L, int nsweeps) {
 // phi (L[0].pphi) <- mg_max_vcycles V-cycles of div(a grad phi) = L[0].prhs
 template <class T>
 void macproject(lmm_handle* h) {
+    NvtxRange nvtx_("macproject (pressure V-cycle)");
     auto& L = levels<T>(h);
     const lmm_knobs& K = h->knobs;
     const int nl = h->nlev_p;
@@ -835,6 +855,7 @@ void visc_schur(lmm_handle* h, T* mac, T* x_p) {
 // may alias the level-0 rhs / phi arrays of the hierarchy).
 template <class T>
 void apply_precon(lmm_handle* h, const T* const b_u[3], const T* b_p, T* const x_u[3], T* x_p) {
+    NvtxRange nvtx_("apply_precon");
     const lmm_knobs& K = h->knobs;
     const int dm = h->dm;
     const int64_t n = h->n;
@@ -1095,6 +1116,7 @@ void push_hist(lmm_stats* st, double v) {
 // (slots 1..i+1) and the copy of those slots to the host, then -- after the
 // caller has enqueued whatever may run meanwhile -- wait for the copy only.
 void arnoldi_column_enqueue(lmm_handle* h, int i) {
+    NvtxRange nvtx_("arnoldi column (MGS)");
     const int64_t len = h->w.size();
     for (int k = 1; k <= i; ++k) {
         stokes_dot(h, h->w, h->V[k - 1], k);
@@ -1125,6 +1147,7 @@ void arnoldi_column(lmm_handle* h, int i, std::vector<double>& col) {
 // (entry 4), |w| into slot i+1 (entry 5); on a batch handle one of each per
 // problem (slot arrays, stride batch * 8 between slots).
 void cgs_column(lmm_handle* h, int i) {
+    NvtxRange nvtx_("arnoldi column (CGS)");
     const int64_t len = h->w.size();
     const int64_t ss = h->batched ? (int64_t)h->batch * 8 : 8;
     const int64_t N = h->batched ? h->n : 0, ni = h->batched ? (int64_t)h->D0.nx * h->D0.ny : 0;
@@ -1159,6 +1182,7 @@ void arnoldi_column_cgs_enqueue(lmm_handle* h, int i) {
 
 // ------------------------------------------------------------ the reference GMRES
 int run_gmres(lmm_handle* h, double* theta_alpha, double* norm_pre_rhs, lmm_stats* st) {
+    NvtxRange nvtx_("gmres");
     const lmm_knobs& K = h->knobs;
     const int m = K.gmres_max_inner;
     const int64_t len = h->b.size();
@@ -1282,6 +1306,7 @@ int run_gmres(lmm_handle* h, double* theta_alpha, double* norm_pre_rhs, lmm_stat
 // otherwise c = 0 and the plain V-cycle result stands.  Mode 2 computes the
 // correction but never accepts it (the stage's cost without its effect).
 void learned_stage(lmm_handle* h, const SVec& c, const SVec& v, int mode) {
+    NvtxRange nvtx_("learned stage");
     const int64_t len = v.size();
     const int S1 = lmm_handle::kLrnSlot, S2 = S1 + 1, S3 = S1 + 2;
     launch_lin(h->lr1.base, v.base, -1.0, h->w.base, len, h->stream);
@@ -1311,6 +1336,7 @@ void learned_stage(lmm_handle* h, const SVec& c, const SVec& v, int mode) {
 }
 
 int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
+    NvtxRange nvtx_("fgmres");
     const lmm_knobs& K = h->knobs;
     const int m = K.gmres_max_inner;
     const int64_t len = h->b.size();
@@ -1471,6 +1497,7 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
 // partition and sum each instance as they would one problem).  An instance that has stopped rides along: its
 // columns are computed and not used, its update coefficients are zero.
 int run_fgmres_batch(lmm_handle* h, int count, lmm_stats* stats, int* status) {
+    NvtxRange nvtx_("fgmres batch");
     const lmm_knobs& K = h->knobs;
     const int m = K.gmres_max_inner, B = h->batch, ni = h->D0.nx * h->D0.ny;
     const int64_t n = h->n, len = h->b.size();
@@ -2062,6 +2089,7 @@ extern "C" int lmm_stokes_solve_device(lmm_handle* h, const lmm_fields_in* in, l
     if (!h || h->batched || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
     if (in->layout != LMM_LAYOUT_COMPACT || out->layout != LMM_LAYOUT_COMPACT) return LMM_ERR_INVALID;
     g_last_error.clear();
+    NvtxRange nvtx_("lmm_stokes_solve_device");
     try {
         LMM_CK(cudaSetDevice(h->device));
         if (st) std::memset(st, 0, sizeof(*st));
@@ -2090,6 +2118,7 @@ extern "C" int lmm_stokes_solve(lmm_handle* h, const lmm_fields_in* in, lmm_fiel
                                 double* norm_pre_rhs, lmm_stats* st) {
     if (!h || h->batched || !in || !out || !theta_alpha) return LMM_ERR_INVALID;
     g_last_error.clear();
+    NvtxRange nvtx_("lmm_stokes_solve");
     const int dm = h->dm;
     const int64_t n = h->n;
     const Dims& D = h->D0;

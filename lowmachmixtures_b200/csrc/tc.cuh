@@ -178,10 +178,21 @@ __device__ bool gemm_tile(const Gather& G, const Epi& E, int m0, int N, int K, u
         }
         issued = c + 1;
     }
-    // every MMA of this tile is complete once the last commit has arrived
-    // (also waited for, within the bound, when the loop stopped early)
-    if (issued > 0 && !mbar_wait(&bars[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
-    ok = __syncthreads_and(ok);
+    // Every MMA of this tile is complete once the last commit has arrived
+    // (MMAs complete in issue order and a commit tracks all earlier ones).
+    // It is waited for also when the loop stopped early; a wait that gives
+    // up is followed by one more bounded wait, so TMEM is freed below only
+    // after the tile's MMAs have drained or two full bounds have passed.
+    // Freeing it even then is deliberate: a CTA that exits holding TMEM
+    // leaves the next CTA on its SM blocked in tcgen05.alloc, and the error
+    // flag makes the host discard every result of this launch.
+    bool drained = true;
+    if (issued > 0) {
+        const unsigned par = ((issued - 1) >> 1) & 1;
+        drained = mbar_wait(&bars[(issued - 1) & 1], par);
+        if (!drained) drained = mbar_wait(&bars[(issued - 1) & 1], par);
+    }
+    ok = __syncthreads_and(ok && drained);
     if (ok) {
         tc_fence_after();
         const int row = m0 + 32 * warp + lane;

@@ -10,8 +10,10 @@
 ! per grid and knob set and rebuilt when either changes.
 !
 ! Restrictions of the library (checked at run time, status -1): one level,
-! one box (max_grid_size >= n_cells), periodic in every direction,
-! visc_schur_approx = 0.
+! one box (max_grid_size >= n_cells); each direction periodic or bounded by
+! walls on both sides (no-slip 100-103 or slip 200-203, from
+! the_bc_tower%domain_bc); on a grid with walls, visc_schur_approx = 0 and no
+! learned stage.
 module gmres_module
 
   use iso_c_binding

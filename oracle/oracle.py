@@ -195,3 +195,9 @@ def macproject(prob, knobs, mac_rhs, alpha_fc=None):
                               abi.ptr(phi))
     assert rc == 0
     return phi
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads of the oracle's parallel loops (the CPU-baseline legs
+    time it on one core and on all)."""
+    lib().omp_set_num_threads(int(n))

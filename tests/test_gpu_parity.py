@@ -257,6 +257,33 @@ def test_gmres_parity_3d_inertial(oracle, pt):
     _assert_solution_parity(ref, got)
 
 
+@pytest.mark.parametrize("method", [0, 1])
+def test_gmres_parity_bench_workload_128(oracle, method):
+    """The solve the benchmark times, at its full size: 3D 128^3 periodic,
+    contrast 100, theta alpha dx^2 = 0.1, precon_type 2, visc_type -2, the
+    seed-0 problem.  The reference's left-preconditioned GMRES (method 0)
+    and FP64 FGMRES (method 1) each match the oracle's solve of the same
+    method within 1e-10 in velocity and mean-removed pressure, iterations
+    +-1 (gmres.f90:30-477, apply_precon.f90:197-279)."""
+    prob = synth.config_3d_128(0)
+    assert prob.n[:3] == (128, 128, 128)
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2, method=method)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
+    if method == 1:
+        assert got[5]["norm_resid_true"] <= 1e-9 * got[5]["norm_b"]
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_gmres_parity_64_steady_contrast_1000(oracle, method):
+    """A problem of the learned-preconditioner family: 3D 64^3, steady
+    (theta = 0), viscosity contrast 1000."""
+    prob = synth.config_3d_64_learned(7, contrast=1000.0)
+    ref, got = _solve_both(oracle, prob, precon_type=2, visc_type=-2, method=method)
+    assert ref[0] == got[0] == 0
+    _assert_solution_parity(ref, got)
+
+
 @pytest.mark.parametrize("visc", [-1, -3, 1])
 def test_gmres_parity_other_visc_types(oracle, visc):
     prob = synth.make_problem(2, 32, 20.0, 3, theta_alpha=100.0, gamma_value=0.25)
