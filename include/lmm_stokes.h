@@ -143,6 +143,13 @@ typedef struct lmm_knobs {
     int    ensemble_batch;         /* lmm_ensemble_*: 0 = 2D problems whose knobs allow it are solved
                                       in batches (lmm_stokes_create_batch), -1 = always the worker
                                       pool of one-problem handles; a solver handle ignores it */
+    int    smoother_tma;           /* 3D Gauss-Seidel (smoother_fusion = 0): 0 = default (both colours
+                                      of a component in one launch, operands staged in shared memory
+                                      by TMA, on the periodic levels that allow it with at least
+                                      smoother_tma_cells cells), -1 = never, k > 0 = the same with k
+                                      rows of faces per tile */
+    int    smoother_tma_slabs;     /* k-slabs of that launch; 0 = about one CTA per SM */
+    int    smoother_tma_cells;     /* smallest level (cells) that uses it; 0 = default (32^3) */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -1461,6 +1461,10 @@ void launch_div_mul(const LevelDev<T>& L, const T* const l[3], const T* const m[
         k_div_mul<T, 3><<<gg.grid, gg.block, 0, s>>>(L.D, l[0], l[1], l[2], m[0], m[1], m[2], out, dxinv);
 }
 
+}  // namespace lmm
+#include "gs_tma.cuh"
+namespace lmm {
+
 #define LMM_INSTANTIATE(T)                                                                                                     \
     template void launch_applyop<T>(const LevelDev<T>&, int, const T* const[3], T* const[3], cudaStream_t, int);              \
     template void launch_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t);     \
@@ -1487,6 +1491,9 @@ void launch_div_mul(const LevelDev<T>& L, const T* const l[3], const T* const m[
     template void launch_recip<T>(const T*, T*, int64_t, cudaStream_t);                                                        \
     template void launch_fill<T>(T*, double, int64_t, cudaStream_t);                                                           \
     template void launch_reduce<T>(const Dims&, int, const T* const[4], const T* const[4], const double[3], double,            \
-                                   double*, unsigned*, double*, int, cudaStream_t, int);
+                                   double*, unsigned*, double*, int, cudaStream_t, int);                                      \
+    template bool gs_tma_supported<T>(const LevelDev<T>&, int, int, int);                                                     \
+    template cudaError_t launch_gs_pair_tma<T>(const LevelDev<T>&, int, int, const T* const[3], const T* const[3], T*, double, \
+                                               int, int, int*, cudaStream_t);
 
 }  // namespace lmm

@@ -57,6 +57,17 @@ bool gs_pair_supported(const LevelDev<T>& L, int kc);
 template <class T>
 void launch_gs_pair(const LevelDev<T>& L, int visc, int comp, const T* const rhs[3], const T* const cur[3], T* out, double omega,
                     int kc, cudaStream_t s);
+// Both Gauss-Seidel colours of component comp in one launch whose operands
+// are staged in shared memory by TMA tensor copies, marching through
+// k-slabs (gs_tma.cuh); out of place like launch_gs_pair.  Periodic 3D
+// levels with even sizes and rows of at most 256 faces (gs_tma_supported).
+// ty_req / slabs_req > 0 force the rows per tile / the k-slabs; *err is set
+// when a bounded wait of the kernel gave up.
+template <class T>
+bool gs_tma_supported(const LevelDev<T>& L, int visc, int ty_req, int slabs_req);
+template <class T>
+cudaError_t launch_gs_pair_tma(const LevelDev<T>& L, int visc, int comp, const T* const rhs[3], const T* const cur[3], T* out,
+                               double omega, int ty_req, int slabs_req, int* err, cudaStream_t s);
 template <class T>
 void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const phi_in[3], T* const phi_out[3],
                    double omega, cudaStream_t s);

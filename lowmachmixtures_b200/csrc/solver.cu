@@ -192,6 +192,10 @@ struct lmm_handle {
     float* lz32 = nullptr;
     int* luses = nullptr;  // [accepted, tried] of the current solve
     static constexpr int kLrnSlot = 250;
+    // error word of the kernels with bounded waits (the TMA smoother): set
+    // on the device when a wait gave up, read and cleared after each solve
+    int* dev_err = nullptr;
+    bool tma_smoother = false;  // a level of this handle runs the TMA smoother
     // a batch of 2D problems (lmm_stokes_create_batch): `batch` instances of
     // one grid stacked along the third index of every array (D0.nz = batch);
     // per-instance scalars in slot arrays of batch x 8 doubles
@@ -324,6 +328,7 @@ size_t plan_bytes(const lmm_grid& g, const lmm_knobs& k, int nlev, int nlev_p, i
     add(vec, sizeof(float));
     add(partials_count(g, batch), sizeof(double));  // reduction partials
     add(std::max(64, batch), sizeof(unsigned));
+    add(64, sizeof(int));  // error word of the kernels with bounded waits
     add(8 * lmm_handle::kSlots, sizeof(double));
     // BoxLib staging: the largest field with up to 4 ghost layers
     int64_t st = 1;
@@ -552,9 +557,35 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
 }
 
 // ------------------------------------------------------------ staggered V-cycle
+// the level runs both colours of each component in one TMA-staged launch
+template <class T>
+bool use_tma_smoother(const lmm_handle* h, const LevelDev<T>& L) {
+    const lmm_knobs& K = h->knobs;
+    const int64_t min_cells = K.smoother_tma_cells > 0 ? K.smoother_tma_cells : 32768;
+    return K.stag_mg_smoother != 0 && K.smoother_fusion == 0 && K.smoother_tma >= 0 && h->dm == 3 && !h->batched &&
+           L.n >= min_cells && gs_tma_supported<T>(L, K.visc_type, K.smoother_tma, K.smoother_tma_slabs);
+}
+
 template <class T>
 void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
     const lmm_knobs& K = h->knobs;
+    if (nsm > 0 && use_tma_smoother<T>(h, L)) {
+        h->tma_smoother = true;
+        // TMA-staged colour pairs, ping-ponging each component between phi and tmp
+        T* cur[3] = {L.phi[0], L.phi[1], L.phi[2]};
+        T* alt[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
+        for (int m = 0; m < nsm; ++m)
+            for (int d = 0; d < 3; ++d) {
+                LMM_CK(launch_gs_pair_tma<T>(L, K.visc_type, d, L.rhs, cur, alt[d], K.stag_mg_omega, K.smoother_tma,
+                                             K.smoother_tma_slabs, h->dev_err, h->stream));
+                check_launch();
+                std::swap(cur[d], alt[d]);
+            }
+        if (cur[0] != L.phi[0])
+            for (int d = 0; d < 3; ++d)
+                LMM_CK(cudaMemcpyAsync(L.phi[d], cur[d], L.n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+        return;
+    }
     if (K.stag_mg_smoother != 0 && K.smoother_fusion > 0 && nsm > 0 && gs_pair_supported<T>(L, K.smoother_fusion)) {
         // fused colour pairs, ping-ponging each component between phi and tmp
         T* cur[3] = {L.phi[0], L.phi[1], L.phi[2]};
@@ -1897,6 +1928,7 @@ static int create_impl(const lmm_grid* g, const lmm_knobs* k, int device, int ba
         h->red_blocks = reduce_blocks(batched ? (int64_t)g->n[0] * g->n[1] : h->n);
         h->partials = h->alloc<double>(partials_count(*g, batch));
         h->counter = h->alloc<unsigned>(std::max(64, batch));
+        h->dev_err = h->alloc<int>(64);
         h->scal = h->alloc<double>(8 * lmm_handle::kSlots);
         int64_t st = 1;
         for (int d = 0; d < dm; ++d) st *= (g->n[d] + 1 + 8);
@@ -1962,7 +1994,8 @@ int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
                       SAME(stag_mg_max_bottom_nlevels) && SAME(stag_mg_omega) && SAME(stag_mg_smoother) &&
                       SAME(gmres_max_inner) && SAME(visc_type) && SAME(method) && SAME(precision) &&
                       SAME(learned_stage) && SAME(tail_cells) && SAME(tail_smem_kb) && SAME(use_graphs) &&
-                      SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait);
+                      SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait) &&
+                      SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells);
 #undef SAME
     if (!same) {
         g_last_error = "lmm_stokes_update_knobs changes only the stopping rules; create a new handle for the rest";
@@ -2072,6 +2105,17 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
     load_coeffs(h, al, beta, bed, gamma, theta);
     h->pvcycles = 0;
     int rc = (K.method == LMM_METHOD_FGMRES) ? run_fgmres(h, norm_pre_rhs, st) : run_gmres(h, theta_alpha, norm_pre_rhs, st);
+    if (h->tma_smoother && rc != LMM_ERR_WATCHDOG) {
+        // a bounded wait of the TMA smoother that gave up makes the solve an error
+        int* herr = reinterpret_cast<int*>(h->hscal + 8 * (lmm_handle::kSlots - 1));
+        LMM_CK(cudaMemcpyAsync(herr, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(host_wait(h));
+        if (*herr != 0) {
+            LMM_CK(cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream));
+            g_last_error = "a bounded wait of the TMA Gauss-Seidel smoother gave up";
+            return LMM_ERR_WATCHDOG;
+        }
+    }
     if (sf != 1.0) {
         theta = theta / sf;
         launch_scale_copy<double>(h->x.p(), h->x.p(), 1.0 / sf, n, h->stream);

@@ -157,6 +157,59 @@ def test_vcycle_fused_smoother_bit_exact(oracle, n, visc, fusion):
     s.close()
 
 
+# (rows per tile, k-slabs): 0 = the library's choice; tiles whose rows wrap
+# around the periodic y boundary, one-tile rows (TY = n) and slabs of one
+# plane are all among them.  FP64 tilings instantiated per row length:
+TMA_FP64 = {128: (4,), 64: (8, 4), 32: (8, 16)}
+TMA_TILINGS = [(0, 0), (8, 1), (8, 5), (4, 16), (16, 3)]
+
+
+@pytest.mark.parametrize("n", [32, 64])
+@pytest.mark.parametrize("visc", [-1, -2, -3])
+@pytest.mark.parametrize("tiling", TMA_TILINGS)
+def test_vcycle_tma_smoother_bit_exact(oracle, n, visc, tiling):
+    """Both Gauss-Seidel colours of a component in one launch with every
+    operand staged in shared memory by TMA, marching through k-slabs,
+    reproduce the reference's colour-by-colour smoother bit for bit
+    (stag_mg_solver.f90:363-401) inside a whole V-cycle."""
+    ty, slabs = tiling
+    if ty and ty not in TMA_FP64[n]:
+        pytest.skip("tiling not instantiated for this row length")
+    p, rng = random_problem(3, n, 19, visc, theta=3.0)
+    kn = dict(visc_type=visc)
+    k = oracle.default_knobs(**kn)
+    s = make_solver(p, **kn, tail_cells=-1, smoother_tma=ty, smoother_tma_slabs=slabs, smoother_tma_cells=1)
+    rhs = [rng.standard_normal(p.shape) for _ in range(3)]
+    ref = oracle.stag_mg_solver(p, k, rhs)
+    phi = [dev(np.zeros(p.shape)) for _ in range(3)]
+    s.stag_mg_solver([dev(a) for a in rhs], phi)
+    for c in range(3):
+        np.testing.assert_array_equal(host(phi[c]), ref[c])
+    s.close()
+
+
+def test_tma_smoother_fp32_solve_matches_colour_launches():
+    """The mixed method with the TMA smoother on its FP32 levels and with one
+    launch per colour: both reach the FP64 tolerance, the same iteration
+    count within one and solutions within 1e-8 of each other (FP32
+    preconditioners, no bit parity asked)."""
+    from lowmachmixtures_b200.gmres import StokesSolver
+    prob = synth.config_3d_128(5, n=64)
+    outs = []
+    for tma in (0, -1):
+        kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32,
+                            smoother_tma=tma)
+        xu, xp = prob.zeros_like_solution()
+        with StokesSolver(3, (64, 64, 64), prob.dx, knobs=kn) as s:
+            _, _, st = s.solve(prob.b_u, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma,
+                               prob.theta_alpha)
+        assert st["status"] == 0 and st["norm_resid_true"] <= 1e-9 * st["norm_b"]
+        outs.append((st["total_iter"], xu))
+    assert abs(outs[0][0] - outs[1][0]) <= 1
+    for c in range(3):
+        assert np.linalg.norm(outs[0][1][c] - outs[1][1][c]) <= 1e-8 * np.linalg.norm(outs[1][1][c])
+
+
 @pytest.mark.parametrize("dm,n", [(2, 32), (3, 16)])
 @pytest.mark.parametrize("visc", VISCS)
 def test_apply_matrix_bit_exact(oracle, dm, n, visc):
