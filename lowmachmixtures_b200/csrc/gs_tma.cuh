@@ -27,8 +27,10 @@
 //    bytes as transaction count; the plane two steps ahead is requested at
 //    the start of a step, so one plane is always in flight while the CTA
 //    computes.  A tile whose rows wrap around the periodic y boundary
-//    requests its rows one by one (a one-row box per copy) at wrapped
-//    coordinates.
+//    fetches each run of consecutive rows with one contiguous bulk copy
+//    (cp.async.bulk), two or three per array instead of one per row: every
+//    TMA operation has a fixed cost, and one copy per row made those CTAs
+//    the stragglers of the launch.
 //  - Row length and tile rows are compile-time, so every shared-memory
 //    operand is a per-step register plus an immediate offset (see the
 //    thread layout at the kernel).
@@ -150,11 +152,11 @@ struct Args {
     T omega, dxsqinv;
     T* out;
     int* err;
+    const T* src[A_N];   // the staged arrays (rows that wrap in y are fetched by bulk copies)
 };
 
 struct Maps {
     CUtensorMap tile[A_N];   // box: nx x (TY + lo + hi) rows x 1 plane
-    CUtensorMap row[A_N];    // box: nx x 1 row x 1 plane (tiles that wrap in y)
 };
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
@@ -179,6 +181,13 @@ __device__ __forceinline__ bool bar_wait(uint64_t* b, unsigned parity) {
         if (it > 32) __nanosleep(32);
     }
     return false;
+}
+// contiguous bulk load (16-byte aligned addresses, size a multiple of 16)
+// completing on mbarrier b
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(su32(dst)),
+                 "l"(src), "r"(bytes), "r"(su32(b))
+                 : "memory");
 }
 // 3D tile load (x, y, z coordinates in elements) completing on mbarrier b
 __device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* b) {
@@ -276,15 +285,19 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
             for (int a = lane; a < A_N; a += 32)
                 if (staged(VISC, a)) tma_load3(dst0 + G::off(a), &M.tile[a], 0, j0 - rows_lo(COMP, a), p, b);
         } else {
-#pragma unroll 1
-            for (int a = 0; a < A_N; ++a) {
+            // rows that wrap around the periodic y boundary: each run of
+            // consecutive rows of one plane is contiguous in memory, one bulk
+            // copy per run (two, or three when the tile spans every row)
+            for (int a = lane; a < A_N; a += 32) {
                 if (!staged(VISC, a)) continue;
-                const int lo = rows_lo(COMP, a), H = G::rows(a);
-                for (int r = lane; r < H; r += 32) {
-                    int jg = j0 - lo + r;
-                    while (jg < 0) jg += ny;
-                    while (jg >= ny) jg -= ny;
-                    tma_load3(dst0 + G::off(a) + r * NX, &M.row[a], 0, jg, p, b);
+                const int H = G::rows(a);
+                int jg = j0 - rows_lo(COMP, a);
+                while (jg < 0) jg += ny;
+                for (int r = 0; r < H;) {
+                    const int run = min(H - r, ny - jg);
+                    bulk_load(dst0 + G::off(a) + r * NX, A.src[a] + ((int64_t)p * ny + jg) * NX, (uint32_t)(run * NX * sizeof(T)), b);
+                    r += run;
+                    jg = 0;
                 }
             }
         }
@@ -605,10 +618,10 @@ cudaError_t launch_gs_pair_tma(const LevelDev<T>& L, int visc, int comp, const T
     Maps m;
     std::memset(&m, 0, sizeof(m));
     for (int q = 0; q < A_N; ++q) {
+        a.src[q] = arr[q];
         if (!staged(visc, q)) continue;
         const int rows = p.TY + rows_lo(comp, q) + rows_hi(comp, q);
-        cudaError_t e = make_map<T>(&m.tile[q], arr[q], L.D, rows);
-        if (e == cudaSuccess) e = make_map<T>(&m.row[q], arr[q], L.D, 1);
+        const cudaError_t e = make_map<T>(&m.tile[q], arr[q], L.D, rows);
         if (e != cudaSuccess) return e;
     }
     const unsigned blocks = (unsigned)((L.D.ny / p.TY) * p.slabs);

@@ -478,20 +478,79 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
     restrict_cell<T, DM, W, 0>(F, f0, f1, f2, Dc, c0, c1, c2, q.i, q.j, q.k, t);
 }
 
-template <class T, int DM, int VISC>
-__global__ void __launch_bounds__(kThreads) k_residual_restrict(Dims F, Coef<T> C, const T* __restrict__ r0,
-                                                                const T* __restrict__ r1, const T* __restrict__ r2,
-                                                                const T* __restrict__ p0, const T* __restrict__ p1,
-                                                                const T* __restrict__ p2, Dims Dc, T* __restrict__ c0,
-                                                                T* __restrict__ c1, T* __restrict__ c2, T dxsqinv) {
-    const Pos q = pos3(Dc.nx, Dc.ny);
-    if (!q.ok) return;
-    const int comp = q.k % DM, k = q.k / DM;  // grid.z covers nz * DM
-    const int t = q.i + Dc.nx * (q.j + Dc.ny * k);
+// Residual and restriction of one 3D periodic level in one pass
+// (stag_mg_solver.f90:406-437 then stag_restriction, :1133-1171): a block
+// owns RCX x RCY x RCZ coarse cells; it evaluates into shared memory every
+// fine residual r = (L phi - rhs) * -1 that their 12-point restrictions read
+// (the fine faces of the tile plus one face layer on the low and high side
+// normal to each component), then forms the coarse faces from shared memory
+// in restrict_cell's order.  The fine residual never goes to global memory,
+// and each one is evaluated once per block (the 2 x 2 x 2-to-1 stencil
+// overlaps only across the block boundary).
+constexpr int RCX = 8, RCY = 4, RCZ = 4;
+template <int COMP>
+struct RTile {  // fine residuals of one component held by the block
+    static constexpr int NX = 2 * RCX + (COMP == 0 ? 1 : 0);
+    static constexpr int NY = 2 * RCY + (COMP == 1 ? 1 : 0);
+    static constexpr int NZ = 2 * RCZ + (COMP == 2 ? 1 : 0);
+    static constexpr int N = NX * NY * NZ;
+};
+
+template <class T, int VISC>
+__global__ void __launch_bounds__(kThreads) k_resid_restrict3(Dims F, Coef<T> C, const T* __restrict__ r0, const T* __restrict__ r1,
+                                                              const T* __restrict__ r2, const T* __restrict__ p0,
+                                                              const T* __restrict__ p1, const T* __restrict__ p2, Dims Dc,
+                                                              T* __restrict__ c0, T* __restrict__ c1, T* __restrict__ c2,
+                                                              T dxsqinv) {
+    pdl_enter();
+    using X = RTile<0>;
+    using Y = RTile<1>;
+    using Z = RTile<2>;
+    __shared__ T rs[X::N + Y::N + Z::N];
+    const int ci0 = blockIdx.x * RCX, cj0 = blockIdx.y * RCY, ck0 = blockIdx.z * RCZ;
     const T* phi[3] = {p0, p1, p2};
-    const T* rhs[3] = {r0, r1, r2};
-    T* out[3] = {c0, c1, c2};
-    restrict_comp<T, DM, VISC, 0>(comp, F, C, rhs, phi, out, t, q.i, q.j, k, dxsqinv);
+    const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
+    // fine residuals: component x from fine i = 2 ci0 - 1, y from j = 2 cj0 - 1,
+    // z from k = 2 ck0 - 1 (one layer below the tile in its own direction)
+    for (int t = threadIdx.x; t < X::N + Y::N + Z::N; t += kThreads) {
+        if (t < X::N) {
+            const int a = t % X::NX, bb = (t / X::NX) % X::NY, cc = t / (X::NX * X::NY);
+            rs[t] = fine_resid<T, 3, VISC, 0>(F, C, phi, r0, 2 * ci0 - 1 + a, 2 * cj0 + bb, 2 * ck0 + cc, dxsqinv, b, c);
+        } else if (t < X::N + Y::N) {
+            const int u = t - X::N;
+            const int a = u % Y::NX, bb = (u / Y::NX) % Y::NY, cc = u / (Y::NX * Y::NY);
+            rs[t] = fine_resid<T, 3, VISC, 1>(F, C, phi, r1, 2 * ci0 + a, 2 * cj0 - 1 + bb, 2 * ck0 + cc, dxsqinv, b, c);
+        } else {
+            const int u = t - X::N - Y::N;
+            const int a = u % Z::NX, bb = (u / Z::NX) % Z::NY, cc = u / (Z::NX * Z::NY);
+            rs[t] = fine_resid<T, 3, VISC, 2>(F, C, phi, r2, 2 * ci0 + a, 2 * cj0 + bb, 2 * ck0 - 1 + cc, dxsqinv, b, c);
+        }
+    }
+    __syncthreads();
+    constexpr int NC = RCX * RCY * RCZ;
+    for (int t = threadIdx.x; t < 3 * NC; t += kThreads) {
+        const int comp = t / NC, u = t - comp * NC;
+        const int i = u % RCX, j = (u / RCX) % RCY, k = u / (RCX * RCY);
+        // fine index of the coarse face's first fine face inside the block's arrays
+        const int I = 2 * i + (comp == 0 ? 1 : 0), J = 2 * j + (comp == 1 ? 1 : 0), K = 2 * k + (comp == 2 ? 1 : 0);
+        const int out = (ci0 + i) + Dc.nx * ((cj0 + j) + Dc.ny * (ck0 + k));
+        if (comp == 0) {
+            auto R = [&](int ii, int jj, int kk) { return rs[ii + X::NX * (jj + X::NY * kk)]; };
+            c0[out] = T(0.125) * (R(I, J, K) + R(I, J + 1, K) + R(I, J, K + 1) + R(I, J + 1, K + 1)) +
+                      T(0.0625) * (R(I + 1, J, K) + R(I + 1, J + 1, K) + R(I + 1, J, K + 1) + R(I + 1, J + 1, K + 1)) +
+                      T(0.0625) * (R(I - 1, J, K) + R(I - 1, J + 1, K) + R(I - 1, J, K + 1) + R(I - 1, J + 1, K + 1));
+        } else if (comp == 1) {
+            auto R = [&](int ii, int jj, int kk) { return rs[X::N + ii + Y::NX * (jj + Y::NY * kk)]; };
+            c1[out] = T(0.125) * (R(I, J, K) + R(I + 1, J, K) + R(I, J, K + 1) + R(I + 1, J, K + 1)) +
+                      T(0.0625) * (R(I, J + 1, K) + R(I + 1, J + 1, K) + R(I, J + 1, K + 1) + R(I + 1, J + 1, K + 1)) +
+                      T(0.0625) * (R(I, J - 1, K) + R(I + 1, J - 1, K) + R(I, J - 1, K + 1) + R(I + 1, J - 1, K + 1));
+        } else {
+            auto R = [&](int ii, int jj, int kk) { return rs[X::N + Y::N + ii + Z::NX * (jj + Z::NY * kk)]; };
+            c2[out] = T(0.125) * (R(I, J, K) + R(I + 1, J, K) + R(I, J + 1, K) + R(I + 1, J + 1, K)) +
+                      T(0.0625) * (R(I, J, K + 1) + R(I + 1, J, K + 1) + R(I, J + 1, K + 1) + R(I + 1, J + 1, K + 1)) +
+                      T(0.0625) * (R(I, J, K - 1) + R(I + 1, J, K - 1) + R(I, J + 1, K - 1) + R(I + 1, J + 1, K - 1));
+        }
+    }
 }
 
 // --------------------------------------------------------------- prolongation
@@ -1254,8 +1313,14 @@ template <class T>
 void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
                               const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s) {
     if (F.D.wall) return wl_residual_restrict<T>(F, Cc, visc, rhs_f, phi_f, rhs_c, s);
-    // residual on every fine face into F.tmp, then the pure restriction
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
+    if (F.D.dm == 3 && Cc.D.nx % RCX == 0 && Cc.D.ny % RCY == 0 && Cc.D.nz % RCZ == 0 && !odd_level(F.D)) {
+        // residual and restriction in one pass, the residual kept in shared memory
+        const dim3 grid(Cc.D.nx / RCX, Cc.D.ny / RCY, Cc.D.nz / RCZ);
+        LMM_VISC_DISPATCH(visc, launch_pdl(k_resid_restrict3<T, V>, grid, dim3(kThreads), 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv))
+        return;
+    }
+    // residual on every fine face into F.tmp, then the pure restriction
     const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz * F.D.dm);
     if (F.D.dm == 2) {
         LMM_VISC_DISPATCH(visc, launch_pdl(k_residual_c<T, 2, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv))
