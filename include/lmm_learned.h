@@ -39,9 +39,12 @@ int lmm_net_train_step(lmm_net* net, const void* x, const float* target, float l
 /* ---- the stage inside the solver (include lmm_stokes.h for lmm_handle) ----
  * A 3D solver handle can carry a network on its own grid (batch 1 is
  * enough).  With knobs.learned_stage = 1, FGMRES with the FP32
- * preconditioner adds the network's correction after every V-cycle
- * application when it reduces the residual, and keeps the plain V-cycle
- * result otherwise.  set_net(h, NULL) detaches. */
+ * preconditioner adds, after every V-cycle column, a second column: the
+ * network's correction of the residual that V-cycle application leaves,
+ * so the least-squares minimisation runs over both (a correction whose
+ * image adds nothing to the basis is dropped).  learned_stage = 3 adds the
+ * correction to the V-cycle's direction instead, when it lowers the
+ * residual.  set_net(h, NULL) detaches. */
 struct lmm_handle;
 int lmm_stokes_set_net(struct lmm_handle* h, lmm_net* net);
 /* count training pairs from the handle's loaded coefficients (see
@@ -51,7 +54,8 @@ int lmm_learned_make_pairs(struct lmm_handle* h, unsigned long long seed, int co
 /* ratios[0] = |r1| / |r0| after the preconditioner, ratios[1] = |r1 - A c| / |r1|
  * after the network's correction, on one fresh random pair */
 int lmm_learned_eval(struct lmm_handle* h, unsigned long long seed, double* ratios);
-/* corrections accepted / tried in the last solve */
+/* corrections kept / computed in the last solve (learned_stage 1: network
+ * columns kept in the basis / computed; 3: corrections accepted / tried) */
 int lmm_learned_stats(struct lmm_handle* h, int* accepted, int* tried);
 
 /* D[M x N] (FP32, row-major) = A[M x K] * B[N x K]^T with BF16 row-major A

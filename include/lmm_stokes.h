@@ -119,8 +119,12 @@ typedef struct lmm_knobs {
     /* additions of this library */
     int    method;                 /* LMM_METHOD_* */
     int    precision;              /* LMM_PRECISION_* */
-    int    learned_stage;          /* 0 off, 1 network correction after each FP32 V-cycle application
-                                      (3D FGMRES; needs lmm_stokes_set_net) */
+    int    learned_stage;          /* 3D FGMRES with the FP32 preconditioner and a network attached
+                                      by lmm_stokes_set_net: 0 off; 1 the network's correction of
+                                      each V-cycle application's residual is an extra FGMRES
+                                      direction; 2 the same corrections computed and not used (the
+                                      stage's cost alone); 3 the correction added to the V-cycle's
+                                      direction when it lowers the residual */
     int    tail_cells;             /* coarse multigrid levels with at most this many cells run in
                                       one single-block launch; 0 = default (512 for the velocity
                                       V-cycle, 1024 for one 2D problem, 4096 for the pressure
@@ -143,13 +147,16 @@ typedef struct lmm_knobs {
     int    ensemble_batch;         /* lmm_ensemble_*: 0 = 2D problems whose knobs allow it are solved
                                       in batches (lmm_stokes_create_batch), -1 = always the worker
                                       pool of one-problem handles; a solver handle ignores it */
-    int    smoother_tma;           /* 3D Gauss-Seidel (smoother_fusion = 0): 0 = default (both colours
-                                      of a component in one launch, operands staged in shared memory
-                                      by TMA, on the periodic levels that allow it with at least
-                                      smoother_tma_cells cells), -1 = never, k > 0 = the same with k
-                                      rows of faces per tile */
+    int    smoother_tma;           /* 3D Gauss-Seidel (smoother_fusion = 0): 1 = both colours of a
+                                      component in one launch with its operands staged in shared
+                                      memory by TMA, on the periodic levels that allow it with at least
+                                      smoother_tma_cells cells (k >= 2: k rows of faces per tile);
+                                      0 = default (off: one launch per colour), -1 = off */
     int    smoother_tma_slabs;     /* k-slabs of that launch; 0 = about one CTA per SM */
     int    smoother_tma_cells;     /* smallest level (cells) that uses it; 0 = default (32^3) */
+    int    smoother_order;         /* Gauss-Seidel with one launch per colour: 0 = default (consecutive
+                                      launches take the planes in alternating order, each starting
+                                      where the last left its operands in L2), -1 = always in +k order */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

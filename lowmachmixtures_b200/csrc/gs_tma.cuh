@@ -120,7 +120,7 @@ __device__ __forceinline__ T face_diag3_vals(T a, T be, T bm, T E1, T E1p, T E2,
 
 namespace gst {
 
-constexpr int kNS = 4;    // plane slots per staged array
+constexpr int kNS = 4;    // plane sets of the ring (5 where one CTA per SM has the room: Geo::NS)
 constexpr int kRNS = 3;   // red-value plane slots
 constexpr unsigned kSpinLimit = 1u << 22;
 
@@ -223,30 +223,37 @@ struct Geo {
     static constexpr int SS = off(A_N);            // elements of one plane set
     static constexpr int RS = HALF + 1;            // red-value row stride (padded: no bank conflicts)
     static constexpr int RP = (TY + 2) * RS;       // red-value plane
-    static constexpr int THREADS = NX;             // two threads per x-pair: one per row parity
+    static constexpr int THREADS = TY * HALF;      // one thread per face pair of the tile
     static constexpr size_t BAR_BYTES = 128;
     static constexpr size_t SET_BYTES = (size_t)SS * sizeof(T);
-    static constexpr size_t SMEM = BAR_BYTES + kNS * SET_BYTES + (size_t)kRNS * RP * sizeof(T);
+    static constexpr size_t smem_for(int ns) { return BAR_BYTES + ns * SET_BYTES + (size_t)kRNS * RP * sizeof(T); }
+    // plane sets: a fifth (two planes requested ahead instead of one) when
+    // four already leave room for a single CTA per SM and five still fit
+    static constexpr int NS = (smem_for(4) > 113 * 1024 && smem_for(5) <= 227 * 1024) ? 5 : 4;
+    static constexpr size_t SMEM = smem_for(NS);
 };
 
-// Thread layout: thread t handles x-pair q = 16 * warp + lane / 2 and the
-// rows of parity g = lane & 1 of the tile, i.e. a fixed column strip.  In
-// one plane all red (black) faces of a strip sit in the same column
-// (i = 2q + parity of j0 + g + k), so a step computes its column and its two
-// periodic neighbours once, and every shared-memory operand is a per-step
-// register plus a compile-time offset.  Adjacent lanes take the two rows of
-// a pair, whose faces lie in different columns: no bank conflicts.
+// Thread layout: one thread per face pair (i = 2q, 2q + 1) of the tile:
+// thread t takes x-pair q = (t / 2) % (NX / 2) in tile row
+// lj = 2 ((t / 2) / (NX / 2)) + (t & 1).  It updates the black face of its
+// pair in each plane and the red face of its pair; the two ring rows' red
+// faces (rows -1 and TY) go to the threads of rows 0 and 1 as a second
+// item.  In one plane a thread's faces sit in one column (i = 2q + the
+// parity of j + k), so a step computes the column and its two periodic
+// neighbours once, and every shared-memory operand is a per-step register
+// plus a compile-time offset.  Adjacent lanes take the two rows of a pair,
+// whose faces lie in different columns: no bank conflicts.
 template <class T, int VISC, int COMP, int NX, int TY>
-__global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __grid_constant__ Maps M) {
+__global__ void __launch_bounds__(TY * NX / 2, 1) k_gs_pair_tma(const Args<T> A, const __grid_constant__ Maps M) {
     using G = Geo<T, VISC, COMP, NX, TY>;
-    constexpr int HALF = G::HALF, SS = G::SS, RS = G::RS, RP = G::RP;
+    constexpr int HALF = G::HALF, SS = G::SS, RS = G::RS, RP = G::RP, NS = G::NS;
     constexpr int D = COMP;
     constexpr int t1 = (D == 0) ? 1 : 0, t2 = (D == 2) ? 1 : 2;
     constexpr int ex[3] = {1, 0, 0}, ey[3] = {0, 1, 0}, ez[3] = {0, 0, 1};
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
-    T* set = reinterpret_cast<T*>(smem + G::BAR_BYTES);               // kNS plane sets
-    T* red = reinterpret_cast<T*>(smem + G::BAR_BYTES + kNS * G::SET_BYTES);  // kRNS red planes
+    T* set = reinterpret_cast<T*>(smem + G::BAR_BYTES);               // NS plane sets
+    T* red = reinterpret_cast<T*>(smem + G::BAR_BYTES + NS * G::SET_BYTES);  // kRNS red planes
     pdl_enter();
     const int ny = A.D.ny, nz = A.D.nz;
     const int tiles_y = ny / TY;
@@ -257,7 +264,9 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
     const int k0 = slab * kb + (slab < krem ? slab : krem);
     const int dir = A.dir;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane & 1, q = warp * 16 + (lane >> 1);
+    const int q = (tid >> 1) % HALF;
+    const int g = 2 * ((tid >> 1) / HALF) + (tid & 1);   // this thread's tile row
+    const bool ring = g < 2;                              // also a ring row's red face (row -1 + TY + 1 + g)
     const int qp = (q == HALF - 1) ? 0 : q + 1, qm = (q == 0) ? HALF - 1 : q - 1;
     auto plane_of = [&](int L) {
         const int p = (dir > 0) ? (k0 - 2 + L) : (k0 + KZ + 1 - L);
@@ -266,16 +275,16 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
     const bool wraps = (j0 - 2 < 0) || (j0 + TY + 2 > ny);
 
     if (tid == 0) {
-        for (int b = 0; b < kNS; ++b) bar_init(&bars[b], 1);
+        for (int b = 0; b < NS; ++b) bar_init(&bars[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    // warp 0 requests plane L of every staged array into plane set L % kNS
+    // warp 0 requests plane L of every staged array into plane set L % NS
     auto issue = [&](int L) {
         const int p = plane_of(L);
-        T* dst0 = set + (L % kNS) * SS;
-        uint64_t* b = &bars[L % kNS];
+        T* dst0 = set + (L % NS) * SS;
+        uint64_t* b = &bars[L % NS];
         if (lane == 0) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             bar_expect_tx(b, (uint32_t)(SS * sizeof(T)));
@@ -303,8 +312,8 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
         }
     };
     if (warp == 0)
-        for (int L = 0; L < kNS; ++L) issue(L);
-    int issued = kNS;
+        for (int L = 0; L < NS && L <= KZ + 3; ++L) issue(L);
+    int issued = NS < KZ + 4 ? NS : KZ + 4;
 
     const T om = A.omega, dxsqinv = A.dxsqinv;
     bool failed = false;
@@ -353,43 +362,46 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
 
 #pragma unroll 1
     for (int s = 0; s <= KZ + 1; ++s) {
-        if (s >= 1 && s + 3 <= KZ + 3) {
-            if (warp == 0) issue(s + 3);
-            issued = s + 4;
+        // request the plane NS - 2 steps ahead into the set freed by step s - 1
+        if (s >= 1 && s + NS - 1 <= KZ + 3) {
+            if (warp == 0) issue(s + NS - 1);
+            issued = s + NS;
         }
         {
             bool ok = true;
-            for (int L = (s == 0 ? 0 : s + 2); L <= s + 2; ++L) ok = ok && bar_wait(&bars[L % kNS], (L / kNS) & 1);
+            for (int L = (s == 0 ? 0 : s + 2); L <= s + 2; ++L) ok = ok && bar_wait(&bars[L % NS], (L / NS) & 1);
             failed = __syncthreads_or(!ok);
             if (failed) break;
         }
-        // red faces of plane L = s + 1: rows rr = g, g + 2, .. (tile rows -1 .. TY)
+        // red faces of plane L = s + 1: red row rr = g (tile row g - 1), and
+        // for the threads of rows 0 and 1 also rr = TY + g (tile row TY + g - 1)
         {
             const int L = s + 1;
             const int r = plane_of(L);
-            const int sb[3] = {((L - dir) % kNS) * SS, (L % kNS) * SS, ((L + dir) % kNS) * SS};
-            const int par = (j0 + g + 1 + r) & 1;   // red: i + j + k even, j = j0 - 1 + g + 2m
+            const int sb[3] = {((L - dir) % NS) * SS, (L % NS) * SS, ((L + dir) % NS) * SS};
+            const int par = (j0 + g + 1 + r) & 1;   // red: i + j + k even, j = j0 - 1 + g (+ TY, even)
             Cols cl;
             cl.c = 2 * q + par;
             cl.p = (cl.c == NX - 1) ? 0 : cl.c + 1;
             cl.m = (cl.c == 0) ? NX - 1 : cl.c - 1;
             T* rs = red + (L % kRNS) * RP + g * RS + q;
 #pragma unroll
-            for (int m = 0; m < (TY + 2) / 2; ++m) {
-                const int rowoff = g + 2 * m - 1;   // tile row lj of this face
+            for (int m = 0; m < 2; ++m) {
+                if (m == 1 && !ring) break;
+                const int rowoff = g - 1 + m * TY;   // tile row lj of this face
                 const T p0 = op(set, A_P, 0, 0, 0, sb, cl, rowoff);
                 const T nb[6] = {op(set, A_P, 0, 0, 1, sb, cl, rowoff), op(set, A_P, 0, 0, -1, sb, cl, rowoff),
                                  op(set, A_P, 0, 1, 0, sb, cl, rowoff), op(set, A_P, 0, -1, 0, sb, cl, rowoff),
                                  op(set, A_P, 1, 0, 0, sb, cl, rowoff), op(set, A_P, -1, 0, 0, sb, cl, rowoff)};
-                rs[2 * m * RS] = face(p0, nb, sb, cl, rowoff);
+                rs[m * TY * RS] = face(p0, nb, sb, cl, rowoff);
             }
         }
         __syncthreads();
-        // black faces of plane L = s: rows lj = g, g + 2, .. < TY, stored with their red partners
+        // black face of plane L = s in tile row g, stored with its red partner
         if (s >= 2) {
             const int L = s;
             const int bpl = plane_of(L);
-            const int sb[3] = {((L - dir) % kNS) * SS, (L % kNS) * SS, ((L + dir) % kNS) * SS};
+            const int sb[3] = {((L - dir) % NS) * SS, (L % NS) * SS, ((L + dir) % NS) * SS};
             const int par = (j0 + g + bpl) & 1;     // the pair's red face is i = 2q + par
             Cols cl;
             cl.c = 2 * q + 1 - par;
@@ -400,10 +412,9 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
             const T* rdn = red + ((L - dir) % kRNS) * RP + g * RS;
             const int xp = par == 0 ? qp : q, xm = par == 0 ? q : qm;   // red neighbours in x
             T* orow = A.out + ((int64_t)bpl * ny + j0 + g) * NX + 2 * q;
-#pragma unroll
-            for (int m = 0; m < TY / 2; ++m) {
-                const int rowoff = g + 2 * m;          // tile row lj
-                const int rr = 2 * m + 1;              // red row of lj (relative to g)
+            {
+                const int rowoff = g;                  // tile row lj
+                constexpr int rr = 1;                  // red row of lj (relative to g)
                 const T nb[6] = {r0[rr * RS + xp], r0[rr * RS + xm], r0[(rr + 1) * RS + q], r0[(rr - 1) * RS + q],
                                  rup[rr * RS + q], rdn[rr * RS + q]};
                 const T p0 = op(set, A_P, 0, 0, 0, sb, cl, rowoff);
@@ -412,7 +423,7 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
                 V2 pr;
                 pr.x = par == 0 ? vr : vb;
                 pr.y = par == 0 ? vb : vr;
-                *reinterpret_cast<V2*>(orow + (int64_t)(2 * m) * NX) = pr;
+                *reinterpret_cast<V2*>(orow) = pr;
             }
         }
         __syncthreads();
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(NX, 1) k_gs_pair_tma(const Args<T> A, const __
         // the copies in flight must land before the CTA's shared memory is
         // released: the last plane requested into each set (earlier ones in
         // a set were waited for before it was reused), bounded again
-        for (int L = (issued > kNS ? issued - kNS : 0); L < issued; ++L) bar_wait(&bars[L % kNS], (L / kNS) & 1);
+        for (int L = (issued > NS ? issued - NS : 0); L < issued; ++L) bar_wait(&bars[L % NS], (L / NS) & 1);
         __syncthreads();
     }
 }
@@ -491,7 +502,8 @@ inline size_t smem_bytes(size_t w, int visc, int comp, int NX, int TY) {
     size_t rows = 0;
     for (int a = 0; a < A_N; ++a)
         if (staged(visc, a)) rows += (size_t)TY + rows_lo(comp, a) + rows_hi(comp, a);
-    return 128 + kNS * rows * NX * w + (size_t)kRNS * (TY + 2) * (NX / 2 + 1) * w;
+    auto with = [&](size_t ns) { return 128 + ns * rows * NX * w + (size_t)kRNS * (TY + 2) * (NX / 2 + 1) * w; };
+    return (with(4) > 113 * 1024 && with(5) <= 227 * 1024) ? with(5) : with(4);
 }
 constexpr size_t kMaxSmem = 227 * 1024;   // dynamic shared memory one CTA may use
 

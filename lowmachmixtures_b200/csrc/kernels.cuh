@@ -153,13 +153,17 @@ __global__ void __launch_bounds__(kThreads) k_residual_c(Dims D, Coef<T> C, cons
 // one colour never read each other (even cell counts), so the in-place
 // update equals the reference's compute-all-then-update order.
 // W: wall faces keep their zero (physbc_domainvel after every colour)
+// reverse: the blocks take the planes (the instances of a 2D batch) in
+// decreasing order, so a launch that follows one in increasing order starts
+// on the planes whose operands that launch left in L2 (the faces of one
+// colour are independent: the order changes no value)
 template <class T, int DM, int VISC, int COMP, bool W = false>
 __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const T* __restrict__ rhs, T* p0, T* p1, T* p2,
-                                                        int parity, T omega, T dxsqinv) {
+                                                        int parity, T omega, T dxsqinv, int reverse) {
     pdl_enter();
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
-    const int j = q.j, k = q.k;
+    const int j = q.j, k = reverse ? (int)gridDim.z - 1 - q.k : q.k;
     const int i = 2 * q.i + ((j + ck<DM>(k) + parity) & 1);
     Nb nb = W ? make_nbw(D, i, j, k) : make_nb(D, i, j, k);
     if (W && wall_face(nb, COMP)) return;
@@ -1208,8 +1212,8 @@ void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* co
 
 template <class T>
 void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega,
-                      cudaStream_t s) {
-    if (L.D.wall) return wl_gs_colour<T>(L, visc, color, rhs, phi, omega, s);
+                      cudaStream_t s, int reverse) {
+    if (L.D.wall) return wl_gs_colour<T>(L, visc, color, rhs, phi, omega, s, reverse);
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const int comp = (color - 1) / 2;
     const int parity = (color % 2 == 1) ? 0 : 1;
@@ -1233,7 +1237,7 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
         return;
     }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
-#define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
+#define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv, reverse)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
         else { LMM_VISC_DISPATCH(visc, GS(2, 1)) }
@@ -1532,7 +1536,7 @@ namespace lmm {
 
 #define LMM_INSTANTIATE(T)                                                                                                     \
     template void launch_applyop<T>(const LevelDev<T>&, int, const T* const[3], T* const[3], cudaStream_t, int);              \
-    template void launch_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t);     \
+    template void launch_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t, int); \
     template void launch_jacobi<T>(const LevelDev<T>&, int, const T* const[3], const T* const[3], T* const[3], double,         \
                                    cudaStream_t);                                                                              \
     template bool gs_pair_supported<T>(const LevelDev<T>&, int);                                                               \

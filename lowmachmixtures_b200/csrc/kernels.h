@@ -45,9 +45,11 @@ struct LevelDev {
 // color 0: every face; 1..2*dm: only the faces of that Gauss-Seidel colour
 template <class T>
 void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color);
+// reverse: the launch takes the planes in decreasing k (same values; see
+// k_gs_colour)
 template <class T>
 void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega,
-                      cudaStream_t s);
+                      cudaStream_t s, int reverse = 0);
 // Both Gauss-Seidel colours of component comp in one launch, out of place:
 // cur[] are read, the new values of component comp go to out (3D levels with
 // even sizes; gs_pair_supported says whether the level qualifies).  kc > 0
@@ -85,7 +87,8 @@ void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pre
 template <class T>
 void wl_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const out[3], cudaStream_t s, int color);
 template <class T>
-void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega, cudaStream_t s);
+void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega, cudaStream_t s,
+                  int reverse = 0);
 template <class T>
 void wl_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const phi_in[3], T* const phi_out[3], double omega,
                cudaStream_t s);

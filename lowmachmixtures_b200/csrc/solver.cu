@@ -557,13 +557,16 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
 }
 
 // ------------------------------------------------------------ staggered V-cycle
+// rows per tile the knobs ask of the TMA smoother (0: the level's default)
+int tma_rows(const lmm_knobs& K) { return K.smoother_tma >= 2 ? K.smoother_tma : 0; }
+
 // the level runs both colours of each component in one TMA-staged launch
 template <class T>
 bool use_tma_smoother(const lmm_handle* h, const LevelDev<T>& L) {
     const lmm_knobs& K = h->knobs;
     const int64_t min_cells = K.smoother_tma_cells > 0 ? K.smoother_tma_cells : 32768;
-    return K.stag_mg_smoother != 0 && K.smoother_fusion == 0 && K.smoother_tma >= 0 && h->dm == 3 && !h->batched &&
-           L.n >= min_cells && gs_tma_supported<T>(L, K.visc_type, K.smoother_tma, K.smoother_tma_slabs);
+    return K.stag_mg_smoother != 0 && K.smoother_fusion == 0 && K.smoother_tma > 0 && h->dm == 3 && !h->batched &&
+           L.n >= min_cells && gs_tma_supported<T>(L, K.visc_type, tma_rows(K), K.smoother_tma_slabs);
 }
 
 template <class T>
@@ -576,7 +579,7 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
         T* alt[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
         for (int m = 0; m < nsm; ++m)
             for (int d = 0; d < 3; ++d) {
-                LMM_CK(launch_gs_pair_tma<T>(L, K.visc_type, d, L.rhs, cur, alt[d], K.stag_mg_omega, K.smoother_tma,
+                LMM_CK(launch_gs_pair_tma<T>(L, K.visc_type, d, L.rhs, cur, alt[d], K.stag_mg_omega, tma_rows(K),
                                              K.smoother_tma_slabs, h->dev_err, h->stream));
                 check_launch();
                 std::swap(cur[d], alt[d]);
@@ -608,8 +611,11 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
             for (int d = 0; d < h->dm; ++d)
                 LMM_CK(cudaMemcpyAsync(L.phi[d], L.tmp[d], L.n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
         } else {
+            // consecutive colour launches take the planes in alternating order
+            // (smoother_order = 0): each starts where the last left its operands in L2
             for (int color = 1; color <= 2 * h->dm; ++color) {
-                launch_gs_colour<T>(L, K.visc_type, color, L.rhs, L.phi, K.stag_mg_omega, h->stream);
+                launch_gs_colour<T>(L, K.visc_type, color, L.rhs, L.phi, K.stag_mg_omega, h->stream,
+                                    (K.smoother_order == 0 && color % 2 == 0) ? 1 : 0);
                 check_launch();
             }
         }
@@ -1366,6 +1372,206 @@ void learned_stage(lmm_handle* h, const SVec& c, const SVec& v, int mode) {
     check_launch();
 }
 
+// The network's estimate of the error left by one preconditioner
+// application: with w = A z1 for z1 = M v, the residual r1 = v - w goes
+// through the network, whose output (scaled back) becomes c, with its
+// constant modes removed like every preconditioner output.
+void network_correction(lmm_handle* h, const SVec& c, const SVec& v) {
+    const int64_t len = v.size();
+    const int S1 = lmm_handle::kLrnSlot, S3 = S1 + 2;
+    launch_lin(h->lr1.base, v.base, -1.0, h->w.base, len, h->stream);
+    check_launch();
+    stokes_norm(h, h->lr1, S1);
+    launch_features(h->D0, h->lr1.base, h->L64[0].beta, h->slot(S1), h->grid.dx, nn::net_input(h->net), h->stream);
+    check_launch();
+    if (nn::net_forward_on(h->net, h->stream) != LMM_OK) throw LmmError(LMM_ERR_CUDA);
+    launch_correction(h->D0, nn::net_output(h->net), h->L64[0].beta, h->slot(S1), h->grid.dx, c.base, h->stream);
+    check_launch();
+    double* cu[3] = {c.c(0), c.c(1), c.c(2)};
+    reduce_means<double>(h, cu, c.p(), S3);
+    double tv = 1.0;
+    for (int d = 0; d < h->dm; ++d) tv *= (double)h->grid.n[d];
+    launch_sub_means<double>(h->D0, cu, c.p(), h->slot(S3), tv, mean_mask(h, h->theta_loaded), h->stream);
+    check_launch();
+}
+
+// FGMRES with the learned stage as an extra direction (learned_stage = 1):
+// every step adds two columns to the flexible Krylov basis, the FP32
+// V-cycle's z1 = M v and the network's correction c of the residual
+// v - A z1, and the least-squares problem minimises over both.  A cycle
+// holds m V-cycle columns (up to 2m columns in all); a network column
+// whose image lies in the span of the basis already (|w| after
+// orthogonalisation below 1e-8 of |A c|) is dropped, so it can neither
+// end a cycle as a false breakdown nor make the Hessenberg matrix
+// singular.  Iterations count V-cycle applications, as without the stage.
+// learned_stage = 2 computes every correction and adds none (the cost of
+// the stage without its effect: bitwise the stage-free solve).
+int run_fgmres_augmented(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
+    NvtxRange nvtx_("fgmres (learned columns)");
+    const lmm_knobs& K = h->knobs;
+    const int m = K.gmres_max_inner;
+    const int mc = 2 * m;  // columns per cycle
+    const int64_t len = h->b.size();
+    const bool add = (K.learned_stage == 1);
+    LMM_CK(cudaMemsetAsync(h->luses, 0, 2 * sizeof(int), h->stream));
+    int net_tried = 0, net_kept = 0;
+    std::vector<double> cs(mc + 2), sn(mc + 2), y(mc + 2), s(mc + 3), col;
+    Hess H{mc + 1, std::vector<double>((size_t)(mc + 1) * mc, 0.0)};
+    std::vector<const void*> zcol(mc + 1);
+    std::vector<int> zkind(mc + 1);  // 0: FP32 V-cycle column, 1: FP64 network column
+    h->vcycles = 0;
+    if (norm_pre_rhs) *norm_pre_rhs = 0.0;
+    stokes_norm(h, h->b, 0);
+    const double norm_b = read_slot(h, 0, 5);
+    if (st) st->norm_b = norm_b;
+    if (!std::isfinite(norm_b)) return LMM_ERR_NONFINITE;
+    if (norm_b <= 0.0) {
+        LMM_CK(cudaMemsetAsync(h->x.base, 0, len * sizeof(double), h->stream));
+        return LMM_OK;
+    }
+    int status = LMM_OK, total_iter = 0, iter = 0;
+    double norm_init = 0.0;
+    auto col_norms_ok = [](const std::vector<double>& c, int i) {
+        for (int k = 1; k <= i + 1; ++k)
+            if (!std::isfinite(c[k])) return false;
+        return true;
+    };
+    for (;;) {
+        launch_apply_matrix(h->L64[0], K.visc_type, h->x, h->tmp, h->stream);
+        check_launch();
+        launch_neg_resid(h->tmp.base, h->b.base, len, h->stream);
+        check_launch();
+        stokes_norm(h, h->tmp, 0);
+        const double norm_r = read_slot(h, 0, 5);
+        if (!std::isfinite(norm_r)) return LMM_ERR_NONFINITE;
+        if (iter == 0) norm_init = norm_r;
+        if (st) {
+            st->norm_resid_true = norm_r;
+            st->norm_init_true = norm_init;
+            st->norm_resid = norm_r;
+        }
+        if (total_iter >= K.gmres_min_iter && (norm_r <= K.gmres_rel_tol * norm_b || norm_r <= K.gmres_abs_tol)) break;
+        if (total_iter >= K.gmres_max_iter) {
+            status = LMM_WARN_MAX_ITER;
+            break;
+        }
+        if (iter >= K.gmres_max_outer) {
+            status = LMM_WARN_MAX_OUTER;
+            break;
+        }
+        iter = iter + 1;
+        launch_div_by_f32(h->tmp.base, h->V[0].base, h->pin32, h->slot(0) + 5, len, h->stream);
+        check_launch();
+        std::fill(s.begin(), s.end(), 0.0);
+        s[1] = norm_r;
+        int i = 0;      // columns of this cycle
+        bool stop = false;
+        // one column: Arnoldi of w against V_0..V_{i-1}, V_i = w / H(i+1,i),
+        // the Hessenberg column to the host; false when the column is dropped
+        // (a network column is orthogonalised by modified Gram-Schmidt whatever
+        // the knob: it is often close to the span of the basis, where one
+        // classical pass loses orthogonality)
+        auto arnoldi = [&](int i1, bool droppable) -> bool {
+            if (K.orthogonalization == 1 && !droppable)
+                arnoldi_column_cgs_enqueue(h, i1);
+            else
+                arnoldi_column_enqueue(h, i1);
+            launch_div_by_f32(h->w.base, h->V[i1].base, h->pin32, h->slot(i1 + 1) + 5, len, h->stream);
+            check_launch();
+            arnoldi_column_collect(h, i1, col);
+            if (!col_norms_ok(col, i1)) throw LmmError(LMM_ERR_NONFINITE);
+            if (droppable) {
+                double proj = 0.0;
+                for (int k = 1; k <= i1; ++k) proj += col[k] * col[k];
+                const double full = std::sqrt(proj + col[i1 + 1] * col[i1 + 1]);
+                if (!(col[i1 + 1] > 1e-8 * full)) return false;
+            }
+            for (int k = 1; k <= i1 + 1; ++k) H(k, i1) = col[k];
+            return true;
+        };
+        auto after_column = [&](int i1) {
+            const bool happy = (H(i1 + 1, i1) == 0.0);
+            least_squares(i1, H, cs, sn, s);
+            const double est = std::fabs(s[i1 + 1]);
+            push_hist(st, est);
+            if (happy || (total_iter >= K.gmres_min_iter && (est <= K.gmres_rel_tol * norm_b || est <= K.gmres_abs_tol)))
+                stop = true;
+        };
+        // The V-cycle is applied to the basis vector its own previous column
+        // produced (vin), never to one a network column produced: without
+        // network columns this is plain FGMRES step for step, and the network
+        // only adds directions to the space the least-squares step minimises
+        // over.
+        int vin = 0;
+        bool pin_ok = true;  // h->pin32 holds V[vin] in FP32 (written with it)
+        for (int k = 0; k < m && !stop; ++k) {
+            // V-cycle column: z = M v (FP32), w = A z
+            total_iter = total_iter + 1;
+            precon32(h, h->V[vin], h->Z32[k], pin_ok);
+            launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[k], h->n, h->dm, h->w, h->stream);
+            check_launch();
+            // the network's correction of what this application leaves (before
+            // the Arnoldi step overwrites w)
+            network_correction(h, h->Zc[k], h->V[vin]);
+            ++net_tried;
+            i = i + 1;
+            zcol[i] = h->Z32[k];
+            zkind[i] = 0;
+            arnoldi(i, false);
+            vin = i;
+            pin_ok = true;
+            after_column(i);
+            if (stop || total_iter >= K.gmres_max_iter) {
+                stop = true;
+                break;
+            }
+            if (!add || i + 1 > mc) continue;
+            // network column: z = c, w = A c
+            launch_apply_matrix(h->L64[0], K.visc_type, h->Zc[k], h->w, h->stream);
+            check_launch();
+            pin_ok = false;  // the network column's V overwrote the FP32 copy of V[vin]
+            if (arnoldi(i + 1, true)) {
+                i = i + 1;
+                zcol[i] = h->Zc[k].base;
+                zkind[i] = 1;
+                ++net_kept;
+                after_column(i);
+            }
+        }
+        solve_utri(i - 1, H, s, y);
+        // update_sol: runs of consecutive V-cycle columns as in run_fgmres
+        // (up to 8 FP32 basis vectors per pass), network columns one by one
+        for (int it = 1; it <= i;) {
+            if (zkind[it] == 1) {
+                launch_add_scaled(h->x.base, static_cast<const double*>(zcol[it]), y[it], len, h->stream);
+                check_launch();
+                ++it;
+                continue;
+            }
+            MZ32 Z{};
+            YS ys{};
+            int J = 0;
+            while (J < 8 && it + J <= i && zkind[it + J] == 0) {
+                Z.p[J] = static_cast<const float*>(zcol[it + J]);
+                ys.y[J] = y[it + J];
+                ++J;
+            }
+            launch_add_scaled_multi_f32(h->x.base, Z, ys, J, len, h->stream);
+            check_launch();
+            it += J;
+        }
+    }
+    int u[2] = {net_kept, net_tried};
+    LMM_CK(cudaMemcpyAsync(h->luses, u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
+    LMM_CK(host_wait(h));
+    if (st) {
+        st->total_iter = total_iter;
+        st->outer_iter = iter;
+        st->vcycles = h->vcycles;
+    }
+    return status;
+}
+
 int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
     NvtxRange nvtx_("fgmres");
     const lmm_knobs& K = h->knobs;
@@ -1373,6 +1579,7 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
     const int64_t len = h->b.size();
     const bool fp32 = (K.precision == LMM_PRECISION_FP32);
     const bool learned = fp32 && K.learned_stage > 0 && h->net != nullptr;
+    if (learned && (K.learned_stage == 1 || K.learned_stage == 2)) return run_fgmres_augmented(h, norm_pre_rhs, st);
     if (learned) LMM_CK(cudaMemsetAsync(h->luses, 0, 2 * sizeof(int), h->stream));
     std::vector<double> cs(m + 2), sn(m + 2), y(m + 2), s(m + 3), col;
     Hess H{m + 1, std::vector<double>((size_t)(m + 1) * m, 0.0)};
@@ -1436,7 +1643,7 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             if (fp32) {
                 precon32(h, h->V[c], h->Z32[c], true);
                 launch_apply_matrix_f32(h->L64[0], K.visc_type, h->Z32[c], h->n, h->dm, h->w, h->stream);
-                if (learned) learned_stage(h, h->Zc[c], h->V[c], K.learned_stage);
+                if (learned) learned_stage(h, h->Zc[c], h->V[c], 1);
             } else {
                 precon64(h, h->V[c], h->Z64[c]);
                 launch_apply_matrix(h->L64[0], K.visc_type, h->Z64[c], h->w, h->stream);
@@ -1995,7 +2202,7 @@ int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
                       SAME(gmres_max_inner) && SAME(visc_type) && SAME(method) && SAME(precision) &&
                       SAME(learned_stage) && SAME(tail_cells) && SAME(tail_smem_kb) && SAME(use_graphs) &&
                       SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait) &&
-                      SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells);
+                      SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells) && SAME(smoother_order);
 #undef SAME
     if (!same) {
         g_last_error = "lmm_stokes_update_knobs changes only the stopping rules; create a new handle for the rest";
@@ -2635,14 +2842,18 @@ extern "C" int lmm_stokes_set_net(lmm_handle* h, lmm_net* net) {
             }
             if (!h->lrn_block) {
                 const int64_t len = (int64_t)(h->dm + 1) * h->n;
-                const int nv = 4 + h->m;
+                // 4 work vectors, m network corrections and m more Krylov
+                // vectors (a cycle with the stage holds up to 2m columns)
+                const int nv = 4 + 2 * h->m;
                 const size_t bytes = (size_t)nv * len * sizeof(double) + (size_t)len * sizeof(float) + 256;
                 LMM_CK(cudaMalloc(&h->lrn_block, bytes));
                 double* p = static_cast<double*>(h->lrn_block);
                 h->Zc.assign(h->m, SVec());
+                const size_t v0 = h->V.size();
+                h->V.resize(v0 + h->m);
                 SVec* v[4] = {&h->lr1, &h->lc, &h->lAc, &h->le};
                 for (int q = 0; q < nv; ++q) {
-                    SVec& t = q < 4 ? *v[q] : h->Zc[q - 4];
+                    SVec& t = q < 4 ? *v[q] : (q < 4 + h->m ? h->Zc[q - 4] : h->V[v0 + (q - 4 - h->m)]);
                     t.base = p + (int64_t)q * len;
                     t.n = h->n;
                     t.dm = h->dm;

@@ -31,7 +31,8 @@ void wl_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* const 
 }
 
 template <class T>
-void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega, cudaStream_t s) {
+void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[3], T* const phi[3], double omega, cudaStream_t s,
+                  int reverse) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     const int comp = (color - 1) / 2;
     const int parity = (color % 2 == 1) ? 0 : 1;
@@ -55,7 +56,7 @@ void wl_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const rhs[
         return;
     }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
-#define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_, true>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv)
+#define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_, true>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv, reverse)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
         else { LMM_VISC_DISPATCH(visc, GS(2, 1)) }
@@ -109,7 +110,7 @@ void wl_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const 
 
 #define LMM_INSTANTIATE_WALLS(T)                                                                                           \
     template void wl_applyop<T>(const LevelDev<T>&, int, const T* const[3], T* const[3], cudaStream_t, int);              \
-    template void wl_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t);     \
+    template void wl_gs_colour<T>(const LevelDev<T>&, int, int, const T* const[3], T* const[3], double, cudaStream_t, int); \
     template void wl_jacobi<T>(const LevelDev<T>&, int, const T* const[3], const T* const[3], T* const[3], double,         \
                                cudaStream_t);                                                                              \
     template void wl_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, int, const T* const[3],                  \

@@ -49,7 +49,7 @@ module lmm_stokes_iface
      integer(c_int) :: tail_cells, tail_smem_kb, use_graphs, smoother_fusion, l2_persist
      integer(c_int) :: orthogonalization, host_wait
      integer(c_int) :: ensemble_batch
-     integer(c_int) :: smoother_tma, smoother_tma_slabs, smoother_tma_cells
+     integer(c_int) :: smoother_tma, smoother_tma_slabs, smoother_tma_cells, smoother_order
   end type lmm_knobs
 
   type, bind(c) :: lmm_fields_in
