@@ -157,6 +157,10 @@ typedef struct lmm_knobs {
     int    smoother_order;         /* Gauss-Seidel with one launch per colour: 0 = default (consecutive
                                       launches take the planes in alternating order, each starting
                                       where the last left its operands in L2), -1 = always in +k order */
+    int    autotune;               /* 0 = default (the first handle of a grid size times candidate block
+                                      shapes of the colour, operator and prolongation kernels and the
+                                      process keeps the fastest; see lmm_autotune_report), -1 = this
+                                      handle times nothing (shapes the process chose already apply) */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.
@@ -306,6 +310,13 @@ int64_t lmm_kernel_launches(void);
  *   5 one staggered V-cycle, FP32
  *   6 one pressure V-cycle, FP64                                        */
 int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_rep);
+
+/* The block-shape autotuner's choices so far (no counterpart in the
+ * reference): one text line per tuned kernel, precision, visc_type and
+ * grid, with its chosen block and the measured ms of the default and the
+ * chosen geometry.  Writes at most cap - 1 bytes and a terminating zero
+ * into buf (cap > 0); returns the length of the full report. */
+int lmm_autotune_report(char* buf, int cap);
 
 #ifdef __cplusplus
 }

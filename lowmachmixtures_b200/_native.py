@@ -80,6 +80,8 @@ def load() -> C.CDLL:
     lib.lmm_op_num_levels.argtypes = [C.c_void_p]
     lib.lmm_kernel_launches.restype = C.c_int64
     lib.lmm_time_op.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_double)]
+    lib.lmm_autotune_report.argtypes = [C.c_char_p, C.c_int]
+    lib.lmm_autotune_report.restype = C.c_int
     _lib = lib
     return lib
 

@@ -30,6 +30,7 @@ UNITS = [
     ("krylov.cu", ["-fmad=false"]),
     ("solver.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("autotune.cu", []),
     ("nn.cu", ["-fmad=true"]),
     ("net.cu", ["-fmad=true"]),
     ("learned.cu", ["-fmad=true"]),

@@ -17,6 +17,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "kernels.h"
@@ -47,6 +48,21 @@ static inline G3 geom3(int nx, int ny, int nz) {
     g.block = dim3(bx, by, 1);
     g.grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
     return g;
+}
+
+// the geometry of a tuned kernel: a shape forced by the autotuner while it
+// times candidates, else the shape it chose for this grid, else geom3's
+static inline G3 geom3_shape(int nx, int ny, int nz, Shape s) {
+    G3 g;
+    const int bx = std::max(1, std::min(s.bx, nx)), by = std::max(1, std::min(s.by, ny));
+    g.block = dim3(bx, by, 1);
+    g.grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+    return g;
+}
+static inline G3 geom3_tuned(int kernel, int wbytes, int visc, const Dims& D, int nx, int ny, int nz) {
+    Shape s = forced_shape();
+    if (!s.bx) s = tuned_shape(kernel, wbytes, visc, D);
+    return s.bx ? geom3_shape(nx, ny, nz, s) : geom3(nx, ny, nz);
 }
 
 // --------------------------------------------------------------- applyop
@@ -1194,7 +1210,7 @@ void launch_applyop(const LevelDev<T>& L, int visc, const T* const phi[3], T* co
     if (L.D.wall) return wl_applyop<T>(L, visc, phi, out, s, color);
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     if (color == 0) {
-        const G3 gc = geom3(L.D.nx, L.D.ny, L.D.nz * L.D.dm);
+        const G3 gc = geom3_tuned(TK_APPLYOP, sizeof(T), visc, L.D, L.D.nx, L.D.ny, L.D.nz * L.D.dm);
         if (L.D.dm == 2) {
             LMM_VISC_DISPATCH(visc, launch_pdl(k_applyop_c<T, 2, V>, gc.grid, gc.block, 0, s, L.D, L.coef(), phi[0], phi[1], phi[2], out[0], out[1], out[2], dxsqinv))
         } else {
@@ -1236,7 +1252,7 @@ void launch_gs_colour(const LevelDev<T>& L, int visc, int color, const T* const 
 #undef CU
         return;
     }
-    const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
+    const G3 g = geom3_tuned(TK_GS_COLOUR, sizeof(T), visc, L.D, L.D.nx / 2, L.D.ny, L.D.nz);
 #define GS(DM_, COMP_) launch_pdl(k_gs_colour<T, DM_, V, COMP_>, g.grid, g.block, 0, s, L.D, L.coef(), rhs[COMP_], phi[0], phi[1], phi[2], parity, om, dxsqinv, reverse)
     if (L.D.dm == 2) {
         if (comp == 0) { LMM_VISC_DISPATCH(visc, GS(2, 0)) }
@@ -1343,7 +1359,7 @@ template <class T>
 void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3],
                         cudaStream_t s) {
     if (F.D.wall) return wl_prolong_add<T>(F, Cc, phi_c, phi_f, s);
-    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz);
+    const G3 g = geom3_tuned(TK_PROLONG, sizeof(T), 0, F.D, F.D.nx, F.D.ny, F.D.nz);
     if (F.D.dm == 2)
         launch_pdl(k_prolong_add<T, 2>, g.grid, g.block, 0, s, F.D, Cc.D, phi_c[0], phi_c[1], phi_c[2], phi_f[0], phi_f[1], phi_f[2]);
     else

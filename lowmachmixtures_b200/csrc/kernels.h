@@ -172,4 +172,18 @@ cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
 void count_launch();
 int64_t launches_total();
 
+// ---- block-shape autotuner (autotune.cu; the timing is solver.cu's) ----
+// Kernels whose launch geometry it picks per (precision, visc_type, grid).
+enum TuneKernel { TK_GS_COLOUR = 0, TK_APPLYOP = 1, TK_PROLONG = 2, TK_N = 3 };
+struct Shape {
+    int bx = 0, by = 0;  // 0 x 0: the default geometry (geom3)
+};
+// the chosen shape, {0, 0} when the kernel was not tuned for this grid
+Shape tuned_shape(int kernel, int wbytes, int visc, const Dims& D);
+bool is_tuned(int kernel, int wbytes, int visc, const Dims& D);
+void set_tuned_shape(int kernel, int wbytes, int visc, const Dims& D, Shape s, double ms_default, double ms_best);
+// a candidate forced on this thread's launches while the autotuner times it
+void force_shape(Shape s);
+Shape forced_shape();
+
 }  // namespace lmm

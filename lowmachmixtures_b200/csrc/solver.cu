@@ -622,6 +622,67 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
     }
 }
 
+// Block-shape autotuner.  On the first handle of a grid size (per
+// precision and visc_type; the table is the process's), time the candidate
+// block shapes of the Gauss-Seidel colour, operator and prolongation
+// kernels on every periodic level with at least 4096 cells -- one warm-up
+// and three launches each, CUDA events on the handle's stream -- and keep
+// the fastest.  It runs at creation, on the fresh arena's zeros; the colour
+// kernel divides by the zero diagonal there, so phi and tmp of a tuned
+// level are zeroed again afterwards.  Shapes change no value.
+template <class T>
+void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
+    static const Shape cands[] = {{0, 0}, {64, 4}, {32, 8}, {128, 2}, {16, 16}, {32, 4}, {64, 2}, {128, 1}, {256, 1}};
+    const int visc = h->knobs.visc_type;
+    for (int l = 0; l < h->nlev && l < (int)Ls.size(); ++l) {
+        LevelDev<T>& L = Ls[l];
+        if (L.n < 4096 || L.D.wall || (L.D.nx & 1) || (L.D.ny & 1) || (L.D.dm == 3 && (L.D.nz & 1))) continue;
+        bool touched = false;
+        for (int kid = 0; kid < TK_N; ++kid) {
+            if (kid == TK_PROLONG && l + 1 >= h->nlev) continue;  // needs a coarser level
+            const int kv = (kid == TK_PROLONG) ? 0 : visc;
+            if (is_tuned(kid, sizeof(T), kv, L.D)) continue;
+            const int nxe = (kid == TK_GS_COLOUR) ? L.D.nx / 2 : L.D.nx;
+            auto launch = [&]() {
+                if (kid == TK_GS_COLOUR)
+                    launch_gs_colour<T>(L, visc, 1, L.rhs, L.phi, 1.0, h->stream, 0);
+                else if (kid == TK_APPLYOP)
+                    launch_applyop<T>(L, visc, L.phi, L.tmp, h->stream, 0);
+                else
+                    launch_prolong_add<T>(L, Ls[l + 1], Ls[l + 1].phi, L.phi, h->stream);
+                check_launch();
+            };
+            double best = 1e300, def = 0.0;
+            Shape bs{};
+            for (const Shape& c : cands) {
+                if (c.bx > std::max(nxe, 32)) continue;
+                force_shape(c);
+                launch();
+                LMM_CK(cudaEventRecord(h->ev0, h->stream));
+                for (int r = 0; r < 3; ++r) launch();
+                LMM_CK(cudaEventRecord(h->ev1, h->stream));
+                LMM_CK(cudaEventSynchronize(h->ev1));
+                float ms = 0.f;
+                LMM_CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+                const double per = ms / 3.0;
+                if (c.bx == 0) def = per;
+                if (per < best) {
+                    best = per;
+                    bs = c;
+                }
+            }
+            force_shape(Shape{});
+            set_tuned_shape(kid, sizeof(T), kv, L.D, bs, def, best);
+            touched = true;
+        }
+        if (touched)
+            for (int d = 0; d < h->dm; ++d) {
+                LMM_CK(cudaMemsetAsync(L.phi[d], 0, L.n * sizeof(T), h->stream));
+                LMM_CK(cudaMemsetAsync(L.tmp[d], 0, L.n * sizeof(T), h->stream));
+            }
+    }
+}
+
 // first level handled by the shared-memory tail kernel (nl: no tail): the
 // largest run of coarse levels with at most tail_cells cells each whose
 // phi/rhs fit the shared-memory budget
@@ -2156,8 +2217,15 @@ static int create_impl(const lmm_grid* g, const lmm_knobs* k, int device, int ba
                 zt[q] = (k->precision == LMM_PRECISION_FP32) ? (void*)h->Z32[q] : (void*)h->Z64[q].base;
             LMM_CK(cudaMemcpyAsync(h->ztab, zt.data(), sizeof(void*) * (h->m + 1), cudaMemcpyHostToDevice, h->stream));
         }
+        if (k->autotune >= 0 && k->stag_mg_smoother != 0) {
+            if (k->precision == LMM_PRECISION_FP32)
+                autotune_levels<float>(h, h->L32);
+            else
+                autotune_levels<double>(h, h->L64);
+        }
         LMM_CK(host_wait(h));
     } catch (const LmmError& e) {
+        force_shape(Shape{});
         lmm_stokes_destroy(h);
         return e.code;
     }
@@ -2202,7 +2270,8 @@ int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
                       SAME(gmres_max_inner) && SAME(visc_type) && SAME(method) && SAME(precision) &&
                       SAME(learned_stage) && SAME(tail_cells) && SAME(tail_smem_kb) && SAME(use_graphs) &&
                       SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait) &&
-                      SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells) && SAME(smoother_order);
+                      SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells) && SAME(smoother_order) &&
+                      SAME(autotune);
 #undef SAME
     if (!same) {
         g_last_error = "lmm_stokes_update_knobs changes only the stopping rules; create a new handle for the rest";

@@ -562,3 +562,35 @@ def test_gmres_parity_bfbt(oracle, pt):
     ref, got = _solve_both(oracle, prob, precon_type=pt, visc_type=-2, visc_schur_approx=1)
     assert ref[0] == got[0] == 0
     _assert_solution_parity(ref, got)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotuned_block_shapes_are_bitwise_neutral_and_reported(precision):
+    """The block-shape autotuner picks launch geometry only: on a grid size
+    no handle has tuned yet, a solve with the default shapes (autotune = -1)
+    and one after tuning (autotune = 0) give the same bits, and
+    lmm_autotune_report lists what was tuned for that grid."""
+    import ctypes as C
+
+    from lowmachmixtures_b200 import _native
+    from lowmachmixtures_b200.gmres import StokesSolver
+    n = 48 if precision == 0 else 40
+    prob = synth.make_problem(3, n, 30.0, 9, theta_alpha=0.1 * n * n)
+    outs = []
+    for at in (-1, 0):
+        kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=precision, autotune=at)
+        with StokesSolver(3, (n, n, n), prob.dx, knobs=kn) as s:
+            xu, xp = prob.zeros_like_solution()
+            s.solve(prob.b_u, prob.b_p, xu, xp, prob.alpha_fc, prob.beta, prob.beta_ed, prob.gamma, prob.theta_alpha)
+        outs.append((xu, xp))
+    for c in range(3):
+        np.testing.assert_array_equal(outs[0][0][c], outs[1][0][c])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    lib = _native.load()
+    need = lib.lmm_autotune_report(None, 0)
+    buf = C.create_string_buffer(need + 1)
+    assert lib.lmm_autotune_report(buf, need + 1) == need
+    rep = buf.value.decode()
+    w = 64 if precision == 0 else 32
+    assert f"gs_colour fp{w} visc -2 3D {n}x{n}x{n}" in rep, rep
+    assert f"applyop fp{w} visc -2 3D {n}x{n}x{n}" in rep, rep
