@@ -3,8 +3,9 @@ seeds and viscosity fields): the units of work that shard across GPUs.
 
 Instances are independent, so a multi-GPU run gives every rank a disjoint
 set of whole instances -- no collective on the data path, only a final
-gather of per-instance statistics.  `shard` balances the ranks by the cost
-of an instance (its cell count).
+gather of per-instance statistics.  `shard` balances the ranks by the
+expected cost of an instance (`instance_cost`: its cell count times the
+FGMRES iterations its viscosity contrast is expected to take).
 """
 from __future__ import annotations
 
@@ -23,6 +24,20 @@ def instance_contrast(i: int, seed: int = 0) -> float:
     """viscosity contrast of instance i: log-uniform in [10, 1000]"""
     u = np.random.Generator(np.random.PCG64(777 + 1000003 * seed + i)).uniform()
     return float(10.0 ** (1.0 + 2.0 * u))
+
+
+def expected_iterations(contrast: float) -> float:
+    """FGMRES + V-cycle iterations to 1e-8 expected at a viscosity contrast:
+    12.7 + 10.6 log10(contrast / 10), fitted to oracle solves of 2D 64^2 and
+    128^2 problems of this family (precon_type 2, visc_type -2; three seeds
+    each at contrasts 10, 30, 100, 300 and 1000: 12.7, 16.5, 21, 26 and 34
+    iterations on average, the same at both sizes)."""
+    return 12.7 + 10.6 * float(np.log10(max(contrast, 1.0) / 10.0))
+
+
+def instance_cost(n: int, contrast: float, dm: int = 2) -> float:
+    """expected work of one instance: cells times expected iterations"""
+    return float(n) ** dm * max(1.0, expected_iterations(contrast))
 
 
 def shard(costs, world: int):
@@ -164,7 +179,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     pool_sizes = tuple(int(v) for v in a.sizes.split(","))
     sizes = instance_sizes(a.count, sizes=pool_sizes)
-    mine = shard([n * n for n in sizes], world)[rank]
+    mine = shard([instance_cost(n, instance_contrast(i)) for i, n in enumerate(sizes)], world)[rank]
     allp = make_instances(a.count, sizes=pool_sizes)
     probs = [allp[i] for i in mine]
     pool = a.mode == "pool"

@@ -66,3 +66,18 @@ def test_shard_balances_cost():
         loads = [sum(costs[i] for i in p) for p in parts]
         assert sorted(i for p in parts for i in p) == list(range(512))
         assert max(loads) - min(loads) <= max(costs)
+
+
+def test_instance_cost_weights_cells_by_expected_iterations():
+    """A 2D instance's expected work grows with its cells and with the log of
+    its viscosity contrast (the iteration count measured on the oracle)."""
+    from lowmachmixtures_b200 import ensemble
+    assert abs(ensemble.expected_iterations(10.0) - 12.7) < 1e-12
+    assert abs(ensemble.expected_iterations(1000.0) - (12.7 + 21.2)) < 1e-9
+    assert ensemble.instance_cost(128, 100.0) > ensemble.instance_cost(128, 10.0)
+    assert ensemble.instance_cost(128, 10.0) == 4 * ensemble.instance_cost(64, 10.0)
+    sizes = ensemble.instance_sizes(512, seed=0)
+    costs = [ensemble.instance_cost(n, ensemble.instance_contrast(i)) for i, n in enumerate(sizes)]
+    parts = ensemble.shard(costs, 4)
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) <= 1.01 * min(loads)
