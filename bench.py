@@ -20,10 +20,11 @@ A step is one full solve.  Reported:
   cpu_baseline  the CPU oracle (C++ restatement of the reference algorithm):
           one full solve of the same problem on every host thread, plus one
           full 64^3 solve of the same family on one core, rank 0 only;
-  learned_stage  the same mixed method with the learned correction stage
-          (network trained on the GPU before the timed region, on 64^3
-          problems of this workload's family) -- measured beside `value`,
-          which is the faster mixed configuration without it;
+  learned_stage  the same mixed method with the learned stage (network
+          trained on the GPU before the timed region, on 64^3 problems of
+          this workload's family, its corrections added as extra FGMRES
+          directions) -- measured beside `value`, which is the faster mixed
+          configuration without it;
   mixed_vs_fp64  relative L2 error of the mixed solution against the FP64 one.
 
 N > 1 GPUs: replicas only (one independent solve per GPU, a different seed
@@ -374,13 +375,22 @@ def run_product(args, world, rank, local):
     bytes_smooth64 = 16 * 8 * nf
     bytes_apply64 = 13 * 8 * nf   # w(3F + N + E): phi, alpha, beta, edges in; L out
     gbs = lambda b, ms: b / (ms * 1e-3) / 1e9  # noqa: E731
-    roofline = {"bound": "hbm", "kernel": "gs_colour_fp32 (one full smooth: 6 colours, 128^3)",
+    roofline = {"bound": "hbm", "kernel": f"gs_colour_fp32 (one full smooth: 6 colour launches in alternating plane order, {n}^3)",
                 "achieved": gbs(bytes_smooth32, ms_smooth32), "peak": peak, "unit": "GB/s",
                 "frac": gbs(bytes_smooth32, ms_smooth32) / peak, "traffic": None,
                 "peak_source": peak_src,
                 "algorithmic_bytes": bytes_smooth32, "ms_per_launch": ms_smooth32 / 6.0,
                 "ms_per_smooth": ms_smooth32}
+    # the opt-in TMA-staged red/black pair smoother on the same level
+    tma_kn = abi.make_knobs(**base, method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32, orthogonalization=1,
+                            smoother_tma=1)
+    with StokesSolver(3, (n, n, n), prob.dx, knobs=tma_kn, device=local) as tma:
+        tma.load_coeffs(d_in["alpha_fc"], d_in["beta"], d_in["beta_ed"], d_in["gamma"], prob.theta_alpha)
+        ms_smooth32_tma = tma.time_op(1, reps=20)
     kernels = {
+        "gs_smooth_fp32_tma_pair": {"ms": ms_smooth32_tma, "GB/s": gbs(bytes_smooth32, ms_smooth32_tma),
+                                    "frac": gbs(bytes_smooth32, ms_smooth32_tma) / peak,
+                                    "note": "opt-in (smoother_tma = 1): slower than the colour launches"},
         "gs_smooth_fp64": {"ms": ms_smooth64, "GB/s": gbs(bytes_smooth64, ms_smooth64),
                            "frac": gbs(bytes_smooth64, ms_smooth64) / peak},
         "stag_applyop_fp64": {"ms": ms_apply64, "GB/s": gbs(bytes_apply64, ms_apply64),
@@ -407,6 +417,7 @@ def run_product(args, world, rank, local):
         "gpu_launches": launches,
         "roofline": roofline,
         "kernels": kernels,
+        "autotune": autotune_choices(n),
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -447,6 +458,16 @@ def run_product(args, world, rank, local):
         s.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def autotune_choices(n):
+    """the block shapes the library's autotuner chose for this grid's levels"""
+    from lowmachmixtures_b200 import _native
+    lib = _native.load()
+    need = lib.lmm_autotune_report(None, 0)
+    buf = ctypes.create_string_buffer(need + 1)
+    lib.lmm_autotune_report(buf, need + 1)
+    return [ln for ln in buf.value.decode().splitlines() if f" {n}x{n}x{n}:" in ln]
 
 
 def profiled_traffic(key):
@@ -499,7 +520,7 @@ def learned_leg(args, prob, n, local, solve_dev, d_in, d_xu, d_xp, world):
         rel = st["norm_resid_true"] / st["norm_b"]
     net.close()
     return {"value": steps / (ms / 1e3), "unit": "solves/s", "ms_per_step": ms / steps, "iterations": iters,
-            "true_rel_residual": rel, "accepted": acc.value, "tried": tried.value,
+            "true_rel_residual": rel, "network_columns_kept": acc.value, "network_corrections": tried.value,
             "train_seconds": train_s, "train_pairs": args.learned_steps * 4, "train_fields": args.learned_fields,
             "train_grid": "64^3", "loss_first": hist[0], "loss_last": sum(hist[-20:]) / 20}
 
