@@ -161,6 +161,9 @@ typedef struct lmm_knobs {
                                       shapes of the colour, operator and prolongation kernels and the
                                       process keeps the fastest; see lmm_autotune_report), -1 = this
                                       handle times nothing (shapes the process chose already apply) */
+    int    residual_fusion;        /* 3D periodic V-cycle: 1 = residual and restriction in one pass
+                                      through shared memory; 0 = default (a residual kernel and a
+                                      restriction kernel: measured faster) */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

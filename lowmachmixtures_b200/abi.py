@@ -94,6 +94,7 @@ _KNOB_FIELDS = [
     ("smoother_tma_cells", C.c_int),
     ("smoother_order", C.c_int),
     ("autotune", C.c_int),
+    ("residual_fusion", C.c_int),
 ]
 
 
@@ -117,7 +118,7 @@ KNOB_DEFAULTS = dict(
     gmres_max_inner=5, gmres_max_iter=100, gmres_min_iter=1,
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
     tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0, orthogonalization=0, host_wait=0,
-    ensemble_batch=0, smoother_tma=0, smoother_tma_slabs=0, smoother_tma_cells=0, smoother_order=0, autotune=0,
+    ensemble_batch=0, smoother_tma=0, smoother_tma_slabs=0, smoother_tma_cells=0, smoother_order=0, autotune=0, residual_fusion=0,
 )
 
 

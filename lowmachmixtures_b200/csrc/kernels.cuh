@@ -499,7 +499,11 @@ __global__ void __launch_bounds__(kThreads) k_restrict(Dims F, const T* __restri
 }
 
 // Residual and restriction of one 3D periodic level in one pass
-// (stag_mg_solver.f90:406-437 then stag_restriction, :1133-1171): a block
+// (stag_mg_solver.f90:406-437 then stag_restriction, :1133-1171), opt-in
+// (knobs.residual_fusion = 1): it saves writing and re-reading the fine
+// residual but evaluates the face layer each block shares with its
+// neighbour twice and launches few blocks on coarse levels, and measured
+// slower than the split pair below on every level of the benchmark.  A block
 // owns RCX x RCY x RCZ coarse cells; it evaluates into shared memory every
 // fine residual r = (L phi - rhs) * -1 that their 12-point restrictions read
 // (the fine faces of the tile plus one face layer on the low and high side
@@ -1331,10 +1335,10 @@ void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const 
 
 template <class T>
 void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
-                              const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s) {
+                              const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s, int fused) {
     if (F.D.wall) return wl_residual_restrict<T>(F, Cc, visc, rhs_f, phi_f, rhs_c, s);
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
-    if (F.D.dm == 3 && Cc.D.nx % RCX == 0 && Cc.D.ny % RCY == 0 && Cc.D.nz % RCZ == 0 && !odd_level(F.D)) {
+    if (fused && F.D.dm == 3 && Cc.D.nx % RCX == 0 && Cc.D.ny % RCY == 0 && Cc.D.nz % RCZ == 0 && !odd_level(F.D)) {
         // residual and restriction in one pass, the residual kept in shared memory
         const dim3 grid(Cc.D.nx / RCX, Cc.D.ny / RCY, Cc.D.nz / RCZ);
         LMM_VISC_DISPATCH(visc, launch_pdl(k_resid_restrict3<T, V>, grid, dim3(kThreads), 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], Cc.D, rhs_c[0], rhs_c[1], rhs_c[2], dxsqinv))
@@ -1562,7 +1566,7 @@ namespace lmm {
     template void launch_gs_pair<T>(const LevelDev<T>&, int, int, const T* const[3], const T* const[3], T*, double, int,        \
                                     cudaStream_t);                                                                             \
     template void launch_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, int, const T* const[3],                  \
-                                              const T* const[3], T* const[3], cudaStream_t);                                   \
+                                              const T* const[3], T* const[3], cudaStream_t, int);                              \
     template void launch_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, const T* const[3], T* const[3], cudaStream_t); \
     template void launch_coarsen_coeffs<T>(const LevelDev<T>&, const LevelDev<T>&, bool, cudaStream_t);                        \
     template void launch_cc_smooth<T>(const LevelDev<T>&, int, cudaStream_t);                                                   \

@@ -73,9 +73,12 @@ cudaError_t launch_gs_pair_tma(const LevelDev<T>& L, int visc, int comp, const T
 template <class T>
 void launch_jacobi(const LevelDev<T>& L, int visc, const T* const rhs[3], const T* const phi_in[3], T* const phi_out[3],
                    double omega, cudaStream_t s);
+// fused = 1: residual and restriction in one pass through shared memory
+// (3D periodic levels whose coarse sizes divide the tile), else a residual
+// kernel into F.tmp and a restriction kernel
 template <class T>
 void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int visc, const T* const rhs_f[3],
-                              const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s);
+                              const T* const phi_f[3], T* const rhs_c[3], cudaStream_t s, int fused = 0);
 template <class T>
 void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* const phi_c[3], T* const phi_f[3],
                         cudaStream_t s);

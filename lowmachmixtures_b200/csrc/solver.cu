@@ -717,7 +717,8 @@ void vcycle(lmm_handle* h, std::vector<LevelDev<T>>& L) {
         for (int d = 0; d < h->dm; ++d) LMM_CK(cudaMemsetAsync(L[l].phi[d], 0, L[l].n * sizeof(T), h->stream));
     for (int l = 0; l < lc && l < nl - 1; ++l) {
         smooth<T>(h, L[l], K.stag_mg_nsmooths_down);
-        launch_residual_restrict<T>(L[l], L[l + 1], K.visc_type, L[l].rhs, L[l].phi, L[l + 1].rhs, h->stream);
+        launch_residual_restrict<T>(L[l], L[l + 1], K.visc_type, L[l].rhs, L[l].phi, L[l + 1].rhs, h->stream,
+                                    K.residual_fusion > 0 ? 1 : 0);
         check_launch();
     }
     if (lc < nl) {
@@ -2271,7 +2272,7 @@ int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
                       SAME(learned_stage) && SAME(tail_cells) && SAME(tail_smem_kb) && SAME(use_graphs) &&
                       SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait) &&
                       SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells) && SAME(smoother_order) &&
-                      SAME(autotune);
+                      SAME(autotune) && SAME(residual_fusion);
 #undef SAME
     if (!same) {
         g_last_error = "lmm_stokes_update_knobs changes only the stopping rules; create a new handle for the rest";
@@ -2812,7 +2813,8 @@ extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* co
                                         double* const rhs_coarse[3]) {
     if (!h || h->batched || !h->coeffs_loaded || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
     try {
-        launch_residual_restrict<double>(h->L64[lev], h->L64[lev + 1], h->knobs.visc_type, rhs, phi, rhs_coarse, h->stream);
+        launch_residual_restrict<double>(h->L64[lev], h->L64[lev + 1], h->knobs.visc_type, rhs, phi, rhs_coarse, h->stream,
+                                         h->knobs.residual_fusion > 0 ? 1 : 0);
         check_launch();
         LMM_CK(host_wait(h));
         return LMM_OK;

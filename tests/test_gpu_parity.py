@@ -89,12 +89,17 @@ def test_smooth_colours_bit_exact(oracle, dm, n, visc, lev):
     s.close()
 
 
-@pytest.mark.parametrize("dm,n", [(2, 16), (3, 16)])
+@pytest.mark.parametrize("dm,n", [(2, 16), (3, 16), (3, 32)])
 @pytest.mark.parametrize("visc", [-1, -2, -3, 2])
-def test_residual_restrict_and_prolong_bit_exact(oracle, dm, n, visc):
+@pytest.mark.parametrize("fusion", [0, 1])
+def test_residual_restrict_and_prolong_bit_exact(oracle, dm, n, visc, fusion):
+    """Residual restriction (split, or with residual_fusion = 1 in one pass
+    through shared memory) and prolongation against the oracle, bit for bit."""
+    if dm == 2 and fusion:
+        pytest.skip("the fused pass is 3D")
     p, rng = random_problem(dm, n, 13, visc)
     k = oracle.default_knobs(visc_type=visc)
-    s = make_solver(p, visc_type=visc)
+    s = make_solver(p, visc_type=visc, residual_fusion=fusion)
     for lev in (0, 1):
         shp = oracle.level_shape(p, lev)
         shc = oracle.level_shape(p, lev + 1)
@@ -141,13 +146,15 @@ def test_vcycle_bit_exact(oracle, dm, n, visc, smoother, tail):
 @pytest.mark.parametrize("visc", VISCS)
 @pytest.mark.parametrize("fusion", [0, 1, 2, 4])
 def test_vcycle_fused_smoother_bit_exact(oracle, n, visc, fusion):
-    """One launch per colour (0), both colours of a component in one
-    out-of-place launch (1) and the same with 2 or 4 planes per block all
-    reproduce the reference's colour-by-colour Gauss-Seidel bit for bit."""
+    """One launch per colour (0; the launches alternate their plane order),
+    both colours of a component in one out-of-place launch (1) and the same
+    with 2 or 4 planes per block all reproduce the reference's
+    colour-by-colour Gauss-Seidel bit for bit (fusion 0 also with the
+    residual and restriction fused)."""
     p, rng = random_problem(3, n, 17, visc, theta=3.0)
     kn = dict(visc_type=visc)
     k = oracle.default_knobs(**kn)
-    s = make_solver(p, **kn, tail_cells=-1, smoother_fusion=fusion)
+    s = make_solver(p, **kn, tail_cells=-1, smoother_fusion=fusion, residual_fusion=1 if fusion == 0 else 0)
     rhs = [rng.standard_normal(p.shape) for _ in range(3)]
     ref = oracle.stag_mg_solver(p, k, rhs)
     phi = [dev(np.zeros(p.shape)) for _ in range(3)]
