@@ -813,19 +813,63 @@ __device__ __forceinline__ T cc_diag(const T* const a[3], const Nb& n, T dxsqinv
     return -(sum * dxsqinv);
 }
 
+// flag = 1 when an entry of a0, a1 or a2 (a1, a2 may be null) differs from
+// a0[0] in its bits
+template <class T>
+__global__ void k_uniform_check(const T* __restrict__ a0, const T* __restrict__ a1, const T* __restrict__ a2, int64_t n,
+                                int* __restrict__ flag) {
+    auto bits = [](T x) -> unsigned long long {
+        if constexpr (sizeof(T) == 8)
+            return (unsigned long long)__double_as_longlong((double)x);
+        else
+            return (unsigned long long)(unsigned)__float_as_int((float)x);
+    };
+    const unsigned long long v = bits(a0[0]);
+    bool diff = false;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n && !diff; t += (int64_t)gridDim.x * blockDim.x)
+        diff = bits(a0[t]) != v || (a1 && bits(a1[t]) != v) || (a2 && bits(a2[t]) != v);
+    if (diff) atomicOr(flag, 1);
+}
+
+// the same two expressions with every face coefficient equal to c (the
+// value each load would return: the same operations, the same bits)
+template <class T, int DM, int LD = 0>
+__device__ __forceinline__ T cc_lap_u(T c, const T* phi, const Nb& n, T dxsqinv) {
+    const int s = n.s;
+    const T p = ldp<LD>(phi, s);
+    T v = (c * (ldp<LD>(phi, s + n.op[0]) - p) - c * (p - ldp<LD>(phi, s + n.om[0]))) +
+          (c * (ldp<LD>(phi, s + n.op[1]) - p) - c * (p - ldp<LD>(phi, s + n.om[1])));
+    if constexpr (DM == 3) v = v + (c * (ldp<LD>(phi, s + n.op[2]) - p) - c * (p - ldp<LD>(phi, s + n.om[2])));
+    return v * dxsqinv;
+}
 template <class T, int DM>
+__device__ __forceinline__ T cc_diag_u(T c, T dxsqinv) {
+    T sum = c + c + c + c;
+    if constexpr (DM == 3) sum = sum + c + c;
+    return -(sum * dxsqinv);
+}
+
+// U: every face coefficient equals cu (the arrays a0..a2 are not read);
+// reverse: the blocks take the planes in decreasing order (see k_gs_colour)
+template <class T, int DM, bool U = false>
 __global__ void __launch_bounds__(kThreads) k_cc_smooth(Dims D, const T* a0, const T* a1, const T* a2, const T* __restrict__ rhs,
-                                                        T* phi, int parity, T dxsqinv) {
+                                                        T* phi, int parity, T dxsqinv, T cu, int reverse) {
     pdl_enter();
     const Pos q = pos3(D.nx >> 1, D.ny);
     if (!q.ok) return;
-    const int j = q.j, k = q.k;
+    const int j = q.j, k = reverse ? (int)gridDim.z - 1 - q.k : q.k;
     const int i = 2 * q.i + ((j + ck<DM>(k) + parity) & 1);
     Nb nb = make_nb(D, i, j, k);
-    const T* a[3] = {a0, a1, a2};
-    T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
-    T cur = phi[nb.s];
-    phi[nb.s] = cur + res / cc_diag<T, DM>(a, nb, dxsqinv);
+    if constexpr (U) {
+        T res = ld(rhs, nb.s) - cc_lap_u<T, DM>(cu, phi, nb, dxsqinv);
+        T cur = phi[nb.s];
+        phi[nb.s] = cur + res / cc_diag_u<T, DM>(cu, dxsqinv);
+    } else {
+        const T* a[3] = {a0, a1, a2};
+        T res = ld(rhs, nb.s) - cc_lap<T, DM>(a, phi, nb, dxsqinv);
+        T cur = phi[nb.s];
+        phi[nb.s] = cur + res / cc_diag<T, DM>(a, nb, dxsqinv);
+    }
 }
 
 // one colour of the pressure smoother on an odd level: new values from the
@@ -859,10 +903,10 @@ __device__ __forceinline__ T cc_res_at(const Dims& F, const T* const a[3], const
     return ldp<LD>(rhs, nb.s) - cc_lap<T, DM, LD>(a, phi, nb, dxsqinv);
 }
 
-template <class T, int DM>
+template <class T, int DM, bool U = false>
 __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const T* a0, const T* a1, const T* a2,
                                                                    const T* __restrict__ rhs, const T* __restrict__ phi, Dims Dc,
-                                                                   T* __restrict__ rc, T dxsqinv) {
+                                                                   T* __restrict__ rc, T dxsqinv, T cu) {
     pdl_enter();
     const Pos q = pos3(Dc.nx, Dc.ny);
     if (!q.ok) return;
@@ -870,7 +914,15 @@ __global__ void __launch_bounds__(kThreads) k_cc_residual_restrict(Dims F, const
     const int t = i + Dc.nx * (j + Dc.ny * k);
     const T* a[3] = {a0, a1, a2};
     const int I = 2 * i, J = 2 * j, K = 2 * k;
-#define R(ii, jj, kk) cc_res_at<T, DM>(F, a, phi, rhs, ii, jj, kk, dxsqinv)
+    auto res_at = [&](int ii, int jj, int kk) -> T {
+        if constexpr (U) {
+            Nb nb = make_nb(F, ii, jj, kk);
+            return ld(rhs, nb.s) - cc_lap_u<T, DM>(cu, phi, nb, dxsqinv);
+        } else {
+            return cc_res_at<T, DM>(F, a, phi, rhs, ii, jj, kk, dxsqinv);
+        }
+    };
+#define R(ii, jj, kk) res_at(ii, jj, kk)
     if constexpr (DM == 2)
         rc[t] = T(0.25) * (R(I, J, k) + R(I + 1, J, k) + R(I, J + 1, k) + R(I + 1, J + 1, k));
     else
@@ -1398,7 +1450,7 @@ void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pre
 }
 
 template <class T>
-void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s) {
+void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s, int reverse) {
     const T dxsqinv = T(1.0 / (L.dx * L.dx));
     if (odd_level(L.D)) {
         const G3 go = geom3(L.D.nx, L.D.ny, L.D.nz);
@@ -1411,20 +1463,42 @@ void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s) {
         return;
     }
     const G3 g = geom3(L.D.nx / 2, L.D.ny, L.D.nz);
+    const int rev = reverse ? 1 : 0;
+    if (L.pa_uniform) {
+        if (L.D.dm == 2)
+            launch_pdl(k_cc_smooth<T, 2, true>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv, L.pa_value, rev);
+        else
+            launch_pdl(k_cc_smooth<T, 3, true>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv, L.pa_value, rev);
+        return;
+    }
     if (L.D.dm == 2)
-        launch_pdl(k_cc_smooth<T, 2>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+        launch_pdl(k_cc_smooth<T, 2>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv, T(0), rev);
     else
-        launch_pdl(k_cc_smooth<T, 3>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv);
+        launch_pdl(k_cc_smooth<T, 3>, g.grid, g.block, 0, s, L.D, L.pa[0], L.pa[1], L.pa[2], L.prhs, L.pphi, parity, dxsqinv, T(0), rev);
+}
+
+template <class T>
+void launch_uniform_check(const LevelDev<T>& L, int* flag, cudaStream_t s) {
+    const int64_t n = L.n;
+    const int blocks = (int)std::min<int64_t>((n + kThreads - 1) / kThreads, 1184);
+    k_uniform_check<T><<<blocks, kThreads, 0, s>>>(L.pa[0], L.pa[1], L.D.dm == 3 ? L.pa[2] : nullptr, n, flag);
 }
 
 template <class T>
 void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s) {
     const T dxsqinv = T(1.0 / (F.dx * F.dx));
     const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
+    if (F.pa_uniform) {
+        if (F.D.dm == 2)
+            launch_pdl(k_cc_residual_restrict<T, 2, true>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv, F.pa_value);
+        else
+            launch_pdl(k_cc_residual_restrict<T, 3, true>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv, F.pa_value);
+        return;
+    }
     if (F.D.dm == 2)
-        launch_pdl(k_cc_residual_restrict<T, 2>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+        launch_pdl(k_cc_residual_restrict<T, 2>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv, T(0));
     else
-        launch_pdl(k_cc_residual_restrict<T, 3>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv);
+        launch_pdl(k_cc_residual_restrict<T, 3>, g.grid, g.block, 0, s, F.D, F.pa[0], F.pa[1], F.pa[2], F.prhs, F.pphi, Cc.D, Cc.prhs, dxsqinv, T(0));
 }
 
 template <class T>
@@ -1569,9 +1643,10 @@ namespace lmm {
                                               const T* const[3], T* const[3], cudaStream_t, int);                              \
     template void launch_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, const T* const[3], T* const[3], cudaStream_t); \
     template void launch_coarsen_coeffs<T>(const LevelDev<T>&, const LevelDev<T>&, bool, cudaStream_t);                        \
-    template void launch_cc_smooth<T>(const LevelDev<T>&, int, cudaStream_t);                                                   \
+    template void launch_cc_smooth<T>(const LevelDev<T>&, int, cudaStream_t, int);                                              \
     template void launch_cc_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, cudaStream_t);                        \
     template void launch_cc_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, cudaStream_t);                              \
+    template void launch_uniform_check<T>(const LevelDev<T>&, int*, cudaStream_t);                                            \
     template void launch_neg_cc_lap<T>(const LevelDev<T>&, const T*, T*, cudaStream_t);                                        \
     template void launch_div_plus<T>(const LevelDev<T>&, const T* const[3], const T*, T*, cudaStream_t);                        \
     template void launch_sub_weighted_grad<T>(const LevelDev<T>&, const T* const[3], const T*, T* const[3], cudaStream_t);     \

@@ -28,6 +28,11 @@ struct LevelDev {
     T* tmp[3];          // Jacobi output / scratch
     // pressure (cell-centred) multigrid level
     T* pa[3];           // face coefficient 1/alpha (coarsened)
+    // every entry of pa holds the same value pa_value (checked on the
+    // device at every coefficient load): the pressure kernels then take it
+    // as a scalar instead of reading three face arrays
+    int pa_uniform;
+    T pa_value;
     T* pmu[3];          // BFBt: face coefficient 1/diag(viscous operator) (coarsened)
     T* pphi;
     T* prhs;
@@ -112,10 +117,15 @@ template <class T>
 size_t tail_smem_bytes(const LevelDev<T>* L, int nl, bool stag, bool jacobi);
 
 // ---- pressure multigrid (this library's cell-centred V-cycle) ----
+// reverse: the launch takes the planes in decreasing order (same values)
 template <class T>
-void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s);
+void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s, int reverse = 0);
 template <class T>
 void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s);
+// *flag |= 1 when the level's pressure face coefficients are not all the
+// same value (bit for bit)
+template <class T>
+void launch_uniform_check(const LevelDev<T>& L, int* flag, cudaStream_t s);
 template <class T>
 void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s);
 template <class T>

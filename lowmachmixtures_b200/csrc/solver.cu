@@ -163,6 +163,7 @@ struct lmm_handle {
     unsigned* counter = nullptr;
     double* scal = nullptr;       // device scalar slots (8 doubles per slot)
     double* hscal = nullptr;      // pinned host mirror
+    double* hmisc = nullptr;      // pinned: per-level pressure coefficients and flags (64 doubles)
     int red_blocks = 0;
     static constexpr int kSlots = 256;
     // BoxLib staging
@@ -552,6 +553,30 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
         for (int d = 0; d < dm; ++d) launch_convert<double, float>(h->alphainv[d], h->alphainv32[d], n, h->stream);
         check_launch();
     }
+    // pressure levels whose face coefficients are one value (constant
+    // density): their smoother and residual take it as a scalar
+    {
+        const int np = std::min(h->nlev_p, 32);
+        int* flags = h->dev_err + 32;
+        LMM_CK(cudaMemsetAsync(flags, 0, 32 * sizeof(int), h->stream));
+        for (int l = 0; l < np; ++l) {
+            launch_uniform_check<double>(h->L64[l], flags + l, h->stream);
+            check_launch();
+            LMM_CK(cudaMemcpyAsync(h->hmisc + l, h->L64[l].pa[0], sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        }
+        int* hflags = reinterpret_cast<int*>(h->hmisc + 32);
+        LMM_CK(cudaMemcpyAsync(hflags, flags, 32 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        LMM_CK(host_wait(h));
+        for (int l = 0; l < (int)h->L64.size(); ++l) {
+            const bool u = l < np && hflags[l] == 0 && !h->D0.wall;
+            h->L64[l].pa_uniform = u ? 1 : 0;
+            h->L64[l].pa_value = u ? h->hmisc[l] : 0.0;
+            if (l < (int)h->L32.size()) {
+                h->L32[l].pa_uniform = h->L64[l].pa_uniform;
+                h->L32[l].pa_value = (float)h->L64[l].pa_value;
+            }
+        }
+    }
     h->coeffs_loaded = true;
     h->theta_loaded = theta;
 }
@@ -805,7 +830,7 @@ template <class T>
 void cc_smooth(lmm_handle* h, LevelDev<T>& L, int nsweeps) {
     for (int s = 0; s < nsweeps; ++s)
         for (int parity = 0; parity < 2; ++parity) {
-            launch_cc_smooth<T>(L, parity, h->stream);
+            launch_cc_smooth<T>(L, parity, h->stream, (h->knobs.smoother_order == 0 && parity == 1) ? 1 : 0);
             check_launch();
         }
 }
@@ -913,9 +938,21 @@ void visc_schur(lmm_handle* h, T* mac, T* x_p) {
     T* lg[3] = {S.bf[5], S.bf[6], S.bf[7]};
     const T* m[3] = {L0.pmu[0], L0.pmu[1], L0.pmu[2]};
     if (std::fabs(theta) > 0.0) LMM_CK(cudaMemcpyAsync(keep, L0.pphi, n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
+    // the pressure solves of BFBt use 1/diag(viscous operator) as face
+    // coefficient: swapped into pa, with the uniform-coefficient path off
+    std::vector<int> uni(h->nlev_p, 0);
+    bool swapped = false;
     auto swap_coefficients = [&]() {
-        for (int l = 0; l < h->nlev_p; ++l)
+        swapped = !swapped;
+        for (int l = 0; l < h->nlev_p; ++l) {
             for (int d = 0; d < dm; ++d) std::swap(L[l].pa[d], L[l].pmu[d]);
+            if (swapped) {
+                uni[l] = L[l].pa_uniform;
+                L[l].pa_uniform = 0;
+            } else {
+                L[l].pa_uniform = uni[l];
+            }
+        }
     };
     swap_coefficients();
     // STEP 1: phi_mu = (D M G)^-1 rhs
@@ -2204,6 +2241,7 @@ static int create_impl(const lmm_grid* g, const lmm_knobs* k, int device, int ba
         h->stage_elems = st;
         h->stage = h->alloc<double>(st);
         LMM_CK(cudaMallocHost(&h->hscal, 8 * sizeof(double) * lmm_handle::kSlots));
+        LMM_CK(cudaMallocHost(&h->hmisc, 64 * sizeof(double)));
         if (batched) {
             h->bslots = h->alloc<double>((int64_t)lmm_handle::kBSlots * batch * 8);
             h->ys = h->alloc<double>((int64_t)(h->m + 1) * batch);
@@ -2303,6 +2341,7 @@ int lmm_stokes_destroy(lmm_handle* h) {
     if (h->arena) cudaFree(h->arena);
     if (h->lrn_block) cudaFree(h->lrn_block);
     if (h->hscal) cudaFreeHost(h->hscal);
+    if (h->hmisc) cudaFreeHost(h->hmisc);
     if (h->bhost) cudaFreeHost(h->bhost);
     if (h->ys_host) cudaFreeHost(h->ys_host);
     if (h->gtab_host) cudaFreeHost(h->gtab_host);

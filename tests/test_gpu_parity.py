@@ -275,6 +275,29 @@ def test_apply_precon(oracle, dm, n, pt, theta, tail_cells):
     s.close()
 
 
+@pytest.mark.parametrize("dm,n", [(2, 32), (3, 16), (3, 32)])
+@pytest.mark.parametrize("pt", [1, 2, -1, 5])
+def test_apply_precon_uniform_density(oracle, dm, n, pt):
+    """With alpha_fc the same on every face (constant density) the pressure
+    multigrid takes its face coefficient as a scalar instead of reading
+    three arrays; same tolerance against the oracle as the general path."""
+    p, rng = random_problem(dm, n, 43, -2, theta=50.0)
+    p.alpha_fc = [np.full(p.shape, 1.25) for _ in range(dm)]
+    k = oracle.default_knobs(visc_type=-2, precon_type=pt)
+    s = make_solver(p, visc_type=-2, precon_type=pt)
+    bu = [rng.standard_normal(p.shape) for _ in range(dm)]
+    bpp = rng.standard_normal(p.shape)
+    ref_u, ref_p = oracle.apply_precon(p, k, bu, bpp)
+    xu = [dev(np.zeros(p.shape)) for _ in range(dm)]
+    xp = dev(np.zeros(p.shape))
+    s.apply_precon([dev(a) for a in bu], dev(bpp), xu, xp)
+    scale = max(np.abs(r).max() for r in ref_u + [ref_p])
+    for c in range(dm):
+        np.testing.assert_allclose(host(xu[c]), ref_u[c], rtol=0, atol=1e-12 * scale)
+    np.testing.assert_allclose(host(xp), ref_p, rtol=0, atol=1e-12 * scale)
+    s.close()
+
+
 def _solve_both(oracle, prob, **kn):
     k = oracle.default_knobs(**kn)
     rc_o, xu_o, xp_o, th_o, npr_o, st_o = oracle.solve(prob, k)
