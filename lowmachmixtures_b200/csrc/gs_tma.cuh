@@ -58,66 +58,6 @@
 
 namespace lmm {
 
-// ------------------------------------------------------------ face arithmetic on values
-// L phi of one 3D face of component D from its loaded operands: p0 and nb =
-// {+x, -x, +y, -y, +z, -z} of the own component, q1/q2 the cross terms
-// {q(s+t), q(s), q(s-d+t), q(s-d)} of components t1, t2, a = theta alpha,
-// be/bm = beta at s and s-d, E1/E1p and E2/E2p the two edge arrays at s and
-// s+t, g/gm = gamma at s and s-d; b, c the constant beta, gamma of |visc|
-// 1..3.  Same expressions, same order as face_L3_own.
-template <class T, int VISC>
-__device__ __forceinline__ T face_L3_vals(T p0, const T (&nb)[6], int D, const T (&q1)[4], const T (&q2)[4], T a, T be, T bm,
-                                          T E1, T E1p, T E2, T E2p, T g, T gm, T dxsqinv, T b, T c) {
-    const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
-    if (VISC == 1) {
-        T nbs = nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5];
-        return p0 * (a + T(6) * b * dxsqinv) - nbs * b * dxsqinv;
-    }
-    const int t1 = (D == 0) ? 1 : 0, t2 = (D == 2) ? 1 : 2;
-    const T ppd = nb[2 * D], pmd = nb[2 * D + 1];
-    const T pp1 = nb[2 * t1], pm1 = nb[2 * t1 + 1];
-    const T pp2 = nb[2 * t2], pm2 = nb[2 * t2 + 1];
-    const T c10 = q1[0], c11 = q1[1], c12 = q1[2], c13 = q1[3];
-    const T c20 = q2[0], c21 = q2[1], c22 = q2[2], c23 = q2[3];
-    if (VISC == 2) {
-        return p0 * (a + T(8) * b * dxsqinv) -
-               (T(2) * ppd + T(2) * pmd + pp1 + pm1 + pp2 + pm2 + c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * b * dxsqinv;
-    }
-    if (VISC == 3) {
-        const T nbt = pp1 + pm1 + pp2 + pm2;
-        return p0 * (a + (T(20) * b * onethird + T(2) * c) * dxsqinv) -
-               ((ppd + pmd) * (fourthirds * b + c) + nbt * b +
-                (c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * (onethird * b + c)) * dxsqinv;
-    }
-    if (VISC == -1) {
-        return p0 * (a + (be + bm + E1 + E1p + E2 + E2p) * dxsqinv) -
-               (ppd * be + pmd * bm + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2) * dxsqinv;
-    }
-    if (VISC == -2) {
-        return p0 * (a + (T(2) * be + T(2) * bm + E1 + E1p + E2 + E2p) * dxsqinv) -
-               (T(2) * ppd * be + T(2) * pmd * bm + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2 + c10 * E1p - c11 * E1 - c12 * E1p +
-                c13 * E1 + c20 * E2p - c21 * E2 - c22 * E2p + c23 * E2) * dxsqinv;
-    }
-    // VISC == -3
-    return p0 * (a + (fourthirds * be + g + fourthirds * bm + gm + E1 + E1p + E2 + E2p) * dxsqinv) -
-           (ppd * (fourthirds * be + g) + pmd * (fourthirds * bm + gm) + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2 +
-            c10 * (E1p - twothirds * be + g) - c11 * (E1 - twothirds * be + g) - c12 * (E1p - twothirds * bm + gm) +
-            c13 * (E1 - twothirds * bm + gm) + c20 * (E2p - twothirds * be + g) - c21 * (E2 - twothirds * be + g) -
-            c22 * (E2p - twothirds * bm + gm) + c23 * (E2 - twothirds * bm + gm)) * dxsqinv;
-}
-
-// the diagonal of the same face (face_diag3's expressions)
-template <class T, int VISC>
-__device__ __forceinline__ T face_diag3_vals(T a, T be, T bm, T E1, T E1p, T E2, T E2p, T g, T gm, T dxsqinv, T b, T c) {
-    if (VISC == 1) return a + T(6) * b * dxsqinv;
-    if (VISC == 2) return a + T(8) * b * dxsqinv;
-    if (VISC == 3) return a + (T(20) / T(3) * b + T(2) * c) * dxsqinv;
-    if (VISC == -1) return a + (be + bm + E1 + E1p + E2 + E2p) * dxsqinv;
-    if (VISC == -2) return a + (T(2) * be + T(2) * bm + E1 + E1p + E2 + E2p) * dxsqinv;
-    const T fourthirds = T(4) / T(3);
-    return a + (fourthirds * be + g + fourthirds * bm + gm + E1 + E1p + E2 + E2p) * dxsqinv;
-}
-
 namespace gst {
 
 constexpr int kNS = 4;    // plane sets of the ring (5 where one CTA per SM has the room: Geo::NS)

@@ -185,11 +185,15 @@ __global__ void __launch_bounds__(kThreads) k_gs_colour(Dims D, Coef<T> C, const
     if (W && wall_face(nb, COMP)) return;
     const T* phi[3] = {p0, p1, p2};
     const T b = ld(C.beta, 0), c = ld(C.gamma, 0);
-    T Lp = face_L<T, DM, VISC, COMP, 0, T, W>(phi, C, nb, dxsqinv, b, c);
-    T fac = face_diag<T, DM, VISC, COMP, W>(C, nb, dxsqinv, b, c);
     T* p = (COMP == 0) ? p0 : (COMP == 1 ? p1 : p2);
-    T cur = p[nb.s];
-    p[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
+    if constexpr (DM == 3 && !W) {
+        p[nb.s] = face_update3<T, VISC, COMP>(phi, C, rhs, nb, dxsqinv, b, c, omega);
+    } else {
+        T Lp = face_L<T, DM, VISC, COMP, 0, T, W>(phi, C, nb, dxsqinv, b, c);
+        T fac = face_diag<T, DM, VISC, COMP, W>(C, nb, dxsqinv, b, c);
+        T cur = p[nb.s];
+        p[nb.s] = cur + omega * (ld(rhs, nb.s) - Lp) / fac;
+    }
 }
 
 // --------------------------------------------------------------- odd levels

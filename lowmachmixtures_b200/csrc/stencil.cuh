@@ -301,6 +301,112 @@ __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv
     return a + (fourthirds * be + g + fourthirds * bm + gm + E1 + E1p + E2 + E2p) * dxsqinv;
 }
 
+// ------------------------------------------------------------ face arithmetic on values
+// L phi of one 3D face of component D from its loaded operands: p0 and nb =
+// {+x, -x, +y, -y, +z, -z} of the own component, q1/q2 the cross terms
+// {q(s+t), q(s), q(s-d+t), q(s-d)} of components t1, t2, a = theta alpha,
+// be/bm = beta at s and s-d, E1/E1p and E2/E2p the two edge arrays at s and
+// s+t, g/gm = gamma at s and s-d; b, c the constant beta, gamma of |visc|
+// 1..3.  Same expressions, same order as face_L3_own.
+template <class T, int VISC>
+__device__ __forceinline__ T face_L3_vals(T p0, const T (&nb)[6], int D, const T (&q1)[4], const T (&q2)[4], T a, T be, T bm,
+                                          T E1, T E1p, T E2, T E2p, T g, T gm, T dxsqinv, T b, T c) {
+    const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
+    if (VISC == 1) {
+        T nbs = nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5];
+        return p0 * (a + T(6) * b * dxsqinv) - nbs * b * dxsqinv;
+    }
+    const int t1 = (D == 0) ? 1 : 0, t2 = (D == 2) ? 1 : 2;
+    const T ppd = nb[2 * D], pmd = nb[2 * D + 1];
+    const T pp1 = nb[2 * t1], pm1 = nb[2 * t1 + 1];
+    const T pp2 = nb[2 * t2], pm2 = nb[2 * t2 + 1];
+    const T c10 = q1[0], c11 = q1[1], c12 = q1[2], c13 = q1[3];
+    const T c20 = q2[0], c21 = q2[1], c22 = q2[2], c23 = q2[3];
+    if (VISC == 2) {
+        return p0 * (a + T(8) * b * dxsqinv) -
+               (T(2) * ppd + T(2) * pmd + pp1 + pm1 + pp2 + pm2 + c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * b * dxsqinv;
+    }
+    if (VISC == 3) {
+        const T nbt = pp1 + pm1 + pp2 + pm2;
+        return p0 * (a + (T(20) * b * onethird + T(2) * c) * dxsqinv) -
+               ((ppd + pmd) * (fourthirds * b + c) + nbt * b +
+                (c10 - c11 - c12 + c13 + c20 - c21 - c22 + c23) * (onethird * b + c)) * dxsqinv;
+    }
+    if (VISC == -1) {
+        return p0 * (a + (be + bm + E1 + E1p + E2 + E2p) * dxsqinv) -
+               (ppd * be + pmd * bm + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2) * dxsqinv;
+    }
+    if (VISC == -2) {
+        return p0 * (a + (T(2) * be + T(2) * bm + E1 + E1p + E2 + E2p) * dxsqinv) -
+               (T(2) * ppd * be + T(2) * pmd * bm + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2 + c10 * E1p - c11 * E1 - c12 * E1p +
+                c13 * E1 + c20 * E2p - c21 * E2 - c22 * E2p + c23 * E2) * dxsqinv;
+    }
+    // VISC == -3
+    return p0 * (a + (fourthirds * be + g + fourthirds * bm + gm + E1 + E1p + E2 + E2p) * dxsqinv) -
+           (ppd * (fourthirds * be + g) + pmd * (fourthirds * bm + gm) + pp1 * E1p + pm1 * E1 + pp2 * E2p + pm2 * E2 +
+            c10 * (E1p - twothirds * be + g) - c11 * (E1 - twothirds * be + g) - c12 * (E1p - twothirds * bm + gm) +
+            c13 * (E1 - twothirds * bm + gm) + c20 * (E2p - twothirds * be + g) - c21 * (E2 - twothirds * be + g) -
+            c22 * (E2p - twothirds * bm + gm) + c23 * (E2 - twothirds * bm + gm)) * dxsqinv;
+}
+
+// the diagonal of the same face (face_diag3's expressions)
+template <class T, int VISC>
+__device__ __forceinline__ T face_diag3_vals(T a, T be, T bm, T E1, T E1p, T E2, T E2p, T g, T gm, T dxsqinv, T b, T c) {
+    if (VISC == 1) return a + T(6) * b * dxsqinv;
+    if (VISC == 2) return a + T(8) * b * dxsqinv;
+    if (VISC == 3) return a + (T(20) / T(3) * b + T(2) * c) * dxsqinv;
+    if (VISC == -1) return a + (be + bm + E1 + E1p + E2 + E2p) * dxsqinv;
+    if (VISC == -2) return a + (T(2) * be + T(2) * bm + E1 + E1p + E2 + E2p) * dxsqinv;
+    const T fourthirds = T(4) / T(3);
+    return a + (fourthirds * be + g + fourthirds * bm + gm + E1 + E1p + E2 + E2p) * dxsqinv;
+}
+
+// One Gauss-Seidel update of a 3D face of component D on a periodic grid,
+// phi + omega (rhs - L phi) / diag, with every operand read once from
+// global memory and L phi and the diagonal formed from the same values
+// (face_L3_vals, face_diag3_vals: face_L3 / face_diag3's expressions, so
+// the same bits).
+template <class T, int VISC, int D>
+__device__ __forceinline__ T face_update3(const T* const phi[3], const Coef<T>& C, const T* rhs, const Nb& n, T dxsqinv, T b,
+                                          T c, T omega) {
+    constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
+    const int s = n.s;
+    const T* p = phi[D];
+    const T p0 = ld(p, s);
+    const T nb[6] = {ld(p, s + n.op[0]), ld(p, s + n.om[0]), ld(p, s + n.op[1]),
+                     ld(p, s + n.om[1]), ld(p, s + n.op[2]), ld(p, s + n.om[2])};
+    T q1[4] = {T(0), T(0), T(0), T(0)}, q2[4] = {T(0), T(0), T(0), T(0)};
+    if constexpr (VISC == 2 || VISC == 3 || VISC == -2 || VISC == -3) {
+        const T* a1 = phi[t1];
+        const T* a2 = phi[t2];
+        q1[0] = ld(a1, s + n.op[t1]);
+        q1[1] = ld(a1, s);
+        q1[2] = ld(a1, s + n.om[D] + n.op[t1]);
+        q1[3] = ld(a1, s + n.om[D]);
+        q2[0] = ld(a2, s + n.op[t2]);
+        q2[1] = ld(a2, s);
+        q2[2] = ld(a2, s + n.om[D] + n.op[t2]);
+        q2[3] = ld(a2, s + n.om[D]);
+    }
+    const T a = ld(C.alpha[D], s);
+    T be = T(0), bm = T(0), E1 = T(0), E1p = T(0), E2 = T(0), E2p = T(0), g = T(0), gm = T(0);
+    if constexpr (VISC < 0) {
+        be = ld(C.beta, s);
+        bm = ld(C.beta, s + n.om[D]);
+        E1 = ld(C.bed[e1], s);
+        E1p = ld(C.bed[e1], s + n.op[t1]);
+        E2 = ld(C.bed[e2], s);
+        E2p = ld(C.bed[e2], s + n.op[t2]);
+    }
+    if constexpr (VISC == -3) {
+        g = ld(C.gamma, s);
+        gm = ld(C.gamma, s + n.om[D]);
+    }
+    const T Lp = face_L3_vals<T, VISC>(p0, nb, D, q1, q2, a, be, bm, E1, E1p, E2, E2p, g, gm, dxsqinv, b, c);
+    const T fac = face_diag3_vals<T, VISC>(a, be, bm, E1, E1p, E2, E2p, g, gm, dxsqinv, b, c);
+    return p0 + omega * (ld(rhs, s) - Lp) / fac;
+}
+
 // ------------------------------------------------------------------ 2D
 template <class T, int VISC, int D, int LD = 0, class TP = T, bool W = false>
 __device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
