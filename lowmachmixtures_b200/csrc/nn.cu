@@ -7,6 +7,7 @@
 #include "../../include/lmm_learned.h"
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
+#include "conv_tile.cuh"
 #include "nn_layers.cuh"
 #include "tc.cuh"
 
@@ -91,6 +92,34 @@ int conv3d(const bf16* x, const bf16* w, const float* bias, const bf16* skip, co
     G.N = round_up(Cout, 16);
     G.K = 27 * Cin;
     ConvEpi E{bias, skip, mask, out, out32, G.Mtot, Cout, Cs, relu};
+    // the shifted-view tile kernel where the grid tiles by 8 x 16 and the
+    // weights and three halo planes fit in shared memory
+    const int cinp = round_up(Cin, 16);
+    if (nx % kTX == 0 && ny % kTY == 0 && G.N <= 64 && (cinp == 16 || cinp == 32 || cinp == 64) &&
+        tile_smem_bytes(cinp, G.N) <= 227 * 1024) {
+        TileConvArgs A{x, w, nx, ny, nz, up, Cin, G.N, B, 1, nx / kTX, ny / kTY, 1};
+        const int tiles = A.tiles_x * A.tiles_y * B;
+        int zch = (148 * 4 + tiles - 1) / tiles;
+        zch = zch < 1 ? 1 : (zch > nz ? nz : zch);
+        A.KZ = (nz + zch - 1) / zch;
+        A.zchunks = (nz + A.KZ - 1) / A.KZ;
+        const size_t smem = tile_smem_bytes(cinp, G.N);
+        const unsigned blocks = (unsigned)(tiles * A.zchunks);
+        cudaError_t e = cudaSuccess;
+        if (cinp == 16) {
+            e = raise_smem_limit((const void*)k_conv3d_tile<16>, smem);
+            if (e == cudaSuccess) k_conv3d_tile<16><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
+        } else if (cinp == 32) {
+            e = raise_smem_limit((const void*)k_conv3d_tile<32>, smem);
+            if (e == cudaSuccess) k_conv3d_tile<32><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
+        } else {
+            e = raise_smem_limit((const void*)k_conv3d_tile<64>, smem);
+            if (e == cudaSuccess) k_conv3d_tile<64><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
+        }
+        if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+        count_launch();
+        return LMM_OK;
+    }
     if (raise_smem_limit((const void*)k_conv3d, tc::smem_bytes(G.N)) != cudaSuccess) return LMM_ERR_CUDA;
     k_conv3d<<<(G.Mtot + tc::kM - 1) / tc::kM, tc::kThreadsTC, tc::smem_bytes(G.N), s>>>(G, E, err);
     if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;

@@ -70,8 +70,14 @@ def _packed(w, with_t=False):
     return wf, wt
 
 
+# grids whose x tiles by 8 and y by 16 run the shifted-view tile kernel
+# (conv_tile.cuh) when its weights fit in shared memory; the others the
+# gathered implicit GEMM
 @pytest.mark.parametrize("B,n,cin,cout,up,relu", [(2, (16, 8, 8), 16, 32, 0, 1), (1, (16, 16, 8), 32, 16, 1, 1),
-                                                  (1, (8, 8, 8), 64, 64, 0, 0), (1, (32, 16, 16), 8, 16, 0, 1)])
+                                                  (1, (8, 8, 8), 64, 64, 0, 0), (1, (32, 16, 16), 8, 16, 0, 1),
+                                                  (2, (16, 32, 8), 16, 16, 0, 1), (1, (32, 32, 8), 64, 32, 1, 1),
+                                                  (1, (16, 16, 16), 32, 64, 0, 1), (1, (24, 16, 6), 16, 48, 0, 0),
+                                                  (1, (16, 16, 4), 64, 64, 0, 1), (1, (16, 16, 8), 8, 16, 0, 0)])
 def test_conv3d_matches_torch(B, n, cin, cout, up, relu):
     import torch
     from lowmachmixtures_b200 import _native
