@@ -7,7 +7,7 @@
 #include "../../include/lmm_learned.h"
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
-#include "conv_tile.cuh"
+#include "conv_tile_zn.cuh"
 #include "nn_layers.cuh"
 #include "tc.cuh"
 
@@ -77,6 +77,98 @@ namespace nn {
 
 static inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
+// persistent launch of a tile kernel (ZN: the z taps in N, else 27 taps):
+// as many CTAs as are resident at once (shared memory, registers and TMEM
+// columns permitting), split evenly over the output-channel slices, each
+// taking an equal run of its slice's (tile, plane) sequence
+template <bool ZN, int CINP, int NS>
+static int launch_tile_n(TileConvArgs A, const ConvEpi& E, int* err, cudaStream_t s) {
+    constexpr int smem_c = ZN ? zn_smem_bytes(CINP, NS) : tile_smem_bytes(CINP, NS);
+    if constexpr (smem_c > 227 * 1024 || (ZN && (CINP > 32 || NS > 32))) {
+        return LMM_ERR_INVALID;
+    } else {
+        const void* kern;
+        if constexpr (ZN)
+            kern = (const void*)k_conv3d_tile_zn<CINP, NS>;
+        else
+            kern = (const void*)k_conv3d_tile<CINP, NS>;
+        const size_t smem = smem_c;
+        if (raise_smem_limit(kern, smem) != cudaSuccess) return LMM_ERR_CUDA;
+        // resident CTAs per SM, from the SM's shared memory (the carveout is
+        // set to its maximum), its register file and its 512 TMEM columns
+        static int per_sm_cached[16] = {};
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return LMM_ERR_CUDA;
+        int per_sm = dev < 16 ? per_sm_cached[dev] : 0;
+        if (per_sm == 0) {
+            int smem_sm = 0, smem_rsv = 0, regs_sm = 0;
+            cudaFuncAttributes fa;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
+                cudaFuncGetAttributes(&fa, kern) != cudaSuccess ||
+                cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess)
+                return LMM_ERR_CUDA;
+            const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + smem_rsv);
+            const int regs_warp = ((fa.numRegs + 7) / 8 * 8) * 32;
+            const int by_regs = regs_sm / (regs_warp * (tc::kThreadsTC / 32));
+            const int by_tmem = 512 / (int)(ZN ? zn_tmem_cols(NS) : tile_tmem_cols(NS));
+            per_sm = by_smem < by_regs ? by_smem : by_regs;
+            per_sm = per_sm < by_tmem ? per_sm : by_tmem;
+            per_sm = per_sm < 16 ? per_sm : 16;
+            if (per_sm < 1) per_sm = 1;
+            if (dev < 16) per_sm_cached[dev] = per_sm;
+        }
+        int64_t cps = (int64_t)sms * per_sm / A.slices;
+        cps = cps < 1 ? 1 : (cps > A.total ? A.total : cps);
+        A.ctas_per_slice = (int)cps;
+        const unsigned blocks = (unsigned)(A.slices * cps);
+        if constexpr (ZN)
+            k_conv3d_tile_zn<CINP, NS><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
+        else
+            k_conv3d_tile<CINP, NS><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
+        if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
+        count_launch();
+        return LMM_OK;
+    }
+}
+template <bool ZN, int CINP>
+static int launch_tile_c(int ns, const TileConvArgs& A, const ConvEpi& E, int* err, cudaStream_t s) {
+    switch (ns) {
+        case 16: return launch_tile_n<ZN, CINP, 16>(A, E, err, s);
+        case 32: return launch_tile_n<ZN, CINP, 32>(A, E, err, s);
+        case 48: return launch_tile_n<ZN, CINP, 48>(A, E, err, s);
+        case 64: return launch_tile_n<ZN, CINP, 64>(A, E, err, s);
+        default: return LMM_ERR_INVALID;
+    }
+}
+// LMM_ERR_INVALID: no tile instantiation for (zn, cinp, ns); the caller gathers
+static int launch_tile(bool zn, int cinp, int ns, const TileConvArgs& A, const ConvEpi& E, int* err, cudaStream_t s) {
+    switch (cinp) {
+        case 16: return zn ? launch_tile_c<true, 16>(ns, A, E, err, s) : launch_tile_c<false, 16>(ns, A, E, err, s);
+        case 32: return zn ? launch_tile_c<true, 32>(ns, A, E, err, s) : launch_tile_c<false, 32>(ns, A, E, err, s);
+        case 64: return launch_tile_c<false, 64>(ns, A, E, err, s);
+        default: return LMM_ERR_INVALID;
+    }
+}
+// the output-channel slice (a multiple of 16 dividing n) of a tile kernel:
+// with the z taps in N (*zn) for 16 or 32 input channels, the widest slice
+// leaving room for two CTAs per SM; else the 27-tap kernel's widest slice
+// that fits in shared memory; 0 when none does
+static int tile_slice(int cinp, int n, bool* zn) {
+    *zn = false;
+    if (cinp <= 32)
+        for (int ns = 32; ns >= 16; ns -= 16)
+            if (ns <= n && n % ns == 0 && zn_smem_bytes(cinp, ns) <= 113 * 1024) {
+                *zn = true;
+                return ns;
+            }
+    for (int ns = 64; ns >= 16; ns -= 16)
+        if (ns <= n && n % ns == 0 && tile_smem_bytes(cinp, ns) <= 227 * 1024) return ns;
+    return 0;
+}
+
 int conv3d(const bf16* x, const bf16* w, const float* bias, const bf16* skip, const bf16* mask, bf16* out, float* out32, int B,
            int nx, int ny, int nz, int up, int Cin, int Cout, int Cs, int relu, int* err, cudaStream_t s) {
     if (!x || !w || !err || (!out && !out32) || B < 1 || nx < 1 || ny < 1 || nz < 1 || Cin < 8 || (Cin % 8) || Cout < 1 ||
@@ -92,33 +184,17 @@ int conv3d(const bf16* x, const bf16* w, const float* bias, const bf16* skip, co
     G.N = round_up(Cout, 16);
     G.K = 27 * Cin;
     ConvEpi E{bias, skip, mask, out, out32, G.Mtot, Cout, Cs, relu};
-    // the shifted-view tile kernel where the grid tiles by 8 x 16 and the
-    // weights and three halo planes fit in shared memory
+    // the shifted-view tile kernel where the grid tiles by 8 x 16, a slice
+    // of the weights and the halo ring fit in shared memory, and skip / mask
+    // rows can be read as 16-byte vectors
     const int cinp = round_up(Cin, 16);
-    if (nx % kTX == 0 && ny % kTY == 0 && G.N <= 64 && (cinp == 16 || cinp == 32 || cinp == 64) &&
-        tile_smem_bytes(cinp, G.N) <= 227 * 1024) {
-        TileConvArgs A{x, w, nx, ny, nz, up, Cin, G.N, B, 1, nx / kTX, ny / kTY, 1};
-        const int tiles = A.tiles_x * A.tiles_y * B;
-        int zch = (148 * 4 + tiles - 1) / tiles;
-        zch = zch < 1 ? 1 : (zch > nz ? nz : zch);
-        A.KZ = (nz + zch - 1) / zch;
-        A.zchunks = (nz + A.KZ - 1) / A.KZ;
-        const size_t smem = tile_smem_bytes(cinp, G.N);
-        const unsigned blocks = (unsigned)(tiles * A.zchunks);
-        cudaError_t e = cudaSuccess;
-        if (cinp == 16) {
-            e = raise_smem_limit((const void*)k_conv3d_tile<16>, smem);
-            if (e == cudaSuccess) k_conv3d_tile<16><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
-        } else if (cinp == 32) {
-            e = raise_smem_limit((const void*)k_conv3d_tile<32>, smem);
-            if (e == cudaSuccess) k_conv3d_tile<32><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
-        } else {
-            e = raise_smem_limit((const void*)k_conv3d_tile<64>, smem);
-            if (e == cudaSuccess) k_conv3d_tile<64><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
-        }
-        if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
-        count_launch();
-        return LMM_OK;
+    bool zn = false;
+    const int ns = (cinp == 16 || cinp == 32 || cinp == 64) && G.N <= 64 ? tile_slice(cinp, G.N, &zn) : 0;
+    if (nx % kTX == 0 && ny % kTY == 0 && ns > 0 && ((!skip && !mask) || Cs % 8 == 0)) {
+        TileConvArgs A{x, w, nx, ny, nz, up, Cin, B, nx / kTX, ny / kTY, 0, G.N / ns, 1};
+        A.total = (int64_t)A.tiles_x * A.tiles_y * B * nz;
+        const int rc = launch_tile(zn, cinp, ns, A, E, err, s);
+        if (rc != LMM_ERR_INVALID) return rc;
     }
     if (raise_smem_limit((const void*)k_conv3d, tc::smem_bytes(G.N)) != cudaSuccess) return LMM_ERR_CUDA;
     k_conv3d<<<(G.Mtot + tc::kM - 1) / tc::kM, tc::kThreadsTC, tc::smem_bytes(G.N), s>>>(G, E, err);

@@ -77,7 +77,14 @@ def _packed(w, with_t=False):
                                                   (1, (8, 8, 8), 64, 64, 0, 0), (1, (32, 16, 16), 8, 16, 0, 1),
                                                   (2, (16, 32, 8), 16, 16, 0, 1), (1, (32, 32, 8), 64, 32, 1, 1),
                                                   (1, (16, 16, 16), 32, 64, 0, 1), (1, (24, 16, 6), 16, 48, 0, 0),
-                                                  (1, (16, 16, 4), 64, 64, 0, 1), (1, (16, 16, 8), 8, 16, 0, 0)])
+                                                  (1, (16, 16, 4), 64, 64, 0, 1), (1, (16, 16, 8), 8, 16, 0, 0),
+                                                  # more planes than resident CTAs: runs of several planes that
+                                                  # cross tile boundaries
+                                                  (1, (64, 64, 64), 16, 16, 0, 1), (2, (32, 48, 40), 32, 16, 1, 1),
+                                                  (1, (64, 32, 64), 64, 32, 1, 1), (3, (8, 16, 5), 16, 32, 0, 1),
+                                                  (1, (128, 128, 24), 16, 16, 0, 0),
+                                                  # output channels in slices: 2 x 32 and 3 x 16
+                                                  (1, (32, 32, 32), 64, 64, 0, 1), (1, (16, 32, 12), 64, 48, 0, 1)])
 def test_conv3d_matches_torch(B, n, cin, cout, up, relu):
     import torch
     from lowmachmixtures_b200 import _native
@@ -104,11 +111,12 @@ def test_conv3d_matches_torch(B, n, cin, cout, up, relu):
     np.testing.assert_allclose(out.float().cpu().numpy(), ref.cpu().numpy(), rtol=1e-2, atol=1e-2 * scale)
 
 
-def test_conv3d_fp32_output_and_mask():
+@pytest.mark.parametrize("n", [16, 64])
+def test_conv3d_fp32_output_and_mask(n):
     import torch
     from lowmachmixtures_b200 import _native
     lib = _native.load()
-    B, nx, ny, nz, cin, cout = 1, 16, 16, 16, 16, 4
+    B, nx, ny, nz, cin, cout = 1, n, n, n, 16, 4
     g = torch.Generator().manual_seed(5)
     x = torch.randn(B, nz, ny, nx, cin, generator=g).to(torch.bfloat16).cuda()
     w = (torch.randn(cout, 27, cin, generator=g) / 20).cuda()
