@@ -140,7 +140,8 @@ __global__ void __launch_bounds__(tc::kThreadsTC, tile_min_blocks(CINP, NS)) k_c
     constexpr int KS = CINP / 16;                       // K=16 steps per tap
     constexpr int NCH = NS / 16;                        // 16-column epilogue chunks
     constexpr int PLANE = tile_plane_bytes(CINP);
-    constexpr int UNITS = (CINP / 8) * kHalo;           // 16-byte units of one halo plane
+    constexpr int NGR = CINP / 8;                       // 8-channel groups
+    constexpr int UNITS = NGR * kHalo;                  // 16-byte units of one halo plane
     constexpr int PER = (UNITS + tc::kThreadsTC - 1) / tc::kThreadsTC;
     constexpr uint32_t NCOLS = tile_tmem_cols(NS);
     constexpr uint32_t ACC = NCOLS / 2;                 // column offset of accumulator 1
@@ -194,16 +195,22 @@ __global__ void __launch_bounds__(tc::kThreadsTC, tile_min_blocks(CINP, NS)) k_c
 
     auto wrapz = [&](int z) { return z < 0 ? z + A.nz : (z >= A.nz ? z - A.nz : z); };
     // asynchronous 16-byte copies of halo plane z into ring slot q (units
-    // of channel groups past Cin stay the zeros written at the start)
-    const uint32_t ring_s = tc::smem_u32(ring) + (uint32_t)tid * 16;
+    // of channel groups past Cin stay the zeros written at the start).  Unit
+    // u = tid + 128 i is channel group u % NGR of halo voxel u / NGR (groups
+    // fastest: a warp's copies cover whole sectors); sdst is its byte offset
+    // in a slot
+    uint32_t sdst[PER];
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int u = tid + tc::kThreadsTC * i, v = u / NGR, g = u - v * NGR;
+        sdst[i] = tc::smem_u32(ring) + (uint32_t)(g * kGStride + v * 16);
+    }
     auto fetch = [&](int z, int q) {
         const bf16* base = A.x + ((int64_t)b * nzi + (wrapz(z) >> A.up)) * in_plane;
-        const uint32_t dst = ring_s + (uint32_t)(q * PLANE);
 #pragma unroll
         for (int i = 0; i < PER; ++i)
             if (off[i] >= 0)
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + (uint32_t)(i * tc::kThreadsTC * 16)),
-                             "l"(base + off[i])
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst[i] + (uint32_t)(q * PLANE)), "l"(base + off[i])
                              : "memory");
     };
     auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
@@ -263,10 +270,9 @@ __global__ void __launch_bounds__(tc::kThreadsTC, tile_min_blocks(CINP, NS)) k_c
         y0 = ty * kTY;
 #pragma unroll
         for (int i = 0; i < PER; ++i) {
-            const int u = tid + tc::kThreadsTC * i;
+            const int u = tid + tc::kThreadsTC * i, v = u / NGR, g = u - v * NGR;
             off[i] = -1;
             if (u < UNITS) {
-                const int g = u / kHalo, v = u - g * kHalo;
                 const int hy = v / kHX, hx = v - hy * kHX;
                 int xx = x0 - 1 + hx, yy = y0 - 1 + hy;
                 xx = xx < 0 ? xx + A.nx : (xx >= A.nx ? xx - A.nx : xx);

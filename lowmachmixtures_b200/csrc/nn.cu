@@ -7,7 +7,7 @@
 #include "../../include/lmm_learned.h"
 #include "../../include/lmm_stokes.h"
 #include "kernels.h"
-#include "conv_tile_zn.cuh"
+#include "conv_tile_ws.cuh"
 #include "nn_layers.cuh"
 #include "tc.cuh"
 
@@ -77,19 +77,21 @@ namespace nn {
 
 static inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-// persistent launch of a tile kernel (ZN: the z taps in N, else 27 taps):
+// persistent launch of a tile kernel (ZN: the warp-specialised kernel with
+// the z taps in N, else 27 taps):
 // as many CTAs as are resident at once (shared memory, registers and TMEM
 // columns permitting), split evenly over the output-channel slices, each
 // taking an equal run of its slice's (tile, plane) sequence
 template <bool ZN, int CINP, int NS>
 static int launch_tile_n(TileConvArgs A, const ConvEpi& E, int* err, cudaStream_t s) {
-    constexpr int smem_c = ZN ? zn_smem_bytes(CINP, NS) : tile_smem_bytes(CINP, NS);
-    if constexpr (smem_c > 227 * 1024 || (ZN && (CINP > 32 || NS > 32))) {
+    constexpr int smem_c = ZN ? ws_smem_bytes(CINP, NS) : tile_smem_bytes(CINP, NS);
+    constexpr int threads = ZN ? kThreadsWS : tc::kThreadsTC;
+    if constexpr (smem_c > 227 * 1024 || (ZN && (CINP > 32 || NS != 16))) {
         return LMM_ERR_INVALID;
     } else {
         const void* kern;
         if constexpr (ZN)
-            kern = (const void*)k_conv3d_tile_zn<CINP, NS>;
+            kern = (const void*)k_conv3d_ws<CINP, NS>;
         else
             kern = (const void*)k_conv3d_tile<CINP, NS>;
         const size_t smem = smem_c;
@@ -112,8 +114,8 @@ static int launch_tile_n(TileConvArgs A, const ConvEpi& E, int* err, cudaStream_
                 return LMM_ERR_CUDA;
             const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + smem_rsv);
             const int regs_warp = ((fa.numRegs + 7) / 8 * 8) * 32;
-            const int by_regs = regs_sm / (regs_warp * (tc::kThreadsTC / 32));
-            const int by_tmem = 512 / (int)(ZN ? zn_tmem_cols(NS) : tile_tmem_cols(NS));
+            const int by_regs = regs_sm / (regs_warp * (threads / 32));
+            const int by_tmem = 512 / (int)(ZN ? ws_tmem_cols(NS) : tile_tmem_cols(NS));
             per_sm = by_smem < by_regs ? by_smem : by_regs;
             per_sm = per_sm < by_tmem ? per_sm : by_tmem;
             per_sm = per_sm < 16 ? per_sm : 16;
@@ -125,7 +127,7 @@ static int launch_tile_n(TileConvArgs A, const ConvEpi& E, int* err, cudaStream_
         A.ctas_per_slice = (int)cps;
         const unsigned blocks = (unsigned)(A.slices * cps);
         if constexpr (ZN)
-            k_conv3d_tile_zn<CINP, NS><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
+            k_conv3d_ws<CINP, NS><<<blocks, threads, smem, s>>>(A, E, err);
         else
             k_conv3d_tile<CINP, NS><<<blocks, tc::kThreadsTC, smem, s>>>(A, E, err);
         if (cudaGetLastError() != cudaSuccess) return LMM_ERR_CUDA;
@@ -153,17 +155,12 @@ static int launch_tile(bool zn, int cinp, int ns, const TileConvArgs& A, const C
     }
 }
 // the output-channel slice (a multiple of 16 dividing n) of a tile kernel:
-// with the z taps in N (*zn) for 16 or 32 input channels, the widest slice
-// leaving room for two CTAs per SM; else the 27-tap kernel's widest slice
-// that fits in shared memory; 0 when none does
+// 16 with the warp-specialised z-taps-in-N kernel (*zn) for 16 or 32 input
+// channels; else the 27-tap kernel's widest slice that fits in shared
+// memory; 0 when none does
 static int tile_slice(int cinp, int n, bool* zn) {
-    *zn = false;
-    if (cinp <= 32)
-        for (int ns = 32; ns >= 16; ns -= 16)
-            if (ns <= n && n % ns == 0 && zn_smem_bytes(cinp, ns) <= 113 * 1024) {
-                *zn = true;
-                return ns;
-            }
+    *zn = cinp <= 32 && n % 16 == 0;
+    if (*zn) return 16;
     for (int ns = 64; ns >= 16; ns -= 16)
         if (ns <= n && n % ns == 0 && tile_smem_bytes(cinp, ns) <= 227 * 1024) return ns;
     return 0;
