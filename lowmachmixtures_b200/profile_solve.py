@@ -6,6 +6,11 @@ Used under ncu to list every kernel launch of a solve, and to capture the
 hot kernels on the benchmark workload (3D n^3, contrast 100, inertial
 theta*alpha*dx^2 = 0.1, precon_type 2, visc_type -2).  --warm solves run
 first so that a capture can skip them with ncu's -s.
+
+    python -m lowmachmixtures_b200.profile_solve --n 128 --op net_forward --solves 5
+
+times forward passes of the learned stage's network (random weights, one
+n^3 field of 8 BF16 channels) instead.
 """
 from __future__ import annotations
 
@@ -28,9 +33,10 @@ def main():
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=INT",
                     help="extra lmm_knobs integer field (repeatable), e.g. --knob tail_cells=512")
     ap.add_argument("--bc", default="", help="BC code per direction, both sides, e.g. -1,100,-1 (default periodic)")
-    ap.add_argument("--op", default="", choices=["", "smooth", "applyop", "apply_matrix", "vcycle", "macproject"],
+    ap.add_argument("--op", default="", choices=["", "smooth", "applyop", "apply_matrix", "vcycle", "macproject", "net_forward"],
                     help="instead of solves: time one operation (lmm_time_op) --solves times after one warm-up; "
-                         "'smooth' and 'vcycle' run in the method's precision")
+                         "'smooth' and 'vcycle' run in the method's precision; 'net_forward': --warm + --solves "
+                         "forward passes of the learned stage's network")
     a = ap.parse_args()
 
     import numpy as np
@@ -38,6 +44,27 @@ def main():
 
     from lowmachmixtures_b200 import abi, synth
     from lowmachmixtures_b200.gmres import StokesSolver
+
+    if a.op == "net_forward":
+        import ctypes
+
+        from lowmachmixtures_b200 import learned
+        net = learned.Net((a.n,) * 3, 1, 0)
+        x = torch.randn(1, a.n, a.n, a.n, 8).to(torch.bfloat16).cuda()
+        y = torch.empty(1, a.n, a.n, a.n, 4, device="cuda")
+        fwd = lambda: net.lib.lmm_net_forward(net.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()))  # noqa: E731
+        for _ in range(a.warm):
+            assert fwd() == 0
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(a.solves):
+            assert fwd() == 0
+        t1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"op": a.op, "n": a.n, "ms_per_forward": t0.elapsed_time(t1) / max(a.solves, 1)}))
+        net.close()
+        return
 
     bc = tuple(int(v) for v in a.bc.split(",")) if a.bc else None
     if a.dm == 2:
