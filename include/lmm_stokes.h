@@ -54,6 +54,8 @@ extern "C" {
 #define LMM_ERR_CUDA          -4  /* CUDA runtime error */
 #define LMM_ERR_WATCHDOG      -5  /* a bounded device wait gave up */
 #define LMM_ERR_NO_DEVICE     -6  /* no CUDA device visible */
+#define LMM_ERR_BOUNDS        -8  /* builds with -DLMM_BOUNDS_CHECK only: a load outside the handle's
+                                     allocations was skipped (lmm_strerror gives the first address) */
 
 /* ---- boundary-condition codes (src_common/bc.f90:23-44) ---- */
 #define LMM_BC_PERIODIC       -1

@@ -1,7 +1,9 @@
 """Loader of the in-tree CUDA library liblmmstokes.so (no fallback).
 
 The product path has no CPU implementation: if the library is missing or no
-CUDA device is present, calls fail loudly.
+CUDA device is present, calls fail loudly.  With LMM_BOUNDS_CHECK=1 in the
+environment the bounds-check build liblmmstokes_bc.so is loaded instead
+(`python -m lowmachmixtures_b200.build --bounds-check`).
 """
 from __future__ import annotations
 
@@ -11,7 +13,7 @@ import os
 from . import abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblmmstokes.so")
+LIB_PATH = os.path.join(_HERE, "liblmmstokes_bc.so" if os.environ.get("LMM_BOUNDS_CHECK") == "1" else "liblmmstokes.so")
 _lib = None
 
 _dp = C.POINTER(C.c_double)

@@ -19,6 +19,7 @@ LMM_ERR_CUDA = -4
 LMM_ERR_WATCHDOG = -5
 LMM_ERR_NO_DEVICE = -6
 LMM_ERR_TOO_LARGE = -7
+LMM_ERR_BOUNDS = -8  # -DLMM_BOUNDS_CHECK builds only
 
 LMM_BC_PERIODIC = -1
 LMM_BC_NO_SLIP_WALL = 100

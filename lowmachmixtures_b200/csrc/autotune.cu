@@ -88,3 +88,7 @@ extern "C" int lmm_autotune_report(char* buf, int cap) {
     }
     return (int)out.size();
 }
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(autotune)

@@ -5,6 +5,7 @@
 // explicitly instantiated in kernels_fp64.cu (built with -fmad=false) and
 // kernels_fp32.cu.
 #pragma once
+#include <initializer_list>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -181,6 +182,31 @@ int reduce_blocks(int64_t n);
 // raise a kernel's dynamic shared-memory limit to at least `bytes` on the
 // current device, once per (device, kernel); safe from several host threads
 cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+
+// bounds-check builds (-DLMM_BOUNDS_CHECK, stencil.cuh): register / forget a
+// device allocation that loads may touch; bc_status reads and clears every
+// translation unit's record (LMM_ERR_BOUNDS when a load fell outside).  In
+// other builds bc_add and bc_remove do nothing and bc_status is LMM_OK.
+void bc_add(const void* p, size_t bytes);
+void bc_remove(const void* p);
+int bc_status();
+// the caller's arrays of one entry point that reads them in place
+struct BcScope {
+    const void* p[8] = {};
+    BcScope(std::initializer_list<const void*> ptrs, size_t bytes) {
+        int k = 0;
+        for (const void* q : ptrs)
+            if (k < 8) {
+                p[k++] = q;
+                bc_add(q, bytes);
+            }
+    }
+    ~BcScope() {
+        for (const void* q : p) bc_remove(q);
+    }
+    BcScope(const BcScope&) = delete;
+    BcScope& operator=(const BcScope&) = delete;
+};
 // one kernel launch issued (counted by check_launch after every launch site)
 void count_launch();
 int64_t launches_total();

@@ -8,3 +8,7 @@ namespace lmm {
 LMM_INSTANTIATE(float)
 LMM_INSTANTIATE_TAIL(float)
 }  // namespace lmm
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(kernels_fp32)

@@ -11,3 +11,7 @@ LMM_INSTANTIATE_TAIL(double)
 template void launch_convert<double, float>(const double*, float*, int64_t, cudaStream_t);
 template void launch_convert<float, double>(const float*, double*, int64_t, cudaStream_t);
 }  // namespace lmm
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(kernels_fp64)

@@ -835,3 +835,7 @@ void launch_scatter_ptrs(const double* src, double* const* dst_dev, int ni, int 
 }
 
 }  // namespace lmm
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(krylov)

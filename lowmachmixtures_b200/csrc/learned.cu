@@ -160,3 +160,7 @@ void launch_accept(double* c, double* w, const double* Ac, const double* n1, con
 }
 
 }  // namespace lmm
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(learned)

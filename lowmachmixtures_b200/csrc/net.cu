@@ -411,3 +411,7 @@ int net_forward_on(lmm_net* h, cudaStream_t s) {
 }
 }  // namespace nn
 }  // namespace lmm
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(net)

@@ -263,3 +263,7 @@ extern "C" int lmm_nn_pack_weights(const float* w, void* wf, void* wt, int Cout,
     using lmm::nn::bf16;
     return lmm::nn::pack_weights(w, static_cast<bf16*>(wf), static_cast<bf16*>(wt), Cout, Cin, static_cast<cudaStream_t>(stream));
 }
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(nn)

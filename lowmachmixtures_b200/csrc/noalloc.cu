@@ -105,6 +105,9 @@ extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* cons
     const int rc = scratch_address(&scr);
     if (rc != LMM_OK) return rc;
 
+    // bounds-check builds: the caller's arrays are read in place
+    lmm::BcScope scope_a({a_u[0], a_u[1], dm == 3 ? a_u[2] : nullptr, a_p}, (size_t)cells * sizeof(double));
+    lmm::BcScope scope_b({b_u[0], b_u[1], dm == 3 ? b_u[2] : nullptr, b_p}, (size_t)cells * sizeof(double));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Dims D;
     D.nx = n[0];
@@ -128,5 +131,9 @@ extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* cons
     if ((e = cudaMemcpyAsync(out_host, scr->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         return cuda_failed("cudaMemcpyAsync", e);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_failed("cudaStreamSynchronize", e);
-    return LMM_OK;
+    return lmm::bc_status();
 }
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(noalloc)

@@ -38,9 +38,110 @@
 
 using namespace lmm;
 
+#ifdef LMM_BOUNDS_CHECK
+#define LMM_BC_DECLARE(name)                                  \
+    cudaError_t lmm_bc_sync_##name(const lmm::bc::Table& t); \
+    cudaError_t lmm_bc_take_##name(lmm::bc::Record* r);
+LMM_BC_UNITS(LMM_BC_DECLARE)
+#undef LMM_BC_DECLARE
+#endif
+
 namespace {
 
 thread_local std::string g_last_error;
+
+}  // namespace
+
+namespace lmm {
+void set_last_error(const std::string& what);
+// bounds-check builds: the device allocations loads may touch, copied into
+// every translation unit's table whenever they change
+#ifdef LMM_BOUNDS_CHECK
+std::mutex g_bc_mu;
+std::map<const void*, size_t> g_bc_ranges;
+cudaError_t bc_sync_locked() {
+    lmm::bc::Table t{};
+    for (const auto& kv : g_bc_ranges) {
+        if (t.n == lmm::bc::kRanges) break;
+        t.lo[t.n] = reinterpret_cast<unsigned long long>(kv.first);
+        t.hi[t.n] = t.lo[t.n] + kv.second;
+        ++t.n;
+    }
+    cudaError_t e = cudaSuccess, f;
+#define LMM_BC_SYNC(name) \
+    if ((f = lmm_bc_sync_##name(t)) != cudaSuccess) e = f;
+    LMM_BC_UNITS(LMM_BC_SYNC)
+#undef LMM_BC_SYNC
+    return e;
+}
+#endif
+void bc_add(const void* p, size_t bytes) {
+#ifdef LMM_BOUNDS_CHECK
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_bc_mu);
+    g_bc_ranges[p] = bytes;
+    bc_sync_locked();
+#else
+    (void)p;
+    (void)bytes;
+#endif
+}
+void bc_remove(const void* p) {
+#ifdef LMM_BOUNDS_CHECK
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_bc_mu);
+    g_bc_ranges.erase(p);
+    bc_sync_locked();
+#else
+    (void)p;
+#endif
+}
+// LMM_OK, or LMM_ERR_BOUNDS (message: count and first address) when a load
+// since the last call fell outside the registered allocations
+int bc_status() {
+#ifdef LMM_BOUNDS_CHECK
+    std::lock_guard<std::mutex> lock(g_bc_mu);
+    unsigned long long count = 0, first = 0;
+    lmm::bc::Record r;
+#define LMM_BC_TAKE(name)                                        \
+    if (lmm_bc_take_##name(&r) == cudaSuccess && r.count) {      \
+        if (!count) first = r.first;                             \
+        count += r.count;                                        \
+    }
+    LMM_BC_UNITS(LMM_BC_TAKE)
+#undef LMM_BC_TAKE
+    if (count) {
+        // where the first one lies against the nearest registered allocation
+        long long best = 0;
+        unsigned long long blo = 0, bhi = 0;
+        bool any = false;
+        for (const auto& kv : g_bc_ranges) {
+            const unsigned long long lo = reinterpret_cast<unsigned long long>(kv.first), hi = lo + kv.second;
+            const long long d = first < lo ? (long long)(first - lo) : (long long)(first - hi);
+            if (!any || std::llabs(d) < std::llabs(best)) {
+                best = d;
+                blo = lo;
+                bhi = hi;
+                any = true;
+            }
+        }
+        char buf[256];
+        std::snprintf(buf, sizeof(buf),
+                      "bounds check: %llu loads outside the registered allocations, the first at 0x%llx (%lld bytes %s the "
+                      "allocation [0x%llx, 0x%llx))",
+                      count, first, std::llabs(best), best < 0 ? "before" : "past", blo, bhi);
+        lmm::set_last_error(buf);
+        return LMM_ERR_BOUNDS;
+    }
+#endif
+    return LMM_OK;
+}
+}  // namespace lmm
+
+namespace {
+using lmm::bc_add;
+using lmm::bc_remove;
+using lmm::bc_status;
 
 // NVTX range over one phase of a solve (solve, Krylov cycle, Arnoldi column,
 // preconditioner, V-cycle, pressure solve, learned stage); a profiler shows
@@ -2104,6 +2205,7 @@ const char* lmm_strerror(int code) {
     case LMM_ERR_CUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
     case LMM_ERR_WATCHDOG: return "a bounded device wait gave up";
     case LMM_ERR_NO_DEVICE: return "no CUDA device";
+    case LMM_ERR_BOUNDS: return g_last_error.empty() ? "a load outside the registered allocations was skipped" : g_last_error.c_str();
     case LMM_ERR_TOO_LARGE: return "grid larger than this fixed-size entry point accepts";
     default: return "unknown status";
     }
@@ -2185,6 +2287,7 @@ static int create_impl(const lmm_grid* g, const lmm_knobs* k, int device, int ba
         LMM_CK(cudaEventCreateWithFlags(&h->col_ev, cudaEventDisableTiming | (k->host_wait == 1 ? cudaEventBlockingSync : 0)));
         h->arena_bytes = plan_bytes(*g, *k, h->nlev, h->nlev_p, batch, batched);
         LMM_CK(cudaMalloc(&h->arena, h->arena_bytes));
+        bc_add(h->arena, h->arena_bytes);
         // zeroed on the handle's own (non-blocking) stream: a cudaMemset on
         // the legacy stream may still run when later copies on h->stream
         // (the batch pointer tables) have landed, and would wipe them
@@ -2338,6 +2441,8 @@ int lmm_stokes_destroy(lmm_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& kv : h->graphs)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    bc_remove(h->arena);
+    bc_remove(h->lrn_block);
     if (h->arena) cudaFree(h->arena);
     if (h->lrn_block) cudaFree(h->lrn_block);
     if (h->hscal) cudaFreeHost(h->hscal);
@@ -2439,7 +2544,8 @@ int solve_core(lmm_handle* h, const lmm_fields_in* in, const double* x0_u[3], co
     }
     *theta_alpha = theta;
     if (st) st->pressure_vcycles = h->pvcycles;
-    return rc;
+    const int bc = bc_status();
+    return bc != LMM_OK ? bc : rc;
 }
 
 }  // namespace
@@ -2683,7 +2789,8 @@ extern "C" int lmm_stokes_solve_batch(lmm_handle* h, lmm_ensemble_item* items, i
             items[q].stats = st[q];
             items[q].status = status[q];
         }
-        return rc;
+        const int bc = bc_status();
+        return bc != LMM_OK ? bc : rc;
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2738,7 +2845,7 @@ extern "C" int lmm_op_load_coeffs(lmm_handle* h, const lmm_fields_in* c, double 
         const double* bed[3] = {c->beta_ed[0], c->beta_ed[1], c->beta_ed[2]};
         load_coeffs(h, al, c->beta, bed, c->gamma, theta_alpha);
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2748,10 +2855,13 @@ extern "C" int lmm_op_stag_applyop(lmm_handle* h, const double* const phi[3], do
     if (!h || h->batched || !h->coeffs_loaded) return LMM_ERR_INVALID;
     try {
         if (color < 0 || color > 2 * h->dm) return LMM_ERR_INVALID;
+        const bool d3 = h->dm == 3;
+        lmm::BcScope scope({phi[0], phi[1], d3 ? phi[2] : nullptr, Lphi[0], Lphi[1], d3 ? Lphi[2] : nullptr},
+                           (size_t)h->L64[0].n * sizeof(double));
         launch_applyop<double>(h->L64[0], h->knobs.visc_type, phi, Lphi, h->stream, color);
         check_launch();
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2772,7 +2882,7 @@ extern "C" int lmm_op_apply_matrix(lmm_handle* h, const double* const x_u[3], co
             LMM_CK(cudaMemcpyAsync(b_u[d], h->tmp.c(d), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(cudaMemcpyAsync(b_p, h->tmp.p(), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2798,7 +2908,7 @@ extern "C" int lmm_op_apply_precon(lmm_handle* h, const double* const b_u[3], co
             LMM_CK(cudaMemcpyAsync(x_u[d], h->w.c(d), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(cudaMemcpyAsync(x_p, h->w.p(), n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2816,7 +2926,7 @@ extern "C" int lmm_op_stag_mg_solver(lmm_handle* h, const double* const rhs[3], 
         for (int d = 0; d < h->dm; ++d)
             LMM_CK(cudaMemcpyAsync(phi[d], L0.phi[d], h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2842,7 +2952,7 @@ extern "C" int lmm_op_smooth(lmm_handle* h, int lev, const double* const rhs[3],
                 LMM_CK(cudaMemcpyAsync(phi[d], L.phi[d], L.n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
         }
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2852,11 +2962,15 @@ extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* co
                                         double* const rhs_coarse[3]) {
     if (!h || h->batched || !h->coeffs_loaded || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
     try {
+        const bool d3 = h->dm == 3;
+        lmm::BcScope fine({rhs[0], rhs[1], d3 ? rhs[2] : nullptr, phi[0], phi[1], d3 ? phi[2] : nullptr},
+                          (size_t)h->L64[lev].n * sizeof(double));
+        lmm::BcScope coarse({rhs_coarse[0], rhs_coarse[1], d3 ? rhs_coarse[2] : nullptr}, (size_t)h->L64[lev + 1].n * sizeof(double));
         launch_residual_restrict<double>(h->L64[lev], h->L64[lev + 1], h->knobs.visc_type, rhs, phi, rhs_coarse, h->stream,
                                          h->knobs.residual_fusion > 0 ? 1 : 0);
         check_launch();
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2865,10 +2979,13 @@ extern "C" int lmm_op_residual_restrict(lmm_handle* h, int lev, const double* co
 extern "C" int lmm_op_prolong_add(lmm_handle* h, int lev, const double* const phi_coarse[3], double* const phi_fine[3]) {
     if (!h || h->batched || lev < 0 || lev + 1 >= h->nlev) return LMM_ERR_INVALID;
     try {
+        const bool d3 = h->dm == 3;
+        lmm::BcScope fine({phi_fine[0], phi_fine[1], d3 ? phi_fine[2] : nullptr}, (size_t)h->L64[lev].n * sizeof(double));
+        lmm::BcScope coarse({phi_coarse[0], phi_coarse[1], d3 ? phi_coarse[2] : nullptr}, (size_t)h->L64[lev + 1].n * sizeof(double));
         launch_prolong_add<double>(h->L64[lev], h->L64[lev + 1], phi_coarse, phi_fine, h->stream);
         check_launch();
         LMM_CK(host_wait(h));
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2880,11 +2997,13 @@ extern "C" int lmm_op_inner_prod(lmm_handle* h, const double* const a_u[3], cons
     try {
         const double* a[4] = {a_u[0], a_u[1], h->dm == 3 ? a_u[2] : nullptr, a_p};
         const double* b[4] = {b_u[0], b_u[1], h->dm == 3 ? b_u[2] : nullptr, b_p};
+        const size_t bytes = (size_t)h->n * sizeof(double);
+        lmm::BcScope scope({a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3]}, bytes);
         stokes_reduce(h, 0, a, b, 2);
         LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(2), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         LMM_CK(host_wait(h));
         for (int c = 0; c <= h->dm; ++c) out_host[c] = h->hscal[c];
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2895,6 +3014,7 @@ extern "C" int lmm_op_sum_umac_press(lmm_handle* h, const double* const u[3], co
     try {
         const double* a[4] = {u[0], u[1], h->dm == 3 ? u[2] : nullptr, p};
         const double* b[4] = {nullptr, nullptr, nullptr, nullptr};
+        lmm::BcScope scope({a[0], a[1], a[2], a[3]}, (size_t)h->n * sizeof(double));
         stokes_reduce(h, 1, a, b, 2);
         LMM_CK(cudaMemcpyAsync(h->hscal, h->slot(2), 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         LMM_CK(host_wait(h));
@@ -2902,7 +3022,7 @@ extern "C" int lmm_op_sum_umac_press(lmm_handle* h, const double* const u[3], co
         for (int d = 0; d < h->dm; ++d) tv *= (double)h->grid.n[d];
         out_host[0] = h->hscal[h->dm] / tv;
         for (int d = 0; d < h->dm; ++d) out_host[1 + d] = h->hscal[d] / tv;
-        return LMM_OK;
+        return bc_status();
     } catch (const LmmError& e) {
         return e.code;
     }
@@ -2957,6 +3077,7 @@ extern "C" int lmm_stokes_set_net(lmm_handle* h, lmm_net* net) {
                 const int nv = 4 + 2 * h->m;
                 const size_t bytes = (size_t)nv * len * sizeof(double) + (size_t)len * sizeof(float) + 256;
                 LMM_CK(cudaMalloc(&h->lrn_block, bytes));
+                bc_add(h->lrn_block, bytes);
                 double* p = static_cast<double*>(h->lrn_block);
                 h->Zc.assign(h->m, SVec());
                 const size_t v0 = h->V.size();
@@ -3080,3 +3201,7 @@ extern "C" int lmm_learned_stats(lmm_handle* h, int* accepted, int* tried) {
     *tried = u[1];
     return LMM_OK;
 }
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(solver)

@@ -23,9 +23,76 @@
 // component's ghost is -interior at a no-slip wall and +interior at a slip
 // wall (physbc_macvel).
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 namespace lmm {
+
+// ------------------------------------------------------------ bounds checks
+// A build with -DLMM_BOUNDS_CHECK tests every load through ld / ldp: a
+// global address must lie in one of the registered device allocations (the
+// arenas and learned-stage blocks of the live handles, and the caller's
+// arrays of an entry point that reads them in place), a shared-memory one
+// (the single-CTA coarse tails) within the CTA's shared memory.  A load outside them is skipped
+// (it reads zero), counted, and the first such address kept; the host reads
+// and clears the record after each solve and reports LMM_ERR_BOUNDS.  Device
+// globals are per translation unit (no relocatable device code), so each
+// unit that includes this header owns a table and a record, reached through
+// the host functions LMM_BC_UNIT(name) defines in it.
+namespace bc {
+constexpr int kRanges = 64;
+struct Table {
+    unsigned long long lo[kRanges], hi[kRanges];
+    int n;
+};
+struct Record {
+    unsigned long long count, first;
+};
+}  // namespace bc
+#ifdef LMM_BOUNDS_CHECK
+static __device__ bc::Table g_bc_table;
+static __device__ bc::Record g_bc_record;
+// a load of `bytes` at p: in shared memory it must lie within this CTA's
+// shared memory (static + dynamic), in global memory within a registered
+// allocation; other windows (local) are not tracked
+__device__ __forceinline__ bool bc_ok(const void* p, unsigned bytes) {
+    const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+    bool ok;
+    if (__isShared(p)) {
+        // the CTA's own shared memory (static, then dynamic) follows the
+        // reserved region: offsets [cap, cap + total)
+        unsigned total, cap;
+        asm("mov.u32 %0, %%total_smem_size;" : "=r"(total));
+        asm("mov.u32 %0, %%reserved_smem_offset_cap;" : "=r"(cap));
+        const unsigned long long off = __cvta_generic_to_shared(p);
+        ok = off >= cap && off + bytes <= (unsigned long long)cap + total;
+    } else if (__isGlobal(p)) {
+        ok = false;
+        const int n = g_bc_table.n;
+        for (int r = 0; r < n && !ok; ++r) ok = a >= g_bc_table.lo[r] && a + bytes <= g_bc_table.hi[r];
+    } else {
+        ok = true;
+    }
+    if (!ok && atomicAdd(&g_bc_record.count, 1ull) == 0ull) g_bc_record.first = a;
+    return ok;
+}
+#define LMM_BC_UNIT(name)                                                                             \
+    cudaError_t lmm_bc_sync_##name(const lmm::bc::Table& t) {                                         \
+        return cudaMemcpyToSymbol(lmm::g_bc_table, &t, sizeof(t));                                    \
+    }                                                                                                 \
+    cudaError_t lmm_bc_take_##name(lmm::bc::Record* r) {                                              \
+        const lmm::bc::Record z{0ull, 0ull};                                                          \
+        cudaError_t e = cudaMemcpyFromSymbol(r, lmm::g_bc_record, sizeof(*r));                        \
+        return e == cudaSuccess ? cudaMemcpyToSymbol(lmm::g_bc_record, &z, sizeof(z)) : e;            \
+    }
+#else
+#define LMM_BC_UNIT(name)
+#endif
+// the translation units that include this header, each ending in
+// LMM_BC_UNIT(its name)
+#define LMM_BC_UNITS(X) \
+    X(autotune) X(kernels_fp32) X(kernels_fp64) X(krylov) X(learned) X(net) X(nn) X(noalloc) X(solver) X(stochastic) X(walls_fp32) X(walls_fp64)
 
 // neighbour offsets (with periodic wrap) of one index; 32-bit indices
 // (a field holds at most 2^31 - 1 entries)
@@ -158,6 +225,9 @@ struct Coef {
 
 template <class T>
 __device__ __forceinline__ T ld(const T* p, int i) {
+#ifdef LMM_BOUNDS_CHECK
+    if (!bc_ok(p + i, sizeof(T))) return T(0);
+#endif
     return __ldg(p + i);
 }
 
@@ -169,6 +239,9 @@ __device__ __forceinline__ T ld(const T* p, int i) {
 //         thread-block cluster between cluster barriers.
 template <int LD, class T>
 __device__ __forceinline__ T ldp(const T* p, int i) {
+#ifdef LMM_BOUNDS_CHECK
+    if (!bc_ok(p + i, sizeof(T))) return T(0);
+#endif
     if constexpr (LD == 0)
         return __ldg(p + i);
     else if constexpr (LD == 1)

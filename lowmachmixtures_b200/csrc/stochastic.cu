@@ -126,3 +126,7 @@ extern "C" int lmm_stochastic_rhs(int dm, const int n[3], double dx, double dt, 
     count_launch();
     return LMM_OK;
 }
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(stochastic)

@@ -5,3 +5,7 @@
 namespace lmm {
 LMM_INSTANTIATE_WALLS(double)
 }  // namespace lmm
+
+// the bounds-check table and record of this translation unit (empty
+// unless built with -DLMM_BOUNDS_CHECK)
+LMM_BC_UNIT(walls_fp64)

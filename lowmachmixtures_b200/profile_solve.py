@@ -27,7 +27,9 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--dm", type=int, default=3, choices=[2, 3],
                     help="2: the 2D steady workload (n^2, contrast 10, theta = 0); 3: 3D n^3, contrast 100, theta*alpha = 0.1/dx^2")
-    ap.add_argument("--method", default="mixed", choices=["mixed", "plain", "reference"])
+    ap.add_argument("--method", default="mixed", choices=["mixed", "plain", "reference", "learned"],
+                    help="learned: mixed with the learned stage, its network trained (--train-steps, 64^3) first")
+    ap.add_argument("--train-steps", type=int, default=200)
     ap.add_argument("--solves", type=int, default=1)
     ap.add_argument("--warm", type=int, default=1)
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=INT",
@@ -72,7 +74,16 @@ def main():
     else:
         prob = synth.config_3d_128(0, n=a.n) if bc is None else synth.make_problem(3, a.n, 100.0, 0, theta_alpha=0.1 * a.n * a.n, bc=bc)
     kn = dict(precon_type=2, visc_type=-2)
-    if a.method == "mixed":
+    net = None
+    if a.method == "learned":
+        from lowmachmixtures_b200 import learned
+        net64, _, _ = learned.train(n=64, fields=20, steps=a.train_steps, batch=4, theta_alpha=0.1)
+        params = net64.params()
+        net64.close()
+        net = learned.Net((a.n,) * 3, 1, 0)
+        net.set_params(params)
+        kn.update(learned_stage=1)
+    if a.method in ("mixed", "learned"):
         kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP32)
     elif a.method == "plain":
         kn.update(method=abi.LMM_METHOD_FGMRES, precision=abi.LMM_PRECISION_FP64)
@@ -84,6 +95,8 @@ def main():
     al, be, bed, ga = [dev(x) for x in prob.alpha_fc], dev(prob.beta), [dev(x) for x in prob.beta_ed], dev(prob.gamma)
     xu, xp = [torch.zeros_like(bu[0]) for _ in range(a.dm)], torch.zeros_like(bp)
     with StokesSolver(a.dm, (a.n,) * a.dm, prob.dx, knobs=abi.make_knobs(**kn), bc=bc) as s:
+        if net is not None:
+            assert s.lib.lmm_stokes_set_net(s._h, net.h) == 0
         if a.op:
             s.load_coeffs(al, be, bed, ga, prob.theta_alpha)
             fp32 = a.method == "mixed"
