@@ -27,6 +27,20 @@ int64_t lmm_net_num_params(lmm_net* net);
 int lmm_net_stream(lmm_net* net, void** stream);
 /* copy the FP32 parameters to (set = 0) or from (set = 1) host memory */
 int lmm_net_params(lmm_net* net, float* host, int set);
+/* Weights on disk, one flat little-endian file:
+ *   offset 0        8 bytes     magic "LMMNET01"
+ *          8        uint32      format version (1)
+ *          12       uint32      layer count L (11)
+ *          16       L x 2 uint32  (Cin, Cout) of each layer, in layer order
+ *          16 + 8L  uint64      parameter count P (lmm_net_num_params)
+ *          24 + 8L  uint64      FNV-1a 64-bit hash of the 4P parameter bytes
+ *          32 + 8L  P x float32 the parameters, in lmm_net_params order
+ * lmm_net_save writes the network's parameters; lmm_net_load checks the
+ * magic, version, layer table, count, file size and hash and then sets
+ * them (any mismatch: LMM_ERR_INVALID, lmm_strerror says which).  The file
+ * does not depend on the grid or batch the network was created for. */
+int lmm_net_save(lmm_net* net, const char* path);
+int lmm_net_load(lmm_net* net, const char* path);
 /* y (device, may be NULL) = network(x), x device BF16 */
 int lmm_net_forward(lmm_net* net, const void* x, float* y);
 /* gradients of sum(gy * network(x)) with respect to every parameter

@@ -65,6 +65,8 @@ def load() -> C.CDLL:
     lib.lmm_net_stream.argtypes = [vp, P(vp)]
     lib.lmm_net_params.argtypes = [vp, vp, ci]
     lib.lmm_net_forward.argtypes = [vp, vp, vp]
+    lib.lmm_net_save.argtypes = [vp, C.c_char_p]
+    lib.lmm_net_load.argtypes = [vp, C.c_char_p]
     lib.lmm_net_gradients.argtypes = [vp, vp, vp, vp]
     lib.lmm_net_train_step.argtypes = [vp, vp, vp, C.c_float, vp]
     lib.lmm_stokes_set_net.argtypes = [vp, vp]

@@ -17,7 +17,9 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/lmm_learned.h"
@@ -342,6 +344,93 @@ extern "C" int lmm_net_params(lmm_net* h, float* host, int set) {
         return LMM_ERR_CUDA;
     }
     return finish(n);
+}
+
+// ------------------------------------------------------------ weight files
+namespace lmm {
+void set_last_error(const std::string& what);  // solver.cu
+}
+namespace {
+constexpr char kMagic[8] = {'L', 'M', 'M', 'N', 'E', 'T', '0', '1'};
+constexpr uint32_t kFormat = 1;
+// FNV-1a, 64-bit (offset basis 14695981039346656037, prime 1099511628211)
+uint64_t fnv1a64(const unsigned char* p, size_t n) {
+    uint64_t h = 14695981039346656037ull;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+int file_error(const std::string& what, const char* path) {
+    lmm::set_last_error(what + ": " + path);
+    return LMM_ERR_INVALID;
+}
+}  // namespace
+
+extern "C" int lmm_net_save(lmm_net* h, const char* path) {
+    using namespace lmm::nn;
+    if (!h || !path) return LMM_ERR_INVALID;
+    Net* n = reinterpret_cast<Net*>(h);
+    std::vector<float> p((size_t)n->nparams);
+    const int rc = lmm_net_params(h, p.data(), 0);
+    if (rc) return rc;
+    std::vector<uint32_t> table;
+    for (int l = 0; l < kLayers; ++l) {
+        table.push_back((uint32_t)kSpec[l].cin);
+        table.push_back((uint32_t)kSpec[l].cout);
+    }
+    const uint32_t head[2] = {kFormat, (uint32_t)kLayers};
+    const uint64_t count = (uint64_t)n->nparams;
+    const uint64_t hash = fnv1a64(reinterpret_cast<const unsigned char*>(p.data()), p.size() * sizeof(float));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return file_error("cannot open for writing", path);
+    bool ok = std::fwrite(kMagic, 1, 8, f) == 8 && std::fwrite(head, 4, 2, f) == 2 &&
+              std::fwrite(table.data(), 4, table.size(), f) == table.size() && std::fwrite(&count, 8, 1, f) == 1 &&
+              std::fwrite(&hash, 8, 1, f) == 1 && std::fwrite(p.data(), sizeof(float), p.size(), f) == p.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? LMM_OK : file_error("write failed", path);
+}
+
+extern "C" int lmm_net_load(lmm_net* h, const char* path) {
+    using namespace lmm::nn;
+    if (!h || !path) return LMM_ERR_INVALID;
+    Net* n = reinterpret_cast<Net*>(h);
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return file_error("cannot open", path);
+    char magic[8];
+    uint32_t head[2] = {0, 0};
+    std::vector<uint32_t> table(2 * kLayers);
+    uint64_t count = 0, hash = 0;
+    std::vector<float> p;
+    std::string err;
+    if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kMagic, 8) != 0) {
+        err = "not a weight file (magic)";
+    } else if (std::fread(head, 4, 2, f) != 2 || head[0] != kFormat) {
+        err = "unsupported weight-file version";
+    } else if (head[1] != (uint32_t)kLayers || std::fread(table.data(), 4, table.size(), f) != table.size()) {
+        err = "weight file for another architecture (layer count)";
+    } else {
+        for (int l = 0; l < kLayers && err.empty(); ++l)
+            if (table[2 * l] != (uint32_t)kSpec[l].cin || table[2 * l + 1] != (uint32_t)kSpec[l].cout)
+                err = "weight file for another architecture (layer " + std::to_string(l) + " channels)";
+        if (err.empty() && (std::fread(&count, 8, 1, f) != 1 || std::fread(&hash, 8, 1, f) != 1))
+            err = "truncated weight file (header)";
+        else if (err.empty() && count != (uint64_t)n->nparams)
+            err = "weight file holds " + std::to_string(count) + " parameters, the network " + std::to_string(n->nparams);
+        if (err.empty()) {
+            p.resize((size_t)count);
+            if (std::fread(p.data(), sizeof(float), p.size(), f) != p.size())
+                err = "truncated weight file (parameters)";
+            else if (std::fgetc(f) != EOF)
+                err = "weight file longer than its header says";
+            else if (fnv1a64(reinterpret_cast<const unsigned char*>(p.data()), p.size() * sizeof(float)) != hash)
+                err = "weight-file checksum mismatch";
+        }
+    }
+    std::fclose(f);
+    if (!err.empty()) return file_error(err, path);
+    return lmm_net_params(h, p.data(), 1);
 }
 
 extern "C" int lmm_net_forward(lmm_net* h, const void* x, float* y) {

@@ -12,6 +12,8 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
+import struct
 import time
 
 import numpy as np
@@ -61,6 +63,18 @@ class Net:
         assert p.size == self.num_params
         assert self.lib.lmm_net_params(self.h, p.ctypes.data_as(C.c_void_p), 1) == 0
 
+    def save(self, path: str):
+        """the weight file of include/lmm_learned.h (lmm_net_save)"""
+        rc = self.lib.lmm_net_save(self.h, os.fsencode(path))
+        if rc != 0:
+            raise RuntimeError(f"lmm_net_save: {self.lib.lmm_strerror(rc).decode()}")
+
+    def load(self, path: str):
+        """set the weights from a weight file, after its checks (lmm_net_load)"""
+        rc = self.lib.lmm_net_load(self.h, os.fsencode(path))
+        if rc != 0:
+            raise RuntimeError(f"lmm_net_load: {self.lib.lmm_strerror(rc).decode()}")
+
     def close(self):
         if self.h:
             self.lib.lmm_net_destroy(self.h)
@@ -71,6 +85,59 @@ class Net:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ------------------------------------------------------------ weight files
+# The flat file of include/lmm_learned.h, read and written without a GPU
+# (lmm_net_save / lmm_net_load are the library's side of the same format).
+WEIGHT_MAGIC = b"LMMNET01"
+WEIGHT_VERSION = 1
+LAYERS = ((8, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 32), (32, 32), (32, 16), (16, 16), (16, 4))
+
+
+def fnv1a64(data: bytes) -> int:
+    """FNV-1a, 64-bit (the weight file's parameter checksum)"""
+    h = 14695981039346656037
+    for b in data:
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def num_params() -> int:
+    return sum(co * 27 * ci + co for ci, co in LAYERS)
+
+
+def write_weights(path: str, params: np.ndarray):
+    p = np.ascontiguousarray(params, dtype="<f4")
+    if p.size != num_params():
+        raise ValueError(f"{p.size} parameters, the network has {num_params()}")
+    payload = p.tobytes()
+    head = WEIGHT_MAGIC + struct.pack("<II", WEIGHT_VERSION, len(LAYERS))
+    head += b"".join(struct.pack("<II", ci, co) for ci, co in LAYERS)
+    head += struct.pack("<QQ", p.size, fnv1a64(payload))
+    with open(path, "wb") as f:
+        f.write(head + payload)
+
+
+def read_weights(path: str) -> np.ndarray:
+    """the parameters of a weight file, after the checks lmm_net_load makes"""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:8] != WEIGHT_MAGIC:
+        raise ValueError("not a weight file (magic)")
+    version, nl = struct.unpack_from("<II", data, 8)
+    if version != WEIGHT_VERSION:
+        raise ValueError("unsupported weight-file version")
+    table = [struct.unpack_from("<II", data, 16 + 8 * l) for l in range(nl)]
+    if tuple(table) != LAYERS:
+        raise ValueError("weight file for another architecture")
+    count, h = struct.unpack_from("<QQ", data, 16 + 8 * nl)
+    payload = data[32 + 8 * nl:]
+    if count != num_params() or len(payload) != 4 * count:
+        raise ValueError("weight file size does not match its header")
+    if fnv1a64(payload) != h:
+        raise ValueError("weight-file checksum mismatch")
+    return np.frombuffer(payload, dtype="<f4").copy()
 
 
 def mixed_knobs(**extra) -> abi.Knobs:
@@ -192,9 +259,17 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-seeds", type=int, default=50)
     ap.add_argument("--out", default="")
+    ap.add_argument("--save-weights", default="", help="write the trained weights (include/lmm_learned.h format)")
+    ap.add_argument("--load-weights", default="", help="evaluate these weights instead of training")
     a = ap.parse_args()
-    net, hist, secs = train(n=a.n, fields=a.fields, steps=a.steps, batch=a.batch, lr=a.lr,
-                            log=lambda m: print(m, flush=True))
+    if a.load_weights:
+        net, hist, secs = Net((a.n,) * 3, 1, 0), [float("nan")], 0.0
+        net.load(a.load_weights)
+    else:
+        net, hist, secs = train(n=a.n, fields=a.fields, steps=a.steps, batch=a.batch, lr=a.lr,
+                                log=lambda m: print(m, flush=True))
+    if a.save_weights:
+        net.save(a.save_weights)
     rows = evaluate(net, range(5000, 5000 + a.eval_seeds), n=a.n, log=lambda r: print(json.dumps(r), flush=True))
     summary = dict(train_seconds=secs, pairs=a.steps * a.batch, fields=a.fields, loss_first=hist[0],
                    loss_last=float(np.mean(hist[-50:])),

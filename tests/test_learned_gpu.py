@@ -295,3 +295,33 @@ def test_trained_stage_gains_on_held_out_seeds():
         assert r["it_learned"] <= r["it_plain"] + 2, msg
         assert r["tried"] == r["it_learned"], msg  # one correction per V-cycle application
     assert sum(r["it_learned"] for r in rows) <= 1.1 * sum(r["it_plain"] for r in rows), msg
+
+
+def test_weight_file_round_trip_through_the_library(tmp_path):
+    """lmm_net_save / lmm_net_load against the format's Python reader and
+    writer (test_learned_weights_cpu.py); the file does not depend on the
+    grid the network was created for"""
+    from lowmachmixtures_b200 import learned
+    a = learned.Net((16, 16, 16), 1, 3)
+    p = a.params()
+    assert p.size == learned.num_params()
+    a.save(str(tmp_path / "a.bin"))
+    assert np.array_equal(learned.read_weights(str(tmp_path / "a.bin")).view(np.uint32), p.view(np.uint32))
+    q = np.random.default_rng(5).standard_normal(p.size).astype(np.float32)
+    learned.write_weights(str(tmp_path / "q.bin"), q)
+    b = learned.Net((32, 32, 16), 2, 0)
+    b.load(str(tmp_path / "q.bin"))
+    assert np.array_equal(b.params().view(np.uint32), q.view(np.uint32))
+    b.load(str(tmp_path / "a.bin"))
+    assert np.array_equal(b.params().view(np.uint32), p.view(np.uint32))
+    # a damaged file leaves the weights as they were
+    d = bytearray((tmp_path / "q.bin").read_bytes())
+    d[-3] ^= 0x10
+    (tmp_path / "bad.bin").write_bytes(bytes(d))
+    with pytest.raises(RuntimeError, match="checksum"):
+        b.load(str(tmp_path / "bad.bin"))
+    with pytest.raises(RuntimeError, match="cannot open"):
+        b.load(str(tmp_path / "missing.bin"))
+    assert np.array_equal(b.params().view(np.uint32), p.view(np.uint32))
+    a.close()
+    b.close()
