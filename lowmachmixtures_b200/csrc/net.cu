@@ -169,10 +169,10 @@ struct Net {
         const bf16* in = xin ? xin : x;
         rc |= conv(0, in, nullptr, nullptr, a0, nullptr, 16);
         rc |= conv(1, a0, nullptr, nullptr, s0, nullptr, 16);
-        k_pool2<<<blocks_for(M(1) * 16), 256, 0, s>>>(s0, p0, B, nx[1], ny[1], nz[1], 16);
+        k_pool2<<<blocks_for(M(1) * 2), 256, 0, s>>>(s0, p0, B, nx[1], ny[1], nz[1], 16);
         rc |= conv(2, p0, nullptr, nullptr, a1, nullptr, 32);
         rc |= conv(3, a1, nullptr, nullptr, s1, nullptr, 32);
-        k_pool2<<<blocks_for(M(2) * 32), 256, 0, s>>>(s1, p1, B, nx[2], ny[2], nz[2], 32);
+        k_pool2<<<blocks_for(M(2) * 4), 256, 0, s>>>(s1, p1, B, nx[2], ny[2], nz[2], 32);
         rc |= conv(4, p1, nullptr, nullptr, a2, nullptr, 64);
         rc |= conv(5, a2, nullptr, nullptr, b2, nullptr, 64);
         rc |= conv(6, b2, s1, nullptr, c1, nullptr, 32);
@@ -197,13 +197,13 @@ struct Net {
         rc |= dgrad(9, g_d0, c0, g_c0);
         rc |= wgrad(8, d1, g_c0, 16);
         rc |= dgrad(8, g_c0, nullptr, gup0);  // fine grid, 32 ch
-        k_downsum<<<blocks_for(M(1) * 32), 256, 0, s>>>(gup0, tmp1, B, nx[1], ny[1], nz[1], 32);
+        k_downsum<<<blocks_for(M(1) * 4), 256, 0, s>>>(gup0, tmp1, B, nx[1], ny[1], nz[1], 32);
         k_grad_combine<<<blocks_for(M(1) * 32), 256, 0, s>>>(tmp1, nullptr, d1, g_d1, B, nx[1], ny[1], nz[1], 32);
         rc |= wgrad(7, c1, g_d1, 32);
         rc |= dgrad(7, g_d1, c1, g_c1);
         rc |= wgrad(6, b2, g_c1, 32);
         rc |= dgrad(6, g_c1, nullptr, gup1);  // level-1 grid, 64 ch
-        k_downsum<<<blocks_for(M(2) * 64), 256, 0, s>>>(gup1, g_b2, B, nx[2], ny[2], nz[2], 64);
+        k_downsum<<<blocks_for(M(2) * 8), 256, 0, s>>>(gup1, g_b2, B, nx[2], ny[2], nz[2], 64);
         k_grad_combine<<<blocks_for(M(2) * 64), 256, 0, s>>>(g_b2, nullptr, b2, g_b2, B, nx[2], ny[2], nz[2], 64);
         rc |= wgrad(5, a2, g_b2, 64);
         rc |= dgrad(5, g_b2, a2, g_a2);

@@ -185,45 +185,70 @@ static __global__ void __launch_bounds__(tc::kThreadsTC) k_conv3d_wgrad(WgradGat
 }
 
 // ------------------------------------------------------------ elementwise
-// 2x2x2 average (fine [B][2nz][2ny][2nx][C] -> coarse), FP32 sum
+// the sum over the 8 fine children of coarse voxel (b, i, j, k), channels
+// 8g .. 8g+7, children in the order d = 0..7 (x fastest), in FP32; C % 8 == 0
+__device__ __forceinline__ void sum_children8(const bf16* __restrict__ f, int64_t b, int i, int j, int k, int g, int nx,
+                                              int ny, int nz, int C, float (&s)[8]) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s[q] = 0.f;
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+        const int fi = 2 * i + (d & 1), fj = 2 * j + ((d >> 1) & 1), fk = 2 * k + (d >> 2);
+        const uint4 u = *reinterpret_cast<const uint4*>(f + (((b * 2 * nz + fk) * 2 * ny + fj) * 2 * nx + fi) * C + 8 * g);
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            s[2 * q] += __uint_as_float(w[q] << 16);
+            s[2 * q + 1] += __uint_as_float(w[q] & 0xFFFF0000u);
+        }
+    }
+}
+__device__ __forceinline__ uint4 pack8_bf16(const float (&s)[8], float scale) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(s[2 * q] * scale, s[2 * q + 1] * scale);
+        w[q] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// 2x2x2 average pooling, [B][nz][ny][nx][C] from the fine grid of twice the
+// extents; one thread per (coarse voxel, group of 8 channels)
 static __global__ void k_pool2(const bf16* __restrict__ f, bf16* __restrict__ c, int B, int nx, int ny, int nz, int C) {
-    const int64_t n = (int64_t)B * nx * ny * nz * C;
+    const int G = C / 8;
+    const int64_t n = (int64_t)B * nx * ny * nz * G;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int ch = (int)(e % C);
-        int64_t v = e / C;
+        const int g = (int)(e % G);
+        int64_t v = e / G;
         const int i = (int)(v % nx);
         v /= nx;
         const int j = (int)(v % ny);
         v /= ny;
         const int k = (int)(v % nz);
-        const int b = (int)(v / nz);
-        float s = 0.f;
-        for (int d = 0; d < 8; ++d) {
-            const int fi = 2 * i + (d & 1), fj = 2 * j + ((d >> 1) & 1), fk = 2 * k + (d >> 2);
-            s += __bfloat162float(f[((((int64_t)b * 2 * nz + fk) * 2 * ny + fj) * 2 * nx + fi) * C + ch]);
-        }
-        c[e] = __float2bfloat16(s * 0.125f);
+        const int64_t b = v / nz;
+        float s[8];
+        sum_children8(f, b, i, j, k, g, nx, ny, nz, C, s);
+        *reinterpret_cast<uint4*>(c + e * 8) = pack8_bf16(s, 0.125f);
     }
 }
 
 // adjoint of nearest upsampling: coarse[v][c] = sum of the 8 fine children
 static __global__ void k_downsum(const bf16* __restrict__ f, bf16* __restrict__ c, int B, int nx, int ny, int nz, int C) {
-    const int64_t n = (int64_t)B * nx * ny * nz * C;
+    const int G = C / 8;
+    const int64_t n = (int64_t)B * nx * ny * nz * G;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int ch = (int)(e % C);
-        int64_t v = e / C;
+        const int g = (int)(e % G);
+        int64_t v = e / G;
         const int i = (int)(v % nx);
         v /= nx;
         const int j = (int)(v % ny);
         v /= ny;
         const int k = (int)(v % nz);
-        const int b = (int)(v / nz);
-        float s = 0.f;
-        for (int d = 0; d < 8; ++d) {
-            const int fi = 2 * i + (d & 1), fj = 2 * j + ((d >> 1) & 1), fk = 2 * k + (d >> 2);
-            s += __bfloat162float(f[((((int64_t)b * 2 * nz + fk) * 2 * ny + fj) * 2 * nx + fi) * C + ch]);
-        }
-        c[e] = __float2bfloat16(s);
+        const int64_t b = v / nz;
+        float s[8];
+        sum_children8(f, b, i, j, k, g, nx, ny, nz, C, s);
+        *reinterpret_cast<uint4*>(c + e * 8) = pack8_bf16(s, 1.f);
     }
 }
 
