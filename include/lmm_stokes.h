@@ -166,6 +166,10 @@ typedef struct lmm_knobs {
     int    residual_fusion;        /* 3D periodic V-cycle: 1 = residual and restriction in one pass
                                       through shared memory; 0 = default (a residual kernel and a
                                       restriction kernel: measured faster) */
+    int    uniform_alpha;          /* 0 = default (a level whose theta*alpha faces all hold one value,
+                                      checked on the device at each coefficient load, has the
+                                      velocity operator take that value as a scalar: the same bits,
+                                      one array fewer per stencil), -1 = always read the arrays */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -1430,6 +1430,7 @@ template <class T>
 void launch_coarsen_coeffs(const LevelDev<T>& F, const LevelDev<T>& Cc, bool pressure_faces, cudaStream_t s) {
     const G3 g = geom3(Cc.D.nx, Cc.D.ny, Cc.D.nz);
     Coef<T> cf = F.coef();
+    cf.alpha_uniform = 0;  // the arrays are read (and may be others below)
     if (pressure_faces) {
         for (int d = 0; d < 3; ++d) cf.alpha[d] = F.pa[d];
         if (F.D.dm == 2)
@@ -1482,10 +1483,11 @@ void launch_cc_smooth(const LevelDev<T>& L, int parity, cudaStream_t s, int reve
 }
 
 template <class T>
-void launch_uniform_check(const LevelDev<T>& L, int* flag, cudaStream_t s) {
+void launch_uniform_check(const LevelDev<T>& L, int* flag, cudaStream_t s, bool velocity) {
     const int64_t n = L.n;
     const int blocks = (int)std::min<int64_t>((n + kThreads - 1) / kThreads, 1184);
-    k_uniform_check<T><<<blocks, kThreads, 0, s>>>(L.pa[0], L.pa[1], L.D.dm == 3 ? L.pa[2] : nullptr, n, flag);
+    T* const* a = velocity ? L.alpha : L.pa;
+    k_uniform_check<T><<<blocks, kThreads, 0, s>>>(a[0], a[1], L.D.dm == 3 ? a[2] : nullptr, n, flag);
 }
 
 template <class T>
@@ -1650,7 +1652,7 @@ namespace lmm {
     template void launch_cc_smooth<T>(const LevelDev<T>&, int, cudaStream_t, int);                                              \
     template void launch_cc_residual_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, cudaStream_t);                        \
     template void launch_cc_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, cudaStream_t);                              \
-    template void launch_uniform_check<T>(const LevelDev<T>&, int*, cudaStream_t);                                            \
+    template void launch_uniform_check<T>(const LevelDev<T>&, int*, cudaStream_t, bool);                                            \
     template void launch_neg_cc_lap<T>(const LevelDev<T>&, const T*, T*, cudaStream_t);                                        \
     template void launch_div_plus<T>(const LevelDev<T>&, const T* const[3], const T*, T*, cudaStream_t);                        \
     template void launch_sub_weighted_grad<T>(const LevelDev<T>&, const T* const[3], const T*, T* const[3], cudaStream_t);     \

@@ -34,6 +34,10 @@ struct LevelDev {
     // as a scalar instead of reading three face arrays
     int pa_uniform;
     T pa_value;
+    // every face of alpha[0..dm-1] holds a_value (checked on the device at
+    // every coefficient load): the velocity operator takes it as a scalar
+    int a_uniform = 0;
+    T a_value = T(0);
     T* pmu[3];          // BFBt: face coefficient 1/diag(viscous operator) (coarsened)
     T* pphi;
     T* prhs;
@@ -41,6 +45,8 @@ struct LevelDev {
     Coef<T> coef() const {
         Coef<T> c;
         for (int d = 0; d < 3; ++d) { c.alpha[d] = alpha[d]; c.bed[d] = bed[d]; }
+        c.alpha_uniform = a_uniform;
+        c.alpha_u = a_value;
         c.beta = beta;
         c.gamma = gamma;
         return c;
@@ -126,7 +132,7 @@ void launch_cc_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, cu
 // *flag |= 1 when the level's pressure face coefficients are not all the
 // same value (bit for bit)
 template <class T>
-void launch_uniform_check(const LevelDev<T>& L, int* flag, cudaStream_t s);
+void launch_uniform_check(const LevelDev<T>& L, int* flag, cudaStream_t s, bool velocity = false);
 template <class T>
 void launch_cc_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, cudaStream_t s);
 template <class T>

@@ -654,16 +654,23 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
         for (int d = 0; d < dm; ++d) launch_convert<double, float>(h->alphainv[d], h->alphainv32[d], n, h->stream);
         check_launch();
     }
-    // pressure levels whose face coefficients are one value (constant
-    // density): their smoother and residual take it as a scalar
+    // levels whose face coefficients are one value (constant density):
+    // the pressure smoother and residual take 1/alpha as a scalar, the
+    // velocity operator theta*alpha (up to 16 levels of each; the flags
+    // and values share the handle's error word block and misc buffer)
     {
-        const int np = std::min(h->nlev_p, 32);
+        const int np = std::min(h->nlev_p, 16), nv = std::min(h->nlev, 16);
         int* flags = h->dev_err + 32;
         LMM_CK(cudaMemsetAsync(flags, 0, 32 * sizeof(int), h->stream));
         for (int l = 0; l < np; ++l) {
             launch_uniform_check<double>(h->L64[l], flags + l, h->stream);
             check_launch();
             LMM_CK(cudaMemcpyAsync(h->hmisc + l, h->L64[l].pa[0], sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        }
+        for (int l = 0; l < nv; ++l) {
+            launch_uniform_check<double>(h->L64[l], flags + 16 + l, h->stream, true);
+            check_launch();
+            LMM_CK(cudaMemcpyAsync(h->hmisc + 16 + l, h->L64[l].alpha[0], sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         }
         int* hflags = reinterpret_cast<int*>(h->hmisc + 32);
         LMM_CK(cudaMemcpyAsync(hflags, flags, 32 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -672,9 +679,14 @@ void load_coeffs(lmm_handle* h, const double* const alpha_dev[3], const double* 
             const bool u = l < np && hflags[l] == 0 && !h->D0.wall;
             h->L64[l].pa_uniform = u ? 1 : 0;
             h->L64[l].pa_value = u ? h->hmisc[l] : 0.0;
+            const bool ua = l < nv && hflags[16 + l] == 0 && h->knobs.uniform_alpha >= 0;
+            h->L64[l].a_uniform = ua ? 1 : 0;
+            h->L64[l].a_value = ua ? h->hmisc[16 + l] : 0.0;
             if (l < (int)h->L32.size()) {
                 h->L32[l].pa_uniform = h->L64[l].pa_uniform;
                 h->L32[l].pa_value = (float)h->L64[l].pa_value;
+                h->L32[l].a_uniform = h->L64[l].a_uniform;
+                h->L32[l].a_value = (float)h->L64[l].a_value;
             }
         }
     }
@@ -1066,6 +1078,7 @@ void visc_schur(lmm_handle* h, T* mac, T* x_p) {
     {
         LevelDev<T> Lv = L0;
         for (int d = 0; d < 3; ++d) Lv.alpha[d] = zero;
+        Lv.a_uniform = 0;  // read the zero arrays
         Lv.gamma = zero;
         const T* gc[3] = {g[0], g[1], g[2]};
         launch_applyop<T>(Lv, h->knobs.visc_type, gc, lg, h->stream, 0);

@@ -221,6 +221,12 @@ struct Coef {
     const T* beta;       // cells
     const T* bed[3];     // 2D: [0] nodal; 3D: xy, xz, yz edges
     const T* gamma;      // cells
+    // every face of every alpha array holds alpha_u (checked on the device
+    // at each coefficient load): the operator takes it as a scalar instead
+    // of reading the arrays -- the value each load would return, so the
+    // same bits.  Set by LevelDev::coef(), the only place a Coef is made.
+    int alpha_uniform;
+    T alpha_u;
 };
 
 template <class T>
@@ -248,6 +254,12 @@ __device__ __forceinline__ T ldp(const T* p, int i) {
         return p[i];
     else
         return __ldcg(p + i);
+}
+
+// theta*alpha of face s of component d
+template <class T>
+__device__ __forceinline__ T alpha_at(const Coef<T>& C, int d, int s) {
+    return C.alpha_uniform ? C.alpha_u : ld(C.alpha[d], s);
 }
 
 // periodic wrap of an index known to lie in [-n, 2n)
@@ -284,7 +296,7 @@ __device__ __forceinline__ T face_L3_own(const T p0, const T (&nb)[6], const TP*
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
     const T onethird = T(1) / T(3), twothirds = T(2) / T(3), fourthirds = T(4) / T(3);
     const int s = n.s;
-    const T a = ld(C.alpha[D], s);
+    const T a = alpha_at(C, D, s);
     if (VISC == 1) {
         T nbs = nb[0] + nb[1] + nb[2] + nb[3] + nb[4] + nb[5];
         return p0 * (a + T(6) * b * dxsqinv) - nbs * b * dxsqinv;
@@ -360,7 +372,7 @@ template <class T, int VISC, int D, bool W = false>
 __device__ __forceinline__ T face_diag3(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t1 = Perm3<D>::t1, t2 = Perm3<D>::t2, e1 = Perm3<D>::e1, e2 = Perm3<D>::e2;
     const int s = n.s;
-    const T a = ld(C.alpha[D], s);
+    const T a = alpha_at(C, D, s);
     if (VISC == 1) return a + T(6) * b * dxsqinv;
     if (VISC == 2) return a + T(8) * b * dxsqinv;
     if (VISC == 3) return a + (T(20) / T(3) * b + T(2) * c) * dxsqinv;
@@ -461,7 +473,7 @@ __device__ __forceinline__ T face_update3(const T* const phi[3], const Coef<T>& 
         q2[2] = ld(a2, s + n.om[D] + n.op[t2]);
         q2[3] = ld(a2, s + n.om[D]);
     }
-    const T a = ld(C.alpha[D], s);
+    const T a = alpha_at(C, D, s);
     T be = T(0), bm = T(0), E1 = T(0), E1p = T(0), E2 = T(0), E2p = T(0), g = T(0), gm = T(0);
     if constexpr (VISC < 0) {
         be = ld(C.beta, s);
@@ -489,7 +501,7 @@ __device__ __forceinline__ T face_L2(const TP* const phi[3], const Coef<T>& C, c
     const TP* q = phi[t];
     const int s = n.s;
     const T p0 = (T)ldp<LD>(p, s);
-    const T a = ld(C.alpha[D], s);
+    const T a = alpha_at(C, D, s);
     T ppd = (T)ldp<LD>(p, s + n.op[D]), pmd = (T)ldp<LD>(p, s + n.om[D]);
     T ppt = (T)ldp<LD>(p, s + n.op[t]), pmt = (T)ldp<LD>(p, s + n.om[t]);
     if constexpr (W) {
@@ -534,7 +546,7 @@ template <class T, int VISC, int D, bool W = false>
 __device__ __forceinline__ T face_diag2(const Coef<T>& C, const Nb& n, T dxsqinv, T b, T c) {
     constexpr int t = 1 - D;
     const int s = n.s;
-    const T a = ld(C.alpha[D], s);
+    const T a = alpha_at(C, D, s);
     if (VISC == 1) return a + T(4) * b * dxsqinv;
     if (VISC == 2) return a + T(6) * b * dxsqinv;
     if (VISC == 3) return a + (T(14) / T(3) * b + T(2) * c) * dxsqinv;

@@ -298,6 +298,34 @@ def test_apply_precon_uniform_density(oracle, dm, n, pt):
     s.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("uniform", [True, False])
+def test_uniform_alpha_scalar_is_bitwise_neutral(precision, uniform):
+    """theta*alpha the same on every face (constant density, the bench's
+    case): the velocity operator takes it as a scalar (knob uniform_alpha =
+    0, the default) instead of reading three face arrays -- the same bits as
+    reading them (uniform_alpha = -1); with alpha varying, the arrays are
+    read either way"""
+    from lowmachmixtures_b200 import synth
+    from lowmachmixtures_b200.gmres import StokesSolver
+    p = synth.make_problem(3, 32, 100.0, 8, theta_alpha=0.1 * 32 * 32)
+    if not uniform:
+        rng = np.random.default_rng(3)
+        p.alpha_fc = [1.0 + 0.5 * rng.random(p.shape) for _ in range(3)]
+    out = []
+    for ua in (0, -1):
+        kn = abi.make_knobs(precon_type=2, visc_type=-2, method=abi.LMM_METHOD_FGMRES, precision=precision, uniform_alpha=ua)
+        with StokesSolver(3, (32, 32, 32), p.dx, knobs=kn) as s:
+            xu, xp = p.zeros_like_solution()
+            _, _, st = s.solve(p.b_u, p.b_p, xu, xp, p.alpha_fc, p.beta, p.beta_ed, p.gamma, p.theta_alpha)
+        assert st["status"] == 0
+        out.append((xu, xp, st["history"]))
+    for c in range(3):
+        np.testing.assert_array_equal(out[0][0][c], out[1][0][c])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+
+
 def _solve_both(oracle, prob, **kn):
     k = oracle.default_knobs(**kn)
     rc_o, xu_o, xp_o, th_o, npr_o, st_o = oracle.solve(prob, k)
