@@ -2815,6 +2815,7 @@ extern "C" int64_t lmm_kernel_launches(void) { return lmm::launches_total(); }
 extern "C" int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_rep) {
     if (!h || !h->coeffs_loaded || reps < 1 || !ms_per_rep) return LMM_ERR_INVALID;
     if ((which == 1 || which == 5) && h->knobs.precision != LMM_PRECISION_FP32) return LMM_ERR_INVALID;
+    NvtxRange nvtx_("lmm_time_op");  // a profiler can select these launches (not the autotuner's)
     try {
         LevelDev<double>& L = h->L64[0];
         auto once = [&]() {
