@@ -70,15 +70,19 @@ __device__ __forceinline__ void unflat3d(const Dims& D, int w, int& i, int& j, i
 
 // W: a grid with walls (wall faces keep their zero; the stencils and ghost
 // rules of the per-level wall kernels)
+// faces of one colour of an even level
+__device__ __forceinline__ int colour_count(const Dims& D) { return (D.nx >> 1) * D.ny * D.nz; }
+
+// threads t0, t0 + stride, ... of the block take the colour's faces
 template <class T, int DM, int VISC, int COMP, bool W>
-__device__ __forceinline__ void tail_colour(const TailView<T>& L, int parity, T omega) {
+__device__ __forceinline__ void tail_colour(const TailView<T>& L, int parity, T omega, int t0, int stride) {
     const T b = ld(L.C.beta, 0), c = ld(L.C.gamma, 0);
     const int half = L.D.nx >> 1;
     const int count = half * L.D.ny * L.D.nz;
     const T* phi[3] = {L.phi[0], L.phi[1], L.phi[2]};
     T* p = L.phi[COMP];
     const T* r = L.rhs[COMP];
-    for (int w = threadIdx.x; w < count; w += blockDim.x) {
+    for (int w = t0; w < count; w += stride) {
         const int ih = w % half;
         const int q = w / half;
         const int j = q % L.D.ny, k = q / L.D.ny;
@@ -127,6 +131,27 @@ template <class T, int DM, int VISC, bool W>
 __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega) {
     const T b = ld(L.C.beta, 0), c = ld(L.C.gamma, 0);
     const int n = ncells(L.D);
+    // Gauss-Seidel on an even level whose colours have at most 32 faces (4^3,
+    // 2^3; 4^2, 2^2): warp 0 takes every sweep, a __syncwarp between colours
+    // instead of the block's barrier (the same faces, the same arithmetic)
+    if (smoother != 0 && !odd_level(L.D) && colour_count(L.D) <= 32) {
+        if (threadIdx.x < 32) {
+            for (int s = 0; s < nsm; ++s)
+                for (int color = 1; color <= 2 * DM; ++color) {
+                    const int comp = (color - 1) / 2;
+                    const int parity = (color % 2 == 1) ? 0 : 1;
+                    if (comp == 0)
+                        tail_colour<T, DM, VISC, 0, W>(L, parity, omega, threadIdx.x, 32);
+                    else if (comp == 1)
+                        tail_colour<T, DM, VISC, 1, W>(L, parity, omega, threadIdx.x, 32);
+                    else if constexpr (DM == 3)
+                        tail_colour<T, DM, VISC, 2, W>(L, parity, omega, threadIdx.x, 32);
+                    __syncwarp();
+                }
+        }
+        __syncthreads();
+        return;
+    }
     for (int s = 0; s < nsm; ++s) {
         if (smoother == 0) {
             const T* phi[3] = {L.phi[0], L.phi[1], L.phi[2]};
@@ -175,11 +200,11 @@ __device__ void tail_smooth(const TailView<T>& L, int nsm, int smoother, T omega
                         tail_colour_odd<T, DM, VISC, 2, W>(L, parity, omega);
                 } else {
                     if (comp == 0)
-                        tail_colour<T, DM, VISC, 0, W>(L, parity, omega);
+                        tail_colour<T, DM, VISC, 0, W>(L, parity, omega, threadIdx.x, blockDim.x);
                     else if (comp == 1)
-                        tail_colour<T, DM, VISC, 1, W>(L, parity, omega);
+                        tail_colour<T, DM, VISC, 1, W>(L, parity, omega, threadIdx.x, blockDim.x);
                     else if constexpr (DM == 3)
-                        tail_colour<T, DM, VISC, 2, W>(L, parity, omega);
+                        tail_colour<T, DM, VISC, 2, W>(L, parity, omega, threadIdx.x, blockDim.x);
                 }
                 __syncthreads();
             }
@@ -354,9 +379,17 @@ __device__ void tail_cc_smooth(const TailView<T>& L, int nsweeps) {
             }
         return;
     }
+    // at most 32 cells per colour: warp 0 takes every sweep, a __syncwarp
+    // between colours instead of the block's barrier
+    const bool narrow = count <= 32;
+    if (narrow && threadIdx.x >= 32) {
+        __syncthreads();
+        return;
+    }
+    const int t0 = threadIdx.x, stride = narrow ? 32 : blockDim.x;
     for (int s = 0; s < nsweeps; ++s)
         for (int parity = 0; parity < 2; ++parity) {
-            for (int w = threadIdx.x; w < count; w += blockDim.x) {
+            for (int w = t0; w < count; w += stride) {
                 const int ih = w % half;
                 const int q = w / half;
                 const int j = q % L.D.ny, k = q / L.D.ny;
@@ -366,8 +399,12 @@ __device__ void tail_cc_smooth(const TailView<T>& L, int nsweeps) {
                 T cur = L.pphi[nb.s];
                 L.pphi[nb.s] = cur + res / cc_diag<T, DM>(L.pa, nb, L.dxsqinv);
             }
-            __syncthreads();
+            if (narrow)
+                __syncwarp();
+            else
+                __syncthreads();
         }
+    if (narrow) __syncthreads();
 }
 
 template <class T, int DM>
