@@ -32,7 +32,7 @@ namespace lmm {
 namespace nn {
 
 constexpr int kRingW = 4;                              // input halo planes held
-constexpr int kThreadsWS = 160;                        // 4 epilogue warps + the feeder
+constexpr int kThreadsWS = 160;                        // 4 epilogue / copy warps + the MMA warp
 constexpr int kBarsWS = kRingW + 4;                    // full per slot; tfull, tempty per buffer
 
 __host__ __device__ constexpr int ws_weight_bytes(int cinp, int ns) { return 9 * (cinp / 16) * 3 * ns * 32; }
