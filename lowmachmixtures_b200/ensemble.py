@@ -197,6 +197,7 @@ def main():
     ens = Ensemble(probs, kn, a.workers, local)
     create_s = time.perf_counter() - t0
     best = None
+    each = []  # seconds of every repeat
     for _ in range(a.repeats):
         if dist is not None:
             dist.barrier()
@@ -205,6 +206,7 @@ def main():
         if bad:
             raise RuntimeError(f"instances of sizes {bad} failed: " + lib.lmm_strerror(min(st)).decode())
         best = secs if best is None else min(best, secs)
+        each.append(secs)
     ens.close()
     ok = [s for s, c in zip(stats, st) if c >= 0]
     errors = {}
@@ -212,6 +214,7 @@ def main():
         if c < 0:
             errors.setdefault(lib.lmm_strerror(c).decode(), []).append(p.n[0])
     out = dict(rank=rank, mode=a.mode, workers=a.workers if pool else None, instances=len(probs), seconds=best,
+               seconds_each=each,
                instances_per_s=len(probs) / best,
                pool_creation_seconds=create_s,
                failed=int(sum(1 for c in st if c < 0)), unconverged=int(sum(1 for c in st if c > 0)), errors=errors,
