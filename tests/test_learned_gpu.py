@@ -84,7 +84,9 @@ def _packed(w, with_t=False):
                                                   (1, (64, 32, 64), 64, 32, 1, 1), (3, (8, 16, 5), 16, 32, 0, 1),
                                                   (1, (128, 128, 24), 16, 16, 0, 0),
                                                   # output channels in slices: 2 x 32 and 3 x 16
-                                                  (1, (32, 32, 32), 64, 64, 0, 1), (1, (16, 32, 12), 64, 48, 0, 1)])
+                                                  (1, (32, 32, 32), 64, 64, 0, 1), (1, (16, 32, 12), 64, 48, 0, 1),
+                                                  # 8 input channels: x taps paired in one K = 16 step
+                                                  (1, (64, 64, 32), 8, 16, 0, 1), (2, (32, 32, 16), 8, 32, 0, 1)])
 def test_conv3d_matches_torch(B, n, cin, cout, up, relu):
     import torch
     from lowmachmixtures_b200 import _native
