@@ -35,6 +35,19 @@ def test_every_declared_symbol_is_exported(lib):
         assert hasattr(lib, name), f"{name} not exported"
 
 
+def test_bounds_check_library_exports_the_same_symbols():
+    """liblmmstokes_bc.so (build.py --bounds-check) is a drop-in for the
+    default library: every declared entry point, and the status code its
+    checks return"""
+    from lowmachmixtures_b200 import build
+    path = build.build(bounds_check=True)
+    bc = C.CDLL(path)
+    for name in declared_functions():
+        assert hasattr(bc, name), f"{name} not exported by {os.path.basename(path)}"
+    bc.lmm_strerror.restype = C.c_char_p
+    assert b"registered allocations" in bc.lmm_strerror(abi.LMM_ERR_BOUNDS)
+
+
 def test_struct_layout_matches_c(lib):
     # sizes of the C structs, computed by the C compiler
     src = r'''
