@@ -160,8 +160,8 @@ typedef struct lmm_knobs {
                                       launches take the planes in alternating order, each starting
                                       where the last left its operands in L2), -1 = always in +k order */
     int    autotune;               /* 0 = default (the first handle of a grid size times candidate block
-                                      shapes of the colour, operator and prolongation kernels and the
-                                      process keeps the fastest; see lmm_autotune_report), -1 = this
+                                      shapes of the colour, operator, residual and prolongation kernels
+                                      and the process keeps the fastest; see lmm_autotune_report), -1 = this
                                       handle times nothing (shapes the process chose already apply) */
     int    residual_fusion;        /* 3D periodic V-cycle: 1 = residual and restriction in one pass
                                       through shared memory; 0 = default (a residual kernel and a
@@ -317,7 +317,11 @@ int64_t lmm_kernel_launches(void);
  *   3 apply_matrix, FP64
  *   4 one staggered V-cycle, FP64
  *   5 one staggered V-cycle, FP32
- *   6 one pressure V-cycle, FP64                                        */
+ *   6 one pressure V-cycle, FP64
+ *   7 the classical Gram-Schmidt passes of one restart cycle (columns
+ *     1..gmres_max_inner: projections, update and norm of w; FGMRES)
+ *   8 one Krylov normalisation V = w / |w| (with its FP32 copy when
+ *     precision is FP32)                                                */
 int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_rep);
 
 /* The block-shape autotuner's choices so far (no counterpart in the

@@ -34,6 +34,7 @@ const char* kernel_name(int k) {
     case TK_GS_COLOUR: return "gs_colour";
     case TK_APPLYOP: return "applyop";
     case TK_PROLONG: return "prolong_add";
+    case TK_RESIDUAL: return "residual";
     default: return "?";
     }
 }

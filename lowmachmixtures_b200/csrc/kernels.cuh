@@ -1401,7 +1401,7 @@ void launch_residual_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, int v
         return;
     }
     // residual on every fine face into F.tmp, then the pure restriction
-    const G3 g = geom3(F.D.nx, F.D.ny, F.D.nz * F.D.dm);
+    const G3 g = geom3_tuned(TK_RESIDUAL, sizeof(T), visc, F.D, F.D.nx, F.D.ny, F.D.nz * F.D.dm);
     if (F.D.dm == 2) {
         LMM_VISC_DISPATCH(visc, launch_pdl(k_residual_c<T, 2, V>, g.grid, g.block, 0, s, F.D, F.coef(), rhs_f[0], rhs_f[1], rhs_f[2], phi_f[0], phi_f[1], phi_f[2], F.tmp[0], F.tmp[1], F.tmp[2], dxsqinv))
     } else {

@@ -219,7 +219,7 @@ int64_t launches_total();
 
 // ---- block-shape autotuner (autotune.cu; the timing is solver.cu's) ----
 // Kernels whose launch geometry it picks per (precision, visc_type, grid).
-enum TuneKernel { TK_GS_COLOUR = 0, TK_APPLYOP = 1, TK_PROLONG = 2, TK_N = 3 };
+enum TuneKernel { TK_GS_COLOUR = 0, TK_APPLYOP = 1, TK_PROLONG = 2, TK_RESIDUAL = 3, TK_N = 4 };
 struct Shape {
     int bx = 0, by = 0;  // 0 x 0: the default geometry (geom3)
 };

@@ -149,8 +149,27 @@ __global__ void k_div_by_f32(const double* __restrict__ w, double* __restrict__ 
         v32[t] = (float)q;
     }
 }
+// the same, four entries per thread by 16-byte loads and stores (n a
+// multiple of 4, every pointer 16-byte aligned)
+__global__ void k_div_by_f32_x4(const double2* __restrict__ w, double2* __restrict__ v, float4* __restrict__ v32,
+                                const double* __restrict__ den, int64_t n4) {
+    pdl_enter();
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n4) {
+        const double d = *den;
+        const double2 a = w[2 * t], b = w[2 * t + 1];
+        const double2 qa = make_double2(a.x / d, a.y / d), qb = make_double2(b.x / d, b.y / d);
+        v[2 * t] = qa;
+        v[2 * t + 1] = qb;
+        v32[t] = make_float4((float)qa.x, (float)qa.y, (float)qb.x, (float)qb.y);
+    }
+}
 void launch_div_by_f32(const double* w, double* v, float* v32, const double* den, int64_t n, cudaStream_t s) {
-    launch_pdl(k_div_by_f32, nb(n), kT, 0, s, w, v, v32, den, n);
+    auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    if (n % 4 == 0 && al(w) && al(v) && al(v32))
+        launch_pdl(k_div_by_f32_x4, nb(n / 4), kT, 0, s, (const double2*)w, (double2*)v, (float4*)v32, den, n / 4);
+    else
+        launch_pdl(k_div_by_f32, nb(n), kT, 0, s, w, v, v32, den, n);
 }
 
 __global__ void k_sub_scaled(double* __restrict__ w, const double* __restrict__ V, const double* __restrict__ h, int64_t n) {
@@ -460,6 +479,20 @@ namespace {
 
 constexpr int kMdotThreads = 256;
 
+// The last block's sum of every block's partials, entry e of E: warp
+// e mod 8 takes it, its lanes stride over the blocks, then a shuffle tree
+// (a fixed order for a given grid).  The result goes to sh[e * ld].
+template <int E>
+__device__ __forceinline__ void sum_partials(const double* partials, double* sh, int ld) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int e = warp; e < E; e += kMdotThreads / 32) {
+        double v = 0.0;
+        for (unsigned b = lane; b < gridDim.x; b += 32) v += ((volatile const double*)partials)[b * E + e];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[e * ld] = v;
+    }
+}
+
 // Stokes inner products <w, V_k>, k < J, in one pass over w: per component
 // the plain sum plus (seam weight - 1) x the seam-plane sum, as k_reduce
 // weighs them; out[k*ss + 4] = sum_d <w_d, V_k,d> + pw^2 <w_p, V_k,p> (ss:
@@ -468,10 +501,12 @@ constexpr int kMdotThreads = 256;
 // 2D batches (D.nz instances): blockIdx.y is the instance, with its own
 // partials, counter and slot entry (+8 per instance); each instance is
 // partitioned and summed as one problem alone.
+// (J = 5 held to three blocks per SM: unbounded, the compiler takes the
+// registers of two, and two blocks per SM keep too few loads in flight)
 template <int DM, int J>
-__global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __restrict__ w, MVecs V, double wseam, double pw,
+__global__ void __launch_bounds__(kMdotThreads, J == 5 ? 3 : 0) k_mdot(Dims D, const double* __restrict__ w, MVecs V, double wseam, double pw,
                                                        double* __restrict__ partials, unsigned* __restrict__ counter,
-                                                       double* __restrict__ out, int64_t ss) {
+                                                       double* __restrict__ out, int64_t ss, int vec) {
     pdl_enter();
     constexpr int NC = DM + 1;
     const int n = D.nx * D.ny * (DM == 3 ? D.nz : 1);  // one instance
@@ -492,12 +527,62 @@ __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __r
         for (int c = 0; c < NC; ++c) acc[k][c] = 0.0;
     const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int t = tid; t < n; t += stride) {
+    if (vec) {
+        // entry pairs by 16-byte loads (every row even, every vector
+        // 16-byte aligned); few vectors: two pairs per thread and pass,
+        // so each thread keeps 8 or more loads in flight
+        constexpr int U = (J <= 2) ? 2 : 1;
+        const int n2 = n >> 1;
+        if constexpr (U == 1) {
+            // per component: its J + 1 loads, then their products (the
+            // compiler overlaps the next component's loads with them)
+            for (int p = tid; p < n2; p += stride) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const double x = __ldg(w + (int64_t)c * N + t);
+                for (int c = 0; c < NC; ++c) {
+                    const double2 x = __ldg(reinterpret_cast<const double2*>(w + (int64_t)c * N) + p);
+                    double2 v[J];
 #pragma unroll
-            for (int k = 0; k < J; ++k) acc[k][c] += x * __ldg(V.p[k] + (int64_t)c * N + t);
+                    for (int k = 0; k < J; ++k) v[k] = __ldg(reinterpret_cast<const double2*>(V.p[k] + (int64_t)c * N) + p);
+#pragma unroll
+                    for (int k = 0; k < J; ++k) {
+                        acc[k][c] += x.x * v[k].x;
+                        acc[k][c] += x.y * v[k].y;
+                    }
+                }
+            }
+        } else
+        for (int p0 = tid; p0 < n2; p0 += U * stride) {
+            double2 x[U][NC], v[U][J][NC];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int p = min(p0 + u * stride, n2 - 1);
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    x[u][c] = __ldg(reinterpret_cast<const double2*>(w + (int64_t)c * N) + p);
+#pragma unroll
+                    for (int k = 0; k < J; ++k) v[u][k][c] = __ldg(reinterpret_cast<const double2*>(V.p[k] + (int64_t)c * N) + p);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (u > 0 && p0 + u * stride >= n2) break;
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int k = 0; k < J; ++k) {
+                        acc[k][c] += x[u][c].x * v[u][k][c].x;
+                        acc[k][c] += x[u][c].y * v[u][k][c].y;
+                    }
+            }
+        }
+    } else {
+        for (int t = tid; t < n; t += stride) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const double x = __ldg(w + (int64_t)c * N + t);
+#pragma unroll
+                for (int k = 0; k < J; ++k) acc[k][c] += x * __ldg(V.p[k] + (int64_t)c * N + t);
+            }
         }
     }
     // seam planes of the face components (x: i == 0, y: j == 0, z: k == 0)
@@ -543,12 +628,7 @@ __global__ void __launch_bounds__(kMdotThreads) k_mdot(Dims D, const double* __r
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (threadIdx.x < J * NC) {
-        // fixed order over the blocks
-        double v = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) v += ((volatile double*)partials)[b * J * NC + threadIdx.x];
-        sh[threadIdx.x][0] = v;
-    }
+    sum_partials<J * NC>(partials, &sh[0][0], kMdotThreads / 32);
     __syncthreads();
     if (threadIdx.x < J) {
         const int k = threadIdx.x;
@@ -579,7 +659,8 @@ __global__ void k_maxpy(double* __restrict__ w, MVecs V, const double* __restric
 template <int DM, int J>
 __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __restrict__ w, MVecs V, const double* __restrict__ hs,
                                                              double wseam, double pw, double* __restrict__ partials,
-                                                             unsigned* __restrict__ counter, double* __restrict__ out, int64_t ss) {
+                                                             unsigned* __restrict__ counter, double* __restrict__ out, int64_t ss,
+                                                             int vec) {
     pdl_enter();
     constexpr int NC = DM + 1;
     const int n = D.nx * D.ny * (DM == 3 ? D.nz : 1);  // one instance (blockIdx.y, as k_mdot)
@@ -601,17 +682,48 @@ __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __r
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] = 0.0;
     const int stride = gridDim.x * blockDim.x;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-        const int i = t % D.nx, r = t / D.nx, j = r % D.ny, kk = r / D.ny;
+    if (vec) {
+        // entry pairs (2p, 2p+1) of one row by 16-byte loads and stores
+        // (every row even, every vector 16-byte aligned)
+        const int n2 = n >> 1;
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n2; p += stride) {
+            const int t = 2 * p;
+            const int i = t % D.nx, r = t / D.nx, j = r % D.ny, kk = r / D.ny;
+            double2 x[NC], v[J][NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const int64_t e = (int64_t)c * N + t;
-            double x = w[e];
+            for (int c = 0; c < NC; ++c) {
+                x[c] = reinterpret_cast<const double2*>(w + (int64_t)c * N)[p];
 #pragma unroll
-            for (int k = 0; k < J; ++k) x = x - V.p[k][e] * h[k];
-            w[e] = x;
-            const bool seam = (c == 0 && i == 0) || (c == 1 && j == 0) || (c == 2 && c < DM && kk == 0);
-            acc[c] += (seam ? wseam : 1.0) * (x * x);
+                for (int k = 0; k < J; ++k) v[k][c] = __ldg(reinterpret_cast<const double2*>(V.p[k] + (int64_t)c * N) + p);
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+#pragma unroll
+                for (int k = 0; k < J; ++k) {
+                    x[c].x = x[c].x - v[k][c].x * h[k];
+                    x[c].y = x[c].y - v[k][c].y * h[k];
+                }
+                reinterpret_cast<double2*>(w + (int64_t)c * N)[p] = x[c];
+                // entry 2p+1 has i > 0: only the y and z seams reach it
+                const bool seam_yz = (c == 1 && j == 0) || (c == 2 && c < DM && kk == 0);
+                const bool seam0 = (c == 0 && i == 0) || seam_yz;
+                acc[c] += (seam0 ? wseam : 1.0) * (x[c].x * x[c].x);
+                acc[c] += (seam_yz ? wseam : 1.0) * (x[c].y * x[c].y);
+            }
+        }
+    } else {
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+            const int i = t % D.nx, r = t / D.nx, j = r % D.ny, kk = r / D.ny;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int64_t e = (int64_t)c * N + t;
+                double x = w[e];
+#pragma unroll
+                for (int k = 0; k < J; ++k) x = x - V.p[k][e] * h[k];
+                w[e] = x;
+                const bool seam = (c == 0 && i == 0) || (c == 1 && j == 0) || (c == 2 && c < DM && kk == 0);
+                acc[c] += (seam ? wseam : 1.0) * (x * x);
+            }
         }
     }
     __shared__ double sh[NC][kMdotThreads / 32];
@@ -635,11 +747,7 @@ __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __r
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (threadIdx.x < NC) {
-        double v = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) v += ((volatile double*)partials)[b * NC + threadIdx.x];
-        sh[threadIdx.x][0] = v;
-    }
+    sum_partials<NC>(partials, &sh[0][0], kMdotThreads / 32);
     __syncthreads();
     if (threadIdx.x == 0) {
         double su = 0.0;
@@ -656,11 +764,20 @@ __global__ void __launch_bounds__(kMdotThreads) k_maxpy_norm(Dims D, double* __r
 namespace {
 template <int DM, int J, bool NORM>
 int cgs_blocks(int64_t n);
+// the Gram-Schmidt passes may take entries in pairs: rows of even length
+// (no pair straddles a row or an instance) and 16-byte aligned vectors
+int pairs_ok(const Dims& D, const void* w, const MVecs& V, int J) {
+    auto al = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    bool ok = (D.nx % 2 == 0) && al(w);
+    for (int k = 0; k < J && k < 8; ++k) ok = ok && al(V.p[k]);
+    return ok ? 1 : 0;
+}
 }
 void launch_maxpy_norm(const Dims& D, double* w, const MVecs& V, int J, const double* hs, double wseam, double pw, double* partials,
                        unsigned* counter, double* out, cudaStream_t s, int ninst, int64_t ss) {
     const int64_t n = (int64_t)D.nx * D.ny * (D.dm == 3 ? D.nz : 1);
-#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, dim3(cgs_blocks<DM_, J_, true>(n), ninst), dim3(kMdotThreads), 0, s, D, w, V, hs, wseam, pw, partials, counter, out, ss)
+    const int vec = pairs_ok(D, w, V, J);
+#define MN(DM_, J_) launch_pdl(k_maxpy_norm<DM_, J_>, dim3(cgs_blocks<DM_, J_, true>(n), ninst), dim3(kMdotThreads), 0, s, D, w, V, hs, wseam, pw, partials, counter, out, ss, vec)
 #define MNJ(DM_)                               \
     switch (J) {                               \
     case 1: MN(DM_, 1); break;                 \
@@ -707,7 +824,8 @@ int cgs_blocks(int64_t n) {
 void launch_mdot(const Dims& D, const double* w, const MVecs& V, int J, double wseam, double pw, double* partials, unsigned* counter,
                  double* out, cudaStream_t s, int ninst, int64_t ss) {
     const int64_t n = (int64_t)D.nx * D.ny * (D.dm == 3 ? D.nz : 1);
-#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, dim3(cgs_blocks<DM_, J_, false>(n), ninst), dim3(kMdotThreads), 0, s, D, w, V, wseam, pw, partials, counter, out, ss)
+    const int vec = pairs_ok(D, w, V, J);
+#define MD(DM_, J_) launch_pdl(k_mdot<DM_, J_>, dim3(cgs_blocks<DM_, J_, false>(n), ninst), dim3(kMdotThreads), 0, s, D, w, V, wseam, pw, partials, counter, out, ss, vec)
 #define MDJ(DM_)                               \
     switch (J) {                               \
     case 1: MD(DM_, 1); break;                 \

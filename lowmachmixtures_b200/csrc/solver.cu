@@ -762,8 +762,8 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
 
 // Block-shape autotuner.  On the first handle of a grid size (per
 // precision and visc_type; the table is the process's), time the candidate
-// block shapes of the Gauss-Seidel colour, operator and prolongation
-// kernels on every periodic level with at least 4096 cells -- one warm-up
+// block shapes of the Gauss-Seidel colour, operator, residual and
+// prolongation kernels on every periodic level with at least 4096 cells -- one warm-up
 // and three launches each, CUDA events on the handle's stream -- and keep
 // the fastest.  It runs at creation, on the fresh arena's zeros; the colour
 // kernel divides by the zero diagonal there, so phi and tmp of a tuned
@@ -777,7 +777,7 @@ void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
         if (L.n < 4096 || L.D.wall || (L.D.nx & 1) || (L.D.ny & 1) || (L.D.dm == 3 && (L.D.nz & 1))) continue;
         bool touched = false;
         for (int kid = 0; kid < TK_N; ++kid) {
-            if (kid == TK_PROLONG && l + 1 >= h->nlev) continue;  // needs a coarser level
+            if ((kid == TK_PROLONG || kid == TK_RESIDUAL) && l + 1 >= h->nlev) continue;  // needs a coarser level
             const int kv = (kid == TK_PROLONG) ? 0 : visc;
             if (is_tuned(kid, sizeof(T), kv, L.D)) continue;
             const int nxe = (kid == TK_GS_COLOUR) ? L.D.nx / 2 : L.D.nx;
@@ -786,6 +786,8 @@ void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
                     launch_gs_colour<T>(L, visc, 1, L.rhs, L.phi, 1.0, h->stream, 0);
                 else if (kid == TK_APPLYOP)
                     launch_applyop<T>(L, visc, L.phi, L.tmp, h->stream, 0);
+                else if (kid == TK_RESIDUAL)  // the split residual (its restriction is timed with it)
+                    launch_residual_restrict<T>(L, Ls[l + 1], visc, L.rhs, L.phi, Ls[l + 1].rhs, h->stream, 0);
                 else
                     launch_prolong_add<T>(L, Ls[l + 1], Ls[l + 1].phi, L.phi, h->stream);
                 check_launch();
@@ -2835,6 +2837,17 @@ extern "C" int lmm_time_op(lmm_handle* h, int which, int reps, double* ms_per_re
             case 4: vcycle<double>(h, h->L64); break;
             case 5: vcycle<float>(h, h->L32); break;
             case 6: macproject<double>(h); break;
+            case 7:
+                // one restart cycle's Gram-Schmidt passes (columns 1..m)
+                for (int i = 1; i <= h->knobs.gmres_max_inner; ++i) cgs_column(h, i);
+                break;
+            case 8:
+                if (h->knobs.precision == LMM_PRECISION_FP32)
+                    launch_div_by_f32(h->w.base, h->V[1].base, h->pin32, h->slot(2) + 5, h->w.size(), h->stream);
+                else
+                    launch_div_by(h->w.base, h->V[1].base, h->slot(2) + 5, h->w.size(), h->stream);
+                check_launch();
+                break;
             default: throw LmmError(LMM_ERR_INVALID);
             }
         };

@@ -35,7 +35,8 @@ def main():
     ap.add_argument("--knob", action="append", default=[], metavar="NAME=INT",
                     help="extra lmm_knobs integer field (repeatable), e.g. --knob tail_cells=512")
     ap.add_argument("--bc", default="", help="BC code per direction, both sides, e.g. -1,100,-1 (default periodic)")
-    ap.add_argument("--op", default="", choices=["", "smooth", "applyop", "apply_matrix", "vcycle", "macproject", "net_forward"],
+    ap.add_argument("--op", default="", choices=["", "smooth", "applyop", "apply_matrix", "vcycle", "macproject", "gram_schmidt",
+                             "normalise", "net_forward"],
                     help="instead of solves: time one operation (lmm_time_op) --solves times after one warm-up; "
                          "'smooth' and 'vcycle' run in the method's precision; 'net_forward': --warm + --solves "
                          "forward passes of the learned stage's network")
@@ -101,7 +102,7 @@ def main():
             s.load_coeffs(al, be, bed, ga, prob.theta_alpha)
             fp32 = a.method == "mixed"
             which = {"smooth": 1 if fp32 else 0, "applyop": 2, "apply_matrix": 3, "vcycle": 5 if fp32 else 4,
-                     "macproject": 6}[a.op]
+                     "macproject": 6, "gram_schmidt": 7, "normalise": 8}[a.op]
             print(json.dumps({"op": a.op, "us": s.time_op(which, reps=a.solves) * 1000.0}))
             return
         out = []
