@@ -161,7 +161,7 @@ typedef struct lmm_knobs {
                                       where the last left its operands in L2), -1 = always in +k order */
     int    autotune;               /* 0 = default (the first handle of a grid size times candidate block
                                       shapes of the colour, operator, residual and prolongation kernels
-                                      and the process keeps the fastest; see lmm_autotune_report), -1 = this
+                                      and of apply_matrix, and the process keeps the fastest; see lmm_autotune_report), -1 = this
                                       handle times nothing (shapes the process chose already apply) */
     int    residual_fusion;        /* 3D periodic V-cycle: 1 = residual and restriction in one pass
                                       through shared memory; 0 = default (a residual kernel and a
@@ -170,6 +170,9 @@ typedef struct lmm_knobs {
                                       checked on the device at each coefficient load, has the
                                       velocity operator take that value as a scalar: the same bits,
                                       one array fewer per stencil), -1 = always read the arrays */
+    int    smoother_fusion_cells;  /* smoother_fusion > 0: only levels with at most this many cells
+                                      take the fused colour pairs (the larger ones one launch per
+                                      colour); 0 = default (every level that allows them) */
 } lmm_knobs;
 
 /* Inputs of gmres(...): b_u, b_p, alpha_fc, beta, beta_ed, gamma.

@@ -97,6 +97,7 @@ _KNOB_FIELDS = [
     ("autotune", C.c_int),
     ("residual_fusion", C.c_int),
     ("uniform_alpha", C.c_int),
+    ("smoother_fusion_cells", C.c_int),
 ]
 
 
@@ -121,7 +122,7 @@ KNOB_DEFAULTS = dict(
     visc_type=1, method=LMM_METHOD_GMRES, precision=LMM_PRECISION_FP64, learned_stage=0,
     tail_cells=0, tail_smem_kb=0, use_graphs=0, smoother_fusion=0, l2_persist=0, orthogonalization=0, host_wait=0,
     ensemble_batch=0, smoother_tma=0, smoother_tma_slabs=0, smoother_tma_cells=0, smoother_order=0, autotune=0, residual_fusion=0,
-    uniform_alpha=0,
+    uniform_alpha=0, smoother_fusion_cells=0,
 )
 
 

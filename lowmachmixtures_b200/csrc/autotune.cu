@@ -35,6 +35,7 @@ const char* kernel_name(int k) {
     case TK_APPLYOP: return "applyop";
     case TK_PROLONG: return "prolong_add";
     case TK_RESIDUAL: return "residual";
+    case TK_APPLY_MATRIX: return "apply_matrix";
     default: return "?";
     }
 }

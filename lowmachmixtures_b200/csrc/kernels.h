@@ -219,7 +219,9 @@ int64_t launches_total();
 
 // ---- block-shape autotuner (autotune.cu; the timing is solver.cu's) ----
 // Kernels whose launch geometry it picks per (precision, visc_type, grid).
-enum TuneKernel { TK_GS_COLOUR = 0, TK_APPLYOP = 1, TK_PROLONG = 2, TK_RESIDUAL = 3, TK_N = 4 };
+// TK_APPLY_MATRIX: the level-0 apply_matrix, keyed by its input width
+// (8: FP64 x, 4: the FP32 preconditioned vector of the mixed method)
+enum TuneKernel { TK_GS_COLOUR = 0, TK_APPLYOP = 1, TK_PROLONG = 2, TK_RESIDUAL = 3, TK_APPLY_MATRIX = 4, TK_N = 5 };
 struct Shape {
     int bx = 0, by = 0;  // 0 x 0: the default geometry (geom3)
 };

@@ -78,8 +78,16 @@ static void apply_matrix_impl(const LevelDev<double>& L0, int visc, const TX* xb
                               cudaStream_t s) {
     const double dxsqinv = 1.0 / (L0.dx * L0.dx);
     const double dxinv = 1.0 / L0.dx;
+    // periodic grids: the block shape the autotuner chose (a shape it
+    // forces while it times them), else 64 x 4
+    Shape sh = forced_shape();
+    if (!sh.bx) sh = tuned_shape(TK_APPLY_MATRIX, sizeof(TX), visc, L0.D);
     int bx = L0.D.nx < 64 ? L0.D.nx : 64;
     int by = 256 / bx;
+    if (!L0.D.wall && sh.bx) {
+        bx = std::min(sh.bx, L0.D.nx);
+        by = sh.by ? sh.by : 256 / bx;
+    }
     if (by > L0.D.ny) by = L0.D.ny;
     const dim3 blk(bx, by, 1), grd((L0.D.nx + bx - 1) / bx, (L0.D.ny + by - 1) / by, L0.D.nz);
     const TX* x0 = xb;

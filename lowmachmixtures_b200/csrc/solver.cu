@@ -727,7 +727,8 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
                 LMM_CK(cudaMemcpyAsync(L.phi[d], cur[d], L.n * sizeof(T), cudaMemcpyDeviceToDevice, h->stream));
         return;
     }
-    if (K.stag_mg_smoother != 0 && K.smoother_fusion > 0 && nsm > 0 && gs_pair_supported<T>(L, K.smoother_fusion)) {
+    if (K.stag_mg_smoother != 0 && K.smoother_fusion > 0 && nsm > 0 && gs_pair_supported<T>(L, K.smoother_fusion) &&
+        (K.smoother_fusion_cells <= 0 || L.n <= K.smoother_fusion_cells)) {
         // fused colour pairs, ping-ponging each component between phi and tmp
         T* cur[3] = {L.phi[0], L.phi[1], L.phi[2]};
         T* alt[3] = {L.tmp[0], L.tmp[1], L.tmp[2]};
@@ -763,7 +764,8 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
 // Block-shape autotuner.  On the first handle of a grid size (per
 // precision and visc_type; the table is the process's), time the candidate
 // block shapes of the Gauss-Seidel colour, operator, residual and
-// prolongation kernels on every periodic level with at least 4096 cells -- one warm-up
+// prolongation kernels on every periodic level with at least 4096 cells,
+// and of apply_matrix on the finest (one problem, not a batch) -- one warm-up
 // and three launches each, CUDA events on the handle's stream -- and keep
 // the fastest.  It runs at creation, on the fresh arena's zeros; the colour
 // kernel divides by the zero diagonal there, so phi and tmp of a tuned
@@ -778,6 +780,8 @@ void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
         bool touched = false;
         for (int kid = 0; kid < TK_N; ++kid) {
             if ((kid == TK_PROLONG || kid == TK_RESIDUAL) && l + 1 >= h->nlev) continue;  // needs a coarser level
+            // apply_matrix: the finest level only, on the vector type this precision feeds it
+            if (kid == TK_APPLY_MATRIX && (l != 0 || h->batched || (sizeof(T) == 4 && h->Z32.empty()))) continue;
             const int kv = (kid == TK_PROLONG) ? 0 : visc;
             if (is_tuned(kid, sizeof(T), kv, L.D)) continue;
             const int nxe = (kid == TK_GS_COLOUR) ? L.D.nx / 2 : L.D.nx;
@@ -788,7 +792,12 @@ void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
                     launch_applyop<T>(L, visc, L.phi, L.tmp, h->stream, 0);
                 else if (kid == TK_RESIDUAL)  // the split residual (its restriction is timed with it)
                     launch_residual_restrict<T>(L, Ls[l + 1], visc, L.rhs, L.phi, Ls[l + 1].rhs, h->stream, 0);
-                else
+                else if (kid == TK_APPLY_MATRIX) {
+                    if constexpr (sizeof(T) == 4)
+                        launch_apply_matrix_f32(h->L64[0], visc, h->Z32[0], h->n, h->dm, h->tmp, h->stream);
+                    else
+                        launch_apply_matrix(h->L64[0], visc, h->x, h->tmp, h->stream);
+                } else
                     launch_prolong_add<T>(L, Ls[l + 1], Ls[l + 1].phi, L.phi, h->stream);
                 check_launch();
             };
@@ -2428,7 +2437,7 @@ int lmm_stokes_update_knobs(lmm_handle* h, const lmm_knobs* k) {
                       SAME(learned_stage) && SAME(tail_cells) && SAME(tail_smem_kb) && SAME(use_graphs) &&
                       SAME(smoother_fusion) && SAME(l2_persist) && SAME(orthogonalization) && SAME(host_wait) &&
                       SAME(smoother_tma) && SAME(smoother_tma_slabs) && SAME(smoother_tma_cells) && SAME(smoother_order) &&
-                      SAME(autotune) && SAME(residual_fusion);
+                      SAME(autotune) && SAME(residual_fusion) && SAME(uniform_alpha) && SAME(smoother_fusion_cells);
 #undef SAME
     if (!same) {
         g_last_error = "lmm_stokes_update_knobs changes only the stopping rules; create a new handle for the rest";

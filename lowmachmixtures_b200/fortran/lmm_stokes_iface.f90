@@ -51,6 +51,7 @@ module lmm_stokes_iface
      integer(c_int) :: ensemble_batch
      integer(c_int) :: smoother_tma, smoother_tma_slabs, smoother_tma_cells, smoother_order
      integer(c_int) :: autotune, residual_fusion, uniform_alpha
+     integer(c_int) :: smoother_fusion_cells
   end type lmm_knobs
 
   type, bind(c) :: lmm_fields_in

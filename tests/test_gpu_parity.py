@@ -653,3 +653,4 @@ def test_autotuned_block_shapes_are_bitwise_neutral_and_reported(precision):
     assert f"gs_colour fp{w} visc -2 3D {n}x{n}x{n}" in rep, rep
     assert f"applyop fp{w} visc -2 3D {n}x{n}x{n}" in rep, rep
     assert f"residual fp{w} visc -2 3D {n}x{n}x{n}" in rep, rep
+    assert f"apply_matrix fp{w} visc -2 3D {n}x{n}x{n}" in rep, rep
