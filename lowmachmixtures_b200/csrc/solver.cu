@@ -766,8 +766,13 @@ void smooth(lmm_handle* h, LevelDev<T>& L, int nsm) {
 // block shapes of the Gauss-Seidel colour, operator, residual and
 // prolongation kernels on every periodic level with at least 4096 cells,
 // and of apply_matrix on the finest (one problem, not a batch) -- one warm-up
-// and three launches each, CUDA events on the handle's stream -- and keep
-// the fastest.  It runs at creation, on the fresh arena's zeros; the colour
+// and five timed repetitions each, CUDA events on the handle's stream; the
+// colour kernel as one whole sweep (its 2 dm colours in the smoother's
+// plane order, so a shape is judged with the L2 reuse between consecutive
+// colours) -- and keep the fastest, but the default geometry unless the
+// fastest beats it by 2% (closer than that is timing noise, and a flip on
+// noise has cost a whole sweep more than it saved).  It runs at creation,
+// on the fresh arena's zeros; the colour
 // kernel divides by the zero diagonal there, so phi and tmp of a tuned
 // level are zeroed again afterwards.  Shapes change no value.
 template <class T>
@@ -786,9 +791,13 @@ void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
             if (is_tuned(kid, sizeof(T), kv, L.D)) continue;
             const int nxe = (kid == TK_GS_COLOUR) ? L.D.nx / 2 : L.D.nx;
             auto launch = [&]() {
-                if (kid == TK_GS_COLOUR)
-                    launch_gs_colour<T>(L, visc, 1, L.rhs, L.phi, 1.0, h->stream, 0);
-                else if (kid == TK_APPLYOP)
+                if (kid == TK_GS_COLOUR) {
+                    for (int color = 1; color <= 2 * h->dm; ++color) {
+                        launch_gs_colour<T>(L, visc, color, L.rhs, L.phi, 1.0, h->stream,
+                                            (h->knobs.smoother_order == 0 && color % 2 == 0) ? 1 : 0);
+                        if (color < 2 * h->dm) check_launch();
+                    }
+                } else if (kid == TK_APPLYOP)
                     launch_applyop<T>(L, visc, L.phi, L.tmp, h->stream, 0);
                 else if (kid == TK_RESIDUAL)  // the split residual (its restriction is timed with it)
                     launch_residual_restrict<T>(L, Ls[l + 1], visc, L.rhs, L.phi, Ls[l + 1].rhs, h->stream, 0);
@@ -807,18 +816,24 @@ void autotune_levels(lmm_handle* h, std::vector<LevelDev<T>>& Ls) {
                 if (c.bx > std::max(nxe, 32)) continue;
                 force_shape(c);
                 launch();
+                constexpr int kReps = 5;
                 LMM_CK(cudaEventRecord(h->ev0, h->stream));
-                for (int r = 0; r < 3; ++r) launch();
+                for (int r = 0; r < kReps; ++r) launch();
                 LMM_CK(cudaEventRecord(h->ev1, h->stream));
                 LMM_CK(cudaEventSynchronize(h->ev1));
                 float ms = 0.f;
                 LMM_CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-                const double per = ms / 3.0;
+                // per launch (a colour sweep is 2 dm launches)
+                const double per = ms / kReps / (kid == TK_GS_COLOUR ? 2 * h->dm : 1);
                 if (c.bx == 0) def = per;
                 if (per < best) {
                     best = per;
                     bs = c;
                 }
+            }
+            if (bs.bx != 0 && best > 0.98 * def) {
+                bs = Shape{};
+                best = def;
             }
             force_shape(Shape{});
             set_tuned_shape(kid, sizeof(T), kv, L.D, bs, def, best);
