@@ -126,7 +126,10 @@ typedef struct lmm_knobs {
                                       each V-cycle application's residual is an extra FGMRES
                                       direction; 2 the same corrections computed and not used (the
                                       stage's cost alone); 3 the correction added to the V-cycle's
-                                      direction when it lowers the residual */
+                                      direction when it lowers the residual; 4 as 1, judged by the
+                                      GMRES residual: after two network columns that lower its
+                                      estimate by less than 10% the solve goes on with the V-cycle
+                                      alone */
     int    tail_cells;             /* coarse multigrid levels with at most this many cells run in
                                       one single-block launch; 0 = default (512 for the velocity
                                       V-cycle, 1024 for one 2D problem, 4096 for the pressure

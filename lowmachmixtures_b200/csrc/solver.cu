@@ -1634,6 +1634,14 @@ void network_correction(lmm_handle* h, const SVec& c, const SVec& v) {
     check_launch();
 }
 
+// Where a solve hands over to the plain restarted FGMRES (run_fgmres) at a
+// restart: the counters so far and the first true residual.
+struct FgmresResume {
+    int total_iter, iter;
+    double norm_init;
+};
+int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st, const FgmresResume* resume = nullptr);
+
 // FGMRES with the learned stage as an extra direction (learned_stage = 1):
 // every step adds two columns to the flexible Krylov basis, the FP32
 // V-cycle's z1 = M v and the network's correction c of the residual
@@ -1645,15 +1653,24 @@ void network_correction(lmm_handle* h, const SVec& c, const SVec& v) {
 // singular.  Iterations count V-cycle applications, as without the stage.
 // learned_stage = 2 computes every correction and adds none (the cost of
 // the stage without its effect: bitwise the stage-free solve).
+// learned_stage = 4 lets the GMRES residual judge the network: a network
+// column that lowers the residual estimate |s_{i+1}| by less than 10%
+// (or is dropped) is a miss, and after two misses the solve goes on with
+// the plain V-cycle alone -- no further forward passes; at the next
+// restart it hands the iterate over to the plain restarted FGMRES (the same
+// V-cycle columns and arithmetic, with its look-ahead).  Each solve judges
+// afresh.
 int run_fgmres_augmented(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
     NvtxRange nvtx_("fgmres (learned columns)");
     const lmm_knobs& K = h->knobs;
     const int m = K.gmres_max_inner;
     const int mc = 2 * m;  // columns per cycle
     const int64_t len = h->b.size();
-    const bool add = (K.learned_stage == 1);
+    const bool judged = (K.learned_stage == 4);
+    const bool add = (K.learned_stage == 1 || judged);
     LMM_CK(cudaMemsetAsync(h->luses, 0, 2 * sizeof(int), h->stream));
-    int net_tried = 0, net_kept = 0;
+    int net_tried = 0, net_kept = 0, net_misses = 0;
+    bool net_on = true;  // judged: false once the network has missed twice
     std::vector<double> cs(mc + 2), sn(mc + 2), y(mc + 2), s(mc + 3), col;
     Hess H{mc + 1, std::vector<double>((size_t)(mc + 1) * mc, 0.0)};
     std::vector<const void*> zcol(mc + 1);
@@ -1676,6 +1693,14 @@ int run_fgmres_augmented(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
         return true;
     };
     for (;;) {
+        if (judged && !net_on) {
+            // the network is out for this solve: the plain FGMRES takes over
+            int u[2] = {net_kept, net_tried};
+            LMM_CK(cudaMemcpyAsync(h->luses, u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
+            LMM_CK(host_wait(h));
+            const FgmresResume r{total_iter, iter, norm_init};
+            return run_fgmres(h, norm_pre_rhs, st, &r);
+        }
         launch_apply_matrix(h->L64[0], K.visc_type, h->x, h->tmp, h->stream);
         check_launch();
         launch_neg_resid(h->tmp.base, h->b.base, len, h->stream);
@@ -1751,8 +1776,10 @@ int run_fgmres_augmented(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
             check_launch();
             // the network's correction of what this application leaves (before
             // the Arnoldi step overwrites w)
-            network_correction(h, h->Zc[k], h->V[vin]);
-            ++net_tried;
+            if (net_on) {
+                network_correction(h, h->Zc[k], h->V[vin]);
+                ++net_tried;
+            }
             i = i + 1;
             zcol[i] = h->Z32[k];
             zkind[i] = 0;
@@ -1764,18 +1791,22 @@ int run_fgmres_augmented(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
                 stop = true;
                 break;
             }
-            if (!add || i + 1 > mc) continue;
+            if (!add || !net_on || i + 1 > mc) continue;
             // network column: z = c, w = A c
+            const double est_before = std::fabs(s[i + 1]);
             launch_apply_matrix(h->L64[0], K.visc_type, h->Zc[k], h->w, h->stream);
             check_launch();
             pin_ok = false;  // the network column's V overwrote the FP32 copy of V[vin]
+            bool helped = false;
             if (arnoldi(i + 1, true)) {
                 i = i + 1;
                 zcol[i] = h->Zc[k].base;
                 zkind[i] = 1;
                 ++net_kept;
                 after_column(i);
+                helped = std::fabs(s[i + 1]) < 0.9 * est_before;
             }
+            if (judged && !helped && ++net_misses >= 2) net_on = false;
         }
         solve_utri(i - 1, H, s, y);
         // update_sol: runs of consecutive V-cycle columns as in run_fgmres
@@ -1811,19 +1842,24 @@ int run_fgmres_augmented(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
     return status;
 }
 
-int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
+// resume: continue a solve that run_fgmres_augmented hands over at a
+// restart (its counters kept, the learned stage off from there on).
+int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st, const FgmresResume* resume) {
     NvtxRange nvtx_("fgmres");
     const lmm_knobs& K = h->knobs;
     const int m = K.gmres_max_inner;
     const int64_t len = h->b.size();
     const bool fp32 = (K.precision == LMM_PRECISION_FP32);
-    const bool learned = fp32 && K.learned_stage > 0 && h->net != nullptr;
-    if (learned && (K.learned_stage == 1 || K.learned_stage == 2)) return run_fgmres_augmented(h, norm_pre_rhs, st);
+    const bool learned = fp32 && K.learned_stage > 0 && h->net != nullptr && !resume;
+    if (learned && (K.learned_stage == 1 || K.learned_stage == 2 || K.learned_stage == 4))
+        return run_fgmres_augmented(h, norm_pre_rhs, st);
     if (learned) LMM_CK(cudaMemsetAsync(h->luses, 0, 2 * sizeof(int), h->stream));
     std::vector<double> cs(m + 2), sn(m + 2), y(m + 2), s(m + 3), col;
     Hess H{m + 1, std::vector<double>((size_t)(m + 1) * m, 0.0)};
-    h->vcycles = 0;
-    if (norm_pre_rhs) *norm_pre_rhs = 0.0;
+    if (!resume) {
+        h->vcycles = 0;
+        if (norm_pre_rhs) *norm_pre_rhs = 0.0;
+    }
     stokes_norm(h, h->b, 0);
     const double norm_b = read_slot(h, 0, 5);
     if (st) st->norm_b = norm_b;
@@ -1832,8 +1868,8 @@ int run_fgmres(lmm_handle* h, double* norm_pre_rhs, lmm_stats* st) {
         LMM_CK(cudaMemsetAsync(h->x.base, 0, len * sizeof(double), h->stream));
         return LMM_OK;
     }
-    int status = LMM_OK, total_iter = 0, iter = 0;
-    double norm_init = 0.0;
+    int status = LMM_OK, total_iter = resume ? resume->total_iter : 0, iter = resume ? resume->iter : 0;
+    double norm_init = resume ? resume->norm_init : 0.0;
     for (;;) {
         launch_apply_matrix(h->L64[0], K.visc_type, h->x, h->tmp, h->stream);
         check_launch();

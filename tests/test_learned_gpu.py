@@ -262,6 +262,27 @@ def test_learned_stage_dry_run_changes_nothing_and_stage_converges():
     assert on[2] <= 1e-9 and on[4] > 0
 
 
+def test_judged_stage_drops_a_network_that_does_not_help():
+    """learned_stage = 4: the GMRES residual judges the network.  A network
+    whose weights are all zero returns a zero correction, so every network
+    column is dropped as a miss: the solve stops asking it after two forward
+    passes and goes on with the plain V-cycle, reaching the tolerance in the
+    stage-free iteration count.  Always on (learned_stage = 1) the same
+    network is asked once per V-cycle application and never kept."""
+    from lowmachmixtures_b200 import learned, synth
+    prob = synth.make_problem(3, 32, 100.0, 23)
+    with learned.Net((32, 32, 32), 1, 5) as net:
+        net.set_params(np.zeros(net.num_params, np.float32))
+        plain = learned.solve_with(prob, None)
+        judged = learned.solve_with(prob, net, knobs=learned.mixed_knobs(learned_stage=4))
+        always = learned.solve_with(prob, net, knobs=learned.mixed_knobs(learned_stage=1))
+    assert plain[0] >= 3
+    assert judged[2] <= 1e-9 and always[2] <= 1e-9
+    assert judged[0] == plain[0] and always[0] == plain[0]
+    assert judged[3] == 0 and judged[4] == 2
+    assert always[3] == 0 and always[4] == always[0]
+
+
 def test_trained_stage_gains_on_held_out_seeds():
     """What training gains, on held-out seeds of the learned-stage family
     (32^3, steady, contrast log-uniform in [10, 1000]).  The network trained
