@@ -1047,10 +1047,35 @@ __global__ void k_fill(T* __restrict__ out, T v, int64_t n) {
 // with its own partials, counter and 8-double output slot out + 8 * b; the
 // grid's x extent and every summation order are those of one instance
 // reduced alone, so each instance's result has the same bits.
+// k_reduce may take entries in pairs: rows of even length and every array
+// aligned to a pair (the same choice in the bounds-check build, whose pair
+// loads are checked as one access each, so both builds sum alike)
+static inline int reduce_pairs(const Dims& D, size_t elem, const void* const a[4], const void* const b[4]) {
+    if (D.nx % 2) return 0;
+    for (int q = 0; q < 4; ++q) {
+        if (q == 2 && D.dm == 2) continue;  // a 2D reduction reads no third face array
+        if ((a[q] && (uintptr_t)a[q] % (2 * elem)) || (b[q] && (uintptr_t)b[q] % (2 * elem))) return 0;
+    }
+    return 1;
+}
+
+template <class T>
+struct Pair2;
+template <>
+struct Pair2<double> {
+    using type = double2;
+};
+template <>
+struct Pair2<float> {
+    using type = float2;
+};
+
+// vec = 1 (reduce_pairs): entries in pairs by one 16- (FP64) or 8-byte
+// (FP32) load per array; the sums change order within a thread's pair only
 template <class T, int DM, int MODE>
 __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const T* a1, const T* a2, const T* a3, const T* b0,
                                                      const T* b1, const T* b2, const T* b3, double w0, double w1, double w2,
-                                                     double pw, double* partials, unsigned* counter, double* out) {
+                                                     double pw, double* partials, unsigned* counter, double* out, int vec) {
     pdl_enter();
     constexpr int NC = DM + 1;
     const int nzi = (DM == 3) ? D.nz : 1;  // third extent of one instance
@@ -1084,16 +1109,47 @@ __global__ void __launch_bounds__(kThreads) k_reduce(Dims D, const T* a0, const 
         AA[c] = (c < DM) ? A[c] : A[3];
         BB[c] = (c < DM) ? B[c] : B[3];
     }
-    for (int t = tid; t < n; t += stride) {
+    if (vec) {
+        using V2 = typename Pair2<T>::type;
+        const int n2 = n >> 1;
+        for (int p = tid; p < n2; p += stride) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            if (!AA[c]) continue;
-            double x = (double)ld(AA[c], t);
-            if (MODE == 2) {
-                acc[c] = fmax(acc[c], fabs(x - (BB[c] ? (double)ld(BB[c], t) : 0.0)));
-            } else {
-                if (MODE == 0) x = x * (double)ld(BB[c], t);
-                acc[c] += x;
+            for (int c = 0; c < NC; ++c) {
+                if (!AA[c]) continue;
+                const V2 xa = ld2(reinterpret_cast<const V2*>(AA[c]), p);
+                double x0 = (double)xa.x, x1 = (double)xa.y;
+                if (MODE == 2) {
+                    double y0 = 0.0, y1 = 0.0;
+                    if (BB[c]) {
+                        const V2 xb = ld2(reinterpret_cast<const V2*>(BB[c]), p);
+                        y0 = (double)xb.x;
+                        y1 = (double)xb.y;
+                    }
+                    acc[c] = fmax(acc[c], fabs(x0 - y0));
+                    acc[c] = fmax(acc[c], fabs(x1 - y1));
+                } else {
+                    if (MODE == 0) {
+                        const V2 xb = ld2(reinterpret_cast<const V2*>(BB[c]), p);
+                        x0 = x0 * (double)xb.x;
+                        x1 = x1 * (double)xb.y;
+                    }
+                    acc[c] += x0;
+                    acc[c] += x1;
+                }
+            }
+        }
+    } else {
+        for (int t = tid; t < n; t += stride) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (!AA[c]) continue;
+                double x = (double)ld(AA[c], t);
+                if (MODE == 2) {
+                    acc[c] = fmax(acc[c], fabs(x - (BB[c] ? (double)ld(BB[c], t) : 0.0)));
+                } else {
+                    if (MODE == 0) x = x * (double)ld(BB[c], t);
+                    acc[c] += x;
+                }
             }
         }
     }
@@ -1589,7 +1645,10 @@ template <class T>
 void launch_reduce(const Dims& D, int mode, const T* const a[4], const T* const b[4], const double wseam[3], double pw,
                    double* partials, unsigned* counter, double* out, int nblocks, cudaStream_t s, int ninst) {
     const dim3 grid(nblocks, ninst);
-#define RED(DM_, M_) launch_pdl(k_reduce<T, DM_, M_>, grid, dim3(kThreads), 0, s, D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out)
+    const void* pa[4] = {a[0], a[1], a[2], a[3]};
+    const void* pb[4] = {b[0], b[1], b[2], b[3]};
+    const int vec = reduce_pairs(D, sizeof(T), pa, pb);
+#define RED(DM_, M_) launch_pdl(k_reduce<T, DM_, M_>, grid, dim3(kThreads), 0, s, D, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], wseam[0], wseam[1], wseam[2], pw, partials, counter, out, vec)
     if (D.dm == 2) {
         if (mode == 0) RED(2, 0); else if (mode == 1) RED(2, 1); else RED(2, 2);
     } else {

@@ -120,12 +120,16 @@ extern "C" int lmm_inner_prod_noalloc(int dm, const int n[3], const double* cons
     const double w = 3.0;
     cudaError_t e = cudaMemsetAsync(&scr->counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return cuda_failed("cudaMemsetAsync", e);
+    // the same load layout as lmm_op_inner_prod, so both give the same bits
+    const void* pa[4] = {a_u[0], a_u[1], dm == 3 ? a_u[2] : nullptr, a_p};
+    const void* pb[4] = {b_u[0], b_u[1], dm == 3 ? b_u[2] : nullptr, b_p};
+    const int vec = reduce_pairs(D, sizeof(double), pa, pb);
     if (dm == 2)
         k_reduce<double, 2, 0><<<nblocks, kThreads, 0, s>>>(D, a_u[0], a_u[1], nullptr, a_p, b_u[0], b_u[1], nullptr, b_p, w, w, w,
-                                                             p_norm_weight, scr->partials, &scr->counter, scr->out);
+                                                             p_norm_weight, scr->partials, &scr->counter, scr->out, vec);
     else
         k_reduce<double, 3, 0><<<nblocks, kThreads, 0, s>>>(D, a_u[0], a_u[1], a_u[2], a_p, b_u[0], b_u[1], b_u[2], b_p, w, w, w,
-                                                             p_norm_weight, scr->partials, &scr->counter, scr->out);
+                                                             p_norm_weight, scr->partials, &scr->counter, scr->out, vec);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_failed("k_reduce launch", e);
     count_launch();
     if ((e = cudaMemcpyAsync(out_host, scr->out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)

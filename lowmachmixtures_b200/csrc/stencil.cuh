@@ -237,6 +237,15 @@ __device__ __forceinline__ T ld(const T* p, int i) {
     return __ldg(p + i);
 }
 
+// a pair of entries (double2 / float2) by one load, checked as one access
+template <class V>
+__device__ __forceinline__ V ld2(const V* p, int i) {
+#ifdef LMM_BOUNDS_CHECK
+    if (!bc_ok(p + i, sizeof(V))) return V{};
+#endif
+    return __ldg(p + i);
+}
+
 // loads of arrays a kernel may also write (phi, rhs):
 //   LD 0  read-only path (__ldg): the array is not written by this kernel;
 //   LD 1  plain load: written by other threads of the same block between
